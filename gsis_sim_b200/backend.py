@@ -1,0 +1,183 @@
+"""Python view of the kinetic backend interface over a C ABI.
+
+`KineticBackendABI` mirrors the reference's `gsis::kinetic::KineticBackend` (src/kinetic/kinetic_backend.hpp:59-100):
+same method names, argument meaning (FP64, internal numbering) and error behaviour (a failed call raises
+`KineticError`, the counterpart of `gsis::Error`). `B200Backend` binds it to the CUDA library
+(libgsis_b200.so, entry points of include/gsis_b200.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import load_library
+
+
+class KineticError(RuntimeError):
+    """A backend call failed (the reference raises gsis::Error in the same places)."""
+
+
+class KineticBackendABI:
+    """Common method layer over a kin_*-style C ABI (`prefix` selects the symbol family)."""
+
+    def __init__(self, lib, prefix: str, handle, setup: abi.SetupArrays, error_fn):
+        self._lib = lib
+        self._prefix = prefix
+        self._h = handle
+        self.setup = setup
+        self._error_fn = error_fn
+        self.n_cells = setup.n_cells
+        self.nv = setup.nv
+        self.n_bfaces = setup.n_bfaces
+
+    def _call(self, name, *args):
+        rc = getattr(self._lib, self._prefix + name)(self._h, *args)
+        if rc != abi.KIN_OK:
+            raise KineticError(f"{self._prefix}{name} failed ({rc}): {self._error_fn()}")
+
+    # --- KineticBackend methods -----------------------------------------------------------------------------
+    def chunk_width(self) -> int:
+        out = C.c_int32()
+        self._call("chunk_width", C.byref(out))
+        return out.value
+
+    def set_equilibrium(self, states) -> None:
+        s = np.ascontiguousarray(states, dtype=np.float64).ravel()
+        self._call("set_equilibrium", abi.as_ptr(s, C.c_double), s.size)
+
+    def set_distribution(self, f) -> None:
+        a = np.ascontiguousarray(f, dtype=np.float64).ravel()
+        self._call("set_distribution", abi.as_ptr(a, C.c_double), a.size)
+
+    def get_distribution(self, out=None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.n_cells * self.nv, dtype=np.float64)
+        self._call("get_distribution", abi.as_ptr(out, C.c_double), out.size)
+        return out.reshape(self.n_cells, self.nv)
+
+    def compute_moments(self, out=None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.n_cells * abi.MOMENTS_PER_CELL, dtype=np.float64)
+        self._call("compute_moments", abi.as_ptr(out, C.c_double), out.size)
+        return out.reshape(self.n_cells, abi.MOMENTS_PER_CELL)
+
+    def scale_distribution(self, s: float) -> None:
+        self._call("scale_distribution", C.c_double(s))
+
+    def update_cell_params(self) -> None:
+        self._call("update_cell_params")
+
+    def set_inflow(self, inflow) -> None:
+        a = np.ascontiguousarray(inflow, dtype=np.float64).reshape(-1, 6)
+        arr = abi.inflow_array(a)
+        self._call("set_inflow", arr, len(a))
+
+    def boundary_sums(self, out=None) -> np.ndarray:
+        if out is None:
+            out = np.empty(max(self.n_bfaces, 0) * abi.BOUNDARY_SUMS_PER_FACE, dtype=np.float64)
+        self._call("boundary_sums", abi.as_ptr(out, C.c_double), out.size)
+        return out.reshape(self.n_bfaces, abi.BOUNDARY_SUMS_PER_FACE)
+
+    def sweep(self, out=None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.n_cells, dtype=np.float64)
+        self._call("sweep", abi.as_ptr(out, C.c_double), out.size)
+        return out
+
+    def gsis_correction(self, w_half, w_new):
+        wh = np.ascontiguousarray(w_half, dtype=np.float64).ravel()
+        wn = np.ascontiguousarray(w_new, dtype=np.float64).ravel()
+        flags = np.zeros(self.n_cells, dtype=np.int32)
+        replaced = C.c_int64()
+        self._call("gsis_correction", abi.as_ptr(wh, C.c_double), abi.as_ptr(wn, C.c_double), wh.size,
+                   abi.as_ptr(flags, C.c_int32), C.byref(replaced))
+        return replaced.value, flags
+
+    def internal_face_mass_flux(self, cells, entries) -> np.ndarray:
+        c = np.ascontiguousarray(cells, dtype=np.int32)
+        e = np.ascontiguousarray(entries, dtype=np.int32)
+        out = np.zeros(c.size, dtype=np.float64)
+        self._call("internal_face_mass_flux", abi.as_ptr(c, C.c_int32), abi.as_ptr(e, C.c_int32), c.size,
+                   abi.as_ptr(out, C.c_double))
+        return out
+
+    def deq_counts(self):
+        d = abi.KinDeqCounts()
+        self._call("deq_counts", C.byref(d))
+        return d.corrected, d.failed, d.max_iterations
+
+
+class B200Backend(KineticBackendABI):
+    """The B200 CUDA backend (libgsis_b200.so). Creating it uploads the setup and allocates f on the device."""
+
+    def __init__(self, setup: abi.SetupArrays, precision: str | None = None, device: int = 0,
+                 velocity_chunk: int | None = None):
+        lib = load_library()
+        s = setup.copy()
+        if precision is not None:
+            s["precision"] = abi.PRECISIONS[precision]
+        if velocity_chunk is not None:
+            s["velocity_chunk"] = int(velocity_chunk)
+        s["device"] = device
+        desc = s.desc()
+        h = C.c_void_p()
+        rc = lib.kin_create(C.byref(desc), C.byref(h))
+        if rc != abi.KIN_OK:
+            raise KineticError(f"kin_create failed ({rc}): {lib.kin_last_error(None).decode()}")
+        super().__init__(lib, "kin_", h, s, lambda: lib.kin_last_error(h).decode())
+        self._owned = True
+
+    def close(self):
+        if getattr(self, "_owned", False) and self._h:
+            self._lib.kin_destroy(self._h)
+            self._h = None
+            self._owned = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- B200 additions -------------------------------------------------------------------------------------
+    def set_stream(self, stream_ptr: int) -> None:
+        self._call("set_stream", C.c_void_p(stream_ptr))
+
+    def launch_count(self) -> int:
+        out = C.c_int64()
+        self._call("launch_count", C.byref(out))
+        return out.value
+
+    def device_f(self):
+        p = C.c_void_p()
+        es = C.c_int32()
+        self._call("device_f", C.byref(p), C.byref(es))
+        return p.value, es.value
+
+    def velocity_permutation(self) -> np.ndarray:
+        out = np.empty(self.nv, dtype=np.int32)
+        self._call("velocity_permutation", abi.as_ptr(out, C.c_int32), out.size)
+        return out
+
+    def schedule_info(self):
+        a, b = C.c_int32(), C.c_int32()
+        self._call("schedule_info", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def take_timings(self) -> dict:
+        t = abi.KinStepTimings()
+        self._call("take_timings", C.byref(t))
+        return {k: getattr(t, k) for k, _ in abi.KinStepTimings._fields_}
+
+    def memory_bytes(self) -> int:
+        out = C.c_uint64()
+        self._call("memory_bytes", C.byref(out))
+        return out.value

@@ -1,0 +1,909 @@
+// Host side of the B200 kinetic backend: device memory, level schedule, launch sequencing, timing, and the C ABI
+// of include/gsis_b200.h. One KinHandle corresponds to one reference `CudaBackend<F>` object
+// (src/kinetic/kinetic_backend_cuda.cpp:89-502).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gsis_b200.h"
+#include "kin_launch.h"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct KinError : std::runtime_error {
+  int code;
+  KinError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define KCHECK(cond, msg)                                     \
+  do {                                                        \
+    if (!(cond)) throw KinError(KIN_E_ARG, std::string(msg)); \
+  } while (0)
+
+#define KCUDA(call)                                                                                              \
+  do {                                                                                                           \
+    cudaError_t err_ = (call);                                                                                   \
+    if (err_ != cudaSuccess)                                                                                     \
+      throw KinError(KIN_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(err_) + " (" __FILE__ ":" +      \
+                                     std::to_string(__LINE__) + ")");                                            \
+  } while (0)
+
+// RAII device array
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw KinError(e == cudaErrorMemoryAllocation ? KIN_E_MEMORY : KIN_E_CUDA,
+                     std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " +
+                         cudaGetErrorString(e));
+    }
+  }
+  void upload(const T* host, size_t count, cudaStream_t st) {
+    alloc(count);
+    if (count) KCUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, st));
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// CUDA-event phase timer on the handle's stream (PhaseTimer, src/kinetic/kinetic_backend_cuda.cpp:29-87)
+struct PhaseTimer {
+  enum Phase { kMoments, kBoundary, kGradient, kResidual, kForward, kBackward, kOther };
+  struct Pending {
+    Phase phase;
+    cudaEvent_t a, b;
+  };
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<Pending> pending;
+  Phase cur = kOther;
+  cudaEvent_t start{};
+  ~PhaseTimer() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+  cudaEvent_t take() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      KCUDA(cudaEventCreate(&e));
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void begin(Phase p, cudaStream_t st) {
+    cur = p;
+    start = take();
+    KCUDA(cudaEventRecord(start, st));
+  }
+  void end(cudaStream_t st) {
+    cudaEvent_t e = take();
+    KCUDA(cudaEventRecord(e, st));
+    pending.push_back({cur, start, e});
+  }
+  void flush(KinStepTimings& t) {
+    if (pending.empty()) return;
+    KCUDA(cudaEventSynchronize(pending.back().b));
+    for (const auto& p : pending) {
+      float ms = 0.f;
+      KCUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+      const double s = 1e-3 * ms;
+      switch (p.phase) {
+        case kMoments: t.moments += s; break;
+        case kBoundary: t.boundary += s; break;
+        case kGradient: t.gradient += s; break;
+        case kResidual: t.residual += s; break;
+        case kForward: t.sweep_forward += s; break;
+        case kBackward: t.sweep_backward += s; break;
+        default: t.other += s; break;
+      }
+    }
+    pending.clear();
+    used = 0;
+  }
+};
+
+}  // namespace
+
+struct KinHandle {
+  virtual ~KinHandle() = default;
+  std::string err;
+  cudaStream_t stream = nullptr;      // stream every kernel of the handle goes to
+  cudaStream_t own_stream = nullptr;  // the stream the handle created (destroyed with it)
+  int64_t launches = 0;
+  int device = 0;
+  virtual const char* name() const = 0;
+  virtual int32_t chunk_width() const = 0;
+  virtual uint64_t memory_bytes() const = 0;
+  virtual void set_equilibrium(const double* s, int64_t n) = 0;
+  virtual void set_distribution(const double* f, int64_t n) = 0;
+  virtual void get_distribution(double* f, int64_t n) = 0;
+  virtual void compute_moments(double* out, int64_t n) = 0;
+  virtual void scale_distribution(double s) = 0;
+  virtual void update_cell_params() = 0;
+  virtual void set_inflow(const KinInflowState* in, int64_t n) = 0;
+  virtual void boundary_sums(double* out, int64_t n) = 0;
+  virtual void sweep(double* residual_cell, int64_t n) = 0;
+  virtual void gsis_correction(const double* wh, const double* wn, int64_t n, int32_t* flags, int64_t* replaced) = 0;
+  virtual void internal_face_mass_flux(const int32_t* cells, const int32_t* entries, int64_t n, double* out) = 0;
+  virtual void take_timings(KinStepTimings* out) = 0;
+  virtual void deq_counts(KinDeqCounts* out) = 0;
+  virtual void device_f(void** f, int32_t* es) = 0;
+  virtual void velocity_permutation(int32_t* perm, int64_t n) const = 0;
+  virtual void schedule_info(int32_t* max_levels, int32_t* n_chains) const = 0;
+};
+
+namespace {
+
+using kin::BFace;
+using kin::CellParams;
+using kin::CsrE;
+using kin::Inflow;
+
+template <class S, class M>
+struct Backend final : KinHandle {
+  using L = kin::Launch<S, M>;
+  static constexpr size_t kMargin = size_t{1} << 30;  // device memory kept free (1 GiB)
+
+  // sizes and parameters
+  int32_t nc = 0, nv = 0, nb = 0, n_blocks = 0, n_groups = 1, precision = 0;
+  int32_t block_passes = 1, discrete_eq = 0, collisionless = 0, negative_mode = 0, n_maxwell = 0;
+  double mu0 = 0, omega = 0, Pr = 0, cold_bgk_T = 0;
+  kin::View<S, M> view{};
+  int32_t chunk = 0, partial_stride = 1, max_levels = 0, n_chains = 0;
+
+  // host copies
+  std::vector<int32_t> perm, inv, group_begin, group_end;
+  std::vector<int32_t> h_block_offsets;
+  // per chunk: sweep items
+  struct ChunkPlan {
+    int32_t k0, kc;
+    DevBuf<int4> items;
+    int32_t n_items;
+  };
+  std::vector<std::unique_ptr<ChunkPlan>> chunks;
+
+  // device arrays
+  DevBuf<M> xi_x, xi_y, xi_z;
+  DevBuf<double> xid_x, xid_y, xid_z, wts;
+  DevBuf<int32_t> csr_off;
+  DevBuf<CsrE<M>> csr;
+  DevBuf<M> eps2;
+  DevBuf<BFace<M>> bfaces;
+  DevBuf<Inflow<M>> inflow;
+  DevBuf<CellParams<M>> cells;
+  DevBuf<int32_t> mirror_map;
+  DevBuf<int64_t> mw_offset;
+  DevBuf<double> mw_frac;
+  DevBuf<M> specular, specular_first;
+  DevBuf<int32_t> grid_to_pos;
+  DevBuf<double> volume, vdt;
+  DevBuf<int32_t> block_offsets, chain_cells, chain_start, lev_bounds, lev_start, lev_count, pos;
+  DevBuf<int32_t> d_perm, d_inv;
+  DevBuf<double> moments, shift, residual_cell, bsums, partial, w_half, w_new, staging;
+  DevBuf<int32_t> flags, face_cells, face_entries;
+  DevBuf<double> face_out;
+  DevBuf<S> f, gx, gy, gz, r;
+
+  bool inflow_set = false;
+  bool deq_valid = false;
+  PhaseTimer timer;
+  KinStepTimings timings{};
+
+  const char* name() const override { return "b200"; }
+  int32_t chunk_width() const override { return chunk; }
+
+  explicit Backend(const KinSetupDesc& d) {
+    device = d.device;
+    KCUDA(cudaSetDevice(device));
+    nc = d.n_cells;
+    nv = d.nv;
+    nb = d.n_bfaces;
+    n_blocks = d.n_blocks;
+    precision = d.precision;
+    KCHECK(nc > 0 && nv > 0 && nb >= 0 && n_blocks >= 1, "invalid sizes in KinSetupDesc");
+    KCHECK(d.xi_x && d.xi_y && d.xi_z && d.csr_offsets && d.csr_other && d.csr_bface && d.csr_geom && d.eps2 &&
+               d.volume && d.vdt && d.block_offsets,
+           "missing array in KinSetupDesc");
+    KCHECK(nb == 0 || (d.bface_owner && d.bface_kind && d.bface_mirror_xor && d.bface_geom),
+           "missing boundary-face array in KinSetupDesc");
+    KCHECK(d.block_offsets[0] == 0 && d.block_offsets[n_blocks] == nc, "block_offsets do not cover the cells");
+    block_passes = std::max(1, d.block_passes);
+    discrete_eq = d.discrete_eq;
+    collisionless = d.deq_fallback_collisionless;
+    negative_mode = d.negative_check_mode;
+    mu0 = d.mu0;
+    omega = d.omega;
+    Pr = d.Pr;
+    cold_bgk_T = d.cold_bgk_temperature;
+    n_maxwell = d.n_maxwell_faces;
+
+    // free device memory check for f (kinetic_backend_cuda.cpp:102-106)
+    size_t free_b = 0, total_b = 0;
+    KCUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t f_bytes = sizeof(S) * static_cast<size_t>(nc) * static_cast<size_t>(nv);
+    if (f_bytes + kMargin >= free_b)
+      throw KinError(KIN_E_MEMORY, "distribution function of " + std::to_string(f_bytes / 1e9) +
+                                       " GB does not fit in the free device memory of " +
+                                       std::to_string(free_b / 1e9) + " GB");
+    KCUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    stream = own_stream;
+
+    build_velocity_layout(d);
+    build_mesh(d);
+    build_schedule(d);
+
+    const size_t ncs = static_cast<size_t>(nc);
+    moments.alloc(ncs * 15);
+    shift.alloc(ncs * 3);
+    KCUDA(cudaMemsetAsync(shift.p, 0, shift.bytes(), stream));
+    residual_cell.alloc(ncs);
+    bsums.alloc(static_cast<size_t>(std::max(nb, 1)) * 20);
+    w_half.alloc(ncs * 5);
+    w_new.alloc(ncs * 5);
+    flags.alloc(ncs);
+    inflow.alloc(static_cast<size_t>(std::max(nb, 1)));
+    KCUDA(cudaMemsetAsync(inflow.p, 0, inflow.bytes(), stream));
+    cells.alloc(ncs);
+    KCUDA(cudaMemsetAsync(cells.p, 0, cells.bytes(), stream));
+    f.alloc(ncs * static_cast<size_t>(nv));
+    KCUDA(cudaMemsetAsync(f.p, 0, f.bytes(), stream));
+
+    // velocity chunk: given (rounded to the mirror-orbit-free width it is) or from the free memory
+    // (kinetic_backend_cuda.cpp:147-161)
+    KCUDA(cudaStreamSynchronize(stream));
+    KCUDA(cudaMemGetInfo(&free_b, &total_b));
+    const double per_velocity = static_cast<double>(nc) * (4.0 * sizeof(S) + 8.0 / (256.0 * kin::kTileIters));
+    int64_t k;
+    if (d.velocity_chunk > 0) {
+      k = d.velocity_chunk;
+    } else {
+      const double avail = static_cast<double>(free_b) - static_cast<double>(kMargin);
+      k = static_cast<int64_t>(avail / per_velocity);
+      k = k / 256 * 256;
+      if (k < 256 && k < nv) throw KinError(KIN_E_MEMORY, "not enough device memory for the velocity-chunk work arrays");
+    }
+    chunk = static_cast<int32_t>(std::min<int64_t>(k, nv));
+    const size_t work = ncs * static_cast<size_t>(chunk);
+    gx.alloc(work);
+    gy.alloc(work);
+    gz.alloc(work);
+    r.alloc(work);
+    partial_stride = L::residual_tiles(chunk);
+    partial.alloc(ncs * static_cast<size_t>(partial_stride));
+    build_chunks();
+    staging_alloc();
+    update_view();
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  ~Backend() override {
+    if (stream) cudaStreamSynchronize(stream);
+    if (own_stream) {
+      cudaStreamSynchronize(own_stream);
+      cudaStreamDestroy(own_stream);
+    }
+  }
+
+  // ---- set-up ----------------------------------------------------------------------------------------------
+  void build_velocity_layout(const KinSetupDesc& d) {
+    // velocities grouped by LU-SGS sweep direction (stable: reference storage order inside a group)
+    n_groups = d.n_sweep_dirs > 0 ? d.n_sweep_dirs : 1;
+    std::vector<int32_t> grp(static_cast<size_t>(nv), 0);
+    if (d.n_sweep_dirs > 0) {
+      KCHECK(d.sweep_dir_of && d.sweep_order && d.sweep_pos, "sweep order arrays missing");
+      for (int p = 0; p < nv; ++p) {
+        grp[p] = d.sweep_dir_of[p];
+        KCHECK(grp[p] < n_groups, "sweep_dir_of out of range");
+      }
+    }
+    perm.resize(nv);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return grp[a] < grp[b]; });
+    inv.assign(nv, -1);
+    for (int q = 0; q < nv; ++q) inv[perm[q]] = q;
+    group_begin.assign(n_groups, 0);
+    group_end.assign(n_groups, 0);
+    for (int g = 0, q = 0; g < n_groups; ++g) {
+      group_begin[g] = q;
+      while (q < nv && grp[perm[q]] == g) ++q;
+      group_end[g] = q;
+    }
+    std::vector<M> hx(nv), hy(nv), hz(nv);
+    std::vector<double> dx(nv), dy(nv), dz(nv), hw;
+    for (int q = 0; q < nv; ++q) {
+      const int p = perm[q];
+      dx[q] = d.xi_x[p];
+      dy[q] = d.xi_y[p];
+      dz[q] = d.xi_z[p];
+      hx[q] = static_cast<M>(dx[q]);
+      hy[q] = static_cast<M>(dy[q]);
+      hz[q] = static_cast<M>(dz[q]);
+    }
+    xi_x.upload(hx.data(), nv, stream);
+    xi_y.upload(hy.data(), nv, stream);
+    xi_z.upload(hz.data(), nv, stream);
+    xid_x.upload(dx.data(), nv, stream);
+    xid_y.upload(dy.data(), nv, stream);
+    xid_z.upload(dz.data(), nv, stream);
+    if (d.weights) {
+      hw.resize(nv);
+      for (int q = 0; q < nv; ++q) hw[q] = d.weights[perm[q]];
+      wts.upload(hw.data(), nv, stream);
+    }
+    d_perm.upload(perm.data(), nv, stream);
+    d_inv.upload(inv.data(), nv, stream);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void build_mesh(const KinSetupDesc& d) {
+    const int64_t n_csr = d.csr_offsets[nc];
+    csr_off.upload(d.csr_offsets, static_cast<size_t>(nc) + 1, stream);
+    std::vector<CsrE<M>> hc(static_cast<size_t>(n_csr));
+    for (int64_t k = 0; k < n_csr; ++k) {
+      CsrE<M>& e = hc[k];
+      e.other = d.csr_other[k];
+      e.bface = d.csr_bface[k];
+      KCHECK(e.other < nc && e.bface < nb && (e.other >= 0) != (e.bface >= 0), "invalid CSR entry");
+      const double* g = d.csr_geom + 12 * k;
+      for (int a = 0; a < 3; ++a) {
+        e.s[a] = static_cast<M>(g[a]);
+        e.ds[a] = static_cast<M>(g[3 + a]);
+        e.dn[a] = static_cast<M>(g[6 + a]);
+        e.c[a] = static_cast<M>(g[9 + a]);
+      }
+    }
+    csr.upload(hc.data(), hc.size(), stream);
+    std::vector<M> he(nc);
+    for (int c = 0; c < nc; ++c) he[c] = static_cast<M>(d.eps2[c]);
+    eps2.upload(he.data(), nc, stream);
+    volume.upload(d.volume, nc, stream);
+    vdt.upload(d.vdt, nc, stream);
+    h_block_offsets.assign(d.block_offsets, d.block_offsets + n_blocks + 1);
+    block_offsets.upload(h_block_offsets.data(), h_block_offsets.size(), stream);
+
+    // mirror maps: one per distinct mirror xor of symmetry / Maxwell faces
+    std::vector<int32_t> xors;
+    std::vector<BFace<M>> hb(static_cast<size_t>(std::max(nb, 1)));
+    for (int b = 0; b < nb; ++b) {
+      BFace<M>& o = hb[b];
+      o.owner = d.bface_owner[b];
+      o.kind = d.bface_kind[b];
+      o.patch = d.bface_patch ? d.bface_patch[b] : 0;
+      KCHECK(o.owner >= 0 && o.owner < nc, "invalid boundary face owner");
+      const int x = d.bface_mirror_xor[b];
+      o.mirror = -1;
+      if (x != 0) {
+        auto it = std::find(xors.begin(), xors.end(), x);
+        if (it == xors.end()) {
+          xors.push_back(x);
+          it = xors.end() - 1;
+        }
+        o.mirror = static_cast<int32_t>(it - xors.begin());
+      }
+      KCHECK(o.kind != kin::kSymmetry || o.mirror >= 0, "symmetry face without a mirror map");
+      const double* g = d.bface_geom + 7 * b;
+      for (int a = 0; a < 3; ++a) {
+        o.n[a] = static_cast<M>(g[a]);
+        o.d[a] = static_cast<M>(g[4 + a]);
+      }
+      o.area = static_cast<M>(g[3]);
+    }
+    bfaces.upload(hb.data(), hb.size(), stream);
+    std::vector<int32_t> mm(std::max<size_t>(xors.size(), 1) * nv, 0);
+    for (size_t s = 0; s < xors.size(); ++s) {
+      for (int q = 0; q < nv; ++q) {
+        const int pm = perm[q] ^ xors[s];
+        KCHECK(pm >= 0 && pm < nv, "mirror xor out of range");
+        mm[s * nv + q] = inv[pm];
+      }
+    }
+    mirror_map.upload(mm.data(), mm.size(), stream);
+
+    if (n_maxwell > 0) {
+      KCHECK(d.maxwell_offset && d.maxwell_specular_fraction && d.grid_to_storage, "Maxwell-wall arrays missing");
+      mw_offset.upload(d.maxwell_offset, nb, stream);
+      mw_frac.upload(d.maxwell_specular_fraction, nb, stream);
+      specular.alloc(static_cast<size_t>(n_maxwell) * nv);
+      specular_first.alloc(static_cast<size_t>(n_maxwell) * nv);
+      KCUDA(cudaMemsetAsync(specular.p, 0, specular.bytes(), stream));
+      KCUDA(cudaMemsetAsync(specular_first.p, 0, specular_first.bytes(), stream));
+      std::vector<int32_t> g2p(nv);
+      for (int k = 0; k < nv; ++k) g2p[k] = inv[d.grid_to_storage[k]];
+      grid_to_pos.upload(g2p.data(), nv, stream);
+    }
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  // level schedule of every (direction group, block) chain: level(c) = 1 + max level of the in-block neighbours
+  // that precede c in the group's sweep order (sweep_order / sweep_pos, kinetic_setup.cpp:474-506)
+  void build_schedule(const KinSetupDesc& d) {
+    const size_t ncs = static_cast<size_t>(nc);
+    std::vector<int32_t> hpos(static_cast<size_t>(n_groups) * ncs);
+    for (int g = 0; g < n_groups; ++g) {
+      for (int c = 0; c < nc; ++c) hpos[g * ncs + c] = d.n_sweep_dirs > 0 ? d.sweep_pos[g * ncs + c] : c;
+    }
+    n_chains = n_groups * n_blocks;
+    std::vector<int32_t> hcells(static_cast<size_t>(n_groups) * ncs), hstart(n_chains), hlev_start(n_chains),
+        hlev_count(n_chains);
+    std::vector<int32_t> hbounds;
+    std::vector<int32_t> level(ncs, 0);
+    max_levels = 0;
+    for (int g = 0; g < n_groups; ++g) {
+      const int32_t* order = d.n_sweep_dirs > 0 ? d.sweep_order + g * ncs : nullptr;
+      const int32_t* pg = hpos.data() + g * ncs;
+      for (int b = 0; b < n_blocks; ++b) {
+        const int cb = h_block_offsets[b], ce = h_block_offsets[b + 1];
+        int nlev = 0;
+        for (int k = cb; k < ce; ++k) {
+          const int c = order ? order[k] : k;
+          KCHECK(c >= cb && c < ce && pg[c] == k, "sweep_order / sweep_pos inconsistent with the blocks");
+          int lv = 0;
+          for (int e = d.csr_offsets[c]; e < d.csr_offsets[c + 1]; ++e) {
+            const int o = d.csr_other[e];
+            if (o >= cb && o < ce && pg[o] < pg[c]) lv = std::max(lv, level[o] + 1);
+          }
+          level[c] = lv;
+          nlev = std::max(nlev, lv + 1);
+        }
+        // bucket the block's cells by level (stable in sweep order)
+        const int chain = g * n_blocks + b;
+        hstart[chain] = static_cast<int32_t>(static_cast<size_t>(g) * ncs + cb);
+        hlev_start[chain] = static_cast<int32_t>(hbounds.size());
+        hlev_count[chain] = nlev;
+        std::vector<int32_t> count(nlev + 1, 0);
+        for (int k = cb; k < ce; ++k) ++count[level[order ? order[k] : k] + 1];
+        for (int l = 0; l < nlev; ++l) count[l + 1] += count[l];
+        for (int l = 0; l <= nlev; ++l) hbounds.push_back(count[l]);
+        std::vector<int32_t> fill(count.begin(), count.end() - 1);
+        for (int k = cb; k < ce; ++k) {
+          const int c = order ? order[k] : k;
+          hcells[static_cast<size_t>(g) * ncs + cb + fill[level[c]]++] = c;
+        }
+        max_levels = std::max(max_levels, nlev);
+      }
+    }
+    chain_cells.upload(hcells.data(), hcells.size(), stream);
+    chain_start.upload(hstart.data(), hstart.size(), stream);
+    lev_bounds.upload(hbounds.data(), hbounds.size(), stream);
+    lev_start.upload(hlev_start.data(), hlev_start.size(), stream);
+    lev_count.upload(hlev_count.data(), hlev_count.size(), stream);
+    pos.upload(hpos.data(), hpos.size(), stream);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void build_chunks() {
+    chunks.clear();
+    for (int k0 = 0; k0 < nv; k0 += chunk) {
+      auto cp = std::make_unique<ChunkPlan>();
+      cp->k0 = k0;
+      cp->kc = std::min(chunk, nv - k0);
+      std::vector<int4> items;
+      for (int g = 0; g < n_groups; ++g) {
+        const int s = std::max(group_begin[g], k0), e = std::min(group_end[g], k0 + cp->kc);
+        if (s >= e) continue;
+        for (int b = 0; b < n_blocks; ++b) {
+          if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
+          for (int t = s; t < e; t += 32) items.push_back(make_int4(g * n_blocks + b, t - k0, std::min(t + 32, e) - k0, 0));
+        }
+      }
+      cp->n_items = static_cast<int32_t>(items.size());
+      cp->items.upload(items.data(), items.size(), stream);
+      chunks.push_back(std::move(cp));
+    }
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  // staging buffer for set/get_distribution (bounded: at most 256 MB of doubles)
+  int32_t staging_cells = 1;
+  void staging_alloc() {
+    staging_cells = static_cast<int32_t>(std::max<int64_t>(1, std::min<int64_t>(nc, (int64_t{32} << 20) / nv)));
+    staging.alloc(static_cast<size_t>(staging_cells) * nv);
+  }
+
+  void update_view() {
+    kin::View<S, M>& v = view;
+    v.n_cells = nc;
+    v.nv = nv;
+    v.n_bfaces = nb;
+    v.xi_x = xi_x.p;
+    v.xi_y = xi_y.p;
+    v.xi_z = xi_z.p;
+    v.xid_x = xid_x.p;
+    v.xid_y = xid_y.p;
+    v.xid_z = xid_z.p;
+    v.wts = wts.p;
+    v.csr_off = csr_off.p;
+    v.csr = csr.p;
+    v.eps2 = eps2.p;
+    v.bf = bfaces.p;
+    v.inflow = inflow.p;
+    v.cp = cells.p;
+    v.f = f.p;
+    v.mirror_map = mirror_map.p;
+    v.mw_offset = mw_offset.p;
+    v.mw_frac = mw_frac.p;
+    v.specular = specular.p;
+    v.specular_first = specular_first.p;
+    v.grid_to_pos = grid_to_pos.p;
+  }
+
+  void set_params(const KinSetupDesc& d) {
+    view.weight = d.weight;
+    view.limiter_mode = d.limiter_mode;
+    view.positivity = d.positivity;
+    view.diag_scale = static_cast<M>(d.diag_scale);
+    view.interface_damping = static_cast<M>(d.interface_damping);
+    for (int a = 0; a < 3; ++a) {
+      view.grid_n[a] = d.grid_n[a];
+      view.deq.lo[a] = d.deq_lo[a];
+      view.deq.hi[a] = d.deq_hi[a];
+      view.deq.d[a] = d.deq_d[a];
+    }
+    view.deq.criterion = d.deq_criterion;
+    view.deq.tolerance = d.deq_tolerance;
+    view.deq.max_iterations = d.deq_max_iterations;
+  }
+
+  void launched(int n = 1) {
+    launches += n;
+    KCUDA(cudaGetLastError());
+  }
+
+  uint64_t memory_bytes() const override {
+    return xi_x.bytes() * 3 + xid_x.bytes() * 3 + wts.bytes() + csr_off.bytes() + csr.bytes() + eps2.bytes() +
+           bfaces.bytes() + inflow.bytes() + cells.bytes() + mirror_map.bytes() + mw_offset.bytes() + mw_frac.bytes() +
+           specular.bytes() * 2 + grid_to_pos.bytes() + volume.bytes() + vdt.bytes() + block_offsets.bytes() +
+           chain_cells.bytes() + chain_start.bytes() + lev_bounds.bytes() + lev_start.bytes() + lev_count.bytes() +
+           pos.bytes() + d_perm.bytes() * 2 + moments.bytes() + shift.bytes() + residual_cell.bytes() + bsums.bytes() +
+           partial.bytes() + w_half.bytes() * 2 + staging.bytes() + flags.bytes() + f.bytes() + gx.bytes() * 4;
+  }
+
+  // ---- KineticBackend methods ------------------------------------------------------------------------------
+  void set_equilibrium(const double* states, int64_t n) override {
+    KCHECK(n == 5LL * nc, "length of the initial states does not match the number of cells");
+    DevBuf<double> d_states;
+    d_states.upload(states, static_cast<size_t>(n), stream);
+    timer.begin(PhaseTimer::kOther, stream);
+    L::set_equilibrium(view, d_states.p, shift.p, discrete_eq, stream);
+    launched();
+    timer.end(stream);
+    timer.flush(timings);
+  }
+
+  void set_distribution(const double* h, int64_t n) override {
+    KCHECK(n == static_cast<int64_t>(nc) * nv, "length of the distribution function does not match");
+    for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
+      const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
+      KCUDA(cudaMemcpyAsync(staging.p, h + c0 * nv, sizeof(double) * cnt * nv, cudaMemcpyHostToDevice, stream));
+      L::import_f(staging.p, f.p, d_perm.p, c0, cnt, nv, stream);
+      launched();
+    }
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void get_distribution(double* h, int64_t n) override {
+    KCHECK(n == static_cast<int64_t>(nc) * nv, "length of the distribution function does not match");
+    for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
+      const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
+      L::export_f(f.p, staging.p, d_inv.p, c0, cnt, nv, stream);
+      launched();
+      KCUDA(cudaMemcpyAsync(h + c0 * nv, staging.p, sizeof(double) * cnt * nv, cudaMemcpyDeviceToHost, stream));
+    }
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void compute_moments(double* out, int64_t n) override {
+    KCHECK(n == 15LL * nc, "length of the moment output does not match");
+    timer.begin(PhaseTimer::kMoments, stream);
+    L::moments(view, shift.p, moments.p, stream);
+    launched();
+    timer.end(stream);
+    KCUDA(cudaMemcpyAsync(out, moments.p, moments.bytes(), cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void scale_distribution(double s) override {
+    timer.begin(PhaseTimer::kOther, stream);
+    L::scale(f.p, static_cast<int64_t>(f.n), s, moments.p, nc, stream);
+    launched(2);
+    timer.end(stream);
+    timer.flush(timings);
+  }
+
+  void update_cell_params() override {
+    timer.begin(PhaseTimer::kOther, stream);
+    L::cell_params(view, moments.p, volume.p, vdt.p, mu0, omega, Pr, cold_bgk_T, discrete_eq, collisionless, cells.p,
+                   flags.p, stream);
+    launched();
+    deq_valid = discrete_eq != 0;
+    timer.end(stream);
+    timer.flush(timings);
+  }
+
+  void deq_counts(KinDeqCounts* out) override {
+    out->corrected = 0;
+    out->failed = 0;
+    out->max_iterations = 0;
+    if (!deq_valid) return;
+    std::vector<int32_t> h(nc);
+    KCUDA(cudaMemcpyAsync(h.data(), flags.p, flags.bytes(), cudaMemcpyDeviceToHost, stream));
+    KCUDA(cudaStreamSynchronize(stream));
+    for (int x : h) {
+      if (x > 0) ++out->corrected;
+      if (x < 0) ++out->failed;
+      out->max_iterations = std::max(out->max_iterations, x);
+    }
+  }
+
+  void set_inflow(const KinInflowState* in, int64_t n) override {
+    KCHECK(n == nb, "length of the inflow states does not match the number of boundary faces");
+    inflow_set = true;
+    if (nb == 0) return;
+    std::vector<Inflow<M>> h(nb);
+    for (int b = 0; b < nb; ++b) {
+      h[b].m = kin::maxwell_from<M>(in[b].rho, in[b].ux, in[b].uy, in[b].uz, in[b].T);
+      h[b].scale = static_cast<M>(in[b].scale);
+    }
+    KCUDA(cudaMemcpyAsync(inflow.p, h.data(), sizeof(Inflow<M>) * nb, cudaMemcpyHostToDevice, stream));
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void boundary_sums(double* out, int64_t n) override {
+    KCHECK(n == 20LL * nb, "length of the boundary-sum output does not match");
+    if (nb == 0) return;
+    timer.begin(PhaseTimer::kBoundary, stream);
+    if (n_maxwell > 0) {
+      L::maxwell_reflection(view, stream);
+      launched(2);
+    }
+    L::boundary_sums(view, bsums.p, stream);
+    launched();
+    timer.end(stream);
+    KCUDA(cudaMemcpyAsync(out, bsums.p, sizeof(double) * 20 * nb, cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void internal_face_mass_flux(const int32_t* hc, const int32_t* he, int64_t n, double* out) override {
+    if (n == 0) return;
+    for (int64_t i = 0; i < n; ++i) {
+      KCHECK(hc[i] >= 0 && hc[i] < nc && he[i] >= 0 && he[i] < static_cast<int64_t>(csr.n),
+             "internal-face cell / entry index out of range");
+    }
+    face_cells.upload(hc, static_cast<size_t>(n), stream);
+    face_entries.upload(he, static_cast<size_t>(n), stream);
+    face_out.alloc(static_cast<size_t>(n));
+    timer.begin(PhaseTimer::kOther, stream);
+    L::internal_face_flux(view, face_cells.p, face_entries.p, face_out.p, static_cast<int>(n), stream);
+    launched();
+    timer.end(stream);
+    KCUDA(cudaMemcpyAsync(out, face_out.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  // gradient, residual and block_passes x (forward + backward) per velocity chunk
+  // (CudaBackend::sweep, kinetic_backend_cuda.cpp:317-372)
+  void sweep(double* residual_out, int64_t n) override {
+    KCHECK(n == nc, "length of the residual output does not match the number of cells");
+    KCUDA(cudaMemsetAsync(residual_cell.p, 0, residual_cell.bytes(), stream));
+    for (const auto& cp : chunks) {
+      kin::Chunk<S> ch{cp->k0, cp->kc, chunk, gx.p, gy.p, gz.p, r.p};
+      timer.begin(PhaseTimer::kGradient, stream);
+      L::gradient(view, ch, stream);
+      launched();
+      timer.end(stream);
+      timer.begin(PhaseTimer::kResidual, stream);
+      L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);
+      launched(2);
+      timer.end(stream);
+      // gradients are dead after the residual: pass k writes Delta f into gz (odd k) / gy (even k) and reads
+      // the previous pass from the other one, R stays in r
+      S* prev = nullptr;
+      for (int pass = 0; pass < block_passes; ++pass) {
+        S* out = (pass % 2 == 0) ? gz.p : gy.p;
+        kin::SweepArgs<S> a{};
+        a.items = cp->items.p;
+        a.n_items = cp->n_items;
+        a.n_blocks = n_blocks;
+        a.block_offsets = block_offsets.p;
+        a.chain_cells = chain_cells.p;
+        a.chain_start = chain_start.p;
+        a.lev_bounds = lev_bounds.p;
+        a.lev_start = lev_start.p;
+        a.lev_count = lev_count.p;
+        a.pos = pos.p;
+        a.R = r.p;
+        a.dprev = prev;
+        a.out = out;
+        a.update_f = pass + 1 == block_passes ? 1 : 0;
+        a.k0 = cp->k0;
+        a.stride = chunk;
+        timer.begin(PhaseTimer::kForward, stream);
+        L::sweep_pass(view, a, stream);
+        launched();
+        timer.end(stream);
+        prev = out;
+      }
+    }
+    KCUDA(cudaMemcpyAsync(residual_out, residual_cell.p, residual_cell.bytes(), cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void gsis_correction(const double* wh, const double* wn, int64_t n, int32_t* out_flags,
+                       int64_t* replaced) override {
+    KCHECK(n == 5LL * nc, "length of the GSIS macroscopic states does not match the number of cells");
+    KCUDA(cudaMemcpyAsync(w_half.p, wh, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+    KCUDA(cudaMemcpyAsync(w_new.p, wn, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+    timer.begin(PhaseTimer::kOther, stream);
+    L::gsis_correction(view, w_half.p, w_new.p, flags.p, shift.p, negative_mode, discrete_eq, collisionless, stream);
+    launched();
+    timer.end(stream);
+    std::vector<int32_t> h(nc);
+    KCUDA(cudaMemcpyAsync(h.data(), flags.p, flags.bytes(), cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+    int64_t cnt = 0;
+    for (int x : h) cnt += x != 0 ? 1 : 0;
+    if (out_flags) std::copy(h.begin(), h.end(), out_flags);
+    *replaced = cnt;
+    deq_valid = false;
+  }
+
+  void take_timings(KinStepTimings* out) override {
+    timer.flush(timings);
+    *out = timings;
+    timings = KinStepTimings{};
+  }
+
+  void device_f(void** p, int32_t* es) override {
+    *p = f.p;
+    *es = static_cast<int32_t>(sizeof(S));
+  }
+
+  void velocity_permutation(int32_t* out, int64_t n) const override {
+    KCHECK(n == nv, "length of the permutation output does not match nv");
+    std::copy(perm.begin(), perm.end(), out);
+  }
+
+  void schedule_info(int32_t* ml, int32_t* nch) const override {
+    *ml = max_levels;
+    *nch = n_chains;
+  }
+};
+
+template <class Fn>
+int guard(KinHandle* h, Fn&& fn) {
+  if (h == nullptr) return KIN_E_ARG;
+  try {
+    cudaSetDevice(h->device);
+    fn();
+    return KIN_OK;
+  } catch (const KinError& e) {
+    h->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    h->err = e.what();
+    return KIN_E_ARG;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int kin_create(const KinSetupDesc* d, KinHandle** out) {
+  if (out == nullptr || d == nullptr) {
+    g_create_error = "kin_create: null argument";
+    return KIN_E_ARG;
+  }
+  *out = nullptr;
+  try {
+    if (d->abi_version != KIN_ABI_VERSION) throw KinError(KIN_E_ARG, "KinSetupDesc ABI version mismatch");
+    KinHandle* h = nullptr;
+    switch (d->precision) {
+      case KIN_PREC_FP32: {
+        auto* b = new Backend<float, float>(*d);
+        b->set_params(*d);
+        h = b;
+        break;
+      }
+      case KIN_PREC_FP64: {
+        auto* b = new Backend<double, double>(*d);
+        b->set_params(*d);
+        h = b;
+        break;
+      }
+      case KIN_PREC_MIXED: {
+        auto* b = new Backend<float, double>(*d);
+        b->set_params(*d);
+        h = b;
+        break;
+      }
+      default:
+        throw KinError(KIN_E_ARG, "unknown precision");
+    }
+    *out = h;
+    return KIN_OK;
+  } catch (const KinError& e) {
+    g_create_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return KIN_E_ARG;
+  }
+}
+
+void kin_destroy(KinHandle* h) { delete h; }
+
+const char* kin_last_error(const KinHandle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+const char* kin_name(const KinHandle* h) { return h ? h->name() : "b200"; }
+
+int kin_chunk_width(const KinHandle* h, int32_t* out) {
+  return guard(const_cast<KinHandle*>(h), [&] { *out = h->chunk_width(); });
+}
+int kin_memory_bytes(const KinHandle* h, uint64_t* out) {
+  return guard(const_cast<KinHandle*>(h), [&] { *out = h->memory_bytes(); });
+}
+int kin_set_equilibrium(KinHandle* h, const double* s, int64_t n) { return guard(h, [&] { h->set_equilibrium(s, n); }); }
+int kin_set_distribution(KinHandle* h, const double* f, int64_t n) {
+  return guard(h, [&] { h->set_distribution(f, n); });
+}
+int kin_get_distribution(KinHandle* h, double* f, int64_t n) { return guard(h, [&] { h->get_distribution(f, n); }); }
+int kin_compute_moments(KinHandle* h, double* out, int64_t n) { return guard(h, [&] { h->compute_moments(out, n); }); }
+int kin_scale_distribution(KinHandle* h, double s) { return guard(h, [&] { h->scale_distribution(s); }); }
+int kin_update_cell_params(KinHandle* h) { return guard(h, [&] { h->update_cell_params(); }); }
+int kin_set_inflow(KinHandle* h, const KinInflowState* in, int64_t n) { return guard(h, [&] { h->set_inflow(in, n); }); }
+int kin_boundary_sums(KinHandle* h, double* out, int64_t n) { return guard(h, [&] { h->boundary_sums(out, n); }); }
+int kin_sweep(KinHandle* h, double* res, int64_t n) { return guard(h, [&] { h->sweep(res, n); }); }
+int kin_gsis_correction(KinHandle* h, const double* wh, const double* wn, int64_t n, int32_t* flags,
+                        int64_t* replaced) {
+  return guard(h, [&] { h->gsis_correction(wh, wn, n, flags, replaced); });
+}
+int kin_internal_face_mass_flux(KinHandle* h, const int32_t* cells, const int32_t* entries, int64_t n, double* out) {
+  return guard(h, [&] { h->internal_face_mass_flux(cells, entries, n, out); });
+}
+int kin_take_timings(KinHandle* h, KinStepTimings* out) { return guard(h, [&] { h->take_timings(out); }); }
+int kin_deq_counts(KinHandle* h, KinDeqCounts* out) { return guard(h, [&] { h->deq_counts(out); }); }
+
+int kin_set_stream(KinHandle* h, void* stream) {
+  return guard(h, [&] {
+    KCUDA(cudaStreamSynchronize(h->stream));
+    h->stream = stream != nullptr ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  });
+}
+int kin_launch_count(const KinHandle* h, int64_t* out) {
+  return guard(const_cast<KinHandle*>(h), [&] { *out = h->launches; });
+}
+int kin_device_f(KinHandle* h, void** f, int32_t* es) { return guard(h, [&] { h->device_f(f, es); }); }
+int kin_velocity_permutation(const KinHandle* h, int32_t* perm, int64_t n) {
+  return guard(const_cast<KinHandle*>(h), [&] { h->velocity_permutation(perm, n); });
+}
+int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains) {
+  return guard(const_cast<KinHandle*>(h), [&] { h->schedule_info(max_levels, n_chains); });
+}
+
+}  // extern "C"

@@ -1,0 +1,720 @@
+// Kernels of the B200 kinetic backend. See kin_kernels.cuh for the data layout; every kernel names the
+// reference routine whose semantics it reproduces.
+#include "kin_kernels.cuh"
+#include "kin_launch.h"
+
+namespace kin {
+
+constexpr int kCellThreads = 256;  // moments / Newton / correction: one CTA per cell
+constexpr int kFaceThreads = 128;  // boundary sums / face fluxes: one CTA per face
+constexpr int kTileThreads = 256;  // gradient / residual: one CTA per (cell, velocity tile)
+
+// ---------------------------------------------------------------------------------------------------------
+// f = f_eq(state), shift = u (k_set_equilibrium / CpuBackend::set_equilibrium,
+// src/kinetic/kinetic_backend_cpu.cpp:64-80)
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__global__ void __launch_bounds__(kCellThreads)
+    k_set_equilibrium(View<S, M> v, const double* __restrict__ states, double* __restrict__ shift, int discrete) {
+  __shared__ double sh_red[kDeqSums * (kCellThreads / 32)];
+  __shared__ double sh_state[12];
+  const int c = blockIdx.x;
+  const double* st = states + 5 * static_cast<int64_t>(c);
+  Maxwell<M> m = maxwell_from<M>(st[0], st[1], st[2], st[3], st[4]);
+  if (discrete) {
+    double gamma[5];
+    block_discrete_maxwell<S, M, kCellThreads>(v, st[0], st[1], st[2], st[3], st[4], nullptr, m, gamma, sh_red,
+                                               sh_state);
+  }
+  S* fc = v.f + static_cast<int64_t>(c) * v.nv;
+  for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+    fc[q] = static_cast<S>(maxwellian(m, v.xi_x[q], v.xi_y[q], v.xi_z[q]));
+  }
+  if (threadIdx.x == 0) {
+    shift[3 * static_cast<int64_t>(c) + 0] = st[1];
+    shift[3 * static_cast<int64_t>(c) + 1] = st[2];
+    shift[3 * static_cast<int64_t>(c) + 2] = st[3];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// 13 shifted sums in FP64 -> 15 moments (CpuBackend::compute_moments, kinetic_backend_cpu.cpp:92-120)
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__global__ void __launch_bounds__(kCellThreads)
+    k_moments(View<S, M> v, double* __restrict__ shift, double* __restrict__ out) {
+  __shared__ double sh[kMomentSums * (kCellThreads / 32)];
+  const int c = blockIdx.x;
+  const double u0x = shift[3 * static_cast<int64_t>(c) + 0];
+  const double u0y = shift[3 * static_cast<int64_t>(c) + 1];
+  const double u0z = shift[3 * static_cast<int64_t>(c) + 2];
+  const S* fc = v.f + static_cast<int64_t>(c) * v.nv;
+  const bool uniform = v.wts == nullptr;
+  double acc[kMomentSums];
+#pragma unroll
+  for (int k = 0; k < kMomentSums; ++k) acc[k] = 0.0;
+  for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+    double f = static_cast<double>(fc[q]);
+    if (!uniform) f *= v.wts[q];
+    const double cx = v.xid_x[q] - u0x, cy = v.xid_y[q] - u0y, cz = v.xid_z[q] - u0z;
+    const double t1 = f * cx, t2 = f * cy, t3 = f * cz;
+    const double fc2 = f * (cx * cx + cy * cy + cz * cz);
+    acc[0] += f;
+    acc[1] += t1;
+    acc[2] += t2;
+    acc[3] += t3;
+    acc[4] += t1 * cx;
+    acc[5] += t2 * cy;
+    acc[6] += t3 * cz;
+    acc[7] += t1 * cy;
+    acc[8] += t2 * cz;
+    acc[9] += t1 * cz;
+    acc[10] += fc2 * cx;
+    acc[11] += fc2 * cy;
+    acc[12] += fc2 * cz;
+  }
+  block_sum<kMomentSums, kCellThreads>(acc, sh);
+  if (threadIdx.x == 0) {
+    double* m = out + 15 * static_cast<int64_t>(c);
+    finalize_moments(acc, uniform ? v.weight : 1.0, u0x, u0y, u0z, m);
+    if (m[0] > 0.0) {
+      shift[3 * static_cast<int64_t>(c) + 0] = m[1];
+      shift[3 * static_cast<int64_t>(c) + 1] = m[2];
+      shift[3 * static_cast<int64_t>(c) + 2] = m[3];
+    }
+  }
+}
+
+// f *= s ; moments (rho, p, sigma, q) *= s   (k_scale / k_scale_moments, kinetic_cuda_kernels.cu:207-219)
+template <class S>
+__global__ void k_scale(S* __restrict__ f, int64_t n, double s) {
+  const S sf = static_cast<S>(s);
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) f[i] *= sf;
+}
+
+__global__ void k_scale_moments(double* __restrict__ m, int n_cells, double s) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  double* mc = m + 15 * static_cast<int64_t>(c);
+  mc[0] *= s;
+  for (int k = 5; k < 15; ++k) mc[k] *= s;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// cell parameters (k_cell_params / k_cell_params_deq, kinetic_cuda_kernels.cu:221-260;
+// CpuBackend::update_cell_params, kinetic_backend_cpu.cpp:134-163)
+// ---------------------------------------------------------------------------------------------------------
+template <class M>
+__global__ void k_cell_params(const double* __restrict__ moments, const double* __restrict__ volume,
+                              const double* __restrict__ vdt, double mu0, double omega, double Pr,
+                              CellParams<M>* __restrict__ out, int n_cells, double cold_bgk_T) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  out[c] = make_cell_params<M>(moments + 15 * static_cast<int64_t>(c), volume[c], vdt[c], mu0, omega, Pr, cold_bgk_T);
+}
+
+template <class S, class M>
+__global__ void __launch_bounds__(kCellThreads)
+    k_cell_params_deq(View<S, M> v, const double* __restrict__ moments, const double* __restrict__ volume,
+                      const double* __restrict__ vdt, double mu0, double omega, double Pr, double cold_bgk_T,
+                      int collisionless, CellParams<M>* __restrict__ out, int* __restrict__ flags) {
+  __shared__ double sh_red[kDeqSums * (kCellThreads / 32)];
+  __shared__ double sh_state[12];
+  const int c = blockIdx.x;
+  const double* m = moments + 15 * static_cast<int64_t>(c);
+  CellParams<M> cp = make_cell_params<M>(m, volume[c], vdt[c], mu0, omega, Pr, cold_bgk_T);
+  Maxwell<M> eq;
+  double gamma[5];
+  const int r = block_discrete_maxwell<S, M, kCellThreads>(v, m[0], m[1], m[2], m[3], m[4], &cp, eq, gamma, sh_red,
+                                                           sh_state);
+  if (threadIdx.x == 0) {
+    if (r > 0) {
+      cp.eq = eq;
+      cp.g0 = static_cast<M>(gamma[0]);
+      cp.gx = static_cast<M>(gamma[1]);
+      cp.gy = static_cast<M>(gamma[2]);
+      cp.gz = static_cast<M>(gamma[3]);
+      cp.g4 = static_cast<M>(gamma[4]);
+    } else if (r < 0 && collisionless) {
+      cp.coll = M(0);
+      cp.diag = static_cast<M>(vdt[c]);
+    }
+    out[c] = cp;
+    flags[c] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// specular cache of partially accommodating walls (k_maxwell_reflection / reflected_value,
+// kinetic_cuda_kernels.cu:262-272, kinetic_kernels.hpp:86-127)
+// ---------------------------------------------------------------------------------------------------------
+template <bool Reconstruct, class S, class M>
+__device__ inline M reflected_value(const View<S, M>& v, const BFace<M>& b, int q, M x, M y, M z) {
+  if (b.mirror >= 0) {
+    const int qm = v.mirror_map[b.mirror * v.nv + q];
+    if (Reconstruct) return reconstruct_at_boundary(v, b, qm);
+    return f_at(v, b.owner, qm);
+  }
+  const M un = x * b.n[0] + y * b.n[1] + z * b.n[2];
+  const M r[3] = {x - M(2) * un * b.n[0], y - M(2) * un * b.n[1], z - M(2) * un * b.n[2]};
+  int base[3];
+  M t[3];
+  for (int a = 0; a < 3; ++a) {
+    const double zz = (static_cast<double>(r[a]) - v.deq.lo[a]) / v.deq.d[a] - 0.5;
+    if (zz < -1e-5 || zz > v.grid_n[a] - 1.0 + 1e-5) return M(0);
+    const double clipped = kmax(0.0, kmin(zz, v.grid_n[a] - 1.0));
+    base[a] = static_cast<int>(clipped);
+    if (base[a] >= v.grid_n[a] - 1) base[a] = v.grid_n[a] - 2;
+    t[a] = static_cast<M>(clipped - base[a]);
+  }
+  M result = M(0);
+  const CellParams<M> ref = v.cp[b.owner];
+  for (int k = 0; k < 8; ++k) {
+    const int ix = base[0] + (k & 1), iy = base[1] + ((k >> 1) & 1), iz = base[2] + ((k >> 2) & 1);
+    const M w = ((k & 1) ? t[0] : M(1) - t[0]) * ((k & 2) ? t[1] : M(1) - t[1]) * ((k & 4) ? t[2] : M(1) - t[2]);
+    if (w == M(0)) continue;
+    const int qq = v.grid_to_pos[ix + v.grid_n[0] * (iy + v.grid_n[1] * iz)];
+    M value;
+    if (Reconstruct) value = reconstruct_at_boundary(v, b, qq);
+    else value = f_at(v, b.owner, qq);
+    const double drx = static_cast<double>(r[0]) - ref.eq.ux, dry = static_cast<double>(r[1]) - ref.eq.uy,
+                 drz = static_cast<double>(r[2]) - ref.eq.uz;
+    const double dqx = static_cast<double>(v.xi_x[qq]) - ref.eq.ux, dqy = static_cast<double>(v.xi_y[qq]) - ref.eq.uy,
+                 dqz = static_cast<double>(v.xi_z[qq]) - ref.eq.uz;
+    const double ratio =
+        exp(-static_cast<double>(ref.eq.B) * (drx * drx + dry * dry + drz * drz - dqx * dqx - dqy * dqy - dqz * dqz));
+    result += w * static_cast<M>(static_cast<double>(value) * ratio);
+  }
+  return result;
+}
+
+template <bool Reconstruct, class S, class M>
+__global__ void k_maxwell_reflection(View<S, M> v) {
+  const int b = blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= v.nv || v.mw_offset[b] < 0) return;
+  const BFace<M> bf = v.bf[b];
+  const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+  M* buffer = Reconstruct ? v.specular : v.specular_first;
+  buffer[v.mw_offset[b] + q] = (x * bf.n[0] + y * bf.n[1] + z * bf.n[2]) < M(0)
+                                   ? reflected_value<Reconstruct>(v, bf, q, x, y, z)
+                                   : M(0);
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// 20 half-space sums per boundary face (CpuBackend::boundary_sums, kinetic_backend_cpu.cpp:184-240;
+// add_boundary_terms, kinetic_kernels.hpp:596-609). Terms in M, sums in FP64.
+// ---------------------------------------------------------------------------------------------------------
+template <class M>
+__device__ __forceinline__ void add_boundary_terms(M wf, M x, M y, M z, M a_n, double* flux5, double* mom5) {
+  const M e = M(0.5) * (x * x + y * y + z * z);
+  const M af = a_n * wf;
+  flux5[0] += static_cast<double>(af);
+  flux5[1] += static_cast<double>(af * x);
+  flux5[2] += static_cast<double>(af * y);
+  flux5[3] += static_cast<double>(af * z);
+  flux5[4] += static_cast<double>(af * e);
+  mom5[0] += static_cast<double>(wf);
+  mom5[1] += static_cast<double>(wf * x);
+  mom5[2] += static_cast<double>(wf * y);
+  mom5[3] += static_cast<double>(wf * z);
+  mom5[4] += static_cast<double>(wf * e);
+}
+
+template <class S, class M>
+__global__ void __launch_bounds__(kFaceThreads) k_boundary_sums(View<S, M> v, double* __restrict__ out) {
+  __shared__ double sh[20 * (kFaceThreads / 32)];
+  const int b = blockIdx.x;
+  const BFace<M> bf = v.bf[b];
+  const Maxwell<M> m_in = v.inflow[b].m;
+  const M wu = static_cast<M>(v.weight);
+  double acc[20];
+#pragma unroll
+  for (int k = 0; k < 20; ++k) acc[k] = 0.0;
+  for (int q = threadIdx.x; q < v.nv; q += kFaceThreads) {
+    const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+    const M w = v.wts == nullptr ? wu : static_cast<M>(v.wts[q]);
+    const M a_n = x * bf.n[0] + y * bf.n[1] + z * bf.n[2];
+    if (a_n >= M(0) || bf.kind == kPeriodic) {
+      const M fb = reconstruct_at_boundary(v, bf, q);
+      add_boundary_terms(w * fb, x, y, z, a_n, acc + 0, acc + 10);
+    } else {
+      M fb;
+      if (bf.kind == kSymmetry) {
+        fb = reconstruct_at_boundary(v, bf, v.mirror_map[bf.mirror * v.nv + q]);
+      } else if (bf.kind == kMaxwellWall) {
+        fb = maxwell_inflow(v, b, q, x, y, z);
+      } else {
+        fb = maxwellian(m_in, x, y, z);  // unit density, without scale
+      }
+      add_boundary_terms(w * fb, x, y, z, a_n, acc + 5, acc + 15);
+    }
+  }
+  block_sum<20, kFaceThreads>(acc, sh);
+  if (threadIdx.x == 0) {
+    double* o = out + 20 * static_cast<int64_t>(b);
+    for (int k = 0; k < 20; ++k) o[k] = acc[k];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// section mass flux through internal faces (internal_face_flux_term, kinetic_kernels.hpp:217-231;
+// CpuBackend::internal_face_mass_flux, kinetic_backend_cpu.cpp:242-260)
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__global__ void __launch_bounds__(kFaceThreads)
+    k_internal_face_flux(View<S, M> v, const int32_t* __restrict__ cells, const int32_t* __restrict__ entries,
+                         double* __restrict__ out) {
+  __shared__ double sh[kFaceThreads / 32];
+  const int i = blockIdx.x;
+  const int c = cells[i];
+  const CsrE<M> ce = v.csr[entries[i]];
+  double acc[1] = {0.0};
+  for (int q = threadIdx.x; q < v.nv; q += kFaceThreads) {
+    const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+    const M a = x * ce.s[0] + y * ce.s[1] + z * ce.s[2];
+    M ff, gx, gy, gz;
+    if (a >= M(0)) {
+      const M fi = f_at(v, c, q);
+      limited_gradient(v, c, q, x, y, z, fi, gx, gy, gz);
+      ff = fi + gx * ce.ds[0] + gy * ce.ds[1] + gz * ce.ds[2];
+    } else {
+      const M fj = f_at(v, ce.other, q);
+      limited_gradient(v, ce.other, q, x, y, z, fj, gx, gy, gz);
+      ff = fj + gx * ce.dn[0] + gy * ce.dn[1] + gz * ce.dn[2];
+    }
+    double term = static_cast<double>(a * ff);
+    if (v.wts != nullptr) term *= v.wts[q];
+    acc[0] += term;
+  }
+  block_sum<1, kFaceThreads>(acc, sh);
+  if (threadIdx.x == 0) out[i] = (v.wts == nullptr ? static_cast<double>(static_cast<M>(v.weight)) : 1.0) * acc[0];
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// limited gradients of one velocity chunk (k_gradient, kinetic_cuda_kernels.cu:343-355)
+// grid: (cell, velocity tile of kTileThreads * kTileIters)
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__global__ void __launch_bounds__(kTileThreads) k_gradient(View<S, M> v, Chunk<S> ch) {
+  const int c = blockIdx.x;
+  const int tb = blockIdx.y * (kTileThreads * kTileIters);
+  const int te = min(ch.kc, tb + kTileThreads * kTileIters);
+  for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
+    const int q = ch.k0 + t;
+    const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+    M gx, gy, gz;
+    limited_gradient(v, c, q, x, y, z, f_at(v, c, q), gx, gy, gz);
+    const int64_t wi = static_cast<int64_t>(c) * ch.stride + t;
+    ch.gx[wi] = static_cast<S>(gx);
+    ch.gy[wi] = static_cast<S>(gy);
+    ch.gz[wi] = static_cast<S>(gz);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// steady residual R = sum_e a f_face - (V/tau)(f^S - f) of one chunk (residual_value, kinetic_kernels.hpp:238-278)
+// and per-(cell, tile) partial sums of R^2 in FP64 (k_residual, kinetic_cuda_kernels.cu:357-372)
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__device__ inline M residual_value(const View<S, M>& v, const Chunk<S>& ch, int cell, int t) {
+  const int q = ch.k0 + t;
+  const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+  const M fi = f_at(v, cell, q);
+  const int64_t wi = static_cast<int64_t>(cell) * ch.stride + t;
+  const M gix = static_cast<M>(ch.gx[wi]), giy = static_cast<M>(ch.gy[wi]), giz = static_cast<M>(ch.gz[wi]);
+  M R = M(0);
+  const int e0 = v.csr_off[cell], e1 = v.csr_off[cell + 1];
+  for (int e = e0; e < e1; ++e) {
+    const CsrE<M>& c = v.csr[e];
+    int kind = -1;
+    if (c.other < 0) {
+      kind = v.bf[c.bface].kind;
+      if (kind == kPeriodic) continue;
+    }
+    const M a = x * c.s[0] + y * c.s[1] + z * c.s[2];
+    M ff;
+    if (a >= M(0)) {
+      ff = fi + gix * c.ds[0] + giy * c.ds[1] + giz * c.ds[2];
+    } else if (c.other >= 0) {
+      const int64_t wj = static_cast<int64_t>(c.other) * ch.stride + t;
+      ff = f_at(v, c.other, q) + static_cast<M>(ch.gx[wj]) * c.dn[0] + static_cast<M>(ch.gy[wj]) * c.dn[1] +
+           static_cast<M>(ch.gz[wj]) * c.dn[2];
+    } else if (kind == kSymmetry) {
+      // outflow reconstruction of the mirrored velocity at the same cell (its gradient recomputed: the mirrored
+      // velocity need not lie in this chunk)
+      const int qm = v.mirror_map[v.bf[c.bface].mirror * v.nv + q];
+      const M fm = f_at(v, cell, qm);
+      M gx, gy, gz;
+      limited_gradient(v, cell, qm, v.xi_x[qm], v.xi_y[qm], v.xi_z[qm], fm, gx, gy, gz);
+      ff = fm + gx * c.ds[0] + gy * c.ds[1] + gz * c.ds[2];
+    } else if (kind == kMaxwellWall) {
+      ff = maxwell_inflow(v, c.bface, q, x, y, z);
+    } else {
+      ff = inflow_value(v.inflow[c.bface], x, y, z);
+    }
+    R += a * ff;
+  }
+  const CellParams<M>& cp = v.cp[cell];
+  R -= cp.coll * (shakhov_target(cp, x, y, z) - fi);
+  return R;
+}
+
+template <class S, class M>
+__global__ void __launch_bounds__(kTileThreads)
+    k_residual(View<S, M> v, Chunk<S> ch, double* __restrict__ partial, int partial_stride) {
+  __shared__ double sh[kTileThreads / 32];
+  const int c = blockIdx.x;
+  const int tb = blockIdx.y * (kTileThreads * kTileIters);
+  const int te = min(ch.kc, tb + kTileThreads * kTileIters);
+  double r2[1] = {0.0};
+  for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
+    const M R = residual_value(v, ch, c, t);
+    ch.r[static_cast<int64_t>(c) * ch.stride + t] = static_cast<S>(R);
+    r2[0] += static_cast<double>(R) * static_cast<double>(R);
+  }
+  block_sum<1, kTileThreads>(r2, sh);
+  if (threadIdx.x == 0) partial[static_cast<int64_t>(c) * partial_stride + blockIdx.y] = r2[0];
+}
+
+__global__ void k_residual_reduce(const double* __restrict__ partial, int partial_stride, int n_tiles,
+                                  double* __restrict__ residual_cell, int n_cells) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  double s = 0.0;
+  for (int k = 0; k < n_tiles; ++k) s += partial[static_cast<int64_t>(c) * partial_stride + k];
+  residual_cell[c] += s;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// one LU-SGS block pass: forward then backward sweep of one (direction group, block) chain per warp, 32
+// velocities per warp (sweep_forward_cell / sweep_backward_cell, kinetic_kernels.hpp:289-358).
+//   pass 1:  R = r,  dprev = nullptr (out-of-block coupling -> beta sum|a-| on the diagonal)
+//   pass k:  R = r,  dprev = Delta f of pass k-1 (out-of-block upwind neighbours on the right-hand side)
+// out receives Delta f* (forward) and then Delta f (backward); the last pass adds Delta f to f.
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__device__ __forceinline__ void sweep_forward_cell(const View<S, M>& v, const SweepArgs<S>& a, int cell, int t,
+                                                   int cb, int ce, const int32_t* pos, M x, M y, M z) {
+  M ap = M(0), am_out = M(0), L = M(0), Lout = M(0);
+  const int e0 = v.csr_off[cell], e1 = v.csr_off[cell + 1];
+  const int pi = pos[cell];
+  for (int e = e0; e < e1; ++e) {
+    const CsrE<M>& c = v.csr[e];
+    if (c.other < 0 && v.bf[c.bface].kind == kPeriodic) continue;
+    const M af = x * c.s[0] + y * c.s[1] + z * c.s[2];
+    if (af > M(0)) {
+      ap += af;
+    } else if (c.other >= 0) {
+      if (c.other < cb || c.other >= ce) {
+        if (a.dprev != nullptr) {
+          Lout += af * static_cast<M>(a.dprev[static_cast<int64_t>(c.other) * a.stride + t]);
+        } else {
+          am_out -= af;
+        }
+      } else if (pos[c.other] < pi) {
+        L += af * static_cast<M>(a.out[static_cast<int64_t>(c.other) * a.stride + t]);
+      }
+    }
+  }
+  const M D = v.cp[cell].diag + v.diag_scale * ap + v.interface_damping * am_out;
+  const int64_t wi = static_cast<int64_t>(cell) * a.stride + t;
+  const M Ri = static_cast<M>(a.R[wi]);
+  a.out[wi] = static_cast<S>((-Ri - Lout - L) / D);
+}
+
+template <class S, class M>
+__device__ __forceinline__ void sweep_backward_cell(const View<S, M>& v, const SweepArgs<S>& a, int cell, int t,
+                                                    int q, int cb, int ce, const int32_t* pos, M x, M y, M z) {
+  M ap = M(0), am_out = M(0), U = M(0);
+  const int e0 = v.csr_off[cell], e1 = v.csr_off[cell + 1];
+  const int pi = pos[cell];
+  for (int e = e0; e < e1; ++e) {
+    const CsrE<M>& c = v.csr[e];
+    if (c.other < 0 && v.bf[c.bface].kind == kPeriodic) continue;
+    const M af = x * c.s[0] + y * c.s[1] + z * c.s[2];
+    if (af > M(0)) {
+      ap += af;
+    } else if (c.other >= 0) {
+      if (c.other < cb || c.other >= ce) {
+        if (a.dprev == nullptr) am_out -= af;
+      } else if (pos[c.other] > pi) {
+        U += af * static_cast<M>(a.out[static_cast<int64_t>(c.other) * a.stride + t]);
+      }
+    }
+  }
+  const M D = v.cp[cell].diag + v.diag_scale * ap + v.interface_damping * am_out;
+  const int64_t wi = static_cast<int64_t>(cell) * a.stride + t;
+  const M df = static_cast<M>(a.out[wi]) - U / D;
+  a.out[wi] = static_cast<S>(df);
+  if (a.update_f) {
+    S* fp = v.f + static_cast<int64_t>(cell) * v.nv + q;
+    *fp = static_cast<S>(static_cast<M>(*fp) + df);
+  }
+}
+
+template <class S, class M>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep_pass(View<S, M> v, SweepArgs<S> a) {
+  const int item = (blockIdx.x * kSweepThreads + threadIdx.x) >> 5;
+  if (item >= a.n_items) return;
+  const int4 it = a.items[item];  // (chain, t0, t1, -)
+  const int lane = threadIdx.x & 31;
+  const int t = it.y + lane;
+  const bool active = t < it.z;
+  const int q = a.k0 + t;
+  const int chain = it.x;
+  const int g = chain / a.n_blocks;
+  const int b = chain - g * a.n_blocks;
+  const int cb = a.block_offsets[b], ce = a.block_offsets[b + 1];
+  const int32_t* cells = a.chain_cells + a.chain_start[chain];
+  const int32_t* lb = a.lev_bounds + a.lev_start[chain];
+  const int nlev = a.lev_count[chain];
+  const int32_t* pos = a.pos + static_cast<int64_t>(g) * v.n_cells;
+  M x = M(0), y = M(0), z = M(0);
+  if (active) {
+    x = v.xi_x[q];
+    y = v.xi_y[q];
+    z = v.xi_z[q];
+  }
+  if (!active) return;  // lanes never exchange data: an idle lane can leave
+  for (int L = 0; L < nlev; ++L) {
+    const int i1 = lb[L + 1];
+    for (int i = lb[L]; i < i1; ++i) sweep_forward_cell(v, a, cells[i], t, cb, ce, pos, x, y, z);
+  }
+  for (int L = nlev - 1; L >= 0; --L) {
+    const int i0 = lb[L];
+    for (int i = lb[L + 1] - 1; i >= i0; --i) sweep_backward_cell(v, a, cells[i], t, q, cb, ce, pos, x, y, z);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// GSIS correction f += f_eq(W_new) - f_eq(W_half) with the negativity rule (CpuBackend::gsis_correction,
+// kinetic_backend_cpu.cpp:346-432; k_gsis_correction, kinetic_cuda_kernels.cu:427-518)
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__global__ void __launch_bounds__(kCellThreads)
+    k_gsis_correction(View<S, M> v, const double* __restrict__ w_half, const double* __restrict__ w_new,
+                      int* __restrict__ flags, double* __restrict__ shift, int mode, int discrete,
+                      int collisionless) {
+  __shared__ double sh_red[kDeqSums * (kCellThreads / 32)];
+  __shared__ double sh_state[12];
+  __shared__ M sh_m[kCellThreads / 32 + 1];
+  const int c = blockIdx.x;
+  const double* wh = w_half + 5 * static_cast<int64_t>(c);
+  const double* wn = w_new + 5 * static_cast<int64_t>(c);
+  Maxwell<M> mh = maxwell_from<M>(wh[0], wh[1], wh[2], wh[3], wh[4]);
+  Maxwell<M> mn = maxwell_from<M>(wn[0], wn[1], wn[2], wn[3], wn[4]);
+  if (discrete) {
+    double gamma[5];
+    const int rh = block_discrete_maxwell<S, M, kCellThreads>(v, wh[0], wh[1], wh[2], wh[3], wh[4], nullptr, mh,
+                                                              gamma, sh_red, sh_state);
+    const int rn = block_discrete_maxwell<S, M, kCellThreads>(v, wn[0], wn[1], wn[2], wn[3], wn[4], nullptr, mn,
+                                                              gamma, sh_red, sh_state);
+    if (collisionless && (rh < 0 || rn < 0)) {
+      if (threadIdx.x == 0) {
+        flags[c] = kCorrectionSkipped;
+        shift[3 * static_cast<int64_t>(c) + 0] = wh[1];
+        shift[3 * static_cast<int64_t>(c) + 1] = wh[2];
+        shift[3 * static_cast<int64_t>(c) + 2] = wh[3];
+      }
+      return;
+    }
+  }
+  S* fc = v.f + static_cast<int64_t>(c) * v.nv;
+  const double threshold = -1e-8 * wn[0] / (wn[4] * sqrt(wn[4]));
+  const M thr = static_cast<M>(threshold);
+  bool replace;
+  if (mode == kNegLimit) {
+    M alpha = M(1);
+    for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+      alpha = kmin(alpha, correction_alpha_limit(static_cast<M>(fc[q]), maxwellian(mn, x, y, z) - maxwellian(mh, x, y, z), thr));
+    }
+    alpha = block_reduce_op<kCellThreads>(alpha, sh_m, [](M p, M r) { return kmin(p, r); });
+    for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+      fc[q] = static_cast<S>(static_cast<M>(fc[q]) + alpha * (maxwellian(mn, x, y, z) - maxwellian(mh, x, y, z)));
+    }
+    replace = alpha < M(1);
+  } else if (mode == kNegBlend) {
+    M theta = M(0);
+    for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+      const M e = maxwellian(mn, x, y, z);
+      theta = kmax(theta, blend_theta(static_cast<M>(fc[q]), e - maxwellian(mh, x, y, z), e, thr));
+    }
+    theta = block_reduce_op<kCellThreads>(theta, sh_m, [](M p, M r) { return kmax(p, r); });
+    for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+      const M e = maxwellian(mn, x, y, z);
+      const M g = static_cast<M>(fc[q]) + (e - maxwellian(mh, x, y, z));
+      fc[q] = static_cast<S>((M(1) - theta) * g + theta * e);
+    }
+    replace = theta > M(0);
+  } else {
+    // minimum of the check value over all points (the first point seeds the minimum)
+    M fmin = M(0);
+    bool first = true;
+    for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+      const M old = static_cast<M>(fc[q]);
+      const M xnew = old + (maxwellian(mn, x, y, z) - maxwellian(mh, x, y, z));
+      fc[q] = static_cast<S>(xnew);
+      const M chk = negative_check_value(old, xnew, mode == kNegCreated);
+      fmin = first ? chk : kmin(fmin, chk);
+      first = false;
+    }
+    if (first) fmin = M(1e30);  // threads without points do not take part in the minimum
+    fmin = block_reduce_op<kCellThreads>(fmin, sh_m, [](M p, M r) { return kmin(p, r); });
+    replace = static_cast<double>(fmin) < threshold;
+    if (replace) {
+      for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+        fc[q] = static_cast<S>(maxwellian(mn, v.xi_x[q], v.xi_y[q], v.xi_z[q]));
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    flags[c] = replace ? 1 : 0;
+    shift[3 * static_cast<int64_t>(c) + 0] = wn[1];
+    shift[3 * static_cast<int64_t>(c) + 1] = wn[2];
+    shift[3 * static_cast<int64_t>(c) + 2] = wn[3];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// f <-> host order (cells c0 .. c0 + n of a staging buffer in the reference storage order)
+// ---------------------------------------------------------------------------------------------------------
+template <class S>
+__global__ void k_import(const double* __restrict__ src, S* __restrict__ f, const int32_t* __restrict__ perm, int64_t c0,
+                         int n_cells, int nv) {
+  const int64_t n = static_cast<int64_t>(n_cells) * nv;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int64_t c = i / nv;
+    const int q = static_cast<int>(i - c * nv);
+    f[(c0 + c) * nv + q] = static_cast<S>(src[c * nv + perm[q]]);
+  }
+}
+
+template <class S>
+__global__ void k_export(const S* __restrict__ f, double* __restrict__ dst, const int32_t* __restrict__ inv, int64_t c0,
+                         int n_cells, int nv) {
+  const int64_t n = static_cast<int64_t>(n_cells) * nv;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int64_t c = i / nv;
+    const int p = static_cast<int>(i - c * nv);
+    dst[c * nv + p] = static_cast<double>(f[(c0 + c) * nv + inv[p]]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------------------------
+inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+template <class S, class M>
+void Launch<S, M>::set_equilibrium(const View<S, M>& v, const double* states, double* shift, int discrete,
+                                   cudaStream_t st) {
+  if (v.n_cells > 0) k_set_equilibrium<S, M><<<v.n_cells, kCellThreads, 0, st>>>(v, states, shift, discrete);
+}
+
+template <class S, class M>
+void Launch<S, M>::moments(const View<S, M>& v, double* shift, double* out, cudaStream_t st) {
+  if (v.n_cells > 0) k_moments<S, M><<<v.n_cells, kCellThreads, 0, st>>>(v, shift, out);
+}
+
+template <class S, class M>
+void Launch<S, M>::scale(S* f, int64_t n, double s, double* moments, int n_cells, cudaStream_t st) {
+  if (n > 0) {
+    const int64_t blocks = (n + 255) / 256;
+    k_scale<S><<<static_cast<unsigned>(blocks < 148 * 64 ? blocks : 148 * 64), 256, 0, st>>>(f, n, s);
+  }
+  if (n_cells > 0) k_scale_moments<<<ceil_div(n_cells, 256), 256, 0, st>>>(moments, n_cells, s);
+}
+
+template <class S, class M>
+void Launch<S, M>::cell_params(const View<S, M>& v, const double* moments, const double* volume, const double* vdt,
+                               double mu0, double omega, double Pr, double cold_bgk_T, int discrete, int collisionless,
+                               CellParams<M>* out, int* flags, cudaStream_t st) {
+  if (v.n_cells <= 0) return;
+  if (discrete) {
+    k_cell_params_deq<S, M><<<v.n_cells, kCellThreads, 0, st>>>(v, moments, volume, vdt, mu0, omega, Pr, cold_bgk_T,
+                                                                collisionless, out, flags);
+  } else {
+    k_cell_params<M><<<ceil_div(v.n_cells, 128), 128, 0, st>>>(moments, volume, vdt, mu0, omega, Pr, out, v.n_cells,
+                                                               cold_bgk_T);
+  }
+}
+
+template <class S, class M>
+void Launch<S, M>::maxwell_reflection(const View<S, M>& v, cudaStream_t st) {
+  if (v.n_bfaces <= 0) return;
+  const dim3 grid(ceil_div(v.nv, 128), v.n_bfaces);
+  k_maxwell_reflection<false, S, M><<<grid, 128, 0, st>>>(v);
+  k_maxwell_reflection<true, S, M><<<grid, 128, 0, st>>>(v);
+}
+
+template <class S, class M>
+void Launch<S, M>::boundary_sums(const View<S, M>& v, double* out, cudaStream_t st) {
+  if (v.n_bfaces > 0) k_boundary_sums<S, M><<<v.n_bfaces, kFaceThreads, 0, st>>>(v, out);
+}
+
+template <class S, class M>
+void Launch<S, M>::internal_face_flux(const View<S, M>& v, const int32_t* cells, const int32_t* entries, double* out,
+                                      int n, cudaStream_t st) {
+  if (n > 0) k_internal_face_flux<S, M><<<n, kFaceThreads, 0, st>>>(v, cells, entries, out);
+}
+
+template <class S, class M>
+int Launch<S, M>::residual_tiles(int kc) {
+  return ceil_div(kc, kTileThreads * kTileIters);
+}
+
+template <class S, class M>
+void Launch<S, M>::gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st) {
+  if (v.n_cells <= 0 || ch.kc <= 0) return;
+  const dim3 grid(v.n_cells, residual_tiles(ch.kc));
+  k_gradient<S, M><<<grid, kTileThreads, 0, st>>>(v, ch);
+}
+
+template <class S, class M>
+void Launch<S, M>::residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
+                            double* residual_cell, cudaStream_t st) {
+  if (v.n_cells <= 0 || ch.kc <= 0) return;
+  const int tiles = residual_tiles(ch.kc);
+  k_residual<S, M><<<dim3(v.n_cells, tiles), kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
+  k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride, tiles, residual_cell,
+                                                             v.n_cells);
+}
+
+template <class S, class M>
+void Launch<S, M>::sweep_pass(const View<S, M>& v, const SweepArgs<S>& a, cudaStream_t st) {
+  if (a.n_items <= 0) return;
+  k_sweep_pass<S, M><<<ceil_div(a.n_items, kSweepThreads / 32), kSweepThreads, 0, st>>>(v, a);
+}
+
+template <class S, class M>
+void Launch<S, M>::gsis_correction(const View<S, M>& v, const double* wh, const double* wn, int* flags, double* shift,
+                                   int mode, int discrete, int collisionless, cudaStream_t st) {
+  if (v.n_cells > 0)
+    k_gsis_correction<S, M><<<v.n_cells, kCellThreads, 0, st>>>(v, wh, wn, flags, shift, mode, discrete,
+                                                                 collisionless);
+}
+
+template <class S, class M>
+void Launch<S, M>::import_f(const double* src, S* f, const int32_t* perm, int64_t c0, int n, int nv, cudaStream_t st) {
+  if (n > 0) k_import<S><<<148 * 16, 256, 0, st>>>(src, f, perm, c0, n, nv);
+}
+
+template <class S, class M>
+void Launch<S, M>::export_f(const S* f, double* dst, const int32_t* inv, int64_t c0, int n, int nv, cudaStream_t st) {
+  if (n > 0) k_export<S><<<148 * 16, 256, 0, st>>>(f, dst, inv, c0, n, nv);
+}
+
+template struct Launch<float, float>;
+template struct Launch<double, double>;
+template struct Launch<float, double>;
+
+}  // namespace kin

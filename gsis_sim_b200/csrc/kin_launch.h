@@ -1,0 +1,58 @@
+// Launch interface of the kinetic kernels (kin_kernels.cu). All launches go to the given stream and do not
+// synchronise.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kin_kernels.cuh"
+
+namespace kin {
+
+constexpr int kTileIters = 4;      // velocities per thread in the gradient / residual tiles
+constexpr int kSweepThreads = 128; // 4 independent sweep chains (warps) per CTA
+
+// arguments of one LU-SGS block pass over a velocity chunk
+template <class S>
+struct SweepArgs {
+  const int4* items;  // per warp: (chain, t0, t1, 0), chunk-local velocity range [t0, t1)
+  int32_t n_items;
+  int32_t n_blocks;
+  const int32_t* block_offsets;
+  const int32_t* chain_cells;  // per chain: the block's cells ordered by level
+  const int32_t* chain_start;  // chain -> first index in chain_cells
+  const int32_t* lev_bounds;   // level boundaries relative to chain_start (n_levels + 1 per chain)
+  const int32_t* lev_start;    // chain -> first index in lev_bounds
+  const int32_t* lev_count;    // chain -> number of levels
+  const int32_t* pos;          // [group][cell] position in the group's sweep order
+  const S* R;                  // steady residual of the chunk
+  const S* dprev;              // Delta f of the previous pass (nullptr in the first pass)
+  S* out;                      // Delta f* then Delta f
+  int32_t update_f;
+  int32_t k0;
+  int32_t stride;
+};
+
+template <class S, class M>
+struct Launch {
+  static void set_equilibrium(const View<S, M>& v, const double* states, double* shift, int discrete, cudaStream_t st);
+  static void moments(const View<S, M>& v, double* shift, double* out, cudaStream_t st);
+  static void scale(S* f, int64_t n, double s, double* moments, int n_cells, cudaStream_t st);
+  static void cell_params(const View<S, M>& v, const double* moments, const double* volume, const double* vdt,
+                          double mu0, double omega, double Pr, double cold_bgk_T, int discrete, int collisionless,
+                          CellParams<M>* out, int* flags, cudaStream_t st);
+  static void maxwell_reflection(const View<S, M>& v, cudaStream_t st);
+  static void boundary_sums(const View<S, M>& v, double* out, cudaStream_t st);
+  static void internal_face_flux(const View<S, M>& v, const int32_t* cells, const int32_t* entries, double* out, int n,
+                                 cudaStream_t st);
+  static int residual_tiles(int kc);
+  static void gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st);
+  static void residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
+                       double* residual_cell, cudaStream_t st);
+  static void sweep_pass(const View<S, M>& v, const SweepArgs<S>& a, cudaStream_t st);
+  static void gsis_correction(const View<S, M>& v, const double* wh, const double* wn, int* flags, double* shift,
+                              int mode, int discrete, int collisionless, cudaStream_t st);
+  static void import_f(const double* src, S* f, const int32_t* perm, int64_t c0, int n, int nv, cudaStream_t st);
+  static void export_f(const S* f, double* dst, const int32_t* inv, int64_t c0, int n, int nv, cudaStream_t st);
+};
+
+}  // namespace kin

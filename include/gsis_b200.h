@@ -1,0 +1,243 @@
+/*
+ * gsis_b200.h — C ABI of the B200 kinetic backend (discrete-velocity Shakhov CIS / LU-SGS).
+ *
+ * This library is a drop-in for the reference's `gsis::kinetic::KineticBackend` CUDA implementation
+ * (src/kinetic/kinetic_backend.hpp:59-105, factory `make_cuda_backend` at src/kinetic/kinetic_backend.hpp:105,
+ * defined in src/kinetic/kinetic_backend_cuda.cpp:506-509). Every entry point below replaces one virtual method
+ * of that interface; the C++ shim that wraps them into a `KineticBackend` lives in
+ * gsis_sim_b200/integration/b200_backend.cpp.
+ *
+ * Conventions (identical to the reference backend interface):
+ *   - every host array is FP64 (or int32) in the solver's INTERNAL numbering: cells and boundary faces as
+ *     renumbered by `build_kinetic_setup` (src/kinetic/kinetic_setup.cpp:293-514), velocities in the reference
+ *     storage order (`VelocityLayout`, src/kinetic/kinetic_setup.hpp:29-38);
+ *   - f is addressed as f[cell * nv + p] with p the reference storage position (kinetic_kernels.hpp:64-67);
+ *   - moments: 15 per cell, rho, ux, uy, uz, T, p, sxx, syy, szz, sxy, syz, sxz, qx, qy, qz
+ *     (src/kinetic/kinetic_types.hpp:107-109);
+ *   - boundary sums: 20 per face (src/kinetic/kinetic_types.hpp:111-116);
+ *   - arrays passed in are owned by the caller and only read during the call.
+ *
+ * Every function returns KIN_OK (0) on success and a negative KIN_E* code on failure; the message of the last
+ * failure on a handle is returned by kin_last_error(handle) (kin_last_error(NULL) for kin_create failures).
+ * Errors replace the reference's `GSIS_CHECK` / `GSIS_CUDA_CHECK` exceptions (src/core/error.hpp:1-47,
+ * src/gpu/cuda_check.hpp:16-24); the C++ shim turns them back into `gsis::Error`.
+ */
+#ifndef GSIS_B200_H
+#define GSIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KIN_ABI_VERSION 1
+
+/* status codes */
+#define KIN_OK 0
+#define KIN_E_ARG (-1)      /* invalid argument or size mismatch (reference: GSIS_CHECK) */
+#define KIN_E_CUDA (-2)     /* CUDA runtime error (reference: GSIS_CUDA_CHECK) */
+#define KIN_E_MEMORY (-3)   /* f or the work arrays do not fit in device memory */
+#define KIN_E_STATE (-4)    /* call out of order (e.g. boundary sums before set_inflow) */
+#define KIN_E_TIMEOUT (-5)  /* a bounded device-side wait gave up (status read back from the device) */
+
+/* storage / arithmetic precision of the distribution function */
+#define KIN_PREC_FP32 0  /* reference precision = "fp32": f and all per-point arithmetic in FP32 */
+#define KIN_PREC_FP64 1  /* reference precision = "fp64" */
+#define KIN_PREC_MIXED 2 /* f, gradients and LU-SGS corrections stored in FP32; residual, gradients, moments and
+                            sums evaluated in FP64 arithmetic (defect correction); no reference counterpart */
+
+/* BoundaryKind (src/kinetic/kinetic_types.hpp:19-26) */
+#define KIN_BC_DIFFUSE_WALL 0
+#define KIN_BC_PRESSURE 1
+#define KIN_BC_VACUUM 2
+#define KIN_BC_SYMMETRY 3
+#define KIN_BC_PERIODIC 4
+#define KIN_BC_MAXWELL_WALL 5
+
+/* LimiterMode (src/kinetic/kinetic_types.hpp:101-105) */
+#define KIN_LIMITER_NONE 0
+#define KIN_LIMITER_VENKAT_ABSOLUTE 1
+#define KIN_LIMITER_VENKAT_RELATIVE 2
+
+/* gsis_negative_check (src/kinetic/kinetic_kernels.hpp:584-587) */
+#define KIN_NEGATIVE_ALL 0
+#define KIN_NEGATIVE_CREATED 1
+#define KIN_NEGATIVE_LIMIT 2
+#define KIN_NEGATIVE_BLEND 3
+
+/* number of values per cell / face in the host arrays */
+#define KIN_MOMENTS_PER_CELL 15
+#define KIN_BOUNDARY_SUMS_PER_FACE 20
+#define KIN_CSR_GEOM 12  /* sx sy sz  dsx dsy dsz  dox doy doz  cx cy cz   (CsrEntry<F>, kinetic_types.hpp:35-42) */
+#define KIN_BFACE_GEOM 7 /* nx ny nz  area  dx dy dz                       (BoundaryFaceInfo<F>, :46-54) */
+
+typedef struct KinHandle KinHandle;
+
+/*
+ * Everything the backend needs from the reference's `KineticSetup` (src/kinetic/kinetic_setup.hpp:56-115) as
+ * flat arrays. The nondimensional geometry is the FP64 value that the reference casts to F in
+ * make_csr_entries / make_bface_infos / make_eps2 (src/kinetic/kinetic_setup.cpp:516-599).
+ */
+typedef struct KinSetupDesc {
+  int32_t abi_version; /* KIN_ABI_VERSION */
+  int32_t precision;   /* KIN_PREC_* */
+  int32_t device;      /* CUDA device ordinal */
+  int32_t n_cells;
+  int32_t nv;
+  int32_t n_bfaces;
+  int32_t n_blocks;
+
+  /* velocity grid in storage order (VelocityLayout::xi_*, ::weight) */
+  const double* xi_x;
+  const double* xi_y;
+  const double* xi_z;
+  const double* weights; /* optional per-velocity quadrature weights (NULL: every point has `weight`) */
+  double weight;         /* uniform weight (used when weights == NULL) */
+
+  /* cell -> face CSR, faces of a cell in ascending face order (CellFaceCsr, src/mesh/fv_geometry.hpp:180-190) */
+  const int32_t* csr_offsets; /* n_cells + 1 */
+  const int32_t* csr_other;   /* neighbour cell or -1 */
+  const int32_t* csr_bface;   /* boundary face index or -1 */
+  const double* csr_geom;     /* n_csr * KIN_CSR_GEOM */
+  const double* eps2;         /* n_cells: K^3 V */
+
+  /* boundary faces */
+  const int32_t* bface_owner;
+  const int32_t* bface_kind;       /* KIN_BC_* */
+  const int32_t* bface_mirror_xor; /* symmetry / Maxwell wall: mirrored storage position p ^ mirror_xor */
+  const int32_t* bface_patch;
+  const double* bface_geom; /* n_bfaces * KIN_BFACE_GEOM */
+
+  /* per-cell nondimensional volume and V / dt */
+  const double* volume;
+  const double* vdt;
+
+  /* LU-SGS blocks and per-direction sweep orders (kinetic_setup.hpp:80-96) */
+  const int32_t* block_offsets; /* n_blocks + 1 */
+  int32_t n_sweep_dirs;         /* 0: "block" order (internal numbering) */
+  const int32_t* sweep_order;   /* n_sweep_dirs * n_cells */
+  const int32_t* sweep_pos;     /* n_sweep_dirs * n_cells */
+  const uint8_t* sweep_dir_of;  /* nv */
+
+  /* scheme parameters (KineticParams, src/kinetic/kinetic_params.hpp:11-117) */
+  int32_t limiter_mode; /* KIN_LIMITER_* */
+  int32_t positivity;   /* positivity_limiter */
+  double diag_scale;
+  double interface_damping;
+  int32_t block_passes;
+  int32_t negative_check_mode; /* KIN_NEGATIVE_* */
+  int64_t velocity_chunk;      /* 0: as large as device memory allows */
+
+  /* gas: mu = mu0 T^omega, Shakhov Prandtl number */
+  double mu0;
+  double omega;
+  double Pr;
+  double cold_bgk_temperature;
+
+  /* conservative discrete equilibrium (DeqGrid, src/kinetic/discrete_equilibrium.hpp:25-32) */
+  int32_t discrete_eq;
+  int32_t deq_fallback_collisionless;
+  double deq_lo[3];
+  double deq_hi[3];
+  double deq_d[3];
+  double deq_criterion;
+  double deq_tolerance;
+  int32_t deq_max_iterations;
+
+  /* partially accommodating walls (MaxwellFace, src/kinetic/kinetic_types.hpp:28-31) */
+  int32_t n_maxwell_faces;
+  const int64_t* maxwell_offset;             /* n_bfaces, -1 for non-Maxwell faces (NULL if none) */
+  const double* maxwell_specular_fraction;   /* n_bfaces */
+  const int32_t* grid_to_storage;            /* nv (NULL if no Maxwell walls) */
+  int32_t grid_n[3];
+} KinSetupDesc;
+
+/* InflowState (src/kinetic/kinetic_backend.hpp:45-50): scale * f_eq(rho, u, T); same memory layout */
+typedef struct KinInflowState {
+  double scale;
+  double rho;
+  double ux, uy, uz;
+  double T;
+} KinInflowState;
+
+/* StepTimings (src/kinetic/kinetic_backend.hpp:19-41), seconds */
+typedef struct KinStepTimings {
+  double moments;
+  double boundary;
+  double gradient;
+  double residual;
+  double sweep_forward;
+  double sweep_backward;
+  double other;
+} KinStepTimings;
+
+/* DeqCounts (src/kinetic/kinetic_backend.hpp:53-57) */
+typedef struct KinDeqCounts {
+  int64_t corrected;
+  int64_t failed;
+  int32_t max_iterations;
+} KinDeqCounts;
+
+/* make_cuda_backend (src/kinetic/kinetic_backend_cuda.cpp:506-509): uploads the setup, allocates f and the
+   velocity-chunk work arrays (CudaBackend ctor, kinetic_backend_cuda.cpp:92-175) */
+int kin_create(const KinSetupDesc* desc, KinHandle** out);
+/* ~CudaBackend */
+void kin_destroy(KinHandle* h);
+/* message of the last failure (NULL handle: the last kin_create failure of this thread) */
+const char* kin_last_error(const KinHandle* h);
+
+/* KineticBackend::name / chunk_width / memory_bytes (kinetic_backend.hpp:63-65) */
+const char* kin_name(const KinHandle* h);
+int kin_chunk_width(const KinHandle* h, int32_t* out);
+int kin_memory_bytes(const KinHandle* h, uint64_t* out);
+
+/* KineticBackend::set_equilibrium (kinetic_backend.hpp:68); states: 5 * n_cells (rho, ux, uy, uz, T) */
+int kin_set_equilibrium(KinHandle* h, const double* states, int64_t n);
+/* KineticBackend::set_distribution / get_distribution (:69-70); f: n_cells * nv */
+int kin_set_distribution(KinHandle* h, const double* f, int64_t n);
+int kin_get_distribution(KinHandle* h, double* f, int64_t n);
+/* KineticBackend::compute_moments (:73); out: 15 * n_cells */
+int kin_compute_moments(KinHandle* h, double* out, int64_t n);
+/* KineticBackend::scale_distribution (:75) */
+int kin_scale_distribution(KinHandle* h, double s);
+/* KineticBackend::update_cell_params (:77) */
+int kin_update_cell_params(KinHandle* h);
+/* KineticBackend::set_inflow (:79); n = n_bfaces */
+int kin_set_inflow(KinHandle* h, const KinInflowState* inflow, int64_t n);
+/* KineticBackend::boundary_sums (:81); out: 20 * n_bfaces */
+int kin_boundary_sums(KinHandle* h, double* out, int64_t n);
+/* KineticBackend::sweep (:83); residual_cell: n_cells, sum over velocities of R^2 */
+int kin_sweep(KinHandle* h, double* residual_cell, int64_t n);
+/* KineticBackend::gsis_correction (:86-87); w_half, w_new: 5 * n_cells; replaced_flags: NULL or n_cells */
+int kin_gsis_correction(KinHandle* h, const double* w_half, const double* w_new, int64_t n,
+                        int32_t* replaced_flags, int64_t* replaced);
+/* KineticBackend::internal_face_mass_flux (:92-93) */
+int kin_internal_face_mass_flux(KinHandle* h, const int32_t* cells, const int32_t* entries, int64_t n,
+                                double* out);
+/* KineticBackend::take_timings (:96) */
+int kin_take_timings(KinHandle* h, KinStepTimings* out);
+/* KineticBackend::deq_counts (:99) */
+int kin_deq_counts(KinHandle* h, KinDeqCounts* out);
+
+/* ---- B200 additions (no reference counterpart) ---------------------------------------------------------- */
+
+/* Run every subsequent kernel of this handle on `stream` (a cudaStream_t; NULL: the legacy default stream). */
+int kin_set_stream(KinHandle* h, void* stream);
+/* Number of kernels this handle has launched since creation. */
+int kin_launch_count(const KinHandle* h, int64_t* out);
+/* Device pointer of f (storage order of the handle, see kin_velocity_permutation) and its element size. */
+int kin_device_f(KinHandle* h, void** f, int32_t* elem_bytes);
+/* The handle stores velocities in its own order (grouped by sweep direction): perm[q] = reference storage
+   position of the handle's velocity q. */
+int kin_velocity_permutation(const KinHandle* h, int32_t* perm, int64_t n);
+/* LU-SGS level schedule statistics: number of levels of the longest (direction, block) chain and the total
+   number of (direction, block) chains. */
+int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSIS_B200_H */

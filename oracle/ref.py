@@ -1,0 +1,280 @@
+"""ctypes wrapper of oracle/_ref/libgsisref.so — the reference's own CPU kinetic path (TEST INFRASTRUCTURE).
+
+Only tests/, tests/golden/make_golden.py and bench.py's CPU-baseline leg use this module. It builds cases of the
+reference (box meshes of tests/support/box_mesh.cpp or meshes given as arrays), exports the reference
+`KineticSetup` as `SetupArrays`, and runs the reference `KineticSolver` (src/kinetic/kinetic_solver.cpp) and
+`CpuBackend` (src/kinetic/kinetic_backend_cpu.cpp).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from gsis_sim_b200 import abi
+from gsis_sim_b200.backend import KineticBackendABI, KineticError
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libgsisref.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    L = C.CDLL(LIB_PATH)
+    L.ref_error.restype = C.c_char_p
+    L.ref_mesh_box.argtypes = [C.c_char_p]
+    L.ref_mesh_box.restype = C.c_void_p
+    L.ref_mesh_arrays.argtypes = [C.c_int32, _dp, C.c_int32, _lp, _ip, _ip, C.c_int32, _ip, C.c_int32, C.c_int32,
+                                  C.c_char_p, _ip, _ip]
+    L.ref_mesh_arrays.restype = C.c_void_p
+    L.ref_mesh_free.argtypes = [C.c_void_p]
+    L.ref_mesh_sizes.argtypes = [C.c_void_p, _lp]
+    L.ref_mesh_export.argtypes = [C.c_void_p, _dp, _lp, _ip, _ip, _ip, _ip, _ip, C.c_char_p, C.c_int32, _dp, _dp,
+                                  _dp, _dp]
+    L.ref_case_create.argtypes = [C.c_void_p, C.c_char_p]
+    L.ref_case_create.restype = C.c_void_p
+    L.ref_case_free.argtypes = [C.c_void_p]
+    L.ref_case_desc.argtypes = [C.c_void_p, C.POINTER(abi.KinSetupDesc)]
+    L.ref_case_info.argtypes = [C.c_void_p, _lp, _dp]
+    L.ref_case_maps.argtypes = [C.c_void_p, _ip, _ip, _ip, _ip, _dp]
+    L.ref_case_geometry.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _ip, _dp, _ip]
+    L.ref_solver_init_uniform.argtypes = [C.c_void_p] + [C.c_double] * 5
+    L.ref_solver_init_states.argtypes = [C.c_void_p, _dp]
+    L.ref_solver_prepare.argtypes = [C.c_void_p, _dp]
+    L.ref_solver_sweep.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ref_solver_patch_mass_flow.argtypes = [C.c_void_p, _dp]
+    L.ref_solver_moments.argtypes = [C.c_void_p, _dp]
+    L.ref_solver_boundary_fluxes.argtypes = [C.c_void_p, _dp, _dp, _dp]
+    L.ref_solver_distribution.argtypes = [C.c_void_p, _dp]
+    L.ref_solver_set_distribution.argtypes = [C.c_void_p, _dp, C.c_int64]
+    L.ref_solver_gsis_correction.argtypes = [C.c_void_p, _dp, _dp, _lp]
+    L.ref_solver_section_mass_flow.argtypes = [C.c_void_p, C.c_int32, _dp, C.c_int32, _dp]
+    abi.declare_backend_api(L, "ref_kin_")
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise KineticError(lib().ref_error().decode())
+
+
+def _p(a, t=C.c_double):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class RefMesh:
+    """A reference PolyMesh + geometry (LoadedMesh)."""
+
+    def __init__(self, handle):
+        if not handle:
+            raise KineticError(lib().ref_error().decode())
+        self.h = handle
+
+    @classmethod
+    def box(cls, n, lo, hi, patches, distortion=0.0, tetrahedra=False, seed=1):
+        spec = (f"mesh.n = {n[0]} {n[1]} {n[2]}\nmesh.lo = {lo[0]!r} {lo[1]!r} {lo[2]!r}\n"
+                f"mesh.hi = {hi[0]!r} {hi[1]!r} {hi[2]!r}\nmesh.patches = {' '.join(patches)}\n"
+                f"mesh.distortion = {distortion!r}\nmesh.tetrahedra = {int(tetrahedra)}\nmesh.seed = {seed}\n")
+        return cls(lib().ref_mesh_box(spec.encode()))
+
+    @classmethod
+    def from_arrays(cls, m: dict):
+        pts = np.ascontiguousarray(m["points"], dtype=np.float64)
+        fo = np.ascontiguousarray(m["face_offsets"], dtype=np.int64)
+        fn = np.ascontiguousarray(m["face_nodes"], dtype=np.int32)
+        ow = np.ascontiguousarray(m["owner"], dtype=np.int32)
+        nb = np.ascontiguousarray(m["neighbour"], dtype=np.int32)
+        ps = np.ascontiguousarray(m["patch_start"], dtype=np.int32)
+        pc = np.ascontiguousarray(m["patch_count"], dtype=np.int32)
+        names = "".join(n + "\n" for n in m["patch_names"]).encode()
+        h = lib().ref_mesh_arrays(len(pts) // 3 if pts.ndim == 1 else len(pts), _p(pts), len(ow), _p(fo, C.c_int64),
+                                  _p(fn, C.c_int32), _p(ow, C.c_int32), len(nb), _p(nb, C.c_int32),
+                                  int(m["n_cells"]), len(ps), names, _p(ps, C.c_int32), _p(pc, C.c_int32))
+        return cls(h)
+
+    def export(self) -> dict:
+        s = np.zeros(6, dtype=np.int64)
+        lib().ref_mesh_sizes(self.h, _p(s, C.c_int64))
+        n_points, n_faces, n_int, n_fn, n_cells, n_patches = (int(x) for x in s)
+        out = dict(points=np.zeros((n_points, 3)), face_offsets=np.zeros(n_faces + 1, np.int64),
+                   face_nodes=np.zeros(n_fn, np.int32), owner=np.zeros(n_faces, np.int32),
+                   neighbour=np.zeros(n_int, np.int32), patch_start=np.zeros(n_patches, np.int32),
+                   patch_count=np.zeros(n_patches, np.int32), cell_volume=np.zeros(n_cells),
+                   cell_center=np.zeros((n_cells, 3)), face_area_vector=np.zeros((n_faces, 3)),
+                   face_center=np.zeros((n_faces, 3)))
+        names = C.create_string_buffer(64 * n_patches + 64)
+        _check(lib().ref_mesh_export(self.h, _p(out["points"]), _p(out["face_offsets"], C.c_int64),
+                                     _p(out["face_nodes"], C.c_int32), _p(out["owner"], C.c_int32),
+                                     _p(out["neighbour"], C.c_int32), _p(out["patch_start"], C.c_int32),
+                                     _p(out["patch_count"], C.c_int32), names, len(names),
+                                     _p(out["cell_volume"]), _p(out["cell_center"]), _p(out["face_area_vector"]),
+                                     _p(out["face_center"])))
+        out["patch_names"] = names.value.decode().split("\n")[:n_patches]
+        out["n_cells"] = n_cells
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.ref_mesh_free(self.h)
+            self.h = None
+
+
+def case_spec(bcs, Kn=None, delta_rp=None, nv=(10, 10, 10), vmax=5.0, vlo=None, vhi=None, kinetic=None,
+              omega=0.66, molecular_mass=6.65e-27, mu_ref=1.916e-5, T_ref=273.15, T0=273.15, L_ref=1.0) -> str:
+    """Config text for ref_case_create (same gas and conditions as tests/kinetic/kinetic_test_cases.cpp:9-32).
+
+    bcs: list of (patch, type, dict(T=, p=, u=(x,y,z), alpha=)) with nondimensional values."""
+    lo = vlo if vlo is not None else (-vmax,) * 3
+    hi = vhi if vhi is not None else (vmax,) * 3
+    lines = [f"gas.molecular_mass = {molecular_mass!r}", f"gas.mu_ref = {mu_ref!r}", f"gas.T_ref = {T_ref!r}",
+             f"gas.omega = {omega!r}", f"conditions.L_ref = {L_ref!r}", f"conditions.T0 = {T0!r}",
+             f"velocity_grid.n = {nv[0]} {nv[1]} {nv[2]}", f"velocity_grid.lo = {lo[0]!r} {lo[1]!r} {lo[2]!r}",
+             f"velocity_grid.hi = {hi[0]!r} {hi[1]!r} {hi[2]!r}"]
+    if Kn is not None:
+        lines.append(f"conditions.Kn = {Kn!r}")
+    if delta_rp is not None:
+        lines.append(f"conditions.delta_rp = {delta_rp!r}")
+    for patch, typ, o in bcs:
+        parts = [patch, typ]
+        if "T" in o:
+            parts.append(f"T={o['T']!r}")
+        if "p" in o:
+            parts.append(f"p={o['p']!r}")
+        if "u" in o:
+            u = o["u"]
+            parts.append(f"u={u[0]!r},{u[1]!r},{u[2]!r}")
+        if "alpha" in o:
+            parts.append(f"alpha={o['alpha']!r}")
+        lines.append("boundary = " + " ".join(parts))
+    for k, v in (kinetic or {}).items():
+        if isinstance(v, bool):
+            v = "true" if v else "false"
+        elif isinstance(v, str):
+            v = f'"{v}"'
+        elif isinstance(v, float):
+            v = repr(v) if ("." in repr(v) or "e" in repr(v)) else repr(v) + ".0"
+        lines.append(f"kinetic.{k} = {v}")
+    return "\n".join(lines) + "\n"
+
+
+class RefCase:
+    """The reference KineticSolver (backend = "cpu") on one mesh + config, and a separate CpuBackend."""
+
+    def __init__(self, mesh: RefMesh, spec: str):
+        self.mesh = mesh
+        self.h = lib().ref_case_create(mesh.h, spec.encode())
+        if not self.h:
+            raise KineticError(lib().ref_error().decode())
+        d = abi.KinSetupDesc()
+        _check(lib().ref_case_desc(self.h, C.byref(d)))
+        self.setup = abi.SetupArrays.from_desc(d)
+        iout = np.zeros(8, np.int64)
+        dout = np.zeros(8)
+        _check(lib().ref_case_info(self.h, _p(iout, C.c_int64), _p(dout)))
+        self.n_csr, closed, self.n_patches, self.n_internal_faces = (int(x) for x in iout[:4])
+        self.inner_sweeps, self.inner_wall_update, self.boundary_iterations, self.orbit_size = \
+            int(iout[4]), bool(iout[5]), int(iout[6]), int(iout[7])
+        self.closed_domain = bool(closed)
+        (self.length_scale, self.gamma, self.limiter_k, self.wall_relaxation, self.convergence_u_floor,
+         self.mass_flow_scale, self.mu_hat0, self.xi_max) = (float(x) for x in dout)
+        nc, nb, nv = self.setup.n_cells, self.setup.n_bfaces, self.setup.nv
+        self.cell_new_to_old = np.zeros(nc, np.int32)
+        self.bface_new_to_old = np.zeros(nb, np.int32)
+        self.storage_to_grid = np.zeros(nv, np.int32)
+        self.patch_int = np.zeros((self.n_patches, 4), np.int32)
+        self.patch_dbl = np.zeros((self.n_patches, 7))
+        _check(lib().ref_case_maps(self.h, _p(self.cell_new_to_old, C.c_int32), _p(self.bface_new_to_old, C.c_int32),
+                                   _p(self.storage_to_grid, C.c_int32), _p(self.patch_int, C.c_int32),
+                                   _p(self.patch_dbl)))
+        n_faces = self.n_internal_faces + nb
+        self.geom = dict(cell_center=np.zeros((nc, 3)), face_center=np.zeros((n_faces, 3)),
+                         face_normal=np.zeros((n_faces, 3)), face_area=np.zeros(n_faces),
+                         owner=np.zeros(n_faces, np.int32), lsq=np.zeros((self.n_csr, 3)),
+                         csr_faces=np.zeros(self.n_csr, np.int32))
+        g = self.geom
+        _check(lib().ref_case_geometry(self.h, _p(g["cell_center"]), _p(g["face_center"]), _p(g["face_normal"]),
+                                       _p(g["face_area"]), _p(g["owner"], C.c_int32), _p(g["lsq"]),
+                                       _p(g["csr_faces"], C.c_int32)))
+        self.backend = RefBackend(self)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.ref_case_free(self.h)
+            self.h = None
+
+    # --- reference KineticSolver ------------------------------------------------------------------------------
+    def init_uniform(self, rho, u, T):
+        _check(lib().ref_solver_init_uniform(self.h, rho, u[0], u[1], u[2], T))
+
+    def init_states(self, states_orig):
+        s = np.ascontiguousarray(states_orig, dtype=np.float64)
+        _check(lib().ref_solver_init_states(self.h, _p(s)))
+
+    def prepare(self):
+        info = np.zeros(12)
+        _check(lib().ref_solver_prepare(self.h, _p(info)))
+        return info
+
+    def sweep(self, update_pressure=True):
+        info = np.zeros(12)
+        _check(lib().ref_solver_sweep(self.h, int(update_pressure), _p(info)))
+        return info
+
+    def patch_mass_flow(self):
+        out = np.zeros(self.n_patches)
+        _check(lib().ref_solver_patch_mass_flow(self.h, _p(out)))
+        return out
+
+    def moments(self):
+        out = np.zeros((self.setup.n_cells, 15))
+        _check(lib().ref_solver_moments(self.h, _p(out)))
+        return out
+
+    def boundary_fluxes(self):
+        nb = self.setup.n_bfaces
+        fp, fm, fs = np.zeros((nb, 5)), np.zeros((nb, 5)), np.zeros((nb, 5))
+        _check(lib().ref_solver_boundary_fluxes(self.h, _p(fp), _p(fm), _p(fs)))
+        return fp, fm, fs
+
+    def distribution(self):
+        out = np.zeros((self.setup.n_cells, self.setup.nv))
+        _check(lib().ref_solver_distribution(self.h, _p(out)))
+        return out
+
+    def set_distribution(self, f):
+        a = np.ascontiguousarray(f, dtype=np.float64).ravel()
+        _check(lib().ref_solver_set_distribution(self.h, _p(a), a.size))
+
+    def gsis_correction(self, w_half_orig, w_new_orig):
+        a = np.ascontiguousarray(w_half_orig, dtype=np.float64)
+        b = np.ascontiguousarray(w_new_orig, dtype=np.float64)
+        r = C.c_int64()
+        _check(lib().ref_solver_gsis_correction(self.h, _p(a), _p(b), C.byref(r)))
+        return r.value
+
+    def section_mass_flow(self, positions, axis=0):
+        p = np.ascontiguousarray(positions, dtype=np.float64)
+        out = np.zeros(len(p))
+        _check(lib().ref_solver_section_mass_flow(self.h, axis, _p(p), len(p), _p(out)))
+        return out
+
+
+class RefBackend(KineticBackendABI):
+    """The reference CpuBackend<F> of a RefCase, called operation by operation."""
+
+    def __init__(self, case: RefCase):
+        super().__init__(lib(), "ref_kin_", C.c_void_p(case.h), case.setup, lambda: lib().ref_error().decode())
+        self._case = case
