@@ -173,7 +173,12 @@ struct Backend final : KinHandle {
   int32_t chunk = 0, partial_stride = 1, max_levels = 0, n_chains = 0;
 
   // host copies
-  std::vector<int32_t> perm, inv, group_begin, group_end;
+  std::vector<int32_t> perm, inv;
+  struct GroupRange {
+    int32_t g, begin, end;  // velocities [begin, end) of the handle's order belong to sweep direction g
+  };
+  std::vector<GroupRange> group_ranges;
+  int32_t orbit_size = 1;
   std::vector<int32_t> h_block_offsets;
   // per chunk: sweep items
   struct ChunkPlan {
@@ -249,6 +254,27 @@ struct Backend final : KinHandle {
     KCUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     stream = own_stream;
 
+    // velocity chunk: given (rounded up to whole mirror orbits, kinetic_backend_cuda.cpp:151-152) or from the
+    // memory left after f (kinetic_backend_cuda.cpp:147-161). Mirror orbits never straddle a chunk, so a chunk
+    // only reads f of its own velocities before updating them and the result does not depend on the chunking.
+    int32_t xor_all = 0;
+    for (int b = 0; b < nb; ++b) xor_all |= d.bface_mirror_xor[b];
+    orbit_size = xor_all + 1;
+    KCHECK((orbit_size & (orbit_size - 1)) == 0 && nv % orbit_size == 0, "mirror orbits do not tile the velocity grid");
+    {
+      const double per_velocity = static_cast<double>(nc) * (4.0 * sizeof(S) + 8.0 / (256.0 * kin::kTileIters));
+      int64_t k;
+      if (d.velocity_chunk > 0) {
+        k = (d.velocity_chunk + orbit_size - 1) / orbit_size * orbit_size;
+      } else {
+        const double avail = static_cast<double>(free_b) - static_cast<double>(f_bytes) - 2.0 * kMargin;
+        k = static_cast<int64_t>(avail / per_velocity);
+        k = k / 256 * 256;
+        if (k < 256 && k < nv) throw KinError(KIN_E_MEMORY, "not enough device memory for the velocity-chunk work arrays");
+      }
+      chunk = static_cast<int32_t>(std::min<int64_t>(k, nv));
+    }
+
     build_velocity_layout(d);
     build_mesh(d);
     build_schedule(d);
@@ -269,21 +295,6 @@ struct Backend final : KinHandle {
     f.alloc(ncs * static_cast<size_t>(nv));
     KCUDA(cudaMemsetAsync(f.p, 0, f.bytes(), stream));
 
-    // velocity chunk: given (rounded to the mirror-orbit-free width it is) or from the free memory
-    // (kinetic_backend_cuda.cpp:147-161)
-    KCUDA(cudaStreamSynchronize(stream));
-    KCUDA(cudaMemGetInfo(&free_b, &total_b));
-    const double per_velocity = static_cast<double>(nc) * (4.0 * sizeof(S) + 8.0 / (256.0 * kin::kTileIters));
-    int64_t k;
-    if (d.velocity_chunk > 0) {
-      k = d.velocity_chunk;
-    } else {
-      const double avail = static_cast<double>(free_b) - static_cast<double>(kMargin);
-      k = static_cast<int64_t>(avail / per_velocity);
-      k = k / 256 * 256;
-      if (k < 256 && k < nv) throw KinError(KIN_E_MEMORY, "not enough device memory for the velocity-chunk work arrays");
-    }
-    chunk = static_cast<int32_t>(std::min<int64_t>(k, nv));
     const size_t work = ncs * static_cast<size_t>(chunk);
     gx.alloc(work);
     gy.alloc(work);
@@ -317,17 +328,23 @@ struct Backend final : KinHandle {
         KCHECK(grp[p] < n_groups, "sweep_dir_of out of range");
       }
     }
+    // order: velocity chunk of the reference storage position first, then sweep direction (stable)
     perm.resize(nv);
     std::iota(perm.begin(), perm.end(), 0);
-    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return grp[a] < grp[b]; });
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+      const int ca = a / chunk, cb = b / chunk;
+      return ca != cb ? ca < cb : grp[a] < grp[b];
+    });
     inv.assign(nv, -1);
     for (int q = 0; q < nv; ++q) inv[perm[q]] = q;
-    group_begin.assign(n_groups, 0);
-    group_end.assign(n_groups, 0);
-    for (int g = 0, q = 0; g < n_groups; ++g) {
-      group_begin[g] = q;
-      while (q < nv && grp[perm[q]] == g) ++q;
-      group_end[g] = q;
+    // contiguous (chunk, group) ranges
+    group_ranges.clear();
+    for (int q = 0; q < nv;) {
+      const int g = grp[perm[q]], ck = perm[q] / chunk;
+      int e = q;
+      while (e < nv && grp[perm[e]] == g && perm[e] / chunk == ck) ++e;
+      group_ranges.push_back({g, q, e});
+      q = e;
     }
     std::vector<M> hx(nv), hy(nv), hz(nv);
     std::vector<double> dx(nv), dy(nv), dz(nv), hw;
@@ -499,12 +516,13 @@ struct Backend final : KinHandle {
       cp->k0 = k0;
       cp->kc = std::min(chunk, nv - k0);
       std::vector<int4> items;
-      for (int g = 0; g < n_groups; ++g) {
-        const int s = std::max(group_begin[g], k0), e = std::min(group_end[g], k0 + cp->kc);
+      for (const GroupRange& gr : group_ranges) {
+        const int s = std::max(gr.begin, k0), e = std::min(gr.end, k0 + cp->kc);
         if (s >= e) continue;
         for (int b = 0; b < n_blocks; ++b) {
           if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
-          for (int t = s; t < e; t += 32) items.push_back(make_int4(g * n_blocks + b, t - k0, std::min(t + 32, e) - k0, 0));
+          for (int t = s; t < e; t += 32)
+            items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + 32, e) - k0, 0));
         }
       }
       cp->n_items = static_cast<int32_t>(items.size());

@@ -1,0 +1,66 @@
+"""Parity of the B200 CUDA backend (through the C ABI) with the reference and with the oracle.
+
+Reference values are the golden vectors of the reference's own CPU backend (tests/golden/*.npz); the tolerances
+are those of the reference's GPU-vs-CPU tests (tests/kinetic/test_kinetic_gpu.cpp:133-158).
+"""
+import numpy as np
+import pytest
+
+from tests import common
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def B200Backend():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("no CUDA device")
+    from gsis_sim_b200.backend import B200Backend as cls
+
+    return cls
+
+
+@pytest.mark.parametrize("name", common.golden_names())
+def test_gpu_matches_reference_ops(B200Backend, name):
+    z, setup = common.load(name)
+    prec = common.precision_of(setup)
+    with B200Backend(setup) as be:
+        out = common.run_op_sequence(be, z)
+        assert be.launch_count() > 0
+    common.check_op_sequence(out, z, common.TOL[prec])
+
+
+@pytest.mark.parametrize("name", ["mixed_strong_fp64", "mixed_strong_fp32", "dir13_fp32"])
+def test_gpu_deterministic_and_chunk_independent(B200Backend, name):
+    """Bitwise determinism and independence of the launch splitting (test_kinetic_gpu.cpp:175-186)."""
+    z, setup = common.load(name)
+    with B200Backend(setup) as be:
+        a = common.run_op_sequence(be, z)
+    with B200Backend(setup) as be:
+        b = common.run_op_sequence(be, z)
+    with B200Backend(setup, velocity_chunk=100) as be:
+        c = common.run_op_sequence(be, z)
+        assert be.chunk_width() == 100
+    for k in ["f1", "f3", "res1", "bsums0", "moments2", "face_flux"]:
+        assert np.array_equal(a[k], b[k]), k
+    for k in ["f1", "f3", "bsums0", "moments2"]:
+        assert np.array_equal(a[k], c[k]), k
+    assert common.max_rel(a["res1"], c["res1"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["mixed_strong_fp64", "maxwell_wall_fp64", "couette_fp64"])
+def test_gpu_mixed_precision_matches_oracle(B200Backend, name):
+    """FP32 storage with FP64 arithmetic: the same scheme on the CPU oracle, FP32-rounding tolerance."""
+    from oracle.kinetic_oracle import OracleBackend
+
+    z, setup = common.load(name)
+    with B200Backend(setup, precision="mixed") as be:
+        g = common.run_op_sequence(be, z)
+    o = common.run_op_sequence(OracleBackend(setup, precision="mixed"), z)
+    for k in ["moments0", "bsums0", "f1", "moments2", "f3", "face_flux"]:
+        assert common.max_rel(g[k], o[k]) < 1e-6, k
+    # and it stays within the FP32 tolerance of the FP64 reference
+    for k in ["f1", "f3"]:
+        assert common.max_rel(g[k], z["op." + k]) < 2e-5, k
