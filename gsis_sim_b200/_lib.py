@@ -42,6 +42,8 @@ def load_library():
         "device_f": [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int32)],
         "velocity_permutation": [C.c_void_p, C.POINTER(C.c_int32), C.c_int64],
         "schedule_info": [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
+        "discrete_maxwell": [C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.c_double, C.POINTER(C.c_double),
+                             C.POINTER(C.c_int32)],
     }.items():
         fn = getattr(lib, "kin_" + name)
         fn.argtypes = args
@@ -56,5 +58,5 @@ EXPORTED_SYMBOLS = [
     "kin_set_equilibrium", "kin_set_distribution", "kin_get_distribution", "kin_compute_moments",
     "kin_scale_distribution", "kin_update_cell_params", "kin_set_inflow", "kin_boundary_sums", "kin_sweep",
     "kin_gsis_correction", "kin_internal_face_mass_flux", "kin_take_timings", "kin_deq_counts",
-    "kin_set_stream", "kin_launch_count", "kin_device_f", "kin_velocity_permutation", "kin_schedule_info",
+    "kin_set_stream", "kin_launch_count", "kin_device_f", "kin_velocity_permutation", "kin_schedule_info", "kin_discrete_maxwell",
 ]

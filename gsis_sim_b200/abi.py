@@ -226,12 +226,11 @@ def declare_backend_api(lib, prefix: str, handle_type=C.c_void_p):
         "internal_face_mass_flux": [h, _ip, _ip, C.c_int64, _dp],
         "deq_counts": [h, C.POINTER(KinDeqCounts)],
         "chunk_width": [h, _ip],
+        "discrete_maxwell": [h, _dp, C.c_int64, C.c_double, _dp, _ip],
     }
     for name, args in sig.items():
+        if not hasattr(lib, prefix + name):
+            continue
         fn = getattr(lib, prefix + name)
         fn.argtypes = args
         fn.restype = C.c_int
-
-
-def scalar_fields():
-    return [f.name for f in fields(SetupArrays)]

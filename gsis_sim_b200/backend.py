@@ -103,6 +103,16 @@ class KineticBackendABI:
                    abi.as_ptr(out, C.c_double))
         return out
 
+    def discrete_maxwell(self, states, tolerance: float):
+        """Conservative discrete Maxwellians of macroscopic states (n, 5) -> (corrected states, Newton result)."""
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 5)
+        out = np.empty_like(st)
+        res = np.empty(len(st), dtype=np.int32)
+        if len(st):
+            self._call("discrete_maxwell", abi.as_ptr(st, C.c_double), len(st), C.c_double(tolerance),
+                       abi.as_ptr(out, C.c_double), abi.as_ptr(res, C.c_int32))
+        return out, res
+
     def deq_counts(self):
         d = abi.KinDeqCounts()
         self._call("deq_counts", C.byref(d))

@@ -151,6 +151,7 @@ struct KinHandle {
   virtual void device_f(void** f, int32_t* es) = 0;
   virtual void velocity_permutation(int32_t* perm, int64_t n) const = 0;
   virtual void schedule_info(int32_t* max_levels, int32_t* n_chains) const = 0;
+  virtual void discrete_maxwell(const double* states, int64_t n, double tol, double* out, int32_t* result) = 0;
 };
 
 namespace {
@@ -791,6 +792,25 @@ struct Backend final : KinHandle {
     deq_valid = false;
   }
 
+  void discrete_maxwell(const double* states, int64_t n, double tol, double* out, int32_t* result) override {
+    if (n <= 0) return;
+    DevBuf<double> d_states, d_out;
+    DevBuf<int32_t> d_res;
+    d_states.upload(states, static_cast<size_t>(5 * n), stream);
+    d_out.alloc(static_cast<size_t>(5 * n));
+    d_res.alloc(static_cast<size_t>(n));
+    kin::DeqGrid g = view.deq;
+    g.tolerance = tol;
+    timer.begin(PhaseTimer::kOther, stream);
+    L::discrete_maxwell_states(view, g, d_states.p, d_out.p, d_res.p, static_cast<int>(n), stream);
+    launched();
+    timer.end(stream);
+    KCUDA(cudaMemcpyAsync(out, d_out.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, stream));
+    KCUDA(cudaMemcpyAsync(result, d_res.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
   void take_timings(KinStepTimings* out) override {
     timer.flush(timings);
     *out = timings;
@@ -919,6 +939,10 @@ int kin_launch_count(const KinHandle* h, int64_t* out) {
 int kin_device_f(KinHandle* h, void** f, int32_t* es) { return guard(h, [&] { h->device_f(f, es); }); }
 int kin_velocity_permutation(const KinHandle* h, int32_t* perm, int64_t n) {
   return guard(const_cast<KinHandle*>(h), [&] { h->velocity_permutation(perm, n); });
+}
+int kin_discrete_maxwell(KinHandle* h, const double* states, int64_t n, double tolerance, double* out,
+                         int32_t* result) {
+  return guard(h, [&] { h->discrete_maxwell(states, n, tolerance, out, result); });
 }
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains) {
   return guard(const_cast<KinHandle*>(h), [&] { h->schedule_info(max_levels, n_chains); });

@@ -582,6 +582,43 @@ __global__ void __launch_bounds__(kCellThreads)
   }
 }
 
+
+// ---------------------------------------------------------------------------------------------------------
+// conservative discrete Maxwellian of given macroscopic states, FP64 on the FP64 velocity grid
+// (correct_inflow, src/kinetic/kinetic_solver.cpp:103-114, and maxwell_params_to_state,
+// src/kinetic/kinetic_kernels.hpp:544-552). out: corrected (rho, ux, uy, uz, T), result: Newton iterations
+// (0: resolved, no correction; -1: failed)
+// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__global__ void __launch_bounds__(kCellThreads)
+    k_discrete_maxwell_states(View<S, M> v, DeqGrid deq, const double* __restrict__ states, double* __restrict__ out,
+                              int* __restrict__ result) {
+  __shared__ double sh_red[kDeqSums * (kCellThreads / 32)];
+  __shared__ double sh_state[12];
+  const int i = blockIdx.x;
+  const double* st = states + 5 * static_cast<int64_t>(i);
+  Maxwell<double> m;
+  double gamma[5];
+  const int r = block_discrete_maxwell_on<double, kCellThreads>(v.xid_x, v.xid_y, v.xid_z, v.wts, v.nv, v.weight, deq,
+                                                               st[0], st[1], st[2], st[3], st[4], nullptr, m, gamma,
+                                                               sh_red, sh_state);
+  if (threadIdx.x == 0) {
+    double* o = out + 5 * static_cast<int64_t>(i);
+    if (r > 0) {
+      const double T = 1.0 / (2.0 * m.B);
+      const double two_pi_T = 2.0 * kPi * T;
+      o[0] = m.A * two_pi_T * sqrt(two_pi_T);
+      o[1] = m.ux;
+      o[2] = m.uy;
+      o[3] = m.uz;
+      o[4] = T;
+    } else {
+      for (int k = 0; k < 5; ++k) o[k] = st[k];
+    }
+    result[i] = r;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------------------
 // f <-> host order (cells c0 .. c0 + n of a staging buffer in the reference storage order)
 // ---------------------------------------------------------------------------------------------------------
@@ -711,6 +748,12 @@ void Launch<S, M>::import_f(const double* src, S* f, const int32_t* perm, int64_
 template <class S, class M>
 void Launch<S, M>::export_f(const S* f, double* dst, const int32_t* inv, int64_t c0, int n, int nv, cudaStream_t st) {
   if (n > 0) k_export<S><<<148 * 16, 256, 0, st>>>(f, dst, inv, c0, n, nv);
+}
+
+template <class S, class M>
+void Launch<S, M>::discrete_maxwell_states(const View<S, M>& v, const DeqGrid& deq, const double* states, double* out,
+                                           int* result, int n, cudaStream_t st) {
+  if (n > 0) k_discrete_maxwell_states<S, M><<<n, kCellThreads, 0, st>>>(v, deq, states, out, result);
 }
 
 template struct Launch<float, float>;

@@ -234,13 +234,15 @@ __device__ inline T block_reduce_op(T val, T* sh, Op op) {
 // src/kinetic/kinetic_cuda_kernels.cu:71-145 and discrete_maxwell_seq, kinetic_kernels.hpp:499-540).
 // Terms in M, sums in double. Returns Newton iterations (0: resolved, -1: failed) in every thread.
 // ---------------------------------------------------------------------------------------------------------
-template <class S, class M, int B>
-__device__ int block_discrete_maxwell(const View<S, M>& v, double rho, double ux, double uy, double uz, double T,
-                                      const CellParams<M>* poly, Maxwell<M>& out, double (&gamma)[5], double* sh_red,
-                                      double* sh_state) {
+template <class M, int B>
+__device__ int block_discrete_maxwell_on(const M* __restrict__ vx, const M* __restrict__ vy, const M* __restrict__ vz,
+                                         const double* __restrict__ wts, int nv, double weight, const DeqGrid& deq,
+                                         double rho, double ux, double uy, double uz, double T,
+                                         const CellParams<M>* poly, Maxwell<M>& out, double (&gamma)[5],
+                                         double* sh_red, double* sh_state) {
   for (double& x : gamma) x = 0.0;
   out = maxwell_from<M>(rho, ux, uy, uz, T);
-  if (deq_resolved(v.deq, ux, uy, uz, T)) return 0;
+  if (deq_resolved(deq, ux, uy, uz, T)) return 0;
   const int tid = threadIdx.x;
   if (tid == 0) {
     double beta[5];
@@ -252,8 +254,8 @@ __device__ int block_discrete_maxwell(const View<S, M>& v, double rho, double ux
   }
   __syncthreads();
   const M fux = static_cast<M>(ux), fuy = static_cast<M>(uy), fuz = static_cast<M>(uz);
-  const bool uniform = v.wts == nullptr;
-  const double w = uniform ? v.weight : 1.0;
+  const bool uniform = wts == nullptr;
+  const double w = uniform ? weight : 1.0;
   for (int it = 0;; ++it) {
     const double beta[5] = {sh_state[0], sh_state[1], sh_state[2], sh_state[3], sh_state[4]};
     const Maxwell<M> m = deq_params<M>(beta, ux, uy, uz);
@@ -261,12 +263,12 @@ __device__ int block_discrete_maxwell(const View<S, M>& v, double rho, double ux
 #pragma unroll
     for (int k = 0; k < kDeqSums; ++k) acc[k] = 0.0;
     M t[kDeqSums];
-    for (int q = tid; q < v.nv; q += B) {
-      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+    for (int q = tid; q < nv; q += B) {
+      const M x = vx[q], y = vy[q], z = vz[q];
       const M cx = x - fux, cy = y - fuy, cz = z - fuz;
       M e = maxwellian(m, x, y, z);
       const M pm = poly != nullptr ? shakhov_poly(*poly, cx, cy, cz, cx * cx + cy * cy + cz * cz) : M(0);
-      if (!uniform) e *= static_cast<M>(v.wts[q]);
+      if (!uniform) e *= static_cast<M>(wts[q]);
       deq_terms<M>(e, pm, cx, cy, cz, t);
 #pragma unroll
       for (int k = 0; k < kDeqSums; ++k) acc[k] += static_cast<double>(t[k]);
@@ -275,8 +277,8 @@ __device__ int block_discrete_maxwell(const View<S, M>& v, double rho, double ux
     if (tid == 0) {
       double b[5] = {beta[0], beta[1], beta[2], beta[3], beta[4]};
       double rel = 0.0;
-      const int r = deq_newton_step(acc, w, rho, T, v.deq.tolerance, b, rel);
-      if (deq_accept(r, rel, sh_state[11], it + 1 == v.deq.max_iterations)) {
+      const int r = deq_newton_step(acc, w, rho, T, deq.tolerance, b, rel);
+      if (deq_accept(r, rel, sh_state[11], it + 1 == deq.max_iterations)) {
         sh_state[5] = 1.0;
         if (poly != nullptr) {
           double gm[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -284,7 +286,7 @@ __device__ int block_discrete_maxwell(const View<S, M>& v, double rho, double ux
             for (int k = 0; k < 5; ++k) sh_state[6 + k] = gm[k];
           }
         }
-      } else if (r < 0 || it + 1 >= v.deq.max_iterations) {
+      } else if (r < 0 || it + 1 >= deq.max_iterations) {
         sh_state[5] = -1.0;
       } else {
         for (int k = 0; k < 5; ++k) sh_state[k] = b[k];
@@ -305,6 +307,15 @@ __device__ int block_discrete_maxwell(const View<S, M>& v, double rho, double ux
       return result;
     }
   }
+}
+
+// the same on the View's velocity grid (storage precision of the per-point terms)
+template <class S, class M, int B>
+__device__ inline int block_discrete_maxwell(const View<S, M>& v, double rho, double ux, double uy, double uz, double T,
+                                             const CellParams<M>* poly, Maxwell<M>& out, double (&gamma)[5],
+                                             double* sh_red, double* sh_state) {
+  return block_discrete_maxwell_on<M, B>(v.xi_x, v.xi_y, v.xi_z, v.wts, v.nv, v.weight, v.deq, rho, ux, uy, uz, T,
+                                         poly, out, gamma, sh_red, sh_state);
 }
 
 }  // namespace kin

@@ -51,6 +51,8 @@ struct Launch {
   static void sweep_pass(const View<S, M>& v, const SweepArgs<S>& a, cudaStream_t st);
   static void gsis_correction(const View<S, M>& v, const double* wh, const double* wn, int* flags, double* shift,
                               int mode, int discrete, int collisionless, cudaStream_t st);
+  static void discrete_maxwell_states(const View<S, M>& v, const DeqGrid& deq, const double* states, double* out,
+                                      int* result, int n, cudaStream_t st);
   static void import_f(const double* src, S* f, const int32_t* perm, int64_t c0, int n, int nv, cudaStream_t st);
   static void export_f(const S* f, double* dst, const int32_t* inv, int64_t c0, int n, int nv, cudaStream_t st);
 };

@@ -232,6 +232,12 @@ int kin_device_f(KinHandle* h, void** f, int32_t* elem_bytes);
 /* The handle stores velocities in its own order (grouped by sweep direction): perm[q] = reference storage
    position of the handle's velocity q. */
 int kin_velocity_permutation(const KinHandle* h, int32_t* perm, int64_t n);
+/* Conservative discrete Maxwellian of n macroscopic states (rho, ux, uy, uz, T), FP64 on the velocity grid with
+   the given Newton tolerance: the host-side correction of inflow states (correct_inflow,
+   src/kinetic/kinetic_solver.cpp:103-114) batched on the device. out: the corrected states (unchanged where
+   result <= 0); result: Newton iterations (0: resolved, no correction; -1: no convergence). */
+int kin_discrete_maxwell(KinHandle* h, const double* states, int64_t n, double tolerance, double* out,
+                         int32_t* result);
 /* LU-SGS level schedule statistics: number of levels of the longest (direction, block) chain and the total
    number of (direction, block) chains. */
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains);

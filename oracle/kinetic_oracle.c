@@ -165,6 +165,60 @@ static void orc_finalize_moments(const double* s, double weight, double u0x, dou
   out[14] = 0.5 * weight * (s[12] - dz * tr2 - 2.0 * s2dz + 2.0 * s0 * du2 * dz);
 }
 
+
+/* discrete_maxwell_seq<double> + maxwell_params_to_state (src/kinetic/kinetic_kernels.hpp:499-552) on the FP64
+   velocity grid: the host-side correction of inflow states (correct_inflow, src/kinetic/kinetic_solver.cpp:103-114) */
+static int orc_deq_state_f64(const double* xx, const double* xy, const double* xz, const double* w8, int nv, double weight,
+                             const double* lo, const double* hi, const double* dd, double crit, int maxit, double tol,
+                             const double* st, double* out) {
+  for (int k = 0; k < 5; ++k) out[k] = st[k];
+  const double rho = st[0], ux = st[1], uy = st[2], uz = st[3], T = st[4];
+  if (orc_deq_resolved(lo, hi, dd, crit, ux, uy, uz, T)) return 0;
+  double beta[5];
+  orc_deq_initial_beta(rho, T, beta);
+  const double w = w8 ? 1.0 : weight;
+  double rel_prev = 1e300;
+  for (int it = 0; it < maxit; ++it) {
+    const double B = -0.5 * beta[4];
+    const double dx = -beta[1] / beta[4], dy = -beta[2] / beta[4], dz = -beta[3] / beta[4];
+    const double mux = ux + dx, muy = uy + dy, muz = uz + dz;
+    const double A = exp(beta[0] + B * (dx * dx + dy * dy + dz * dz));
+    double sums[20] = {0};
+    for (int p = 0; p < nv; ++p) {
+      const double cx = xx[p] - ux, cy = xy[p] - uy, cz = xz[p] - uz;
+      const double ex = xx[p] - mux, ey = xy[p] - muy, ez = xz[p] - muz;
+      double e = A * exp(-B * (ex * ex + ey * ey + ez * ez));
+      if (w8) e *= w8[p];
+      const double h = 0.5 * (cx * cx + cy * cy + cz * cz);
+      double t[20];
+      t[0] = e; t[1] = e * cx; t[2] = e * cy; t[3] = e * cz; t[4] = e * h;
+      t[5] = t[1] * cx; t[6] = t[1] * cy; t[7] = t[1] * cz; t[8] = t[1] * h;
+      t[9] = t[2] * cy; t[10] = t[2] * cz; t[11] = t[2] * h;
+      t[12] = t[3] * cz; t[13] = t[3] * h; t[14] = t[4] * h;
+      for (int k = 15; k < 20; ++k) t[k] = 0.0;
+      for (int k = 0; k < 20; ++k) sums[k] += t[k];
+    }
+    double b[5] = {beta[0], beta[1], beta[2], beta[3], beta[4]};
+    double rel = 0.0;
+    const int r = orc_deq_newton_step(sums, w, rho, T, tol, b, &rel);
+    if (orc_deq_accept(r, rel, rel_prev, it + 1 == maxit)) {
+      const double Tn = 1.0 / (2.0 * B);
+      const double tp = 2.0 * ORC_PI * Tn;
+      out[0] = A * tp * sqrt(tp);
+      out[1] = mux;
+      out[2] = muy;
+      out[3] = muz;
+      out[4] = Tn;
+      return it + 1;
+    }
+    if (r < 0) break;
+    for (int k = 0; k < 5; ++k) beta[k] = b[k];
+    rel_prev = rel;
+  }
+  for (int k = 0; k < 5; ++k) out[k] = st[k];
+  return -1;
+}
+
 #define S float
 #define M float
 #define SFX _f32
@@ -321,5 +375,21 @@ int orc_deq_counts(OrcHandle* h, KinDeqCounts* out) {
     if (fl[c] < 0) ++out->failed;
     if (fl[c] > out->max_iterations) out->max_iterations = fl[c];
   }
+  return KIN_OK;
+}
+
+#define DEQ_STATES(SF)                                                                                         \
+  static void deq_states##SF(State##SF* s, const double* st, int64_t n, double tol, double* out, int32_t* res) { \
+    _Pragma("omp parallel for schedule(dynamic, 1)")                                                           \
+    for (int64_t i = 0; i < n; ++i)                                                                            \
+      res[i] = orc_deq_state_f64(s->xd_x, s->xd_y, s->xd_z, s->w, s->nv, s->weight, s->deq_lo, s->deq_hi,      \
+                                 s->deq_d, s->deq_crit, s->deq_maxit, tol, st + 5 * i, out + 5 * i);           \
+  }
+DEQ_STATES(_f32)
+DEQ_STATES(_f64)
+DEQ_STATES(_mix)
+
+int orc_discrete_maxwell(OrcHandle* h, const double* states, int64_t n, double tol, double* out, int32_t* result) {
+  DISPATCH(h, deq_states, states, n, tol, out, result);
   return KIN_OK;
 }
