@@ -1,0 +1,313 @@
+"""Benchmark of the B200 kinetic backend: one CIS iteration of the tube case per step.
+
+Workload (the 3-D tube case, plain FP64 on the GPU): O-grid hex tube of radius 1 and length 5 with a downstream
+reservoir, 134,528 cells; inlet p = 1, outlet p = 0.01, T = 1, diffuse walls; delta = 10, omega = 0.81; uniform
+32^3 velocity grid on [-5, 5]^3 (the parity variant of the case's velocity grid); default strong CIS settings
+(octant sweep order, 4 inner sweeps with wall refresh, 2 block passes, discrete equilibrium). Synthetic: the mesh
+and the uniform initial state are generated here; f (35 GB in FP64) is far larger than L2, so no flush is needed.
+
+A step = KineticSolver.sweep(): moments, cell parameters (discrete-equilibrium Newton), pressure-boundary inflow,
+boundary sums, then 4 x (gradient, residual, 2 LU-SGS block passes) with wall refreshes.
+metric = cell-velocity updates per second = n_cells * n_velocities * inner_sweeps / step time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32|mixed] [--impl b200|reference]
+Under torchrun (N > 1) every rank runs an independent replica of the case on its own GPU (the kinetic path of one
+case does not shard across GPUs here; value = all ranks' updates / the slowest rank's time).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0
+    import datetime
+
+    import torch.distributed as dist
+
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    import torch
+
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, ws, local
+
+
+def build_case(args):
+    from gsis_sim_b200 import tube
+
+    t0 = time.time()
+    setup, host = tube.tube_case(delta=10.0, nv=args.nv, precision=args.precision)
+    return setup, host, time.time() - t0
+
+
+def cpu_baseline(args, setup_time_budget=30.0):
+    """The reference's own CPU kinetic path (oracle/_ref/libgsisref.so: KineticSolver + OpenMP CpuBackend) on the
+    same tube mesh with a reduced velocity grid (a bounded sample); falls back to the C port of oracle/."""
+    import numpy as np
+
+    from gsis_sim_b200 import tube
+
+    nv_s = args.cpu_nv
+    cores = os.cpu_count() or 1
+    mesh = tube.tube_mesh()
+    sample = f"tube 134,528 cells x {nv_s}^3 velocities, {args.cpu_steps} CIS iteration(s), FP64"
+    try:
+        from oracle import ref
+
+        if not ref.available():
+            raise FileNotFoundError("oracle/_ref/libgsisref.so not built")
+        rm = ref.RefMesh.from_arrays(mesh.as_dict())
+        spec = ref.case_spec([("inlet", "pressure_inlet", dict(T=1.0, p=1.0)), ("wall", "diffuse_wall", dict(T=1.0)),
+                              ("back", "diffuse_wall", dict(T=1.0)), ("outlet", "pressure_outlet", dict(p=0.01))],
+                             delta_rp=10.0, nv=(nv_s,) * 3, vmax=5.0, omega=0.81,
+                             kinetic={"precision": args.precision if args.precision != "mixed" else "fp32"})
+        case = ref.RefCase(rm, spec)
+        case.init_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
+        case.sweep()  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(args.cpu_steps):
+            case.sweep()
+        dt = (time.perf_counter() - t0) / args.cpu_steps
+        kind = "reference"
+        inner = case.inner_sweeps
+        nc = case.setup.n_cells
+    except (FileNotFoundError, OSError) as e:
+        from oracle.kinetic_oracle import OracleBackend
+        from gsis_sim_b200.solver import KineticSolver
+
+        setup, host = tube.tube_case(delta=10.0, nv=nv_s, precision=args.precision)
+        sol = KineticSolver(setup, host, OracleBackend(setup))
+        sol.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
+        sol.sweep()
+        t0 = time.perf_counter()
+        for _ in range(args.cpu_steps):
+            sol.sweep()
+        dt = (time.perf_counter() - t0) / args.cpu_steps
+        kind = "port"
+        inner = host.inner_sweeps
+        nc = setup.n_cells
+        sample += f" (reference library unavailable: {e})"
+    value = nc * nv_s ** 3 * inner / dt
+    return {"value": value, "unit": "cell*velocity updates/s", "cores": cores, "kind": kind, "sample": sample,
+            "seconds_per_iteration": dt}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    cb = cpu_baseline(args)
+    line = {"impl": "reference", "metric": "cell_velocity_updates_per_s", "value": cb["value"],
+            "unit": cb["unit"], "n_gpus": args.gpus, "steps": args.cpu_steps, "warmup": 1,
+            "ms_per_step": 1e3 * cb["seconds_per_iteration"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32"}[args.precision],
+            "data": "synthetic", "config": workload_config(args),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, cb_nv=None):
+    return {"workload": f"kinetic CIS iteration, O-grid tube + reservoir 134528 cells, uniform {args.nv}^3 velocities "
+                        f"on [-5,5]^3, delta 10, {args.precision}",
+            "cells": 134528, "velocities": (cb_nv or args.nv) ** 3, "inner_sweeps": 4, "block_passes": 2,
+            "sweep_order": "octant", "equilibrium": "discrete",
+            "l2": "no flush: f and the work arrays (tens of GB) exceed the 126 MB L2"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"])
+    ap.add_argument("--nv", type=int, default=32)
+    ap.add_argument("--cpu-nv", type=int, default=8)
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank, ws, local = dist_init() if args.gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1 else (0, 1, 0)
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    from gsis_sim_b200.backend import B200Backend
+    from gsis_sim_b200.solver import KineticSolver
+
+    torch.cuda.set_device(local)
+    setup, host, t_setup = build_case(args)
+    nc, nv = setup.n_cells, setup.nv
+    inner = host.inner_sweeps
+    be = B200Backend(setup, device=local)
+    sol = KineticSolver(setup, host, be)
+    sol.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
+    for _ in range(args.warmup):
+        sol.sweep()
+    be.take_timings()
+    launches0 = be.launch_count()
+    bytes_h2d = bytes_d2h = 0
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    # timed region: K CIS iterations through the public host loop (host buffers, H2D/D2H inside)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sol.sweep()
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t0
+    barrier()
+    timings = be.take_timings()
+    launches = be.launch_count() - launches0
+    device_busy = sum(timings.values())
+    # per-step host<->device traffic of the host loop (moments, deq flags, inflow tables, boundary sums, residuals,
+    # discrete-Maxwellian inflow states)
+    nb = setup.n_bfaces
+    n_pres = len(sol.pres_faces)
+    per_prepare_d2h = 15 * nc * 8 + nc * 4 + 20 * nb * 8 + n_pres * (5 * 8 + 4)
+    per_prepare_h2d = 2 * nb * 6 * 8 + n_pres * 5 * 8
+    bytes_d2h = per_prepare_d2h + inner * nc * 8 + (inner - 1) * 20 * nb * 8
+    bytes_h2d = per_prepare_h2d + (inner - 1) * nb * 6 * 8
+
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([t_wall, device_busy], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_wall, device_busy = float(t[0]), float(t[1])
+
+    updates = float(nc) * nv * inner * args.steps
+    value = updates * ws / device_busy
+    e2e = updates * ws / t_wall
+    hbm, peak_kind = peaks()
+    s = 8 if args.precision == "fp64" else 4
+    # dominant kernel: gradient, residual or LU-SGS pass (per-launch algorithmic bytes in DESIGN.md)
+    n_sweeps = inner * args.steps
+    kernels = {
+        "k_gradient": (timings["gradient"] / n_sweeps, nc * nv * 4 * s),
+        "k_residual": (timings["residual"] / n_sweeps, nc * nv * 5 * s),
+        "k_sweep_pass": (timings["sweep_forward"] / (2 * n_sweeps), nc * nv * 3 * s),
+    }
+    dom = max(kernels, key=lambda k: kernels[k][0])
+    t_launch, bytes_launch = kernels[dom]
+    achieved = bytes_launch / t_launch / 1e9
+    clocks = clk.summary()
+    line = {
+        "metric": "cell_velocity_updates_per_s", "value": value, "unit": "cell*velocity updates/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32 storage / f64 arithmetic"}[args.precision],
+        "data": "synthetic", "config": workload_config(args),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": 1e3 * t_launch},
+        "e2e": {"value": e2e, "unit": "cell*velocity updates/s", "h2d_bytes_per_step": bytes_h2d,
+                "d2h_bytes_per_step": bytes_d2h},
+        "gpu_launches": launches, "clocks": clocks,
+        "phase_seconds_per_step": {k: v / args.steps for k, v in timings.items()},
+        "mass_flow": sol.mass_flow()[2], "setup_seconds": t_setup,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+        line["cpu_baseline"].pop("seconds_per_iteration", None)
+    be.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
