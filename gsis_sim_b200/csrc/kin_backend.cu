@@ -204,7 +204,9 @@ struct Backend final : KinHandle {
   DevBuf<M> specular, specular_first;
   DevBuf<int32_t> grid_to_pos;
   DevBuf<double> volume, vdt;
-  DevBuf<int32_t> block_offsets, chain_cells, chain_start, lev_bounds, lev_start, lev_count, pos;
+  DevBuf<int32_t> block_offsets, chain_start, lev_bounds, lev_start, lev_count;
+  DevBuf<int4> prog;
+  DevBuf<kin::SweepE<M>> sweep_entries;
   DevBuf<int32_t> d_perm, d_inv;
   DevBuf<double> moments, shift, residual_cell, bsums, partial, w_half, w_new, staging;
   DevBuf<int32_t> flags, face_cells, face_entries;
@@ -501,12 +503,40 @@ struct Backend final : KinHandle {
         max_levels = std::max(max_levels, nlev);
       }
     }
-    chain_cells.upload(hcells.data(), hcells.size(), stream);
+    // per-chain program: (cell, first CSR entry, number of entries, bitmask of the in-block neighbours that precede
+    // the cell in the group's sweep order); the stencil entries keep only what the sweep reads
+    std::vector<int4> hprog(hcells.size());
+    for (int g = 0; g < n_groups; ++g) {
+      const int32_t* pg = hpos.data() + g * ncs;
+      for (int b = 0; b < n_blocks; ++b) {
+        const int cb = h_block_offsets[b], ce = h_block_offsets[b + 1];
+        for (int k = cb; k < ce; ++k) {
+          const size_t i = static_cast<size_t>(g) * ncs + k;
+          const int c = hcells[i];
+          const int e0 = d.csr_offsets[c], ne = d.csr_offsets[c + 1] - e0;
+          KCHECK(ne <= 32, "a cell with more than 32 faces is not supported by the LU-SGS sweep kernel");
+          uint32_t mask = 0;
+          for (int j = 0; j < ne; ++j) {
+            const int o = d.csr_other[e0 + j];
+            if (o >= cb && o < ce && pg[o] < pg[c]) mask |= 1u << j;
+          }
+          hprog[i] = make_int4(c, e0, ne, static_cast<int>(mask));
+        }
+      }
+    }
+    const int64_t n_csr = d.csr_offsets[nc];
+    std::vector<kin::SweepE<M>> hse(static_cast<size_t>(std::max<int64_t>(n_csr, 1)));
+    for (int64_t e = 0; e < n_csr; ++e) {
+      const int o = d.csr_other[e];
+      hse[e].other = o >= 0 ? o : (d.bface_kind[d.csr_bface[e]] == kin::kPeriodic ? -2 : -1);
+      for (int a = 0; a < 3; ++a) hse[e].s[a] = static_cast<M>(d.csr_geom[12 * e + a]);
+    }
+    prog.upload(hprog.data(), hprog.size(), stream);
+    sweep_entries.upload(hse.data(), hse.size(), stream);
     chain_start.upload(hstart.data(), hstart.size(), stream);
     lev_bounds.upload(hbounds.data(), hbounds.size(), stream);
     lev_start.upload(hlev_start.data(), hlev_start.size(), stream);
     lev_count.upload(hlev_count.data(), hlev_count.size(), stream);
-    pos.upload(hpos.data(), hpos.size(), stream);
     KCUDA(cudaStreamSynchronize(stream));
   }
 
@@ -522,8 +552,8 @@ struct Backend final : KinHandle {
         if (s >= e) continue;
         for (int b = 0; b < n_blocks; ++b) {
           if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
-          for (int t = s; t < e; t += 32)
-            items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + 32, e) - k0, 0));
+          for (int t = s; t < e; t += kin::kSweepTile)
+            items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + kin::kSweepTile, e) - k0, 0));
         }
       }
       cp->n_items = static_cast<int32_t>(items.size());
@@ -593,8 +623,8 @@ struct Backend final : KinHandle {
     return xi_x.bytes() * 3 + xid_x.bytes() * 3 + wts.bytes() + csr_off.bytes() + csr.bytes() + eps2.bytes() +
            bfaces.bytes() + inflow.bytes() + cells.bytes() + mirror_map.bytes() + mw_offset.bytes() + mw_frac.bytes() +
            specular.bytes() * 2 + grid_to_pos.bytes() + volume.bytes() + vdt.bytes() + block_offsets.bytes() +
-           chain_cells.bytes() + chain_start.bytes() + lev_bounds.bytes() + lev_start.bytes() + lev_count.bytes() +
-           pos.bytes() + d_perm.bytes() * 2 + moments.bytes() + shift.bytes() + residual_cell.bytes() + bsums.bytes() +
+           prog.bytes() + sweep_entries.bytes() + chain_start.bytes() + lev_bounds.bytes() + lev_start.bytes() +
+           lev_count.bytes() + d_perm.bytes() * 2 + moments.bytes() + shift.bytes() + residual_cell.bytes() + bsums.bytes() +
            partial.bytes() + w_half.bytes() * 2 + staging.bytes() + flags.bytes() + f.bytes() + gx.bytes() * 4;
   }
 
@@ -743,17 +773,17 @@ struct Backend final : KinHandle {
       S* prev = nullptr;
       for (int pass = 0; pass < block_passes; ++pass) {
         S* out = (pass % 2 == 0) ? gz.p : gy.p;
-        kin::SweepArgs<S> a{};
+        kin::SweepArgs<S, M> a{};
         a.items = cp->items.p;
         a.n_items = cp->n_items;
         a.n_blocks = n_blocks;
         a.block_offsets = block_offsets.p;
-        a.chain_cells = chain_cells.p;
+        a.prog = prog.p;
         a.chain_start = chain_start.p;
         a.lev_bounds = lev_bounds.p;
         a.lev_start = lev_start.p;
         a.lev_count = lev_count.p;
-        a.pos = pos.p;
+        a.se = sweep_entries.p;
         a.R = r.p;
         a.dprev = prev;
         a.out = out;

@@ -293,30 +293,161 @@ __global__ void __launch_bounds__(kFaceThreads)
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// limited gradients of one velocity chunk (k_gradient, kinetic_cuda_kernels.cu:343-355)
-// grid: (cell, velocity tile of kTileThreads * kTileIters)
+// limited gradients and steady residual of one velocity chunk (k_gradient / k_residual,
+// kinetic_cuda_kernels.cu:343-372; limited_gradient / residual_value, kinetic_kernels.hpp:161-201, 238-278).
+// grid: (cell, velocity tile of kTileThreads * kTileIters). The CTA stages its cell's CSR entries in shared
+// memory once; every thread then carries its kTileIters velocities through each entry together, so an entry is
+// read once per thread (not once per velocity) and the velocities give independent FP64 chains. The arithmetic
+// of every velocity is that of the reference routines, entry by entry in CSR order.
 // ---------------------------------------------------------------------------------------------------------
+constexpr int kStageMax = 32;
+
+template <class M>
+struct StagedEntry {
+  CsrE<M> e;
+  int32_t kind;  // -1 internal face, else the boundary kind
+};
+
 template <class S, class M>
-__global__ void __launch_bounds__(kTileThreads) k_gradient(View<S, M> v, Chunk<S> ch) {
-  const int c = blockIdx.x;
-  const int tb = blockIdx.y * (kTileThreads * kTileIters);
-  const int te = min(ch.kc, tb + kTileThreads * kTileIters);
-  for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
-    const int q = ch.k0 + t;
-    const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
-    M gx, gy, gz;
-    limited_gradient(v, c, q, x, y, z, f_at(v, c, q), gx, gy, gz);
-    const int64_t wi = static_cast<int64_t>(c) * ch.stride + t;
-    ch.gx[wi] = static_cast<S>(gx);
-    ch.gy[wi] = static_cast<S>(gy);
-    ch.gz[wi] = static_cast<S>(gz);
+__device__ __forceinline__ int stage_cell(const View<S, M>& v, int cell, StagedEntry<M>* sh) {
+  const int e0 = v.csr_off[cell], ne = v.csr_off[cell + 1] - e0;
+  if (ne <= kStageMax && static_cast<int>(threadIdx.x) < ne) {
+    StagedEntry<M> se;
+    se.e = v.csr[e0 + threadIdx.x];
+    se.kind = se.e.other >= 0 ? -1 : v.bf[se.e.bface].kind;
+    sh[threadIdx.x] = se;
+  }
+  __syncthreads();
+  return ne;
+}
+
+template <class S>
+__device__ __forceinline__ S ldg_s(const S* p) { return __ldg(p); }
+
+// limited_gradient for U velocities of one cell at once (same arithmetic per velocity)
+template <class S, class M, int U>
+__device__ inline void limited_gradient_multi(const View<S, M>& v, int cell, const StagedEntry<M>* E, int ne,
+                                              const int (&q)[U], const bool (&ok)[U], const M (&x)[U],
+                                              const M (&y)[U], const M (&z)[U], const M (&fi)[U], M (&gx)[U],
+                                              M (&gy)[U], M (&gz)[U]) {
+  M sx[U], sy[U], sz[U], fmax[U], fmin[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    sx[u] = sy[u] = sz[u] = M(0);
+    fmax[u] = fmin[u] = fi[u];
+  }
+  for (int j = 0; j < ne; ++j) {
+    const CsrE<M>& c = E[j].e;
+    M fk[U];
+    if (c.other >= 0) {
+      const S* fo = v.f + static_cast<int64_t>(c.other) * v.nv;
+#pragma unroll
+      for (int u = 0; u < U; ++u) fk[u] = ok[u] ? static_cast<M>(ldg_s(fo + q[u])) : fi[u];
+    } else {
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        fk[u] = ok[u] ? boundary_value_first_order(v, c, cell, q[u], x[u], y[u], z[u], fi[u]) : fi[u];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const M d = fk[u] - fi[u];
+      sx[u] += c.c[0] * d;
+      sy[u] += c.c[1] * d;
+      sz[u] += c.c[2] * d;
+      fmax[u] = kmax(fmax[u], fk[u]);
+      fmin[u] = kmin(fmin[u], fk[u]);
+    }
+  }
+  if (v.limiter_mode == kLimNone && v.positivity == 0) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      gx[u] = sx[u];
+      gy[u] = sy[u];
+      gz[u] = sz[u];
+    }
+    return;
+  }
+  const M eps2c = v.eps2[cell];
+  M eps2[U], phi[U], pmin[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    eps2[u] = eps2c;
+    if (v.limiter_mode == kLimRel) {
+      const M sc = kmax(kabs(fmax[u]), kabs(fmin[u]));
+      eps2[u] *= sc * sc;
+    }
+    phi[u] = M(1);
+    pmin[u] = M(0);
+  }
+  for (int j = 0; j < ne; ++j) {
+    const CsrE<M>& c = E[j].e;
+    if (E[j].kind == kPeriodic) continue;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const M proj = sx[u] * c.ds[0] + sy[u] * c.ds[1] + sz[u] * c.ds[2];
+      if (v.limiter_mode != kLimNone) phi[u] = kmin(phi[u], venkat_face(proj, fmax[u] - fi[u], fmin[u] - fi[u], eps2[u]));
+      pmin[u] = kmin(pmin[u], proj);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    M ph = phi[u];
+    if (v.positivity != 0) {
+      if (!(fi[u] > M(0))) ph = M(0);
+      else if (pmin[u] < M(0)) ph = kmin(ph, fi[u] / (-pmin[u]));
+    }
+    gx[u] = ph * sx[u];
+    gy[u] = ph * sy[u];
+    gz[u] = ph * sz[u];
   }
 }
 
-// ---------------------------------------------------------------------------------------------------------
-// steady residual R = sum_e a f_face - (V/tau)(f^S - f) of one chunk (residual_value, kinetic_kernels.hpp:238-278)
-// and per-(cell, tile) partial sums of R^2 in FP64 (k_residual, kinetic_cuda_kernels.cu:357-372)
-// ---------------------------------------------------------------------------------------------------------
+template <class S, class M>
+__global__ void __launch_bounds__(kTileThreads, 2) k_gradient(View<S, M> v, Chunk<S> ch) {
+  __shared__ StagedEntry<M> E[kStageMax];
+  const int c = blockIdx.x;
+  const int tb = blockIdx.y * (kTileThreads * kTileIters);
+  const int te = min(ch.kc, tb + kTileThreads * kTileIters);
+  const int ne = stage_cell(v, c, E);
+  if (ne > kStageMax) {  // general polyhedra with many faces: one velocity at a time
+    for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
+      const int q = ch.k0 + t;
+      M gx, gy, gz;
+      limited_gradient(v, c, q, v.xi_x[q], v.xi_y[q], v.xi_z[q], f_at(v, c, q), gx, gy, gz);
+      const int64_t wi = static_cast<int64_t>(c) * ch.stride + t;
+      ch.gx[wi] = static_cast<S>(gx);
+      ch.gy[wi] = static_cast<S>(gy);
+      ch.gz[wi] = static_cast<S>(gz);
+    }
+    return;
+  }
+  constexpr int U = kTileIters;
+  int q[U];
+  bool ok[U];
+  M x[U], y[U], z[U], fi[U], gx[U], gy[U], gz[U];
+  const S* fc = v.f + static_cast<int64_t>(c) * v.nv;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int t = tb + threadIdx.x + u * kTileThreads;
+    ok[u] = t < te;
+    q[u] = ch.k0 + (ok[u] ? t : tb);
+    x[u] = v.xi_x[q[u]];
+    y[u] = v.xi_y[q[u]];
+    z[u] = v.xi_z[q[u]];
+    fi[u] = static_cast<M>(ldg_s(fc + q[u]));
+  }
+  limited_gradient_multi<S, M, U>(v, c, E, ne, q, ok, x, y, z, fi, gx, gy, gz);
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (!ok[u]) continue;
+    const int64_t wi = static_cast<int64_t>(c) * ch.stride + (q[u] - ch.k0);
+    ch.gx[wi] = static_cast<S>(gx[u]);
+    ch.gy[wi] = static_cast<S>(gy[u]);
+    ch.gz[wi] = static_cast<S>(gz[u]);
+  }
+}
+
+// residual_value for one velocity (general path and the symmetry face term)
 template <class S, class M>
 __device__ inline M residual_value(const View<S, M>& v, const Chunk<S>& ch, int cell, int t) {
   const int q = ch.k0 + t;
@@ -362,17 +493,81 @@ __device__ inline M residual_value(const View<S, M>& v, const Chunk<S>& ch, int 
 }
 
 template <class S, class M>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, 2)
     k_residual(View<S, M> v, Chunk<S> ch, double* __restrict__ partial, int partial_stride) {
+  __shared__ StagedEntry<M> E[kStageMax];
   __shared__ double sh[kTileThreads / 32];
   const int c = blockIdx.x;
   const int tb = blockIdx.y * (kTileThreads * kTileIters);
   const int te = min(ch.kc, tb + kTileThreads * kTileIters);
+  const int ne = stage_cell(v, c, E);
   double r2[1] = {0.0};
-  for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
-    const M R = residual_value(v, ch, c, t);
-    ch.r[static_cast<int64_t>(c) * ch.stride + t] = static_cast<S>(R);
-    r2[0] += static_cast<double>(R) * static_cast<double>(R);
+  if (ne > kStageMax) {
+    for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
+      const M R = residual_value(v, ch, c, t);
+      ch.r[static_cast<int64_t>(c) * ch.stride + t] = static_cast<S>(R);
+      r2[0] += static_cast<double>(R) * static_cast<double>(R);
+    }
+  } else {
+    constexpr int U = kTileIters;
+    int t[U];
+    bool ok[U];
+    M x[U], y[U], z[U], fi[U], gix[U], giy[U], giz[U], R[U];
+    const S* fc = v.f + static_cast<int64_t>(c) * v.nv;
+    const int64_t row = static_cast<int64_t>(c) * ch.stride;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      t[u] = tb + threadIdx.x + u * kTileThreads;
+      ok[u] = t[u] < te;
+      if (!ok[u]) t[u] = tb;
+      const int q = ch.k0 + t[u];
+      x[u] = v.xi_x[q];
+      y[u] = v.xi_y[q];
+      z[u] = v.xi_z[q];
+      fi[u] = static_cast<M>(ldg_s(fc + q));
+      gix[u] = static_cast<M>(ldg_s(ch.gx + row + t[u]));
+      giy[u] = static_cast<M>(ldg_s(ch.gy + row + t[u]));
+      giz[u] = static_cast<M>(ldg_s(ch.gz + row + t[u]));
+      R[u] = M(0);
+    }
+    for (int j = 0; j < ne; ++j) {
+      const CsrE<M>& ce = E[j].e;
+      const int kind = E[j].kind;
+      if (kind == kPeriodic) continue;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const M a = x[u] * ce.s[0] + y[u] * ce.s[1] + z[u] * ce.s[2];
+        M ff;
+        if (a >= M(0)) {
+          ff = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
+        } else if (ce.other >= 0) {
+          const int64_t wj = static_cast<int64_t>(ce.other) * ch.stride + t[u];
+          ff = static_cast<M>(ldg_s(v.f + static_cast<int64_t>(ce.other) * v.nv + ch.k0 + t[u])) +
+               static_cast<M>(ldg_s(ch.gx + wj)) * ce.dn[0] + static_cast<M>(ldg_s(ch.gy + wj)) * ce.dn[1] +
+               static_cast<M>(ldg_s(ch.gz + wj)) * ce.dn[2];
+        } else if (kind == kSymmetry) {
+          const int q = ch.k0 + t[u];
+          const int qm = v.mirror_map[v.bf[ce.bface].mirror * v.nv + q];
+          const M fm = f_at(v, c, qm);
+          M gx, gy, gz;
+          limited_gradient(v, c, qm, v.xi_x[qm], v.xi_y[qm], v.xi_z[qm], fm, gx, gy, gz);
+          ff = fm + gx * ce.ds[0] + gy * ce.ds[1] + gz * ce.ds[2];
+        } else if (kind == kMaxwellWall) {
+          ff = maxwell_inflow(v, ce.bface, ch.k0 + t[u], x[u], y[u], z[u]);
+        } else {
+          ff = inflow_value(v.inflow[ce.bface], x[u], y[u], z[u]);
+        }
+        R[u] += a * ff;
+      }
+    }
+    const CellParams<M> cp = v.cp[c];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!ok[u]) continue;
+      const M Ru = R[u] - cp.coll * (shakhov_target(cp, x[u], y[u], z[u]) - fi[u]);
+      ch.r[row + t[u]] = static_cast<S>(Ru);
+      r2[0] += static_cast<double>(Ru) * static_cast<double>(Ru);
+    }
   }
   block_sum<1, kTileThreads>(r2, sh);
   if (threadIdx.x == 0) partial[static_cast<int64_t>(c) * partial_stride + blockIdx.y] = r2[0];
@@ -388,66 +583,70 @@ __global__ void k_residual_reduce(const double* __restrict__ partial, int partia
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// one LU-SGS block pass: forward then backward sweep of one (direction group, block) chain per warp, 32
-// velocities per warp (sweep_forward_cell / sweep_backward_cell, kinetic_kernels.hpp:289-358).
+// one LU-SGS block pass (sweep_forward_cell / sweep_backward_cell, kinetic_kernels.hpp:289-358):
+// forward then backward sweep of one (direction group, block) chain for one tile of 32 velocities per CTA.
 //   pass 1:  R = r,  dprev = nullptr (out-of-block coupling -> beta sum|a-| on the diagonal)
 //   pass k:  R = r,  dprev = Delta f of pass k-1 (out-of-block upwind neighbours on the right-hand side)
 // out receives Delta f* (forward) and then Delta f (backward); the last pass adds Delta f to f.
+// The chain's cells are visited level by level; the 8 warps share the cells of a level (two cells in flight per
+// warp, lane = velocity) and meet at a barrier before the next level, so every in-block upwind neighbour has
+// been finished, exactly as in the reference's cell-by-cell order (same per-cell arithmetic, same entry order).
 // ---------------------------------------------------------------------------------------------------------
 template <class S, class M>
-__device__ __forceinline__ void sweep_forward_cell(const View<S, M>& v, const SweepArgs<S>& a, int cell, int t,
-                                                   int cb, int ce, const int32_t* pos, M x, M y, M z) {
+__device__ __forceinline__ M sweep_forward_value(const View<S, M>& v, const SweepArgs<S, M>& a, int4 p, int t, int cb,
+                                                 int ce, M x, M y, M z) {
   M ap = M(0), am_out = M(0), L = M(0), Lout = M(0);
-  const int e0 = v.csr_off[cell], e1 = v.csr_off[cell + 1];
-  const int pi = pos[cell];
-  for (int e = e0; e < e1; ++e) {
-    const CsrE<M>& c = v.csr[e];
-    if (c.other < 0 && v.bf[c.bface].kind == kPeriodic) continue;
-    const M af = x * c.s[0] + y * c.s[1] + z * c.s[2];
+  const SweepE<M>* se = a.se + p.y;
+  for (int j = 0; j < p.z; ++j) {
+    const SweepE<M> e = se[j];
+    if (e.other == -2) continue;
+    const M af = x * e.s[0] + y * e.s[1] + z * e.s[2];
     if (af > M(0)) {
       ap += af;
-    } else if (c.other >= 0) {
-      if (c.other < cb || c.other >= ce) {
+    } else if (e.other >= 0) {
+      if (e.other < cb || e.other >= ce) {
         if (a.dprev != nullptr) {
-          Lout += af * static_cast<M>(a.dprev[static_cast<int64_t>(c.other) * a.stride + t]);
+          Lout += af * static_cast<M>(a.dprev[static_cast<int64_t>(e.other) * a.stride + t]);
         } else {
           am_out -= af;
         }
-      } else if (pos[c.other] < pi) {
-        L += af * static_cast<M>(a.out[static_cast<int64_t>(c.other) * a.stride + t]);
+      } else if ((p.w >> j) & 1) {
+        L += af * static_cast<M>(a.out[static_cast<int64_t>(e.other) * a.stride + t]);
       }
     }
   }
-  const M D = v.cp[cell].diag + v.diag_scale * ap + v.interface_damping * am_out;
-  const int64_t wi = static_cast<int64_t>(cell) * a.stride + t;
-  const M Ri = static_cast<M>(a.R[wi]);
-  a.out[wi] = static_cast<S>((-Ri - Lout - L) / D);
+  const M D = v.cp[p.x].diag + v.diag_scale * ap + v.interface_damping * am_out;
+  const M Ri = static_cast<M>(a.R[static_cast<int64_t>(p.x) * a.stride + t]);
+  return (-Ri - Lout - L) / D;
 }
 
 template <class S, class M>
-__device__ __forceinline__ void sweep_backward_cell(const View<S, M>& v, const SweepArgs<S>& a, int cell, int t,
-                                                    int q, int cb, int ce, const int32_t* pos, M x, M y, M z) {
+__device__ __forceinline__ M sweep_backward_value(const View<S, M>& v, const SweepArgs<S, M>& a, int4 p, int t, int cb,
+                                                  int ce, M x, M y, M z) {
   M ap = M(0), am_out = M(0), U = M(0);
-  const int e0 = v.csr_off[cell], e1 = v.csr_off[cell + 1];
-  const int pi = pos[cell];
-  for (int e = e0; e < e1; ++e) {
-    const CsrE<M>& c = v.csr[e];
-    if (c.other < 0 && v.bf[c.bface].kind == kPeriodic) continue;
-    const M af = x * c.s[0] + y * c.s[1] + z * c.s[2];
+  const SweepE<M>* se = a.se + p.y;
+  for (int j = 0; j < p.z; ++j) {
+    const SweepE<M> e = se[j];
+    if (e.other == -2) continue;
+    const M af = x * e.s[0] + y * e.s[1] + z * e.s[2];
     if (af > M(0)) {
       ap += af;
-    } else if (c.other >= 0) {
-      if (c.other < cb || c.other >= ce) {
+    } else if (e.other >= 0) {
+      if (e.other < cb || e.other >= ce) {
         if (a.dprev == nullptr) am_out -= af;
-      } else if (pos[c.other] > pi) {
-        U += af * static_cast<M>(a.out[static_cast<int64_t>(c.other) * a.stride + t]);
+      } else if (!((p.w >> j) & 1)) {
+        U += af * static_cast<M>(a.out[static_cast<int64_t>(e.other) * a.stride + t]);
       }
     }
   }
-  const M D = v.cp[cell].diag + v.diag_scale * ap + v.interface_damping * am_out;
-  const int64_t wi = static_cast<int64_t>(cell) * a.stride + t;
-  const M df = static_cast<M>(a.out[wi]) - U / D;
-  a.out[wi] = static_cast<S>(df);
+  const M D = v.cp[p.x].diag + v.diag_scale * ap + v.interface_damping * am_out;
+  return static_cast<M>(a.out[static_cast<int64_t>(p.x) * a.stride + t]) - U / D;
+}
+
+template <class S, class M>
+__device__ __forceinline__ void sweep_backward_store(const View<S, M>& v, const SweepArgs<S, M>& a, int cell, int t,
+                                                     int q, M df) {
+  a.out[static_cast<int64_t>(cell) * a.stride + t] = static_cast<S>(df);
   if (a.update_f) {
     S* fp = v.f + static_cast<int64_t>(cell) * v.nv + q;
     *fp = static_cast<S>(static_cast<M>(*fp) + df);
@@ -455,36 +654,54 @@ __device__ __forceinline__ void sweep_backward_cell(const View<S, M>& v, const S
 }
 
 template <class S, class M>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep_pass(View<S, M> v, SweepArgs<S> a) {
-  const int item = (blockIdx.x * kSweepThreads + threadIdx.x) >> 5;
-  if (item >= a.n_items) return;
-  const int4 it = a.items[item];  // (chain, t0, t1, -)
-  const int lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kSweepThreads, 4) k_sweep_pass(View<S, M> v, SweepArgs<S, M> a) {
+  constexpr int W = kSweepThreads / 32;
+  const int4 it = a.items[blockIdx.x];  // (chain, t0, t1, -)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int t = it.y + lane;
   const bool active = t < it.z;
   const int q = a.k0 + t;
   const int chain = it.x;
-  const int g = chain / a.n_blocks;
-  const int b = chain - g * a.n_blocks;
+  const int b = chain % a.n_blocks;
   const int cb = a.block_offsets[b], ce = a.block_offsets[b + 1];
-  const int32_t* cells = a.chain_cells + a.chain_start[chain];
+  const int4* prog = a.prog + a.chain_start[chain];
   const int32_t* lb = a.lev_bounds + a.lev_start[chain];
   const int nlev = a.lev_count[chain];
-  const int32_t* pos = a.pos + static_cast<int64_t>(g) * v.n_cells;
   M x = M(0), y = M(0), z = M(0);
   if (active) {
     x = v.xi_x[q];
     y = v.xi_y[q];
     z = v.xi_z[q];
   }
-  if (!active) return;  // lanes never exchange data: an idle lane can leave
   for (int L = 0; L < nlev; ++L) {
     const int i1 = lb[L + 1];
-    for (int i = lb[L]; i < i1; ++i) sweep_forward_cell(v, a, cells[i], t, cb, ce, pos, x, y, z);
+    if (active) {
+      for (int i = lb[L] + warp; i < i1; i += 2 * W) {
+        const int4 pa = prog[i];
+        const bool two = i + W < i1;
+        const int4 pb = two ? prog[i + W] : pa;
+        const M va = sweep_forward_value(v, a, pa, t, cb, ce, x, y, z);
+        const M vb = two ? sweep_forward_value(v, a, pb, t, cb, ce, x, y, z) : M(0);
+        a.out[static_cast<int64_t>(pa.x) * a.stride + t] = static_cast<S>(va);
+        if (two) a.out[static_cast<int64_t>(pb.x) * a.stride + t] = static_cast<S>(vb);
+      }
+    }
+    __syncthreads();
   }
   for (int L = nlev - 1; L >= 0; --L) {
-    const int i0 = lb[L];
-    for (int i = lb[L + 1] - 1; i >= i0; --i) sweep_backward_cell(v, a, cells[i], t, q, cb, ce, pos, x, y, z);
+    const int i1 = lb[L + 1];
+    if (active) {
+      for (int i = lb[L] + warp; i < i1; i += 2 * W) {
+        const int4 pa = prog[i];
+        const bool two = i + W < i1;
+        const int4 pb = two ? prog[i + W] : pa;
+        const M da = sweep_backward_value(v, a, pa, t, cb, ce, x, y, z);
+        const M db = two ? sweep_backward_value(v, a, pb, t, cb, ce, x, y, z) : M(0);
+        sweep_backward_store(v, a, pa.x, t, q, da);
+        if (two) sweep_backward_store(v, a, pb.x, t, q, db);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -727,9 +944,9 @@ void Launch<S, M>::residual(const View<S, M>& v, const Chunk<S>& ch, double* par
 }
 
 template <class S, class M>
-void Launch<S, M>::sweep_pass(const View<S, M>& v, const SweepArgs<S>& a, cudaStream_t st) {
+void Launch<S, M>::sweep_pass(const View<S, M>& v, const SweepArgs<S, M>& a, cudaStream_t st) {
   if (a.n_items <= 0) return;
-  k_sweep_pass<S, M><<<ceil_div(a.n_items, kSweepThreads / 32), kSweepThreads, 0, st>>>(v, a);
+  k_sweep_pass<S, M><<<a.n_items, kSweepThreads, 0, st>>>(v, a);
 }
 
 template <class S, class M>

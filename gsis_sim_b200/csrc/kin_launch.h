@@ -9,21 +9,29 @@
 namespace kin {
 
 constexpr int kTileIters = 4;      // velocities per thread in the gradient / residual tiles
-constexpr int kSweepThreads = 128; // 4 independent sweep chains (warps) per CTA
+constexpr int kSweepThreads = 256;  // one CTA per (direction, block, velocity tile): 8 warps share every level
+constexpr int kSweepTile = 32;      // velocities of one sweep CTA (one per lane)
+
+// compact LU-SGS stencil entry: neighbour cell (>= 0), -1 boundary face, -2 periodic face (no coupling)
+template <class M>
+struct SweepE {
+  int32_t other;
+  M s[3];
+};
 
 // arguments of one LU-SGS block pass over a velocity chunk
-template <class S>
+template <class S, class M>
 struct SweepArgs {
-  const int4* items;  // per warp: (chain, t0, t1, 0), chunk-local velocity range [t0, t1)
+  const int4* items;  // per CTA: (chain, t0, t1, 0), chunk-local velocity range [t0, t1)
   int32_t n_items;
   int32_t n_blocks;
   const int32_t* block_offsets;
-  const int32_t* chain_cells;  // per chain: the block's cells ordered by level
-  const int32_t* chain_start;  // chain -> first index in chain_cells
+  const int4* prog;            // per chain, in level order: (cell, first CSR entry, entries, in-block-lower bitmask)
+  const int32_t* chain_start;  // chain -> first index in prog
   const int32_t* lev_bounds;   // level boundaries relative to chain_start (n_levels + 1 per chain)
   const int32_t* lev_start;    // chain -> first index in lev_bounds
   const int32_t* lev_count;    // chain -> number of levels
-  const int32_t* pos;          // [group][cell] position in the group's sweep order
+  const SweepE<M>* se;         // compact stencil entries, CSR order
   const S* R;                  // steady residual of the chunk
   const S* dprev;              // Delta f of the previous pass (nullptr in the first pass)
   S* out;                      // Delta f* then Delta f
@@ -48,7 +56,7 @@ struct Launch {
   static void gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st);
   static void residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
                        double* residual_cell, cudaStream_t st);
-  static void sweep_pass(const View<S, M>& v, const SweepArgs<S>& a, cudaStream_t st);
+  static void sweep_pass(const View<S, M>& v, const SweepArgs<S, M>& a, cudaStream_t st);
   static void gsis_correction(const View<S, M>& v, const double* wh, const double* wn, int* flags, double* shift,
                               int mode, int discrete, int collisionless, cudaStream_t st);
   static void discrete_maxwell_states(const View<S, M>& v, const DeqGrid& deq, const double* states, double* out,

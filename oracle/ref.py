@@ -17,22 +17,24 @@ from gsis_sim_b200.backend import KineticBackendABI, KineticError
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libgsisref.so")
-_lib = None
+# the reference KineticSolver linked with the B200 KineticBackend shim (gsis_sim_b200/integration/b200_backend.cpp)
+DROPIN_PATH = os.path.join(HERE, "_ref", "libgsisdropin.so")
+_libs = {}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 _lp = C.POINTER(C.c_int64)
 
 
-def available() -> bool:
-    return os.path.exists(LIB_PATH)
+def available(dropin: bool = False) -> bool:
+    return os.path.exists(DROPIN_PATH if dropin else LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is not None:
-        return _lib
-    L = C.CDLL(LIB_PATH)
+def lib(dropin: bool = False):
+    path = DROPIN_PATH if dropin else LIB_PATH
+    if path in _libs:
+        return _libs[path]
+    L = C.CDLL(path)
     L.ref_error.restype = C.c_char_p
     L.ref_mesh_box.argtypes = [C.c_char_p]
     L.ref_mesh_box.restype = C.c_void_p
@@ -62,13 +64,13 @@ def lib():
     L.ref_solver_gsis_correction.argtypes = [C.c_void_p, _dp, _dp, _lp]
     L.ref_solver_section_mass_flow.argtypes = [C.c_void_p, C.c_int32, _dp, C.c_int32, _dp]
     abi.declare_backend_api(L, "ref_kin_")
-    _lib = L
+    _libs[path] = L
     return L
 
 
-def _check(rc):
+def _check(rc, L=None):
     if rc != 0:
-        raise KineticError(lib().ref_error().decode())
+        raise KineticError((L or lib()).ref_error().decode())
 
 
 def _p(a, t=C.c_double):
@@ -127,8 +129,8 @@ class RefMesh:
         return out
 
     def __del__(self):
-        if getattr(self, "h", None) and _lib is not None:
-            _lib.ref_mesh_free(self.h)
+        if getattr(self, "h", None) and LIB_PATH in _libs:
+            _libs[LIB_PATH].ref_mesh_free(self.h)
             self.h = None
 
 
@@ -173,17 +175,33 @@ def case_spec(bcs, Kn=None, delta_rp=None, nv=(10, 10, 10), vmax=5.0, vlo=None, 
 class RefCase:
     """The reference KineticSolver (backend = "cpu") on one mesh + config, and a separate CpuBackend."""
 
-    def __init__(self, mesh: RefMesh, spec: str):
+    def __init__(self, mesh: RefMesh, spec: str, dropin: bool = False):
         self.mesh = mesh
-        self.h = lib().ref_case_create(mesh.h, spec.encode())
+        self.L = lib(dropin)
+        if dropin:
+            # the drop-in library has its own copy of the mesh types: rebuild the mesh there from arrays
+            self._mesh_arrays = mesh.export()
+            m = self._mesh_arrays
+            pts = np.ascontiguousarray(m["points"], dtype=np.float64)
+            names = "".join(n + "\n" for n in m["patch_names"]).encode()
+            self._dmesh = self.L.ref_mesh_arrays(len(pts), _p(pts), len(m["owner"]), _p(m["face_offsets"], C.c_int64),
+                                                 _p(m["face_nodes"], C.c_int32), _p(m["owner"], C.c_int32),
+                                                 len(m["neighbour"]), _p(m["neighbour"], C.c_int32), int(m["n_cells"]),
+                                                 len(m["patch_start"]), names, _p(m["patch_start"], C.c_int32),
+                                                 _p(m["patch_count"], C.c_int32))
+            if not self._dmesh:
+                raise KineticError(self.L.ref_error().decode())
+            self.h = self.L.ref_case_create(self._dmesh, spec.encode())
+        else:
+            self.h = self.L.ref_case_create(mesh.h, spec.encode())
         if not self.h:
-            raise KineticError(lib().ref_error().decode())
+            raise KineticError(self.L.ref_error().decode())
         d = abi.KinSetupDesc()
-        _check(lib().ref_case_desc(self.h, C.byref(d)))
+        self._chk(self.L.ref_case_desc(self.h, C.byref(d)))
         self.setup = abi.SetupArrays.from_desc(d)
         iout = np.zeros(8, np.int64)
         dout = np.zeros(8)
-        _check(lib().ref_case_info(self.h, _p(iout, C.c_int64), _p(dout)))
+        self._chk(self.L.ref_case_info(self.h, _p(iout, C.c_int64), _p(dout)))
         self.n_csr, closed, self.n_patches, self.n_internal_faces = (int(x) for x in iout[:4])
         self.inner_sweeps, self.inner_wall_update, self.boundary_iterations, self.orbit_size = \
             int(iout[4]), bool(iout[5]), int(iout[6]), int(iout[7])
@@ -196,7 +214,7 @@ class RefCase:
         self.storage_to_grid = np.zeros(nv, np.int32)
         self.patch_int = np.zeros((self.n_patches, 4), np.int32)
         self.patch_dbl = np.zeros((self.n_patches, 7))
-        _check(lib().ref_case_maps(self.h, _p(self.cell_new_to_old, C.c_int32), _p(self.bface_new_to_old, C.c_int32),
+        self._chk(self.L.ref_case_maps(self.h, _p(self.cell_new_to_old, C.c_int32), _p(self.bface_new_to_old, C.c_int32),
                                    _p(self.storage_to_grid, C.c_int32), _p(self.patch_int, C.c_int32),
                                    _p(self.patch_dbl)))
         n_faces = self.n_internal_faces + nb
@@ -205,76 +223,85 @@ class RefCase:
                          owner=np.zeros(n_faces, np.int32), lsq=np.zeros((self.n_csr, 3)),
                          csr_faces=np.zeros(self.n_csr, np.int32))
         g = self.geom
-        _check(lib().ref_case_geometry(self.h, _p(g["cell_center"]), _p(g["face_center"]), _p(g["face_normal"]),
+        self._chk(self.L.ref_case_geometry(self.h, _p(g["cell_center"]), _p(g["face_center"]), _p(g["face_normal"]),
                                        _p(g["face_area"]), _p(g["owner"], C.c_int32), _p(g["lsq"]),
                                        _p(g["csr_faces"], C.c_int32)))
         self.backend = RefBackend(self)
 
+    def _chk(self, rc):
+        if rc != 0:
+            raise KineticError(self.L.ref_error().decode())
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise KineticError(self.L.ref_error().decode())
+
     def __del__(self):
-        if getattr(self, "h", None) and _lib is not None:
-            _lib.ref_case_free(self.h)
+        if getattr(self, "h", None):
+            self.L.ref_case_free(self.h)
             self.h = None
 
     # --- reference KineticSolver ------------------------------------------------------------------------------
     def init_uniform(self, rho, u, T):
-        _check(lib().ref_solver_init_uniform(self.h, rho, u[0], u[1], u[2], T))
+        self._chk(self.L.ref_solver_init_uniform(self.h, rho, u[0], u[1], u[2], T))
 
     def init_states(self, states_orig):
         s = np.ascontiguousarray(states_orig, dtype=np.float64)
-        _check(lib().ref_solver_init_states(self.h, _p(s)))
+        self._chk(self.L.ref_solver_init_states(self.h, _p(s)))
 
     def prepare(self):
         info = np.zeros(12)
-        _check(lib().ref_solver_prepare(self.h, _p(info)))
+        self._chk(self.L.ref_solver_prepare(self.h, _p(info)))
         return info
 
     def sweep(self, update_pressure=True):
         info = np.zeros(12)
-        _check(lib().ref_solver_sweep(self.h, int(update_pressure), _p(info)))
+        self._chk(self.L.ref_solver_sweep(self.h, int(update_pressure), _p(info)))
         return info
 
     def patch_mass_flow(self):
         out = np.zeros(self.n_patches)
-        _check(lib().ref_solver_patch_mass_flow(self.h, _p(out)))
+        self._chk(self.L.ref_solver_patch_mass_flow(self.h, _p(out)))
         return out
 
     def moments(self):
         out = np.zeros((self.setup.n_cells, 15))
-        _check(lib().ref_solver_moments(self.h, _p(out)))
+        self._chk(self.L.ref_solver_moments(self.h, _p(out)))
         return out
 
     def boundary_fluxes(self):
         nb = self.setup.n_bfaces
         fp, fm, fs = np.zeros((nb, 5)), np.zeros((nb, 5)), np.zeros((nb, 5))
-        _check(lib().ref_solver_boundary_fluxes(self.h, _p(fp), _p(fm), _p(fs)))
+        self._chk(self.L.ref_solver_boundary_fluxes(self.h, _p(fp), _p(fm), _p(fs)))
         return fp, fm, fs
 
     def distribution(self):
         out = np.zeros((self.setup.n_cells, self.setup.nv))
-        _check(lib().ref_solver_distribution(self.h, _p(out)))
+        self._chk(self.L.ref_solver_distribution(self.h, _p(out)))
         return out
 
     def set_distribution(self, f):
         a = np.ascontiguousarray(f, dtype=np.float64).ravel()
-        _check(lib().ref_solver_set_distribution(self.h, _p(a), a.size))
+        self._chk(self.L.ref_solver_set_distribution(self.h, _p(a), a.size))
 
     def gsis_correction(self, w_half_orig, w_new_orig):
         a = np.ascontiguousarray(w_half_orig, dtype=np.float64)
         b = np.ascontiguousarray(w_new_orig, dtype=np.float64)
         r = C.c_int64()
-        _check(lib().ref_solver_gsis_correction(self.h, _p(a), _p(b), C.byref(r)))
+        self._chk(self.L.ref_solver_gsis_correction(self.h, _p(a), _p(b), C.byref(r)))
         return r.value
 
     def section_mass_flow(self, positions, axis=0):
         p = np.ascontiguousarray(positions, dtype=np.float64)
         out = np.zeros(len(p))
-        _check(lib().ref_solver_section_mass_flow(self.h, axis, _p(p), len(p), _p(out)))
+        self._chk(self.L.ref_solver_section_mass_flow(self.h, axis, _p(p), len(p), _p(out)))
         return out
 
 
 class RefBackend(KineticBackendABI):
-    """The reference CpuBackend<F> of a RefCase, called operation by operation."""
+    """The backend of a RefCase (the reference CpuBackend<F>; in the drop-in build the B200 shim), called operation
+    by operation."""
 
     def __init__(self, case: RefCase):
-        super().__init__(lib(), "ref_kin_", C.c_void_p(case.h), case.setup, lambda: lib().ref_error().decode())
+        super().__init__(case.L, "ref_kin_", C.c_void_p(case.h), case.setup, lambda: case.L.ref_error().decode())
         self._case = case

@@ -300,11 +300,20 @@ void* ref_case_create(void* mp, const char* spec) {
     const LoadedMesh& lm = *static_cast<LoadedMesh*>(mp);
     auto rc = std::make_unique<RefCase>();
     rc->cfg = make_config(spec);
+#ifdef REF_HARNESS_DROPIN
+    // drop-in build: the reference KineticSolver on the B200 backend (gsis_sim_b200/integration/b200_backend.cpp)
+    rc->cfg.module_sections["kinetic"].values["backend"] = std::string("cuda");
+#else
     rc->cfg.module_sections["kinetic"].values["backend"] = std::string("cpu");
+#endif
     rc->params = parse_kinetic_params(rc->cfg);
     rc->solver = std::make_unique<KineticSolver>(rc->cfg, lm.mesh, lm.geometry, rc->params);
     const kinetic::KineticSetup& s = rc->solver->setup();
+#ifdef REF_HARNESS_DROPIN
+    rc->backend = kinetic::make_cuda_backend(s);
+#else
     rc->backend = kinetic::make_cpu_backend(s);
+#endif
     // flatten the setup
     rc->xi_x = s.velocity.xi_x;
     rc->xi_y = s.velocity.xi_y;

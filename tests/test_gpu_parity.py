@@ -45,9 +45,11 @@ def test_gpu_deterministic_and_chunk_independent(B200Backend, name):
         assert be.chunk_width() == 100
     for k in ["f1", "f3", "res1", "bsums0", "moments2", "face_flux"]:
         assert np.array_equal(a[k], b[k]), k
-    for k in ["f1", "f3", "bsums0", "moments2"]:
-        assert np.array_equal(a[k], c[k]), k
-    assert common.max_rel(a["res1"], c["res1"]) < 1e-13
+    # With mirror orbits (symmetry planes) the backend orders velocities by (chunk, sweep direction), so a
+    # different chunk width only changes the summation order of the velocity sums: agreement to rounding.
+    tol = 1e-13 if common.precision_of(setup) == "fp64" else 1e-6
+    for k in ["f1", "f3", "bsums0", "moments2", "res1"]:
+        assert common.max_rel(a[k], c[k]) < tol, k
 
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "maxwell_wall_fp64", "couette_fp64"])
