@@ -116,7 +116,8 @@ def build_case(args):
     from gsis_sim_b200 import tube
 
     t0 = time.time()
-    setup, host = tube.tube_case(delta=10.0, nv=args.nv, precision=args.precision)
+    mesh_kw = None if args.nx == 100 else {"n_x": args.nx}
+    setup, host = tube.tube_case(delta=10.0, nv=args.nv, precision=args.precision, mesh_kw=mesh_kw)
     return setup, host, time.time() - t0
 
 
@@ -186,10 +187,10 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def workload_config(args, cb_nv=None):
-    return {"workload": f"kinetic CIS iteration, O-grid tube + reservoir 134528 cells, uniform {args.nv}^3 velocities "
-                        f"on [-5,5]^3, delta 10, {args.precision}",
-            "cells": 134528, "velocities": (cb_nv or args.nv) ** 3, "inner_sweeps": 4, "block_passes": 2,
+def workload_config(args, cb_nv=None, n_cells=134528):
+    return {"workload": f"kinetic CIS iteration, O-grid tube + reservoir {n_cells} cells, uniform {args.nv}^3 "
+                        f"velocities on [-5,5]^3, delta 10, {args.precision}",
+            "cells": n_cells, "velocities": (cb_nv or args.nv) ** 3, "inner_sweeps": 4, "block_passes": 2,
             "sweep_order": "octant", "equilibrium": "discrete",
             "l2": "no flush: f and the work arrays (tens of GB) exceed the 126 MB L2"}
 
@@ -205,6 +206,9 @@ def main():
     ap.add_argument("--cpu-nv", type=int, default=8)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # smaller variants of the tube case for profiler captures (the benchmark itself uses the defaults)
+    ap.add_argument("--nx", type=int, default=100, help="axial cells of the tube (100: 134,528 cells)")
+    ap.add_argument("--velocity-chunk", type=int, default=None, help="velocities per chunk (default: all that fit)")
     args = ap.parse_args()
 
     rank, ws, local = dist_init() if args.gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1 else (0, 1, 0)
@@ -222,7 +226,7 @@ def main():
     setup, host, t_setup = build_case(args)
     nc, nv = setup.n_cells, setup.nv
     inner = host.inner_sweeps
-    be = B200Backend(setup, device=local)
+    be = B200Backend(setup, device=local, velocity_chunk=args.velocity_chunk)
     sol = KineticSolver(setup, host, be)
     sol.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
     for _ in range(args.warmup):
@@ -287,7 +291,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32 storage / f64 arithmetic"}[args.precision],
-        "data": "synthetic", "config": workload_config(args),
+        "data": "synthetic", "config": workload_config(args, n_cells=nc),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": 1e3 * t_launch},
