@@ -13,6 +13,8 @@ import numpy as np
 
 KIN_ABI_VERSION = 1
 KIN_OK = 0
+KIN_E_ARG, KIN_E_CUDA, KIN_E_MEMORY, KIN_E_STATE, KIN_E_TIMEOUT = -1, -2, -3, -4, -5
+KIN_NOALLOC_MAX_STATES = 4096
 KIN_PREC_FP32, KIN_PREC_FP64, KIN_PREC_MIXED = 0, 1, 2
 PRECISIONS = {"fp32": KIN_PREC_FP32, "fp64": KIN_PREC_FP64, "mixed": KIN_PREC_MIXED}
 
@@ -227,6 +229,7 @@ def declare_backend_api(lib, prefix: str, handle_type=C.c_void_p):
         "deq_counts": [h, C.POINTER(KinDeqCounts)],
         "chunk_width": [h, _ip],
         "discrete_maxwell": [h, _dp, C.c_int64, C.c_double, _dp, _ip],
+        "discrete_maxwell_noalloc": [h, _dp, C.c_int64, C.c_double, _dp, _ip],
     }
     for name, args in sig.items():
         if not hasattr(lib, prefix + name):

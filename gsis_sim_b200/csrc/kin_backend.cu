@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -152,7 +153,37 @@ struct KinHandle {
   virtual void velocity_permutation(int32_t* perm, int64_t n) const = 0;
   virtual void schedule_info(int32_t* max_levels, int32_t* n_chains) const = 0;
   virtual void discrete_maxwell(const double* states, int64_t n, double tol, double* out, int32_t* result) = 0;
+  virtual void discrete_maxwell_noalloc(const double* states, int64_t n, double tol, double* out,
+                                        int32_t* result) = 0;
 };
+
+// Scratch of kin_discrete_maxwell_noalloc: static device memory of this module (one copy per device), laid out as
+// [input states: 5 doubles x KIN_NOALLOC_MAX_STATES][corrected states: same][Newton results: int32 x same].
+static constexpr size_t kNoAllocStatesBytes = sizeof(double) * 5 * KIN_NOALLOC_MAX_STATES;
+static constexpr size_t kNoAllocScratchBytes = 2 * kNoAllocStatesBytes + sizeof(int32_t) * KIN_NOALLOC_MAX_STATES;
+static_assert(kNoAllocStatesBytes % 256 == 0, "each part of the scratch starts on a 256-byte boundary");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on `device`, looked up once per device (with that device current) and kept.
+unsigned char* noalloc_scratch(int device) {
+  KCHECK(device >= 0 && device < kNoAllocMaxDevices, "kin_discrete_maxwell_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_address[device] == nullptr) {
+    KCUDA(cudaSetDevice(device));
+    void* p = nullptr;
+    KCUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_address[device] = p;
+  }
+  return static_cast<unsigned char*>(g_noalloc_address[device]);
+}
+
+}  // namespace
 
 namespace {
 
@@ -841,6 +872,30 @@ struct Backend final : KinHandle {
     KCUDA(cudaStreamSynchronize(stream));
   }
 
+  // discrete_maxwell in the static scratch: no device or host allocation, no phase timer (its events may grow a
+  // pool). Nothing in the scratch has to start at zero: the kernel writes all five values and the result of each
+  // of the n states before they are copied back.
+  void discrete_maxwell_noalloc(const double* states, int64_t n, double tol, double* out, int32_t* result) override {
+    KCHECK(n >= 0, "kin_discrete_maxwell_noalloc: negative number of states");
+    KCHECK(n <= KIN_NOALLOC_MAX_STATES, "kin_discrete_maxwell_noalloc: " + std::to_string(n) +
+                                            " states exceed the static scratch of " +
+                                            std::to_string(KIN_NOALLOC_MAX_STATES) + " states; split the batch");
+    if (n == 0) return;
+    KCHECK(states != nullptr && out != nullptr && result != nullptr, "kin_discrete_maxwell_noalloc: null pointer");
+    unsigned char* base = noalloc_scratch(device);
+    double* d_states = reinterpret_cast<double*>(base);
+    double* d_out = reinterpret_cast<double*>(base + kNoAllocStatesBytes);
+    int32_t* d_res = reinterpret_cast<int32_t*>(base + 2 * kNoAllocStatesBytes);
+    KCUDA(cudaMemcpyAsync(d_states, states, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, stream));
+    kin::DeqGrid g = view.deq;
+    g.tolerance = tol;
+    L::discrete_maxwell_states(view, g, d_states, d_out, d_res, static_cast<int>(n), stream);
+    launched();
+    KCUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, stream));
+    KCUDA(cudaMemcpyAsync(result, d_res, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, stream));
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
   void take_timings(KinStepTimings* out) override {
     timer.flush(timings);
     *out = timings;
@@ -973,6 +1028,10 @@ int kin_velocity_permutation(const KinHandle* h, int32_t* perm, int64_t n) {
 int kin_discrete_maxwell(KinHandle* h, const double* states, int64_t n, double tolerance, double* out,
                          int32_t* result) {
   return guard(h, [&] { h->discrete_maxwell(states, n, tolerance, out, result); });
+}
+int kin_discrete_maxwell_noalloc(KinHandle* h, const double* states, int64_t n, double tolerance, double* out,
+                                 int32_t* result) {
+  return guard(h, [&] { h->discrete_maxwell_noalloc(states, n, tolerance, out, result); });
 }
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains) {
   return guard(const_cast<KinHandle*>(h), [&] { h->schedule_info(max_levels, n_chains); });

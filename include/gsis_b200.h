@@ -238,6 +238,25 @@ int kin_velocity_permutation(const KinHandle* h, int32_t* perm, int64_t n);
    result <= 0); result: Newton iterations (0: resolved, no correction; -1: no convergence). */
 int kin_discrete_maxwell(KinHandle* h, const double* states, int64_t n, double tolerance, double* out,
                          int32_t* result);
+
+/* Largest batch kin_discrete_maxwell_noalloc accepts, in states. */
+#define KIN_NOALLOC_MAX_STATES 4096
+/* kin_discrete_maxwell without allocating anything (no reference counterpart): same arguments, same results.
+   kin_discrete_maxwell allocates (and frees) device buffers for the states on every call. That does not suit two
+   kinds of caller: one that has given nearly all of the device memory to f and the sweep work arrays (a handle sizes
+   its velocity chunk to the memory that is free when it is created), for which even a small cudaMalloc can fail;
+   and one that keeps other streams of the device busy, which cudaFree would stall because it waits for the whole
+   device. This entry point works in a fixed scratch area in the library's static device memory (about 336 KB per
+   device: the input states, the corrected states and the Newton results of KIN_NOALLOC_MAX_STATES states), so it
+   only copies, launches one kernel and waits for the handle's stream.
+   - n > KIN_NOALLOC_MAX_STATES is refused with KIN_E_ARG and a message (split the batch); n == 0 does nothing.
+   - The first call on a device looks up the scratch address (cudaGetSymbolAddress) and keeps it; make that first
+     call before capturing any stream.
+   - There is ONE scratch per device, shared by every handle on it: calls whose copies or kernels overlap on the
+     GPU (from different host threads, or handles on different streams) race and overwrite each other's states.
+     Calls made one after another from one thread do not overlap: each returns after its stream is done. */
+int kin_discrete_maxwell_noalloc(KinHandle* h, const double* states, int64_t n, double tolerance, double* out,
+                                 int32_t* result);
 /* LU-SGS level schedule statistics: number of levels of the longest (direction, block) chain and the total
    number of (direction, block) chains. */
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains);
