@@ -3,6 +3,7 @@
 // (src/kinetic/kinetic_backend_cuda.cpp:89-502).
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -238,6 +239,11 @@ struct Backend final : KinHandle {
   DevBuf<int32_t> block_offsets, chain_start, lev_bounds, lev_start, lev_count;
   DevBuf<int4> prog;
   DevBuf<kin::SweepE<M>> sweep_entries;
+  // staged schedule of k_sweep_staged (staged_ne == 0: not usable for this mesh, k_sweep_pass runs instead)
+  int32_t staged_ne = 0;
+  DevBuf<int4> sprog;
+  DevBuf<kin::StageE<M>> sse;
+  DevBuf<int32_t> sub_cells, sub_entries, sub_start, sub_count;
   DevBuf<int32_t> d_perm, d_inv;
   DevBuf<double> moments, shift, residual_cell, bsums, partial, w_half, w_new, staging;
   DevBuf<int32_t> flags, face_cells, face_entries;
@@ -562,6 +568,7 @@ struct Backend final : KinHandle {
       hse[e].other = o >= 0 ? o : (d.bface_kind[d.csr_bface[e]] == kin::kPeriodic ? -2 : -1);
       for (int a = 0; a < 3; ++a) hse[e].s[a] = static_cast<M>(d.csr_geom[12 * e + a]);
     }
+    build_staged_schedule(hprog, hse, hstart, hlev_start, hlev_count, hbounds);
     prog.upload(hprog.data(), hprog.size(), stream);
     sweep_entries.upload(hse.data(), hse.size(), stream);
     chain_start.upload(hstart.data(), hstart.size(), stream);
@@ -569,6 +576,83 @@ struct Backend final : KinHandle {
     lev_start.upload(hlev_start.data(), hlev_start.size(), stream);
     lev_count.upload(hlev_count.data(), hlev_count.size(), stream);
     KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  // Sub-levels of the staged sweep: each level of a chain cut (in its order) into pieces of at most kStageCells
+  // cells and kStageEntries entries; the program refers to entries relative to its sub-level, and the entries are
+  // stored again in program order so that a sub-level is one contiguous range of each.
+  void build_staged_schedule(const std::vector<int4>& hprog, const std::vector<kin::SweepE<M>>& hse,
+                             const std::vector<int32_t>& hstart, const std::vector<int32_t>& hlev_start,
+                             const std::vector<int32_t>& hlev_count, const std::vector<int32_t>& hbounds) {
+    // entry kinds of the staged stencil (k_sweep_tiles): code = kind << 28 | neighbour cell
+    constexpr uint32_t kKindPeriodic = 0, kKindBoundary = 1, kKindLower = 2, kKindUpper = 3, kKindOther = 4;
+    constexpr uint32_t kKindShift = 28;
+    staged_ne = 0;
+    if (nc >= (1 << kKindShift)) return;
+    int max_ne = 0;
+    for (const int4& p : hprog) max_ne = std::max(max_ne, p.z);
+    const int ne_bound = max_ne <= 6 ? 6 : (max_ne <= 8 ? 8 : 0);
+    if (ne_bound == 0) return;
+    std::vector<int4> sp;
+    std::vector<kin::StageE<M>> se;
+    std::vector<int32_t> sc, sen, sst(n_chains), scnt(n_chains);
+    sp.reserve(hprog.size());
+    se.reserve(hprog.size() * static_cast<size_t>(max_ne));
+    for (int ch = 0; ch < n_chains; ++ch) {
+      sst[ch] = static_cast<int32_t>(sc.size());
+      int nsub = 0;
+      const int blk = ch % n_blocks;
+      const int cb = h_block_offsets[blk], ce = h_block_offsets[blk + 1];
+      for (int l = 0; l < hlev_count[ch]; ++l) {
+        const size_t pb = static_cast<size_t>(hstart[ch]) + hbounds[hlev_start[ch] + l];
+        const size_t pe = static_cast<size_t>(hstart[ch]) + hbounds[hlev_start[ch] + l + 1];
+        size_t k = pb;
+        while (k < pe) {
+          sc.push_back(static_cast<int32_t>(sp.size()));
+          sen.push_back(static_cast<int32_t>(se.size()));
+          int ncell = 0, nent = 0;
+          while (k < pe && ncell < kin::kStageCells && nent + hprog[k].z <= kin::kStageEntries) {
+            const int4 p = hprog[k];
+            sp.push_back(make_int4(p.x, nent, p.z, 0));
+            for (int j = 0; j < p.z; ++j) {
+              const kin::SweepE<M>& e = hse[static_cast<size_t>(p.y) + j];
+              uint32_t kind;
+              if (e.other == -2) kind = kKindPeriodic;
+              else if (e.other < 0) kind = kKindBoundary;
+              else if (e.other < cb || e.other >= ce) kind = kKindOther;
+              else kind = ((p.w >> j) & 1) ? kKindLower : kKindUpper;
+              kin::StageE<M> st{};
+              st.code = (kind << kKindShift) | static_cast<uint32_t>(e.other >= 0 ? e.other : 0);
+              for (int a3 = 0; a3 < 3; ++a3) st.s[a3] = e.s[a3];
+              se.push_back(st);
+            }
+            nent += p.z;
+            ++ncell;
+            ++k;
+          }
+          ++nsub;
+        }
+      }
+      sc.push_back(static_cast<int32_t>(sp.size()));
+      sen.push_back(static_cast<int32_t>(se.size()));
+      scnt[ch] = nsub;
+      if (nsub > kin::kMaxSubLevels) return;  // too many sub-levels for the kernel's table: k_sweep_pass
+    }
+    if (sp.empty() || se.empty()) return;
+    KCHECK(se.size() < static_cast<size_t>(INT32_MAX), "staged LU-SGS schedule too large");
+    sprog.upload(sp.data(), sp.size(), stream);
+    sse.upload(se.data(), se.size(), stream);
+    sub_cells.upload(sc.data(), sc.size(), stream);
+    sub_entries.upload(sen.data(), sen.size(), stream);
+    sub_start.upload(sst.data(), sst.size(), stream);
+    sub_count.upload(scnt.data(), scnt.size(), stream);
+    staged_ne = ne_bound;
+    // KIN_SWEEP_KERNEL=legacy selects k_sweep_pass, =staged8 the 8-entry instantiation of k_sweep_staged (both
+    // give the same results; the tests use this to cover every sweep kernel on the available meshes)
+    if (const char* e = std::getenv("KIN_SWEEP_KERNEL")) {
+      if (std::strcmp(e, "legacy") == 0) staged_ne = 0;
+      if (std::strcmp(e, "staged8") == 0) staged_ne = 8;
+    }
   }
 
   void build_chunks() {
@@ -583,8 +667,9 @@ struct Backend final : KinHandle {
         if (s >= e) continue;
         for (int b = 0; b < n_blocks; ++b) {
           if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
-          for (int t = s; t < e; t += kin::kSweepTile)
-            items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + kin::kSweepTile, e) - k0, 0));
+          const int tile = staged_ne != 0 ? kin::kTileVel : kin::kSweepTile;
+          for (int t = s; t < e; t += tile)
+            items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + tile, e) - k0, 0));
         }
       }
       cp->n_items = static_cast<int32_t>(items.size());
@@ -655,7 +740,8 @@ struct Backend final : KinHandle {
            bfaces.bytes() + inflow.bytes() + cells.bytes() + mirror_map.bytes() + mw_offset.bytes() + mw_frac.bytes() +
            specular.bytes() * 2 + grid_to_pos.bytes() + volume.bytes() + vdt.bytes() + block_offsets.bytes() +
            prog.bytes() + sweep_entries.bytes() + chain_start.bytes() + lev_bounds.bytes() + lev_start.bytes() +
-           lev_count.bytes() + d_perm.bytes() * 2 + moments.bytes() + shift.bytes() + residual_cell.bytes() + bsums.bytes() +
+           lev_count.bytes() + sprog.bytes() + sse.bytes() + sub_cells.bytes() + sub_entries.bytes() +
+           sub_start.bytes() + sub_count.bytes() + d_perm.bytes() * 2 + moments.bytes() + shift.bytes() + residual_cell.bytes() + bsums.bytes() +
            partial.bytes() + w_half.bytes() * 2 + staging.bytes() + flags.bytes() + f.bytes() + gx.bytes() * 4;
   }
 
@@ -815,6 +901,13 @@ struct Backend final : KinHandle {
         a.lev_start = lev_start.p;
         a.lev_count = lev_count.p;
         a.se = sweep_entries.p;
+        a.staged_ne = staged_ne;
+        a.sprog = sprog.p;
+        a.sse = sse.p;
+        a.sub_cells = sub_cells.p;
+        a.sub_entries = sub_entries.p;
+        a.sub_start = sub_start.p;
+        a.sub_count = sub_count.p;
         a.R = r.p;
         a.dprev = prev;
         a.out = out;

@@ -300,7 +300,8 @@ __global__ void __launch_bounds__(kFaceThreads)
 // read once per thread (not once per velocity) and the velocities give independent FP64 chains. The arithmetic
 // of every velocity is that of the reference routines, entry by entry in CSR order.
 // ---------------------------------------------------------------------------------------------------------
-constexpr int kStageMax = 32;
+constexpr int kCellsPerCta = 8;   // consecutive cells of one gradient / residual CTA
+constexpr int kStageMulti = 96;   // CSR entries of those cells staged in shared memory
 
 template <class M>
 struct StagedEntry {
@@ -308,14 +309,19 @@ struct StagedEntry {
   int32_t kind;  // -1 internal face, else the boundary kind
 };
 
+// Stage the CSR entries of cells [c0, c1) (contiguous in CSR order) and their per-cell offsets in shared memory.
+// Returns the number of entries; more than kStageMulti means nothing was staged (the caller reads global memory).
 template <class S, class M>
-__device__ __forceinline__ int stage_cell(const View<S, M>& v, int cell, StagedEntry<M>* sh) {
-  const int e0 = v.csr_off[cell], ne = v.csr_off[cell + 1] - e0;
-  if (ne <= kStageMax && static_cast<int>(threadIdx.x) < ne) {
-    StagedEntry<M> se;
-    se.e = v.csr[e0 + threadIdx.x];
-    se.kind = se.e.other >= 0 ? -1 : v.bf[se.e.bface].kind;
-    sh[threadIdx.x] = se;
+__device__ __forceinline__ int stage_cells(const View<S, M>& v, int c0, int c1, StagedEntry<M>* sh, int* sh_off) {
+  const int e0 = v.csr_off[c0], ne = v.csr_off[c1] - e0;
+  if (static_cast<int>(threadIdx.x) <= c1 - c0) sh_off[threadIdx.x] = v.csr_off[c0 + threadIdx.x] - e0;
+  if (ne <= kStageMulti) {
+    for (int k = threadIdx.x; k < ne; k += blockDim.x) {
+      StagedEntry<M> se;
+      se.e = v.csr[e0 + k];
+      se.kind = se.e.other >= 0 ? -1 : v.bf[se.e.bface].kind;
+      sh[k] = se;
+    }
   }
   __syncthreads();
   return ne;
@@ -404,28 +410,16 @@ __device__ inline void limited_gradient_multi(const View<S, M>& v, int cell, con
 
 template <class S, class M>
 __global__ void __launch_bounds__(kTileThreads, 2) k_gradient(View<S, M> v, Chunk<S> ch) {
-  __shared__ StagedEntry<M> E[kStageMax];
-  const int c = blockIdx.x;
+  __shared__ StagedEntry<M> E[kStageMulti];
+  __shared__ int off[kCellsPerCta + 1];
+  const int c0 = blockIdx.x * kCellsPerCta, c1 = min(v.n_cells, c0 + kCellsPerCta);
   const int tb = blockIdx.y * (kTileThreads * kTileIters);
   const int te = min(ch.kc, tb + kTileThreads * kTileIters);
-  const int ne = stage_cell(v, c, E);
-  if (ne > kStageMax) {  // general polyhedra with many faces: one velocity at a time
-    for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
-      const int q = ch.k0 + t;
-      M gx, gy, gz;
-      limited_gradient(v, c, q, v.xi_x[q], v.xi_y[q], v.xi_z[q], f_at(v, c, q), gx, gy, gz);
-      const int64_t wi = static_cast<int64_t>(c) * ch.stride + t;
-      ch.gx[wi] = static_cast<S>(gx);
-      ch.gy[wi] = static_cast<S>(gy);
-      ch.gz[wi] = static_cast<S>(gz);
-    }
-    return;
-  }
+  const bool staged = stage_cells(v, c0, c1, E, off) <= kStageMulti;
   constexpr int U = kTileIters;
   int q[U];
   bool ok[U];
-  M x[U], y[U], z[U], fi[U], gx[U], gy[U], gz[U];
-  const S* fc = v.f + static_cast<int64_t>(c) * v.nv;
+  M x[U], y[U], z[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     const int t = tb + threadIdx.x + u * kTileThreads;
@@ -434,16 +428,34 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gradient(View<S, M> v, Chun
     x[u] = v.xi_x[q[u]];
     y[u] = v.xi_y[q[u]];
     z[u] = v.xi_z[q[u]];
-    fi[u] = static_cast<M>(ldg_s(fc + q[u]));
   }
-  limited_gradient_multi<S, M, U>(v, c, E, ne, q, ok, x, y, z, fi, gx, gy, gz);
+  for (int c = c0; c < c1; ++c) {
+    const int64_t row = static_cast<int64_t>(c) * ch.stride - ch.k0;
+    if (!staged) {  // many faces: one velocity at a time from global memory
 #pragma unroll
-  for (int u = 0; u < U; ++u) {
-    if (!ok[u]) continue;
-    const int64_t wi = static_cast<int64_t>(c) * ch.stride + (q[u] - ch.k0);
-    ch.gx[wi] = static_cast<S>(gx[u]);
-    ch.gy[wi] = static_cast<S>(gy[u]);
-    ch.gz[wi] = static_cast<S>(gz[u]);
+      for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
+        M gx, gy, gz;
+        limited_gradient(v, c, q[u], x[u], y[u], z[u], f_at(v, c, q[u]), gx, gy, gz);
+        ch.gx[row + q[u]] = static_cast<S>(gx);
+        ch.gy[row + q[u]] = static_cast<S>(gy);
+        ch.gz[row + q[u]] = static_cast<S>(gz);
+      }
+      continue;
+    }
+    const S* fc = v.f + static_cast<int64_t>(c) * v.nv;
+    M fi[U], gx[U], gy[U], gz[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) fi[u] = static_cast<M>(ldg_s(fc + q[u]));
+    limited_gradient_multi<S, M, U>(v, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], q, ok, x, y, z, fi, gx,
+                                    gy, gz);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!ok[u]) continue;
+      ch.gx[row + q[u]] = static_cast<S>(gx[u]);
+      ch.gy[row + q[u]] = static_cast<S>(gy[u]);
+      ch.gz[row + q[u]] = static_cast<S>(gz[u]);
+    }
   }
 }
 
@@ -492,85 +504,111 @@ __device__ inline M residual_value(const View<S, M>& v, const Chunk<S>& ch, int 
   return R;
 }
 
+// residual of U velocities of one cell from staged entries
+template <class S, class M, int U>
+__device__ __forceinline__ void residual_multi(const View<S, M>& v, const Chunk<S>& ch, int c,
+                                               const StagedEntry<M>* E, int ne, const int (&t)[U],
+                                               const bool (&ok)[U], const M (&x)[U], const M (&y)[U],
+                                               const M (&z)[U], M (&R)[U]) {
+  M fi[U], gix[U], giy[U], giz[U];
+  const S* fc = v.f + static_cast<int64_t>(c) * v.nv + ch.k0;
+  const int64_t row = static_cast<int64_t>(c) * ch.stride;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    fi[u] = static_cast<M>(ldg_s(fc + t[u]));
+    gix[u] = static_cast<M>(ldg_s(ch.gx + row + t[u]));
+    giy[u] = static_cast<M>(ldg_s(ch.gy + row + t[u]));
+    giz[u] = static_cast<M>(ldg_s(ch.gz + row + t[u]));
+    R[u] = M(0);
+  }
+  for (int j = 0; j < ne; ++j) {
+    const CsrE<M>& ce = E[j].e;
+    const int kind = E[j].kind;
+    if (kind == kPeriodic) continue;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const M a = x[u] * ce.s[0] + y[u] * ce.s[1] + z[u] * ce.s[2];
+      M ff;
+      if (a >= M(0)) {
+        ff = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
+      } else if (ce.other >= 0) {
+        const int64_t wj = static_cast<int64_t>(ce.other) * ch.stride + t[u];
+        ff = static_cast<M>(ldg_s(v.f + static_cast<int64_t>(ce.other) * v.nv + ch.k0 + t[u])) +
+             static_cast<M>(ldg_s(ch.gx + wj)) * ce.dn[0] + static_cast<M>(ldg_s(ch.gy + wj)) * ce.dn[1] +
+             static_cast<M>(ldg_s(ch.gz + wj)) * ce.dn[2];
+      } else if (kind == kSymmetry) {
+        const int q = ch.k0 + t[u];
+        const int qm = v.mirror_map[v.bf[ce.bface].mirror * v.nv + q];
+        const M fm = f_at(v, c, qm);
+        M gx, gy, gz;
+        limited_gradient(v, c, qm, v.xi_x[qm], v.xi_y[qm], v.xi_z[qm], fm, gx, gy, gz);
+        ff = fm + gx * ce.ds[0] + gy * ce.ds[1] + gz * ce.ds[2];
+      } else if (kind == kMaxwellWall) {
+        ff = maxwell_inflow(v, ce.bface, ch.k0 + t[u], x[u], y[u], z[u]);
+      } else {
+        ff = inflow_value(v.inflow[ce.bface], x[u], y[u], z[u]);
+      }
+      R[u] += a * ff;
+    }
+  }
+  const CellParams<M> cp = v.cp[c];
+#pragma unroll
+  for (int u = 0; u < U; ++u) R[u] = R[u] - cp.coll * (shakhov_target(cp, x[u], y[u], z[u]) - fi[u]);
+  (void)ok;
+}
+
+// residual of one chunk; partial[c * partial_stride + tile * warps + warp] = sum of R^2 over the warp's velocities
+// (summed in a fixed order by k_residual_reduce: deterministic)
 template <class S, class M>
 __global__ void __launch_bounds__(kTileThreads, 2)
     k_residual(View<S, M> v, Chunk<S> ch, double* __restrict__ partial, int partial_stride) {
-  __shared__ StagedEntry<M> E[kStageMax];
-  __shared__ double sh[kTileThreads / 32];
-  const int c = blockIdx.x;
+  constexpr int kWarps = kTileThreads / 32;
+  __shared__ StagedEntry<M> E[kStageMulti];
+  __shared__ int off[kCellsPerCta + 1];
+  const int c0 = blockIdx.x * kCellsPerCta, c1 = min(v.n_cells, c0 + kCellsPerCta);
   const int tb = blockIdx.y * (kTileThreads * kTileIters);
   const int te = min(ch.kc, tb + kTileThreads * kTileIters);
-  const int ne = stage_cell(v, c, E);
-  double r2[1] = {0.0};
-  if (ne > kStageMax) {
-    for (int t = tb + threadIdx.x; t < te; t += kTileThreads) {
-      const M R = residual_value(v, ch, c, t);
-      ch.r[static_cast<int64_t>(c) * ch.stride + t] = static_cast<S>(R);
-      r2[0] += static_cast<double>(R) * static_cast<double>(R);
-    }
-  } else {
-    constexpr int U = kTileIters;
-    int t[U];
-    bool ok[U];
-    M x[U], y[U], z[U], fi[U], gix[U], giy[U], giz[U], R[U];
-    const S* fc = v.f + static_cast<int64_t>(c) * v.nv;
-    const int64_t row = static_cast<int64_t>(c) * ch.stride;
+  const bool staged = stage_cells(v, c0, c1, E, off) <= kStageMulti;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int U = kTileIters;
+  int t[U];
+  bool ok[U];
+  M x[U], y[U], z[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      t[u] = tb + threadIdx.x + u * kTileThreads;
-      ok[u] = t[u] < te;
-      if (!ok[u]) t[u] = tb;
-      const int q = ch.k0 + t[u];
-      x[u] = v.xi_x[q];
-      y[u] = v.xi_y[q];
-      z[u] = v.xi_z[q];
-      fi[u] = static_cast<M>(ldg_s(fc + q));
-      gix[u] = static_cast<M>(ldg_s(ch.gx + row + t[u]));
-      giy[u] = static_cast<M>(ldg_s(ch.gy + row + t[u]));
-      giz[u] = static_cast<M>(ldg_s(ch.gz + row + t[u]));
-      R[u] = M(0);
-    }
-    for (int j = 0; j < ne; ++j) {
-      const CsrE<M>& ce = E[j].e;
-      const int kind = E[j].kind;
-      if (kind == kPeriodic) continue;
+  for (int u = 0; u < U; ++u) {
+    t[u] = tb + threadIdx.x + u * kTileThreads;
+    ok[u] = t[u] < te;
+    if (!ok[u]) t[u] = tb;
+    const int q = ch.k0 + t[u];
+    x[u] = v.xi_x[q];
+    y[u] = v.xi_y[q];
+    z[u] = v.xi_z[q];
+  }
+  for (int c = c0; c < c1; ++c) {
+    const int64_t row = static_cast<int64_t>(c) * ch.stride;
+    double r2 = 0.0;
+    if (!staged) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const M a = x[u] * ce.s[0] + y[u] * ce.s[1] + z[u] * ce.s[2];
-        M ff;
-        if (a >= M(0)) {
-          ff = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
-        } else if (ce.other >= 0) {
-          const int64_t wj = static_cast<int64_t>(ce.other) * ch.stride + t[u];
-          ff = static_cast<M>(ldg_s(v.f + static_cast<int64_t>(ce.other) * v.nv + ch.k0 + t[u])) +
-               static_cast<M>(ldg_s(ch.gx + wj)) * ce.dn[0] + static_cast<M>(ldg_s(ch.gy + wj)) * ce.dn[1] +
-               static_cast<M>(ldg_s(ch.gz + wj)) * ce.dn[2];
-        } else if (kind == kSymmetry) {
-          const int q = ch.k0 + t[u];
-          const int qm = v.mirror_map[v.bf[ce.bface].mirror * v.nv + q];
-          const M fm = f_at(v, c, qm);
-          M gx, gy, gz;
-          limited_gradient(v, c, qm, v.xi_x[qm], v.xi_y[qm], v.xi_z[qm], fm, gx, gy, gz);
-          ff = fm + gx * ce.ds[0] + gy * ce.ds[1] + gz * ce.ds[2];
-        } else if (kind == kMaxwellWall) {
-          ff = maxwell_inflow(v, ce.bface, ch.k0 + t[u], x[u], y[u], z[u]);
-        } else {
-          ff = inflow_value(v.inflow[ce.bface], x[u], y[u], z[u]);
-        }
-        R[u] += a * ff;
+        if (!ok[u]) continue;
+        const M R = residual_value(v, ch, c, t[u]);
+        ch.r[row + t[u]] = static_cast<S>(R);
+        r2 += static_cast<double>(R) * static_cast<double>(R);
+      }
+    } else {
+      M R[U];
+      residual_multi<S, M, U>(v, ch, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], t, ok, x, y, z, R);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
+        ch.r[row + t[u]] = static_cast<S>(R[u]);
+        r2 += static_cast<double>(R[u]) * static_cast<double>(R[u]);
       }
     }
-    const CellParams<M> cp = v.cp[c];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (!ok[u]) continue;
-      const M Ru = R[u] - cp.coll * (shakhov_target(cp, x[u], y[u], z[u]) - fi[u]);
-      ch.r[row + t[u]] = static_cast<S>(Ru);
-      r2[0] += static_cast<double>(Ru) * static_cast<double>(Ru);
-    }
+    for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+    if (lane == 0) partial[static_cast<int64_t>(c) * partial_stride + blockIdx.y * kWarps + warp] = r2;
   }
-  block_sum<1, kTileThreads>(r2, sh);
-  if (threadIdx.x == 0) partial[static_cast<int64_t>(c) * partial_stride + blockIdx.y] = r2[0];
 }
 
 __global__ void k_residual_reduce(const double* __restrict__ partial, int partial_stride, int n_tiles,
@@ -701,6 +739,215 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep_pass(View<S, M> v, S
         if (two) sweep_backward_store(v, a, pb.x, t, q, db);
       }
     }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// staged LU-SGS block pass (k_sweep_tiles): the recurrence of k_sweep_pass, organised for instruction economy.
+//  * One CTA of kTileWarps warps per (direction group, block, tile of kTileVel velocities); a thread carries
+//    kTileU velocities (lane, lane + 32, ...) through every stencil entry, so the per-entry work that does not
+//    depend on the velocity (entry fetch, kind decode, addressing) is shared by kTileU velocities.
+//  * The chain's levels are split on the host into sub-levels of at most kStageCells cells and kStageEntries
+//    entries, stored contiguously with each entry's kind for this chain precomputed (periodic, boundary,
+//    in-block lower, in-block upper, other block); the next sub-level is copied into shared memory with
+//    cp.async while the current one computes (double buffer, one barrier per step).
+//  * For each cell a warp first issues every load it needs (upwind Delta f, the previous pass at out-of-block
+//    neighbours, R or Delta f*, f), then accumulates entry by entry in CSR order with the reference's arithmetic
+//    (sweep_forward_cell / sweep_backward_cell, kinetic_kernels.hpp:289-358). The sign test of a = xi . S picks
+//    between the two branches of the reference with selects: ap += (a > 0 ? a : 0) adds an exact zero where the
+//    reference adds nothing, and the coupling terms use (a > 0 ? 0 : a), so every sum equals the reference's.
+// ---------------------------------------------------------------------------------------------------------
+enum : uint32_t { kKindPeriodic = 0, kKindBoundary = 1, kKindLower = 2, kKindUpper = 3, kKindOther = 4 };
+constexpr uint32_t kKindShift = 28, kIndexMask = (1u << kKindShift) - 1;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <class M>
+struct StageBuf {
+  int4 prog[kStageCells];
+  StageE<M> se[kStageEntries];
+};
+static_assert(sizeof(StageE<float>) == 16 && sizeof(StageE<double>) == 32, "stage entries are whole 16-byte words");
+
+// copy sub-level `l` (chain-relative) of the staged schedule into `dst` (every thread issues its share)
+template <class S, class M>
+__device__ __forceinline__ void stage_sublevel(const SweepArgs<S, M>& a, const int32_t* sh_sc, const int32_t* sh_se,
+                                               int l, StageBuf<M>* dst) {
+  constexpr int kWords = static_cast<int>(sizeof(StageE<M>) / 16);
+  const int p0 = sh_sc[l], np = sh_sc[l + 1] - p0;
+  const int e0 = sh_se[l], ne = sh_se[l + 1] - e0;
+  const int n16 = np + ne * kWords;
+  const char* src_e = reinterpret_cast<const char*>(a.sse + e0);
+  char* dst_e = reinterpret_cast<char*>(dst->se);
+  for (int k = threadIdx.x; k < n16; k += kTileThreadsSweep) {
+    if (k < np) {
+      cp_async16(&dst->prog[k], a.sprog + p0 + k);
+    } else {
+      const int w = k - np;
+      cp_async16(dst_e + 16 * w, src_e + 16 * static_cast<int64_t>(w));
+    }
+  }
+  cp_async_commit();
+}
+
+template <class M>
+__device__ __forceinline__ M pos_part(M af) { return af > M(0) ? af : M(0); }
+template <class M>
+__device__ __forceinline__ M neg_part(M af) { return af > M(0) ? M(0) : af; }
+
+// forward value of kTileU velocities of one cell; First: first block pass (no previous Delta f)
+template <class S, class M, int NE, bool First>
+__device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
+                                                  const StageE<M>* E, int4 p, const int (&t)[kTileU],
+                                                  const bool (&ok)[kTileU], const M (&x)[kTileU],
+                                                  const M (&y)[kTileU], const M (&z)[kTileU]) {
+  M val[NE][kTileU];
+#pragma unroll
+  for (int j = 0; j < NE; ++j) {
+    const uint32_t code = j < p.z ? E[p.y + j].code : 0u;
+    const uint32_t kind = code >> kKindShift;
+    const int64_t row = static_cast<int64_t>(code & kIndexMask) * a.stride;
+    const bool load = kind == kKindLower || (!First && kind == kKindOther);
+    const S* src = kind == kKindLower ? a.out : a.dprev;
+#pragma unroll
+    for (int u = 0; u < kTileU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(src[row + t[u]]) : M(0);
+  }
+  const int64_t crow = static_cast<int64_t>(p.x) * a.stride;
+  M own[kTileU];
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) own[u] = ok[u] ? static_cast<M>(__ldcs(a.R + crow + t[u])) : M(0);
+  const M diag = v.cp[p.x].diag;
+  M ap[kTileU], lo[kTileU], ext[kTileU];  // ext: am_out (first pass) or Lout (later passes)
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) ap[u] = lo[u] = ext[u] = M(0);
+#pragma unroll
+  for (int j = 0; j < NE; ++j) {
+    if (j >= p.z) break;
+    const StageE<M>& e = E[p.y + j];
+    const uint32_t kind = e.code >> kKindShift;
+    if (kind == kKindPeriodic) continue;
+    const M s0 = e.s[0], s1 = e.s[1], s2 = e.s[2];
+#pragma unroll
+    for (int u = 0; u < kTileU; ++u) {
+      const M af = x[u] * s0 + y[u] * s1 + z[u] * s2;
+      ap[u] += pos_part(af);
+      if (kind == kKindLower) lo[u] += neg_part(af) * val[j][u];
+      else if (kind == kKindOther) {
+        if (First) ext[u] -= neg_part(af);
+        else ext[u] += neg_part(af) * val[j][u];
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) {
+    if (!ok[u]) continue;
+    const M am_out = First ? ext[u] : M(0), Lout = First ? M(0) : ext[u];
+    const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out;
+    a.out[crow + t[u]] = static_cast<S>((-own[u] - Lout - lo[u]) / D);
+  }
+}
+
+// backward value of kTileU velocities of one cell (and f += Delta f in the last pass)
+template <class S, class M, int NE, bool First>
+__device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
+                                                   const StageE<M>* E, int4 p, const int (&t)[kTileU],
+                                                   const bool (&ok)[kTileU], const M (&x)[kTileU],
+                                                   const M (&y)[kTileU], const M (&z)[kTileU]) {
+  M val[NE][kTileU];
+#pragma unroll
+  for (int j = 0; j < NE; ++j) {
+    const uint32_t code = j < p.z ? E[p.y + j].code : 0u;
+    const bool load = (code >> kKindShift) == kKindUpper;
+    const int64_t row = static_cast<int64_t>(code & kIndexMask) * a.stride;
+#pragma unroll
+    for (int u = 0; u < kTileU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(a.out[row + t[u]]) : M(0);
+  }
+  const int64_t crow = static_cast<int64_t>(p.x) * a.stride;
+  const int64_t frow = static_cast<int64_t>(p.x) * v.nv + a.k0;
+  M own[kTileU], fv[kTileU];
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) {
+    own[u] = ok[u] ? static_cast<M>(a.out[crow + t[u]]) : M(0);
+    fv[u] = (ok[u] && a.update_f) ? static_cast<M>(__ldcs(v.f + frow + t[u])) : M(0);
+  }
+  const M diag = v.cp[p.x].diag;
+  M ap[kTileU], up[kTileU], am_out[kTileU];
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) ap[u] = up[u] = am_out[u] = M(0);
+#pragma unroll
+  for (int j = 0; j < NE; ++j) {
+    if (j >= p.z) break;
+    const StageE<M>& e = E[p.y + j];
+    const uint32_t kind = e.code >> kKindShift;
+    if (kind == kKindPeriodic) continue;
+    const M s0 = e.s[0], s1 = e.s[1], s2 = e.s[2];
+#pragma unroll
+    for (int u = 0; u < kTileU; ++u) {
+      const M af = x[u] * s0 + y[u] * s1 + z[u] * s2;
+      ap[u] += pos_part(af);
+      if (kind == kKindUpper) up[u] += neg_part(af) * val[j][u];
+      else if (First && kind == kKindOther) am_out[u] -= neg_part(af);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) {
+    if (!ok[u]) continue;
+    const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out[u];
+    const M df = own[u] - up[u] / D;
+    a.out[crow + t[u]] = static_cast<S>(df);
+    if (a.update_f) __stcs(v.f + frow + t[u], static_cast<S>(fv[u] + df));
+  }
+}
+
+template <class S, class M, int NE, bool First>
+__global__ void __launch_bounds__(kTileThreadsSweep, kTileMinBlocks) k_sweep_tiles(View<S, M> v, SweepArgs<S, M> a) {
+  constexpr int W = kTileThreadsSweep / 32;
+  __shared__ __align__(16) StageBuf<M> sh_buf[2];
+  __shared__ int32_t sh_sc[kMaxSubLevels + 1], sh_se[kMaxSubLevels + 1];
+  const int4 it = a.items[blockIdx.x];  // (chain, t0, t1, -)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int chain = it.x;
+  const int nsub = a.sub_count[chain];
+  if (nsub <= 0) return;
+  const int s0 = a.sub_start[chain];
+  for (int k = threadIdx.x; k <= nsub; k += kTileThreadsSweep) {
+    sh_sc[k] = a.sub_cells[s0 + k];
+    sh_se[k] = a.sub_entries[s0 + k];
+  }
+  int t[kTileU];
+  bool ok[kTileU];
+  M x[kTileU], y[kTileU], z[kTileU];
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) {
+    t[u] = it.y + lane + 32 * u;
+    ok[u] = t[u] < it.z;
+    const int q = a.k0 + (ok[u] ? t[u] : it.y);
+    x[u] = v.xi_x[q];
+    y[u] = v.xi_y[q];
+    z[u] = v.xi_z[q];
+  }
+  __syncthreads();
+  stage_sublevel(a, sh_sc, sh_se, 0, &sh_buf[0]);
+  cp_async_wait_all();
+  __syncthreads();
+  const int nsteps = 2 * nsub;  // forward over sub-levels 0..nsub-1, then backward over nsub-1..0
+  for (int s = 0; s < nsteps; ++s) {
+    const StageBuf<M>& cur = sh_buf[s & 1];
+    if (s + 1 < nsteps) stage_sublevel(a, sh_sc, sh_se, s + 1 < nsub ? s + 1 : nsteps - 2 - s, &sh_buf[(s + 1) & 1]);
+    const int l = s < nsub ? s : nsteps - 1 - s;
+    const int ncl = sh_sc[l + 1] - sh_sc[l];
+    if (s < nsub) {
+      for (int k = warp; k < ncl; k += W) tile_forward_cell<S, M, NE, First>(v, a, cur.se, cur.prog[k], t, ok, x, y, z);
+    } else {
+      for (int k = warp; k < ncl; k += W) tile_backward_cell<S, M, NE, First>(v, a, cur.se, cur.prog[k], t, ok, x, y, z);
+    }
+    cp_async_wait_all();
     __syncthreads();
   }
 }
@@ -923,13 +1170,13 @@ void Launch<S, M>::internal_face_flux(const View<S, M>& v, const int32_t* cells,
 
 template <class S, class M>
 int Launch<S, M>::residual_tiles(int kc) {
-  return ceil_div(kc, kTileThreads * kTileIters);
+  return ceil_div(kc, kTileThreads * kTileIters) * (kTileThreads / 32);
 }
 
 template <class S, class M>
 void Launch<S, M>::gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st) {
   if (v.n_cells <= 0 || ch.kc <= 0) return;
-  const dim3 grid(v.n_cells, residual_tiles(ch.kc));
+  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * kTileIters));
   k_gradient<S, M><<<grid, kTileThreads, 0, st>>>(v, ch);
 }
 
@@ -937,16 +1184,27 @@ template <class S, class M>
 void Launch<S, M>::residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
                             double* residual_cell, cudaStream_t st) {
   if (v.n_cells <= 0 || ch.kc <= 0) return;
-  const int tiles = residual_tiles(ch.kc);
-  k_residual<S, M><<<dim3(v.n_cells, tiles), kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
-  k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride, tiles, residual_cell,
-                                                             v.n_cells);
+  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * kTileIters));
+  k_residual<S, M><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
+  k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride, residual_tiles(ch.kc),
+                                                             residual_cell, v.n_cells);
 }
 
 template <class S, class M>
 void Launch<S, M>::sweep_pass(const View<S, M>& v, const SweepArgs<S, M>& a, cudaStream_t st) {
   if (a.n_items <= 0) return;
-  k_sweep_pass<S, M><<<a.n_items, kSweepThreads, 0, st>>>(v, a);
+#define KIN_TILES(NE, FIRST) \
+  k_sweep_tiles<S, M, NE, FIRST><<<a.n_items, kTileThreadsSweep, 0, st>>>(v, a)
+  if (a.staged_ne == 6 && a.dprev == nullptr)
+    KIN_TILES(6, true);
+  else if (a.staged_ne == 6)
+    KIN_TILES(6, false);
+  else if (a.staged_ne == 8 && a.dprev == nullptr)
+    KIN_TILES(8, true);
+  else if (a.staged_ne == 8)
+    KIN_TILES(8, false);
+  else
+    k_sweep_pass<S, M><<<a.n_items, kSweepThreads, 0, st>>>(v, a);
 }
 
 template <class S, class M>

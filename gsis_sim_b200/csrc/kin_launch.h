@@ -19,6 +19,19 @@ struct SweepE {
   M s[3];
 };
 
+// staged stencil entry of one chain: code = kind << 28 | neighbour cell (kinds in kin_kernels.cu: periodic,
+// boundary, in-block lower, in-block upper, other block)
+template <class M>
+struct StageE {
+  uint32_t code;
+  M s[3];
+};
+
+constexpr int kTileU = 4;                    // velocities per thread of k_sweep_tiles
+constexpr int kTileThreadsSweep = 128;       // threads of one k_sweep_tiles CTA
+constexpr int kTileMinBlocks = 4;            // resident CTAs per SM the register budget is sized for
+constexpr int kTileVel = 32 * kTileU;        // velocities of one k_sweep_tiles CTA
+
 // arguments of one LU-SGS block pass over a velocity chunk
 template <class S, class M>
 struct SweepArgs {
@@ -38,7 +51,20 @@ struct SweepArgs {
   int32_t update_f;
   int32_t k0;
   int32_t stride;
+  // staged schedule (k_sweep_tiles): every level split into sub-levels of at most kStageCells cells and
+  // kStageEntries stencil entries, stored contiguously per chain so one sub-level is one copy into shared memory
+  int32_t staged_ne;            // 0: use k_sweep_pass; else the entry bound of k_sweep_tiles (6 or 8)
+  const int4* sprog;            // (cell, entry offset within the sub-level, entries, -)
+  const StageE<M>* sse;         // stencil entries with their kind, in sub-level order (one copy per chain)
+  const int32_t* sub_cells;     // absolute sub-level boundaries in sprog (n_sub + 1 per chain)
+  const int32_t* sub_entries;   // absolute sub-level boundaries in sse (n_sub + 1 per chain)
+  const int32_t* sub_start;     // chain -> first index in sub_cells / sub_entries
+  const int32_t* sub_count;     // chain -> number of sub-levels
 };
+
+constexpr int kStageCells = 64;     // cells of one staged sub-level
+constexpr int kStageEntries = 384;  // stencil entries of one staged sub-level
+constexpr int kMaxSubLevels = 512;  // sub-levels of one chain the staged kernel accepts
 
 template <class S, class M>
 struct Launch {

@@ -132,6 +132,8 @@ __host__ __device__ inline M venkat_face(M d2, M dmax, M dmin, M eps2) {
   const M num = (d1 * d1 + eps2) + M(2) * d1 * d2;
   const M den = d1 * d1 + M(2) * d2 * d2 + d1 * d2 + eps2;
   if (!(den > M(0))) return M(0);
+  // num >= den > 0: the quotient rounds to >= 1 and the clamp gives exactly 1, so the division can be skipped
+  if (num >= den) return M(1);
   return kclamp(num / den, M(0), M(1));
 }
 

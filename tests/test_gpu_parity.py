@@ -66,3 +66,18 @@ def test_gpu_mixed_precision_matches_oracle(B200Backend, name):
     # and it stays within the FP32 tolerance of the FP64 reference
     for k in ["f1", "f3"]:
         assert common.max_rel(g[k], z["op." + k]) < 2e-5, k
+
+
+@pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64", "tet_positivity_fp32", "dir13_fp32", "vacuum_tube_fp64"])
+def test_gpu_sweep_kernels_agree(B200Backend, name, monkeypatch):
+    """The staged LU-SGS kernel (6- and 8-entry instantiations) and the plain level kernel give the same sweep."""
+    z, setup = common.load(name)
+    runs = {}
+    for kernel in ["auto", "legacy", "staged8"]:
+        monkeypatch.setenv("KIN_SWEEP_KERNEL", kernel)
+        with B200Backend(setup) as be:
+            runs[kernel] = common.run_op_sequence(be, z)
+    tol = 1e-14 if common.precision_of(setup) == "fp64" else 1e-6
+    for kernel in ["legacy", "staged8"]:
+        for k in ["f1", "f3", "res1"]:
+            assert common.max_rel(runs["auto"][k], runs[kernel][k]) < tol, (kernel, k)
