@@ -290,7 +290,7 @@ def main():
         "metric": "cell_velocity_updates_per_s", "value": value, "unit": "cell*velocity updates/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32 storage / f64 arithmetic"}[args.precision],
+        "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32 (f, gradient, LU-SGS) / f64 (residual, sums)"}[args.precision],
         "data": "synthetic", "config": workload_config(args, n_cells=nc),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": peak_kind, "traffic": None,

@@ -10,6 +10,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "gsis_b200.h"
@@ -196,6 +197,11 @@ using kin::Inflow;
 template <class S, class M>
 struct Backend final : KinHandle {
   using L = kin::Launch<S, M>;
+  // arithmetic of the gradient and the LU-SGS passes: FP32 in the mixed mode (f in FP32, residual and every sum in
+  // FP64: the FP32 sweeps are a defect correction of the FP64 residual), M otherwise
+  using P = typename std::conditional<std::is_same<S, float>::value && std::is_same<M, double>::value, float, M>::type;
+  using LP = kin::Launch<S, P>;
+  static constexpr bool kSplit = !std::is_same<P, M>::value;
   static constexpr size_t kMargin = size_t{1} << 30;  // device memory kept free (1 GiB)
 
   // sizes and parameters
@@ -203,6 +209,7 @@ struct Backend final : KinHandle {
   int32_t block_passes = 1, discrete_eq = 0, collisionless = 0, negative_mode = 0, n_maxwell = 0;
   double mu0 = 0, omega = 0, Pr = 0, cold_bgk_T = 0;
   kin::View<S, M> view{};
+  kin::View<S, P> pview{};  // mixed mode: the FP32 view of the gradient and the LU-SGS passes
   int32_t chunk = 0, partial_stride = 1, max_levels = 0, n_chains = 0;
 
   // host copies
@@ -238,11 +245,17 @@ struct Backend final : KinHandle {
   DevBuf<double> volume, vdt;
   DevBuf<int32_t> block_offsets, chain_start, lev_bounds, lev_start, lev_count;
   DevBuf<int4> prog;
-  DevBuf<kin::SweepE<M>> sweep_entries;
+  DevBuf<kin::SweepE<P>> sweep_entries;
   // staged schedule of k_sweep_staged (staged_ne == 0: not usable for this mesh, k_sweep_pass runs instead)
   int32_t staged_ne = 0;
   DevBuf<int4> sprog;
-  DevBuf<kin::StageE<M>> sse;
+  DevBuf<kin::StageE<P>> sse;
+  // mixed mode: FP32 copies of the tables the FP32 kernels read
+  DevBuf<P> pxi_x, pxi_y, pxi_z, peps2, pspecular, pspecular_first;
+  DevBuf<CsrE<P>> pcsr;
+  DevBuf<BFace<P>> pbfaces;
+  DevBuf<Inflow<P>> pinflow;
+  DevBuf<CellParams<P>> pcells;
   DevBuf<int32_t> sub_cells, sub_entries, sub_start, sub_count;
   DevBuf<int32_t> d_perm, d_inv;
   DevBuf<double> moments, shift, residual_cell, bsums, partial, w_half, w_new, staging;
@@ -254,6 +267,11 @@ struct Backend final : KinHandle {
   bool deq_valid = false;
   PhaseTimer timer;
   KinStepTimings timings{};
+
+  const kin::View<S, P>& sweep_view() const {
+    if constexpr (kSplit) return pview;
+    else return view;
+  }
 
   const char* name() const override { return "b200"; }
   int32_t chunk_width() const override { return chunk; }
@@ -332,6 +350,12 @@ struct Backend final : KinHandle {
     KCUDA(cudaMemsetAsync(inflow.p, 0, inflow.bytes(), stream));
     cells.alloc(ncs);
     KCUDA(cudaMemsetAsync(cells.p, 0, cells.bytes(), stream));
+    if constexpr (kSplit) {
+      pinflow.alloc(static_cast<size_t>(std::max(nb, 1)));
+      KCUDA(cudaMemsetAsync(pinflow.p, 0, pinflow.bytes(), stream));
+      pcells.alloc(ncs);
+      KCUDA(cudaMemsetAsync(pcells.p, 0, pcells.bytes(), stream));
+    }
     f.alloc(ncs * static_cast<size_t>(nv));
     KCUDA(cudaMemsetAsync(f.p, 0, f.bytes(), stream));
 
@@ -400,6 +424,13 @@ struct Backend final : KinHandle {
     xi_x.upload(hx.data(), nv, stream);
     xi_y.upload(hy.data(), nv, stream);
     xi_z.upload(hz.data(), nv, stream);
+    if constexpr (kSplit) {
+      std::vector<P> px(dx.begin(), dx.end()), py(dy.begin(), dy.end()), pz(dz.begin(), dz.end());
+      pxi_x.upload(px.data(), nv, stream);
+      pxi_y.upload(py.data(), nv, stream);
+      pxi_z.upload(pz.data(), nv, stream);
+      KCUDA(cudaStreamSynchronize(stream));
+    }
     xid_x.upload(dx.data(), nv, stream);
     xid_y.upload(dy.data(), nv, stream);
     xid_z.upload(dz.data(), nv, stream);
@@ -434,6 +465,25 @@ struct Backend final : KinHandle {
     std::vector<M> he(nc);
     for (int c = 0; c < nc; ++c) he[c] = static_cast<M>(d.eps2[c]);
     eps2.upload(he.data(), nc, stream);
+    if constexpr (kSplit) {
+      std::vector<CsrE<P>> pc(hc.size());
+      for (size_t k = 0; k < hc.size(); ++k) {
+        pc[k].other = hc[k].other;
+        pc[k].bface = hc[k].bface;
+        const double* g = d.csr_geom + 12 * k;
+        for (int a = 0; a < 3; ++a) {
+          pc[k].s[a] = static_cast<P>(g[a]);
+          pc[k].ds[a] = static_cast<P>(g[3 + a]);
+          pc[k].dn[a] = static_cast<P>(g[6 + a]);
+          pc[k].c[a] = static_cast<P>(g[9 + a]);
+        }
+      }
+      pcsr.upload(pc.data(), pc.size(), stream);
+      std::vector<P> pe(nc);
+      for (int c = 0; c < nc; ++c) pe[c] = static_cast<P>(d.eps2[c]);
+      peps2.upload(pe.data(), nc, stream);
+      KCUDA(cudaStreamSynchronize(stream));
+    }
     volume.upload(d.volume, nc, stream);
     vdt.upload(d.vdt, nc, stream);
     h_block_offsets.assign(d.block_offsets, d.block_offsets + n_blocks + 1);
@@ -467,6 +517,23 @@ struct Backend final : KinHandle {
       o.area = static_cast<M>(g[3]);
     }
     bfaces.upload(hb.data(), hb.size(), stream);
+    if constexpr (kSplit) {
+      std::vector<BFace<P>> pb(hb.size());
+      for (size_t b = 0; b < hb.size(); ++b) {
+        pb[b].owner = hb[b].owner;
+        pb[b].kind = hb[b].kind;
+        pb[b].mirror = hb[b].mirror;
+        pb[b].patch = hb[b].patch;
+        const double* g = b < static_cast<size_t>(nb) ? d.bface_geom + 7 * b : nullptr;
+        for (int a = 0; a < 3; ++a) {
+          pb[b].n[a] = g ? static_cast<P>(g[a]) : P(0);
+          pb[b].d[a] = g ? static_cast<P>(g[4 + a]) : P(0);
+        }
+        pb[b].area = g ? static_cast<P>(g[3]) : P(0);
+      }
+      pbfaces.upload(pb.data(), pb.size(), stream);
+      KCUDA(cudaStreamSynchronize(stream));
+    }
     std::vector<int32_t> mm(std::max<size_t>(xors.size(), 1) * nv, 0);
     for (size_t s = 0; s < xors.size(); ++s) {
       for (int q = 0; q < nv; ++q) {
@@ -485,6 +552,12 @@ struct Backend final : KinHandle {
       specular_first.alloc(static_cast<size_t>(n_maxwell) * nv);
       KCUDA(cudaMemsetAsync(specular.p, 0, specular.bytes(), stream));
       KCUDA(cudaMemsetAsync(specular_first.p, 0, specular_first.bytes(), stream));
+      if constexpr (kSplit) {
+        pspecular.alloc(static_cast<size_t>(n_maxwell) * nv);
+        pspecular_first.alloc(static_cast<size_t>(n_maxwell) * nv);
+        KCUDA(cudaMemsetAsync(pspecular.p, 0, pspecular.bytes(), stream));
+        KCUDA(cudaMemsetAsync(pspecular_first.p, 0, pspecular_first.bytes(), stream));
+      }
       std::vector<int32_t> g2p(nv);
       for (int k = 0; k < nv; ++k) g2p[k] = inv[d.grid_to_storage[k]];
       grid_to_pos.upload(g2p.data(), nv, stream);
@@ -562,11 +635,11 @@ struct Backend final : KinHandle {
       }
     }
     const int64_t n_csr = d.csr_offsets[nc];
-    std::vector<kin::SweepE<M>> hse(static_cast<size_t>(std::max<int64_t>(n_csr, 1)));
+    std::vector<kin::SweepE<P>> hse(static_cast<size_t>(std::max<int64_t>(n_csr, 1)));
     for (int64_t e = 0; e < n_csr; ++e) {
       const int o = d.csr_other[e];
       hse[e].other = o >= 0 ? o : (d.bface_kind[d.csr_bface[e]] == kin::kPeriodic ? -2 : -1);
-      for (int a = 0; a < 3; ++a) hse[e].s[a] = static_cast<M>(d.csr_geom[12 * e + a]);
+      for (int a = 0; a < 3; ++a) hse[e].s[a] = static_cast<P>(d.csr_geom[12 * e + a]);
     }
     build_staged_schedule(hprog, hse, hstart, hlev_start, hlev_count, hbounds);
     prog.upload(hprog.data(), hprog.size(), stream);
@@ -581,7 +654,7 @@ struct Backend final : KinHandle {
   // Sub-levels of the staged sweep: each level of a chain cut (in its order) into pieces of at most kStageCells
   // cells and kStageEntries entries; the program refers to entries relative to its sub-level, and the entries are
   // stored again in program order so that a sub-level is one contiguous range of each.
-  void build_staged_schedule(const std::vector<int4>& hprog, const std::vector<kin::SweepE<M>>& hse,
+  void build_staged_schedule(const std::vector<int4>& hprog, const std::vector<kin::SweepE<P>>& hse,
                              const std::vector<int32_t>& hstart, const std::vector<int32_t>& hlev_start,
                              const std::vector<int32_t>& hlev_count, const std::vector<int32_t>& hbounds) {
     // entry kinds of the staged stencil (k_sweep_tiles): code = kind << 28 | neighbour cell
@@ -594,7 +667,7 @@ struct Backend final : KinHandle {
     const int ne_bound = max_ne <= 6 ? 6 : (max_ne <= 8 ? 8 : 0);
     if (ne_bound == 0) return;
     std::vector<int4> sp;
-    std::vector<kin::StageE<M>> se;
+    std::vector<kin::StageE<P>> se;
     std::vector<int32_t> sc, sen, sst(n_chains), scnt(n_chains);
     sp.reserve(hprog.size());
     se.reserve(hprog.size() * static_cast<size_t>(max_ne));
@@ -615,13 +688,13 @@ struct Backend final : KinHandle {
             const int4 p = hprog[k];
             sp.push_back(make_int4(p.x, nent, p.z, 0));
             for (int j = 0; j < p.z; ++j) {
-              const kin::SweepE<M>& e = hse[static_cast<size_t>(p.y) + j];
+              const kin::SweepE<P>& e = hse[static_cast<size_t>(p.y) + j];
               uint32_t kind;
               if (e.other == -2) kind = kKindPeriodic;
               else if (e.other < 0) kind = kKindBoundary;
               else if (e.other < cb || e.other >= ce) kind = kKindOther;
               else kind = ((p.w >> j) & 1) ? kKindLower : kKindUpper;
-              kin::StageE<M> st{};
+              kin::StageE<P> st{};
               st.code = (kind << kKindShift) | static_cast<uint32_t>(e.other >= 0 ? e.other : 0);
               for (int a3 = 0; a3 < 3; ++a3) st.s[a3] = e.s[a3];
               se.push_back(st);
@@ -711,6 +784,32 @@ struct Backend final : KinHandle {
     v.specular = specular.p;
     v.specular_first = specular_first.p;
     v.grid_to_pos = grid_to_pos.p;
+    if constexpr (kSplit) {
+      kin::View<S, P>& w = pview;
+      w.n_cells = nc;
+      w.nv = nv;
+      w.n_bfaces = nb;
+      w.xi_x = pxi_x.p;
+      w.xi_y = pxi_y.p;
+      w.xi_z = pxi_z.p;
+      w.xid_x = xid_x.p;
+      w.xid_y = xid_y.p;
+      w.xid_z = xid_z.p;
+      w.wts = wts.p;
+      w.csr_off = csr_off.p;
+      w.csr = pcsr.p;
+      w.eps2 = peps2.p;
+      w.bf = pbfaces.p;
+      w.inflow = pinflow.p;
+      w.cp = pcells.p;
+      w.f = f.p;
+      w.mirror_map = mirror_map.p;
+      w.mw_offset = mw_offset.p;
+      w.mw_frac = mw_frac.p;
+      w.specular = pspecular.p;
+      w.specular_first = pspecular_first.p;
+      w.grid_to_pos = grid_to_pos.p;
+    }
   }
 
   void set_params(const KinSetupDesc& d) {
@@ -728,6 +827,15 @@ struct Backend final : KinHandle {
     view.deq.criterion = d.deq_criterion;
     view.deq.tolerance = d.deq_tolerance;
     view.deq.max_iterations = d.deq_max_iterations;
+    if constexpr (kSplit) {
+      pview.weight = view.weight;
+      pview.limiter_mode = view.limiter_mode;
+      pview.positivity = view.positivity;
+      pview.diag_scale = static_cast<P>(d.diag_scale);
+      pview.interface_damping = static_cast<P>(d.interface_damping);
+      for (int a = 0; a < 3; ++a) pview.grid_n[a] = view.grid_n[a];
+      pview.deq = view.deq;
+    }
   }
 
   void launched(int n = 1) {
@@ -742,7 +850,9 @@ struct Backend final : KinHandle {
            prog.bytes() + sweep_entries.bytes() + chain_start.bytes() + lev_bounds.bytes() + lev_start.bytes() +
            lev_count.bytes() + sprog.bytes() + sse.bytes() + sub_cells.bytes() + sub_entries.bytes() +
            sub_start.bytes() + sub_count.bytes() + d_perm.bytes() * 2 + moments.bytes() + shift.bytes() + residual_cell.bytes() + bsums.bytes() +
-           partial.bytes() + w_half.bytes() * 2 + staging.bytes() + flags.bytes() + f.bytes() + gx.bytes() * 4;
+           partial.bytes() + w_half.bytes() * 2 + staging.bytes() + flags.bytes() + f.bytes() + gx.bytes() * 4 +
+           pxi_x.bytes() * 3 + peps2.bytes() + pspecular.bytes() * 2 + pcsr.bytes() + pbfaces.bytes() +
+           pinflow.bytes() + pcells.bytes();
   }
 
   // ---- KineticBackend methods ------------------------------------------------------------------------------
@@ -803,6 +913,10 @@ struct Backend final : KinHandle {
     L::cell_params(view, moments.p, volume.p, vdt.p, mu0, omega, Pr, cold_bgk_T, discrete_eq, collisionless, cells.p,
                    flags.p, stream);
     launched();
+    if constexpr (kSplit) {
+      L::cast_cell_params(cells.p, pcells.p, nc, stream);
+      launched();
+    }
     deq_valid = discrete_eq != 0;
     timer.end(stream);
     timer.flush(timings);
@@ -833,6 +947,15 @@ struct Backend final : KinHandle {
       h[b].scale = static_cast<M>(in[b].scale);
     }
     KCUDA(cudaMemcpyAsync(inflow.p, h.data(), sizeof(Inflow<M>) * nb, cudaMemcpyHostToDevice, stream));
+    if constexpr (kSplit) {
+      std::vector<Inflow<P>> hp(nb);
+      for (int b = 0; b < nb; ++b) {
+        hp[b].m = kin::maxwell_from<P>(in[b].rho, in[b].ux, in[b].uy, in[b].uz, in[b].T);
+        hp[b].scale = static_cast<P>(in[b].scale);
+      }
+      KCUDA(cudaMemcpyAsync(pinflow.p, hp.data(), sizeof(Inflow<P>) * nb, cudaMemcpyHostToDevice, stream));
+      KCUDA(cudaStreamSynchronize(stream));
+    }
     KCUDA(cudaStreamSynchronize(stream));
   }
 
@@ -843,6 +966,10 @@ struct Backend final : KinHandle {
     if (n_maxwell > 0) {
       L::maxwell_reflection(view, stream);
       launched(2);
+      if constexpr (kSplit) {
+        LP::maxwell_reflection(pview, stream);
+        launched(2);
+      }
     }
     L::boundary_sums(view, bsums.p, stream);
     launched();
@@ -878,7 +1005,7 @@ struct Backend final : KinHandle {
     for (const auto& cp : chunks) {
       kin::Chunk<S> ch{cp->k0, cp->kc, chunk, gx.p, gy.p, gz.p, r.p};
       timer.begin(PhaseTimer::kGradient, stream);
-      L::gradient(view, ch, stream);
+      LP::gradient(sweep_view(), ch, stream);
       launched();
       timer.end(stream);
       timer.begin(PhaseTimer::kResidual, stream);
@@ -890,7 +1017,7 @@ struct Backend final : KinHandle {
       S* prev = nullptr;
       for (int pass = 0; pass < block_passes; ++pass) {
         S* out = (pass % 2 == 0) ? gz.p : gy.p;
-        kin::SweepArgs<S, M> a{};
+        kin::SweepArgs<S, P> a{};
         a.items = cp->items.p;
         a.n_items = cp->n_items;
         a.n_blocks = n_blocks;
@@ -915,7 +1042,7 @@ struct Backend final : KinHandle {
         a.k0 = cp->k0;
         a.stride = chunk;
         timer.begin(PhaseTimer::kForward, stream);
-        L::sweep_pass(view, a, stream);
+        LP::sweep_pass(sweep_view(), a, stream);
         launched();
         timer.end(stream);
         prev = out;

@@ -1231,6 +1231,17 @@ void Launch<S, M>::discrete_maxwell_states(const View<S, M>& v, const DeqGrid& d
   if (n > 0) k_discrete_maxwell_states<S, M><<<n, kCellThreads, 0, st>>>(v, deq, states, out, result);
 }
 
+template <class M>
+__global__ void k_cast_cell_params(const CellParams<M>* __restrict__ src, CellParams<float>* __restrict__ dst, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) dst[c] = cast_cell_params<float>(src[c]);
+}
+
+template <class S, class M>
+void Launch<S, M>::cast_cell_params(const CellParams<M>* src, CellParams<float>* dst, int n, cudaStream_t st) {
+  if (n > 0) k_cast_cell_params<M><<<ceil_div(n, 256), 256, 0, st>>>(src, dst, n);
+}
+
 template struct Launch<float, float>;
 template struct Launch<double, double>;
 template struct Launch<float, double>;

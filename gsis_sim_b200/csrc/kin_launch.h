@@ -75,6 +75,7 @@ struct Launch {
                           double mu0, double omega, double Pr, double cold_bgk_T, int discrete, int collisionless,
                           CellParams<M>* out, int* flags, cudaStream_t st);
   static void maxwell_reflection(const View<S, M>& v, cudaStream_t st);
+  static void cast_cell_params(const CellParams<M>* src, CellParams<float>* dst, int n, cudaStream_t st);
   static void boundary_sums(const View<S, M>& v, double* out, cudaStream_t st);
   static void internal_face_flux(const View<S, M>& v, const int32_t* cells, const int32_t* entries, double* out, int n,
                                  cudaStream_t st);

@@ -73,6 +73,33 @@ struct CellParams {
   M coll, diag;
 };
 
+// cell parameters in another precision (member by member)
+template <class To, class From>
+__host__ __device__ inline CellParams<To> cast_cell_params(const CellParams<From>& s) {
+  CellParams<To> o;
+  o.eq.ux = static_cast<To>(s.eq.ux);
+  o.eq.uy = static_cast<To>(s.eq.uy);
+  o.eq.uz = static_cast<To>(s.eq.uz);
+  o.eq.A = static_cast<To>(s.eq.A);
+  o.eq.B = static_cast<To>(s.eq.B);
+  o.ucx = static_cast<To>(s.ucx);
+  o.ucy = static_cast<To>(s.ucy);
+  o.ucz = static_cast<To>(s.ucz);
+  o.qx = static_cast<To>(s.qx);
+  o.qy = static_cast<To>(s.qy);
+  o.qz = static_cast<To>(s.qz);
+  o.theta = static_cast<To>(s.theta);
+  o.coef = static_cast<To>(s.coef);
+  o.g0 = static_cast<To>(s.g0);
+  o.g4 = static_cast<To>(s.g4);
+  o.gx = static_cast<To>(s.gx);
+  o.gy = static_cast<To>(s.gy);
+  o.gz = static_cast<To>(s.gz);
+  o.coll = static_cast<To>(s.coll);
+  o.diag = static_cast<To>(s.diag);
+  return o;
+}
+
 template <class M>
 __host__ __device__ inline M shakhov_poly(const CellParams<M>& s, M cx, M cy, M cz, M c2) {
   return s.coef * (cx * s.qx + cy * s.qy + cz * s.qz) * (c2 / s.theta - M(5));

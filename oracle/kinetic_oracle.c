@@ -246,8 +246,60 @@ static int orc_deq_state_f64(const double* xx, const double* xy, const double* x
 struct OrcHandle {
   int precision;
   void* state;
+  /* mixed precision: an FP32-arithmetic state that shares f and the chunk work arrays with the FP64-arithmetic
+     state; it runs the gradient and the LU-SGS passes, the FP64 state everything else (residual included) */
+  State_f32* fast;
   char err[512];
 };
+
+/* mixed precision: share the FP32 storage of the FP64-arithmetic state with the FP32-arithmetic state */
+static State_f32* mixed_fast_state(const KinSetupDesc* d, State_mix* m) {
+  State_f32* f = create_f32(d);
+  free(f->f);
+  free(f->gx);
+  free(f->gy);
+  free(f->gz);
+  free(f->r);
+  f->f = m->f;
+  f->gx = m->gx;
+  f->gy = m->gy;
+  f->gz = m->gz;
+  f->r = m->r;
+  return f;
+}
+
+static void mixed_fast_destroy(State_f32* f) {
+  f->f = f->gx = f->gy = f->gz = f->r = NULL;
+  destroy_f32(f);
+}
+
+/* FP32 copy of the FP64 cell parameters (the LU-SGS diagonal and the Maxwell-wall reconstruction use them) */
+static void mixed_cast_cell_params(State_f32* f, const State_mix* m) {
+  for (int c = 0; c < m->nc; ++c) {
+    const Cp_mix* a = &m->cp[c];
+    Cp_f32* b = &f->cp[c];
+    b->eq.ux = (float)a->eq.ux;
+    b->eq.uy = (float)a->eq.uy;
+    b->eq.uz = (float)a->eq.uz;
+    b->eq.A = (float)a->eq.A;
+    b->eq.B = (float)a->eq.B;
+    b->ucx = (float)a->ucx;
+    b->ucy = (float)a->ucy;
+    b->ucz = (float)a->ucz;
+    b->qx = (float)a->qx;
+    b->qy = (float)a->qy;
+    b->qz = (float)a->qz;
+    b->theta = (float)a->theta;
+    b->coef = (float)a->coef;
+    b->g0 = (float)a->g0;
+    b->g4 = (float)a->g4;
+    b->gx = (float)a->gx;
+    b->gy = (float)a->gy;
+    b->gz = (float)a->gz;
+    b->coll = (float)a->coll;
+    b->diag = (float)a->diag;
+  }
+}
 
 #define DISPATCH(h, fn, ...)                                      \
   do {                                                            \
@@ -272,7 +324,10 @@ int orc_create(const KinSetupDesc* d, OrcHandle** out) {
   h->precision = d->precision;
   if (d->precision == KIN_PREC_FP32) h->state = create_f32(d);
   else if (d->precision == KIN_PREC_FP64) h->state = create_f64(d);
-  else h->state = create_mix(d);
+  else {
+    h->state = create_mix(d);
+    h->fast = mixed_fast_state(d, (State_mix*)h->state);
+  }
   *out = h;
   return KIN_OK;
 }
@@ -281,7 +336,10 @@ void orc_destroy(OrcHandle* h) {
   if (!h) return;
   if (h->precision == KIN_PREC_FP32) destroy_f32((State_f32*)h->state);
   else if (h->precision == KIN_PREC_FP64) destroy_f64((State_f64*)h->state);
-  else destroy_mix((State_mix*)h->state);
+  else {
+    mixed_fast_destroy(h->fast);
+    destroy_mix((State_mix*)h->state);
+  }
   free(h);
 }
 
@@ -332,20 +390,34 @@ int orc_scale_distribution(OrcHandle* h, double s) {
 }
 int orc_update_cell_params(OrcHandle* h) {
   DISPATCH(h, update_cell_params);
+  if (h->fast) mixed_cast_cell_params(h->fast, (State_mix*)h->state);
   return KIN_OK;
 }
 int orc_set_inflow(OrcHandle* h, const KinInflowState* in, int64_t n) {
   if (n != orc_nb(h)) return orc_fail(h, "length of the inflow states does not match the number of boundary faces");
   DISPATCH(h, set_inflow, in);
+  if (h->fast) set_inflow_f32(h->fast, in);
   return KIN_OK;
 }
 int orc_boundary_sums(OrcHandle* h, double* out, int64_t n) {
   if (n != 20LL * orc_nb(h)) return orc_fail(h, "length of the boundary-sum output does not match");
   DISPATCH(h, boundary_sums, out);
+  if (h->fast) reflect_f32(h->fast);
   return KIN_OK;
 }
 int orc_sweep(OrcHandle* h, double* res, int64_t n) {
   if (n != orc_nc(h)) return orc_fail(h, "length of the residual output does not match the number of cells");
+  if (h->fast) {
+    State_mix* m = (State_mix*)h->state;
+    for (int c = 0; c < m->nc; ++c) res[c] = 0.0;
+    for (int k0 = 0; k0 < m->nv; k0 += m->chunk) {
+      const int kc = m->chunk < m->nv - k0 ? m->chunk : m->nv - k0;
+      sweep_gradient_f32(h->fast, k0, kc);
+      sweep_residual_mix(m, k0, kc, res);
+      sweep_passes_f32(h->fast, k0, kc);
+    }
+    return KIN_OK;
+  }
   DISPATCH(h, sweep, res);
   return KIN_OK;
 }

@@ -383,7 +383,8 @@ static void N(add_terms)(M wf, M x, M y, M z, M an, double* flux5, double* mom5)
   mom5[3] += (double)(wf * z); mom5[4] += (double)(wf * e);
 }
 
-static void N(boundary_sums)(N(State) * s, double* out) {
+/* specular caches of partially accommodating walls (k_maxwell_reflection, kinetic_cuda_kernels.cu:262-272) */
+static void N(reflect)(N(State) * s) {
   if (s->n_maxwell > 0) {
     for (int pass = 0; pass < 2; ++pass) {
 #pragma omp parallel for schedule(dynamic, 1)
@@ -398,6 +399,10 @@ static void N(boundary_sums)(N(State) * s, double* out) {
       }
     }
   }
+}
+
+static void N(boundary_sums)(N(State) * s, double* out) {
+  N(reflect)(s);
   const M wu = (M)s->weight;
 #pragma omp parallel for schedule(dynamic, 4)
   for (int b = 0; b < s->nb; ++b) {
@@ -543,66 +548,80 @@ static void N(bwd_cell)(N(State) * s, int stride, int k0, S* r, const S* dprev, 
   }
 }
 
-/* CpuBackend::sweep (src/kinetic/kinetic_backend_cpu.cpp:262-344) */
-static void N(sweep)(N(State) * s, double* residual_cell) {
-  for (int c = 0; c < s->nc; ++c) residual_cell[c] = 0.0;
+/* CpuBackend::sweep (src/kinetic/kinetic_backend_cpu.cpp:262-344), in three parts per velocity chunk */
+static void N(sweep_gradient)(N(State) * s, int k0, int kc) {
+  const int stride = s->chunk;
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < s->nc; ++c) {
+    for (int t = 0; t < kc; ++t) {
+      const int p = k0 + t;
+      M g[3];
+      N(lgrad)(s, c, p, s->xi_x[p], s->xi_y[p], s->xi_z[p], N(fat)(s, c, p), g);
+      const int64_t wi = (int64_t)c * stride + t;
+      s->gx[wi] = (S)g[0];
+      s->gy[wi] = (S)g[1];
+      s->gz[wi] = (S)g[2];
+    }
+  }
+}
+
+static void N(sweep_residual)(N(State) * s, int k0, int kc, double* residual_cell) {
+  const int stride = s->chunk;
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < s->nc; ++c) {
+    double r2 = 0.0;
+    for (int t = 0; t < kc; ++t) {
+      const M R = N(residual)(s, k0, stride, c, t);
+      s->r[(int64_t)c * stride + t] = (S)R;
+      r2 += (double)R * (double)R;
+    }
+    residual_cell[c] += r2;
+  }
+}
+
+static void N(sweep_passes)(N(State) * s, int k0, int kc) {
   const int stride = s->chunk;
   const size_t work = (size_t)s->nc * (size_t)stride;
+  /* block passes: gx holds R, gy the previous pass (the reference's buffer use) */
+  if (s->passes > 1) memcpy(s->gx, s->r, sizeof(S) * work);
+  const int n_lanes = s->n_blocks * kc;
+  for (int pass = 0; pass < s->passes; ++pass) {
+    const S* r0 = NULL;
+    const S* dprev = NULL;
+    if (pass > 0) {
+      memcpy(s->gy, s->r, sizeof(S) * work);
+      r0 = s->gx;
+      dprev = s->gy;
+    }
+    const int upd = pass + 1 == s->passes;
+#pragma omp parallel for schedule(static)
+    for (int lane = 0; lane < n_lanes; ++lane) {
+      const int b = lane / kc, t = lane % kc, p = k0 + t;
+      const int cb = s->block_off[b], ce = s->block_off[b + 1];
+      const int32_t* order = s->n_dirs > 0 ? s->order + (int64_t)s->dir_of[p] * s->nc : NULL;
+      const int32_t* pos = s->n_dirs > 0 ? s->pos + (int64_t)s->dir_of[p] * s->nc : NULL;
+      for (int k = cb; k < ce; ++k)
+        N(fwd_cell)(s, stride, s->r, r0, dprev, order ? order[k] : k, t, cb, ce, s->xi_x[p], s->xi_y[p], s->xi_z[p], pos);
+    }
+#pragma omp parallel for schedule(static)
+    for (int lane = 0; lane < n_lanes; ++lane) {
+      const int b = lane / kc, t = lane % kc, p = k0 + t;
+      const int cb = s->block_off[b], ce = s->block_off[b + 1];
+      const int32_t* order = s->n_dirs > 0 ? s->order + (int64_t)s->dir_of[p] * s->nc : NULL;
+      const int32_t* pos = s->n_dirs > 0 ? s->pos + (int64_t)s->dir_of[p] * s->nc : NULL;
+      for (int k = ce - 1; k >= cb; --k)
+        N(bwd_cell)(s, stride, k0, s->r, dprev, upd, order ? order[k] : k, t, cb, ce, s->xi_x[p], s->xi_y[p], s->xi_z[p], pos);
+    }
+  }
+}
+
+static void N(sweep)(N(State) * s, double* residual_cell) {
+  for (int c = 0; c < s->nc; ++c) residual_cell[c] = 0.0;
   for (int k0 = 0; k0 < s->nv; k0 += s->chunk) {
     const int kc = s->chunk < s->nv - k0 ? s->chunk : s->nv - k0;
-#pragma omp parallel for schedule(static)
-    for (int c = 0; c < s->nc; ++c) {
-      for (int t = 0; t < kc; ++t) {
-        const int p = k0 + t;
-        M g[3];
-        N(lgrad)(s, c, p, s->xi_x[p], s->xi_y[p], s->xi_z[p], N(fat)(s, c, p), g);
-        const int64_t wi = (int64_t)c * stride + t;
-        s->gx[wi] = (S)g[0];
-        s->gy[wi] = (S)g[1];
-        s->gz[wi] = (S)g[2];
-      }
-    }
-#pragma omp parallel for schedule(static)
-    for (int c = 0; c < s->nc; ++c) {
-      double r2 = 0.0;
-      for (int t = 0; t < kc; ++t) {
-        const M R = N(residual)(s, k0, stride, c, t);
-        s->r[(int64_t)c * stride + t] = (S)R;
-        r2 += (double)R * (double)R;
-      }
-      residual_cell[c] += r2;
-    }
-    /* block passes: gx holds R, gy the previous pass (the reference's buffer use) */
-    if (s->passes > 1) memcpy(s->gx, s->r, sizeof(S) * work);
-    const int n_lanes = s->n_blocks * kc;
-    for (int pass = 0; pass < s->passes; ++pass) {
-      const S* r0 = NULL;
-      const S* dprev = NULL;
-      if (pass > 0) {
-        memcpy(s->gy, s->r, sizeof(S) * work);
-        r0 = s->gx;
-        dprev = s->gy;
-      }
-      const int upd = pass + 1 == s->passes;
-#pragma omp parallel for schedule(static)
-      for (int lane = 0; lane < n_lanes; ++lane) {
-        const int b = lane / kc, t = lane % kc, p = k0 + t;
-        const int cb = s->block_off[b], ce = s->block_off[b + 1];
-        const int32_t* order = s->n_dirs > 0 ? s->order + (int64_t)s->dir_of[p] * s->nc : NULL;
-        const int32_t* pos = s->n_dirs > 0 ? s->pos + (int64_t)s->dir_of[p] * s->nc : NULL;
-        for (int k = cb; k < ce; ++k)
-          N(fwd_cell)(s, stride, s->r, r0, dprev, order ? order[k] : k, t, cb, ce, s->xi_x[p], s->xi_y[p], s->xi_z[p], pos);
-      }
-#pragma omp parallel for schedule(static)
-      for (int lane = 0; lane < n_lanes; ++lane) {
-        const int b = lane / kc, t = lane % kc, p = k0 + t;
-        const int cb = s->block_off[b], ce = s->block_off[b + 1];
-        const int32_t* order = s->n_dirs > 0 ? s->order + (int64_t)s->dir_of[p] * s->nc : NULL;
-        const int32_t* pos = s->n_dirs > 0 ? s->pos + (int64_t)s->dir_of[p] * s->nc : NULL;
-        for (int k = ce - 1; k >= cb; --k)
-          N(bwd_cell)(s, stride, k0, s->r, dprev, upd, order ? order[k] : k, t, cb, ce, s->xi_x[p], s->xi_y[p], s->xi_z[p], pos);
-      }
-    }
+    N(sweep_gradient)(s, k0, kc);
+    N(sweep_residual)(s, k0, kc, residual_cell);
+    N(sweep_passes)(s, k0, kc);
   }
 }
 

@@ -54,18 +54,22 @@ def test_gpu_deterministic_and_chunk_independent(B200Backend, name):
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "maxwell_wall_fp64", "couette_fp64"])
 def test_gpu_mixed_precision_matches_oracle(B200Backend, name):
-    """FP32 storage with FP64 arithmetic: the same scheme on the CPU oracle, FP32-rounding tolerance."""
+    """Mixed precision (f, gradients and LU-SGS passes in FP32; residual, moments and sums in FP64) against the
+    same scheme on the CPU oracle. Quantities computed in FP64 from the same FP32 f agree to 1e-6; the FP32
+    arithmetic of the sweeps gets the reference's FP32 tolerance (FMA contraction differs between the two)."""
     from oracle.kinetic_oracle import OracleBackend
 
     z, setup = common.load(name)
     with B200Backend(setup, precision="mixed") as be:
         g = common.run_op_sequence(be, z)
     o = common.run_op_sequence(OracleBackend(setup, precision="mixed"), z)
-    for k in ["moments0", "bsums0", "f1", "moments2", "f3", "face_flux"]:
+    for k in ["moments0", "bsums0"]:
         assert common.max_rel(g[k], o[k]) < 1e-6, k
+    for k in ["f1", "moments2", "f3", "face_flux", "res1"]:
+        assert common.max_rel(g[k], o[k]) < common.TOL["fp32"], k
     # and it stays within the FP32 tolerance of the FP64 reference
-    for k in ["f1", "f3"]:
-        assert common.max_rel(g[k], z["op." + k]) < 2e-5, k
+    for k in ["f1", "f3", "res1"]:
+        assert common.max_rel(g[k], z["op." + k]) < common.TOL["fp32"], k
 
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64", "tet_positivity_fp32", "dir13_fp32", "vacuum_tube_fp64"])
