@@ -45,8 +45,9 @@ extern "C" {
 /* storage / arithmetic precision of the distribution function */
 #define KIN_PREC_FP32 0  /* reference precision = "fp32": f and all per-point arithmetic in FP32 */
 #define KIN_PREC_FP64 1  /* reference precision = "fp64" */
-#define KIN_PREC_MIXED 2 /* f, gradients and LU-SGS corrections stored in FP32; residual, gradients, moments and
-                            sums evaluated in FP64 arithmetic (defect correction); no reference counterpart */
+#define KIN_PREC_MIXED 2 /* f stored in FP32; limited gradients and LU-SGS passes in FP32 arithmetic; steady residual,
+                            moments, boundary sums, equilibrium and GSIS correction in FP64 arithmetic (the FP32
+                            sweeps are a defect correction of the FP64 residual); no reference counterpart */
 
 /* BoundaryKind (src/kinetic/kinetic_types.hpp:19-26) */
 #define KIN_BC_DIFFUSE_WALL 0
