@@ -210,7 +210,7 @@ struct Backend final : KinHandle {
   double mu0 = 0, omega = 0, Pr = 0, cold_bgk_T = 0;
   kin::View<S, M> view{};
   kin::View<S, P> pview{};  // mixed mode: the FP32 view of the gradient and the LU-SGS passes
-  int32_t chunk = 0, partial_stride = 1, max_levels = 0, n_chains = 0;
+  int32_t chunk = 0, partial_stride = 1, max_levels = 0, n_chains = 0, max_entries = 0;
 
   // host copies
   std::vector<int32_t> perm, inv;
@@ -447,6 +447,7 @@ struct Backend final : KinHandle {
   void build_mesh(const KinSetupDesc& d) {
     const int64_t n_csr = d.csr_offsets[nc];
     csr_off.upload(d.csr_offsets, static_cast<size_t>(nc) + 1, stream);
+    for (int c = 0; c < nc; ++c) max_entries = std::max(max_entries, d.csr_offsets[c + 1] - d.csr_offsets[c]);
     std::vector<CsrE<M>> hc(static_cast<size_t>(n_csr));
     for (int64_t k = 0; k < n_csr; ++k) {
       CsrE<M>& e = hc[k];
@@ -764,6 +765,7 @@ struct Backend final : KinHandle {
     v.n_cells = nc;
     v.nv = nv;
     v.n_bfaces = nb;
+    v.max_entries = max_entries;
     v.xi_x = xi_x.p;
     v.xi_y = xi_y.p;
     v.xi_z = xi_z.p;
@@ -789,6 +791,7 @@ struct Backend final : KinHandle {
       w.n_cells = nc;
       w.nv = nv;
       w.n_bfaces = nb;
+      w.max_entries = max_entries;
       w.xi_x = pxi_x.p;
       w.xi_y = pxi_y.p;
       w.xi_z = pxi_z.p;

@@ -330,19 +330,46 @@ __device__ __forceinline__ int stage_cells(const View<S, M>& v, int c0, int c1, 
 template <class S>
 __device__ __forceinline__ S ldg_s(const S* p) { return __ldg(p); }
 
-// limited_gradient for U velocities of one cell at once (same arithmetic per velocity)
-template <class S, class M, int U>
-__device__ inline void limited_gradient_multi(const View<S, M>& v, int cell, const StagedEntry<M>* E, int ne,
-                                              const int (&q)[U], const bool (&ok)[U], const M (&x)[U],
-                                              const M (&y)[U], const M (&z)[U], const M (&fi)[U], M (&gx)[U],
-                                              M (&gy)[U], M (&gz)[U]) {
+// Loop over the entries of one cell: unrolled with a compile-time bound NE (hexahedra, prisms, tetrahedra:
+// NE = 6) so that loads of later entries can be issued before earlier ones are used, or a plain loop (NE = 0).
+template <int NE, class F>
+__device__ __forceinline__ void for_entries(int ne, F&& body) {
+  if constexpr (NE > 0) {
+#pragma unroll
+    for (int j = 0; j < NE; ++j)
+      if (j < ne) body(j);
+  } else {
+    for (int j = 0; j < ne; ++j) body(j);
+  }
+}
+
+// venkat_face written with selects: the one division is taken only where its value can lower phi (0 <= num < den;
+// otherwise the reference routine returns 1, 0, or a quotient that the clamp makes 1), so min(phi, .) is the same
+template <class M>
+__device__ __forceinline__ M venkat_face_sel(M d2, M dmax, M dmin, M eps2) {
+  const bool pos = d2 > M(0), neg = d2 < M(0);
+  const M d1 = pos ? dmax : dmin;
+  const M num = (d1 * d1 + eps2) + M(2) * d1 * d2;
+  const M den = d1 * d1 + M(2) * d2 * d2 + d1 * d2 + eps2;
+  const bool sided = pos || neg;
+  M r = (sided && !(den > M(0))) ? M(0) : M(1);
+  if (sided && den > M(0) && num < den) r = kclamp(num / den, M(0), M(1));
+  return r;
+}
+
+// limited_gradient for U velocities of one cell at once (same arithmetic per velocity, entries in CSR order)
+template <class S, class M, int U, int NE>
+__device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int cell, const StagedEntry<M>* E, int ne,
+                                                      const int (&q)[U], const bool (&ok)[U], const M (&x)[U],
+                                                      const M (&y)[U], const M (&z)[U], const M (&fi)[U],
+                                                      M (&gx)[U], M (&gy)[U], M (&gz)[U]) {
   M sx[U], sy[U], sz[U], fmax[U], fmin[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     sx[u] = sy[u] = sz[u] = M(0);
     fmax[u] = fmin[u] = fi[u];
   }
-  for (int j = 0; j < ne; ++j) {
+  for_entries<NE>(ne, [&](int j) {
     const CsrE<M>& c = E[j].e;
     M fk[U];
     if (c.other >= 0) {
@@ -363,7 +390,7 @@ __device__ inline void limited_gradient_multi(const View<S, M>& v, int cell, con
       fmax[u] = kmax(fmax[u], fk[u]);
       fmin[u] = kmin(fmin[u], fk[u]);
     }
-  }
+  });
   if (v.limiter_mode == kLimNone && v.positivity == 0) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -374,7 +401,7 @@ __device__ inline void limited_gradient_multi(const View<S, M>& v, int cell, con
     return;
   }
   const M eps2c = v.eps2[cell];
-  M eps2[U], phi[U], pmin[U];
+  M eps2[U], phi[U], pmin[U], dmx[U], dmn[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     eps2[u] = eps2c;
@@ -384,17 +411,21 @@ __device__ inline void limited_gradient_multi(const View<S, M>& v, int cell, con
     }
     phi[u] = M(1);
     pmin[u] = M(0);
+    dmx[u] = fmax[u] - fi[u];
+    dmn[u] = fmin[u] - fi[u];
   }
-  for (int j = 0; j < ne; ++j) {
+  const bool limit = v.limiter_mode != kLimNone;
+  for_entries<NE>(ne, [&](int j) {
+    if (E[j].kind == kPeriodic) return;
     const CsrE<M>& c = E[j].e;
-    if (E[j].kind == kPeriodic) continue;
+    const M ds0 = c.ds[0], ds1 = c.ds[1], ds2 = c.ds[2];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const M proj = sx[u] * c.ds[0] + sy[u] * c.ds[1] + sz[u] * c.ds[2];
-      if (v.limiter_mode != kLimNone) phi[u] = kmin(phi[u], venkat_face(proj, fmax[u] - fi[u], fmin[u] - fi[u], eps2[u]));
+      const M proj = sx[u] * ds0 + sy[u] * ds1 + sz[u] * ds2;
+      if (limit) phi[u] = kmin(phi[u], venkat_face_sel(proj, dmx[u], dmn[u], eps2[u]));
       pmin[u] = kmin(pmin[u], proj);
     }
-  }
+  });
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     M ph = phi[u];
@@ -408,15 +439,30 @@ __device__ inline void limited_gradient_multi(const View<S, M>& v, int cell, con
   }
 }
 
-template <class S, class M>
-__global__ void __launch_bounds__(kTileThreads, 2) k_gradient(View<S, M> v, Chunk<S> ch) {
+// resident CTAs per SM the gradient / residual kernels are register-budgeted for (FP32 arithmetic needs fewer
+// registers per velocity, so three CTAs fit)
+template <class M>
+struct TileOcc {
+  static constexpr int kGradient = 3;
+  static constexpr int kResidual = 3;
+  static constexpr int kGradientU = 4;  // velocities per thread of the gradient
+};
+template <>
+struct TileOcc<double> {
+  static constexpr int kGradient = 3;
+  static constexpr int kResidual = 2;
+  static constexpr int kGradientU = 2;
+};
+
+template <class S, class M, int NE>
+__global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kGradient) k_gradient(View<S, M> v, Chunk<S> ch) {
   __shared__ StagedEntry<M> E[kStageMulti];
   __shared__ int off[kCellsPerCta + 1];
   const int c0 = blockIdx.x * kCellsPerCta, c1 = min(v.n_cells, c0 + kCellsPerCta);
-  const int tb = blockIdx.y * (kTileThreads * kTileIters);
-  const int te = min(ch.kc, tb + kTileThreads * kTileIters);
+  constexpr int U = TileOcc<M>::kGradientU;
+  const int tb = blockIdx.y * (kTileThreads * U);
+  const int te = min(ch.kc, tb + kTileThreads * U);
   const bool staged = stage_cells(v, c0, c1, E, off) <= kStageMulti;
-  constexpr int U = kTileIters;
   int q[U];
   bool ok[U];
   M x[U], y[U], z[U];
@@ -424,10 +470,10 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gradient(View<S, M> v, Chun
   for (int u = 0; u < U; ++u) {
     const int t = tb + threadIdx.x + u * kTileThreads;
     ok[u] = t < te;
-    q[u] = ch.k0 + (ok[u] ? t : tb);
-    x[u] = v.xi_x[q[u]];
-    y[u] = v.xi_y[q[u]];
-    z[u] = v.xi_z[q[u]];
+    q[u] = ch.k0 + t;  // affine in u: one address per neighbour serves all U velocities; used only where ok[u]
+    x[u] = ok[u] ? v.xi_x[q[u]] : M(0);
+    y[u] = ok[u] ? v.xi_y[q[u]] : M(0);
+    z[u] = ok[u] ? v.xi_z[q[u]] : M(0);
   }
   for (int c = c0; c < c1; ++c) {
     const int64_t row = static_cast<int64_t>(c) * ch.stride - ch.k0;
@@ -446,9 +492,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gradient(View<S, M> v, Chun
     const S* fc = v.f + static_cast<int64_t>(c) * v.nv;
     M fi[U], gx[U], gy[U], gz[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) fi[u] = static_cast<M>(ldg_s(fc + q[u]));
-    limited_gradient_multi<S, M, U>(v, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], q, ok, x, y, z, fi, gx,
-                                    gy, gz);
+    for (int u = 0; u < U; ++u) fi[u] = ok[u] ? static_cast<M>(ldg_s(fc + q[u])) : M(0);
+    limited_gradient_tile<S, M, U, NE>(v, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], q, ok, x, y, z, fi,
+                                       gx, gy, gz);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (!ok[u]) continue;
@@ -504,63 +550,81 @@ __device__ inline M residual_value(const View<S, M>& v, const Chunk<S>& ch, int 
   return R;
 }
 
-// residual of U velocities of one cell from staged entries
-template <class S, class M, int U>
-__device__ __forceinline__ void residual_multi(const View<S, M>& v, const Chunk<S>& ch, int c,
-                                               const StagedEntry<M>* E, int ne, const int (&t)[U],
-                                               const bool (&ok)[U], const M (&x)[U], const M (&y)[U],
-                                               const M (&z)[U], M (&R)[U]) {
-  M fi[U], gix[U], giy[U], giz[U];
+// residual of U velocities of one cell from staged entries (residual_value, kinetic_kernels.hpp:238-278). At an
+// internal face the upwind value is chosen with a select between the two reconstructions (the neighbour's loads are
+// predicated on a < 0), so the U velocities never branch apart; boundary faces follow the reference branches.
+template <class S, class M, int U, int NE>
+__device__ __forceinline__ void residual_tile(const View<S, M>& v, const Chunk<S>& ch, int c, const StagedEntry<M>* E,
+                                              int ne, const int (&t)[U], const bool (&ok)[U], const M (&x)[U],
+                                              const M (&y)[U], const M (&z)[U], M (&R)[U], M (&fi)[U]) {
+  M gix[U], giy[U], giz[U];
   const S* fc = v.f + static_cast<int64_t>(c) * v.nv + ch.k0;
   const int64_t row = static_cast<int64_t>(c) * ch.stride;
 #pragma unroll
   for (int u = 0; u < U; ++u) {
-    fi[u] = static_cast<M>(ldg_s(fc + t[u]));
-    gix[u] = static_cast<M>(ldg_s(ch.gx + row + t[u]));
-    giy[u] = static_cast<M>(ldg_s(ch.gy + row + t[u]));
-    giz[u] = static_cast<M>(ldg_s(ch.gz + row + t[u]));
+    fi[u] = ok[u] ? static_cast<M>(ldg_s(fc + t[u])) : M(0);
+    gix[u] = ok[u] ? static_cast<M>(ldg_s(ch.gx + row + t[u])) : M(0);
+    giy[u] = ok[u] ? static_cast<M>(ldg_s(ch.gy + row + t[u])) : M(0);
+    giz[u] = ok[u] ? static_cast<M>(ldg_s(ch.gz + row + t[u])) : M(0);
     R[u] = M(0);
   }
-  for (int j = 0; j < ne; ++j) {
+  for_entries<NE>(ne, [&](int j) {
     const CsrE<M>& ce = E[j].e;
     const int kind = E[j].kind;
-    if (kind == kPeriodic) continue;
+    if (kind == kPeriodic) return;
+    const M s0 = ce.s[0], s1 = ce.s[1], s2 = ce.s[2];
+    if (ce.other >= 0) {
+      const S* fo = v.f + static_cast<int64_t>(ce.other) * v.nv + ch.k0;
+      const int64_t wj = static_cast<int64_t>(ce.other) * ch.stride;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const M a = x[u] * ce.s[0] + y[u] * ce.s[1] + z[u] * ce.s[2];
-      M ff;
-      if (a >= M(0)) {
-        ff = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
-      } else if (ce.other >= 0) {
-        const int64_t wj = static_cast<int64_t>(ce.other) * ch.stride + t[u];
-        ff = static_cast<M>(ldg_s(v.f + static_cast<int64_t>(ce.other) * v.nv + ch.k0 + t[u])) +
-             static_cast<M>(ldg_s(ch.gx + wj)) * ce.dn[0] + static_cast<M>(ldg_s(ch.gy + wj)) * ce.dn[1] +
-             static_cast<M>(ldg_s(ch.gz + wj)) * ce.dn[2];
-      } else if (kind == kSymmetry) {
-        const int q = ch.k0 + t[u];
-        const int qm = v.mirror_map[v.bf[ce.bface].mirror * v.nv + q];
-        const M fm = f_at(v, c, qm);
-        M gx, gy, gz;
-        limited_gradient(v, c, qm, v.xi_x[qm], v.xi_y[qm], v.xi_z[qm], fm, gx, gy, gz);
-        ff = fm + gx * ce.ds[0] + gy * ce.ds[1] + gz * ce.ds[2];
-      } else if (kind == kMaxwellWall) {
-        ff = maxwell_inflow(v, ce.bface, ch.k0 + t[u], x[u], y[u], z[u]);
-      } else {
-        ff = inflow_value(v.inflow[ce.bface], x[u], y[u], z[u]);
+      for (int u = 0; u < U; ++u) {
+        const M a = x[u] * s0 + y[u] * s1 + z[u] * s2;
+        const bool up = a >= M(0);
+        const bool ld = ok[u] && !up;
+        const M fj = ld ? static_cast<M>(ldg_s(fo + t[u])) : M(0);
+        const M gxj = ld ? static_cast<M>(ldg_s(ch.gx + wj + t[u])) : M(0);
+        const M gyj = ld ? static_cast<M>(ldg_s(ch.gy + wj + t[u])) : M(0);
+        const M gzj = ld ? static_cast<M>(ldg_s(ch.gz + wj + t[u])) : M(0);
+        const M f_up = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
+        const M f_dn = fj + gxj * ce.dn[0] + gyj * ce.dn[1] + gzj * ce.dn[2];
+        R[u] += a * (up ? f_up : f_dn);
       }
-      R[u] += a * ff;
+    } else {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const M a = x[u] * s0 + y[u] * s1 + z[u] * s2;
+        M ff;
+        if (a >= M(0)) {
+          ff = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
+        } else if (!ok[u]) {
+          ff = M(0);
+        } else if (kind == kSymmetry) {
+          // outflow reconstruction of the mirrored velocity at the same cell (its gradient recomputed: the
+          // mirrored velocity need not lie in this chunk)
+          const int q = ch.k0 + t[u];
+          const int qm = v.mirror_map[v.bf[ce.bface].mirror * v.nv + q];
+          const M fm = f_at(v, c, qm);
+          M gx, gy, gz;
+          limited_gradient(v, c, qm, v.xi_x[qm], v.xi_y[qm], v.xi_z[qm], fm, gx, gy, gz);
+          ff = fm + gx * ce.ds[0] + gy * ce.ds[1] + gz * ce.ds[2];
+        } else if (kind == kMaxwellWall) {
+          ff = maxwell_inflow(v, ce.bface, ch.k0 + t[u], x[u], y[u], z[u]);
+        } else {
+          ff = inflow_value(v.inflow[ce.bface], x[u], y[u], z[u]);
+        }
+        R[u] += a * ff;
+      }
     }
-  }
+  });
   const CellParams<M> cp = v.cp[c];
 #pragma unroll
   for (int u = 0; u < U; ++u) R[u] = R[u] - cp.coll * (shakhov_target(cp, x[u], y[u], z[u]) - fi[u]);
-  (void)ok;
 }
 
 // residual of one chunk; partial[c * partial_stride + tile * warps + warp] = sum of R^2 over the warp's velocities
 // (summed in a fixed order by k_residual_reduce: deterministic)
-template <class S, class M>
-__global__ void __launch_bounds__(kTileThreads, 2)
+template <class S, class M, int NE>
+__global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
     k_residual(View<S, M> v, Chunk<S> ch, double* __restrict__ partial, int partial_stride) {
   constexpr int kWarps = kTileThreads / 32;
   __shared__ StagedEntry<M> E[kStageMulti];
@@ -576,13 +640,12 @@ __global__ void __launch_bounds__(kTileThreads, 2)
   M x[U], y[U], z[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
-    t[u] = tb + threadIdx.x + u * kTileThreads;
+    t[u] = tb + threadIdx.x + u * kTileThreads;  // affine in u; used only where ok[u]
     ok[u] = t[u] < te;
-    if (!ok[u]) t[u] = tb;
     const int q = ch.k0 + t[u];
-    x[u] = v.xi_x[q];
-    y[u] = v.xi_y[q];
-    z[u] = v.xi_z[q];
+    x[u] = ok[u] ? v.xi_x[q] : M(0);
+    y[u] = ok[u] ? v.xi_y[q] : M(0);
+    z[u] = ok[u] ? v.xi_z[q] : M(0);
   }
   for (int c = c0; c < c1; ++c) {
     const int64_t row = static_cast<int64_t>(c) * ch.stride;
@@ -596,8 +659,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         r2 += static_cast<double>(R) * static_cast<double>(R);
       }
     } else {
-      M R[U];
-      residual_multi<S, M, U>(v, ch, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], t, ok, x, y, z, R);
+      M R[U], fi[U];
+      residual_tile<S, M, U, NE>(v, ch, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], t, ok, x, y, z, R, fi);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;
@@ -1176,8 +1239,11 @@ int Launch<S, M>::residual_tiles(int kc) {
 template <class S, class M>
 void Launch<S, M>::gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st) {
   if (v.n_cells <= 0 || ch.kc <= 0) return;
-  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * kTileIters));
-  k_gradient<S, M><<<grid, kTileThreads, 0, st>>>(v, ch);
+  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * TileOcc<M>::kGradientU));
+  if (v.max_entries <= 6)
+    k_gradient<S, M, 6><<<grid, kTileThreads, 0, st>>>(v, ch);
+  else
+    k_gradient<S, M, 0><<<grid, kTileThreads, 0, st>>>(v, ch);
 }
 
 template <class S, class M>
@@ -1185,7 +1251,10 @@ void Launch<S, M>::residual(const View<S, M>& v, const Chunk<S>& ch, double* par
                             double* residual_cell, cudaStream_t st) {
   if (v.n_cells <= 0 || ch.kc <= 0) return;
   const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * kTileIters));
-  k_residual<S, M><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
+  if (v.max_entries <= 6)
+    k_residual<S, M, 6><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
+  else
+    k_residual<S, M, 0><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
   k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride, residual_tiles(ch.kc),
                                                              residual_cell, v.n_cells);
 }

@@ -46,6 +46,7 @@ struct Inflow {
 template <class S, class M>
 struct View {
   int32_t n_cells, nv, n_bfaces;
+  int32_t max_entries;  // largest number of CSR entries of a cell
   const M* xi_x;
   const M* xi_y;
   const M* xi_z;
