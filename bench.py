@@ -32,6 +32,12 @@ sys.path.insert(0, ROOT)
 HBM_FALLBACK_GBS = 6650.0
 
 
+# DRAM bytes (read + write) per (cell, velocity) per launch from one ncu capture of the tube case at 62,848 cells x
+# 12^3 velocities in FP64 (profiles/gradient_residual_sweep_tiles_tube63k_12cube_fp64.md); the LU-SGS figure is
+# that of the first block pass. Scaled by the units of a full launch for roofline.traffic.
+DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 34.9, ("fp64", "k_residual"): 57.5, ("fp64", "k_sweep_tiles"): 36.5}
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -280,11 +286,13 @@ def main():
     kernels = {
         "k_gradient": (timings["gradient"] / n_sweeps, nc * nv * 4 * s),
         "k_residual": (timings["residual"] / n_sweeps, nc * nv * 5 * s),
-        "k_sweep_pass": (timings["sweep_forward"] / (2 * n_sweeps), nc * nv * 3 * s),
+        "k_sweep_tiles": (timings["sweep_forward"] / (2 * n_sweeps), nc * nv * 3 * s),
     }
     dom = max(kernels, key=lambda k: kernels[k][0])
     t_launch, bytes_launch = kernels[dom]
     achieved = bytes_launch / t_launch / 1e9
+    per_unit = DRAM_BYTES_PER_UNIT.get((args.precision, dom))
+    traffic = per_unit * nc * nv if per_unit is not None else None
     clocks = clk.summary()
     line = {
         "metric": "cell_velocity_updates_per_s", "value": value, "unit": "cell*velocity updates/s", "n_gpus": ws,
@@ -293,7 +301,9 @@ def main():
         "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32 (f, gradient, LU-SGS) / f64 (residual, sums)"}[args.precision],
         "data": "synthetic", "config": workload_config(args, n_cells=nc),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
+                     "traffic_source": ("ncu DRAM bytes per cell-velocity of the 62,848-cell 12^3 capture, scaled "
+                                        "to this launch" if traffic is not None else None),
                      "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": 1e3 * t_launch},
         "e2e": {"value": e2e, "unit": "cell*velocity updates/s", "h2d_bytes_per_step": bytes_h2d,
                 "d2h_bytes_per_step": bytes_d2h},

@@ -968,8 +968,18 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
   }
 }
 
+// resident CTAs per SM of k_sweep_tiles: FP32 arithmetic leaves room for six (measured 9% faster than four)
+template <class M>
+struct SweepOcc {
+  static constexpr int kBlocks = 6;
+};
+template <>
+struct SweepOcc<double> {
+  static constexpr int kBlocks = kTileMinBlocks;
+};
+
 template <class S, class M, int NE, bool First>
-__global__ void __launch_bounds__(kTileThreadsSweep, kTileMinBlocks) k_sweep_tiles(View<S, M> v, SweepArgs<S, M> a) {
+__global__ void __launch_bounds__(kTileThreadsSweep, SweepOcc<M>::kBlocks) k_sweep_tiles(View<S, M> v, SweepArgs<S, M> a) {
   constexpr int W = kTileThreadsSweep / 32;
   __shared__ __align__(16) StageBuf<M> sh_buf[2];
   __shared__ int32_t sh_sc[kMaxSubLevels + 1], sh_se[kMaxSubLevels + 1];

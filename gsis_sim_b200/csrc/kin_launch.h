@@ -29,7 +29,7 @@ struct StageE {
 
 constexpr int kTileU = 4;                    // velocities per thread of k_sweep_tiles
 constexpr int kTileThreadsSweep = 128;       // threads of one k_sweep_tiles CTA
-constexpr int kTileMinBlocks = 4;            // resident CTAs per SM the register budget is sized for
+constexpr int kTileMinBlocks = 4;            // resident CTAs per SM the FP64 register budget is sized for
 constexpr int kTileVel = 32 * kTileU;        // velocities of one k_sweep_tiles CTA
 
 // arguments of one LU-SGS block pass over a velocity chunk

@@ -23,7 +23,6 @@ static int32_t* orc_dup_i(const int32_t* a, int64_t n) {
   if (n > 0) memcpy(o, a, sizeof(int32_t) * n);
   return o;
 }
-static double orc_min(double a, double b) { return b < a ? b : a; }
 static double orc_max(double a, double b) { return a < b ? b : a; }
 
 /* deq_resolved (src/kinetic/discrete_equilibrium.hpp:35-48) */
