@@ -201,6 +201,86 @@ def workload_config(args, cb_nv=None, n_cells=134528):
             "l2": "no flush: f and the work arrays (tens of GB) exceed the 126 MB L2"}
 
 
+def mdot_of_last_prepare(sol):
+    """M_dot of the state the last CIS iteration started from (the patch sums of its prepare step; the same formula as
+    KineticSolver.mass_flow without an extra prepare)."""
+    import math
+
+    from gsis_sim_b200.solver import T_MASS_FLOW_INLET, T_PRESSURE_INLET, T_PRESSURE_OUTLET, T_VACUUM
+
+    pm = sol.info.patch_mass_flow
+    mdot_in = -sum(pm[p] for p in range(len(pm)) if sol.ptype[p] in (T_PRESSURE_INLET, T_MASS_FLOW_INLET))
+    mdot_out = sum(pm[p] for p in range(len(pm)) if sol.ptype[p] in (T_PRESSURE_OUTLET, T_VACUUM))
+    return 0.5 * (mdot_in + mdot_out) * math.sqrt(2.0 / math.pi)
+
+
+def settle_time(hist, ref, tol):
+    """Wall time of the first iteration after which every recorded M_dot stays within tol of ref (None if never)."""
+    t = None
+    for (tw, m, _) in hist:
+        if abs(m - ref) <= tol * abs(ref):
+            if t is None:
+                t = tw
+        else:
+            t = None
+    return t
+
+
+def run_time_to_mdot(args, local):
+    """Solve time to M_dot within --mdot-tol of the converged FP64 M_dot, FP64 against mixed precision, plain CIS
+    iterations through the public host loop (wall clock, host logic included). The FP64 run continues until M_dot
+    changes by less than 1e-8 (relative) per iteration over 5 iterations, or --max-iters; its last M_dot is the
+    reference. Each iteration's M_dot is that of the state it started from (the patch sums of its prepare step)."""
+    import numpy as np
+    import torch
+
+    from gsis_sim_b200.backend import B200Backend
+    from gsis_sim_b200.solver import KineticSolver
+
+    torch.cuda.set_device(local)
+    out = {}
+    ref = None
+    for prec in ("fp64", "mixed"):
+        args.precision = prec
+        setup, host, _ = build_case(args)
+        n_cells = setup.n_cells
+        with B200Backend(setup, device=local) as be:
+            sol = KineticSolver(setup, host, be)
+            sol.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
+            hist = []
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for it in range(args.max_iters):
+                info = sol.sweep()
+                hist.append((time.perf_counter() - t0, mdot_of_last_prepare(sol), info.residual))
+                if prec == "fp64" and len(hist) > 6:
+                    ch = [abs(hist[-k][1] - hist[-k - 1][1]) / abs(hist[-1][1]) for k in range(1, 6)]
+                    if max(ch) < 1e-8:
+                        break
+                if prec == "mixed" and ref is not None and len(hist) > 10:
+                    # stop once M_dot has stayed within a hundredth of the tolerance for 10 iterations
+                    if all(abs(h[1] - ref) <= 0.01 * args.mdot_tol * abs(ref) for h in hist[-10:]):
+                        break
+        if prec == "fp64":
+            ref = hist[-1][1]
+        out[prec] = hist
+        if args.history:
+            np.savetxt(f"{args.history}_{prec}.txt", np.array(hist), header="wall_s mdot residual")
+    t64 = settle_time(out["fp64"], ref, args.mdot_tol)
+    tmx = settle_time(out["mixed"], ref, args.mdot_tol)
+    line = {"metric": f"solve time to M_dot within {args.mdot_tol:g} of the converged FP64 M_dot (mixed)",
+            "value": tmx, "unit": "s", "higher_is_better": False, "fp64_seconds": t64,
+            "speedup_mixed_vs_fp64": (t64 / tmx) if (t64 and tmx) else None, "mdot_fp64_converged": ref,
+            "mdot_mixed_final": out["mixed"][-1][1],
+            "mdot_mixed_rel_error": abs(out["mixed"][-1][1] - ref) / abs(ref),
+            "iterations": {"fp64": len(out["fp64"]), "mixed": len(out["mixed"])},
+            "seconds_per_iteration": {k: out[k][-1][0] / len(out[k]) for k in out},
+            "final_residual": {k: out[k][-1][2] for k in out},
+            "data": "synthetic", "config": workload_config(args, n_cells=n_cells)}
+    line["config"]["workload"] = line["config"]["workload"].replace(", mixed", "")
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,11 +295,20 @@ def main():
     # smaller variants of the tube case for profiler captures (the benchmark itself uses the defaults)
     ap.add_argument("--nx", type=int, default=100, help="axial cells of the tube (100: 134,528 cells)")
     ap.add_argument("--velocity-chunk", type=int, default=None, help="velocities per chunk (default: all that fit)")
+    # second headline metric: solve time to M_dot within a tolerance of the converged FP64 M_dot, mixed vs FP64
+    ap.add_argument("--time-to-mdot", action="store_true")
+    ap.add_argument("--mdot-tol", type=float, default=1e-4)
+    ap.add_argument("--max-iters", type=int, default=2000)
+    ap.add_argument("--history", default=None, help="write per-iteration (wall s, M_dot, residual) to <prefix>_<prec>.txt")
     args = ap.parse_args()
 
     rank, ws, local = dist_init() if args.gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1 else (0, 1, 0)
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.time_to_mdot:
+        if rank == 0:
+            run_time_to_mdot(args, local)
         return
 
     import numpy as np

@@ -306,7 +306,8 @@ constexpr int kStageMulti = 96;   // CSR entries of those cells staged in shared
 template <class M>
 struct StagedEntry {
   CsrE<M> e;
-  int32_t kind;  // -1 internal face, else the boundary kind
+  int32_t kind;          // -1 internal face, else the boundary kind
+  float dsf[3], dnf[3];  // FP32 copies of ds, dn (mixed-precision face reconstruction)
 };
 
 // Stage the CSR entries of cells [c0, c1) (contiguous in CSR order) and their per-cell offsets in shared memory.
@@ -320,6 +321,10 @@ __device__ __forceinline__ int stage_cells(const View<S, M>& v, int c0, int c1, 
       StagedEntry<M> se;
       se.e = v.csr[e0 + k];
       se.kind = se.e.other >= 0 ? -1 : v.bf[se.e.bface].kind;
+      for (int a = 0; a < 3; ++a) {
+        se.dsf[a] = static_cast<float>(se.e.ds[a]);
+        se.dnf[a] = static_cast<float>(se.e.dn[a]);
+      }
       sh[k] = se;
     }
   }
@@ -557,16 +562,27 @@ template <class S, class M, int U, int NE>
 __device__ __forceinline__ void residual_tile(const View<S, M>& v, const Chunk<S>& ch, int c, const StagedEntry<M>* E,
                                               int ne, const int (&t)[U], const bool (&ok)[U], const M (&x)[U],
                                               const M (&y)[U], const M (&z)[U], M (&R)[U], M (&fi)[U]) {
-  M gix[U], giy[U], giz[U];
+  // mixed precision (FP32 storage, FP64 arithmetic): the face reconstructions f + g . d are formed in the storage
+  // precision of their inputs; the flux balance and the collision term are summed in FP64
+  constexpr bool kLowRecon = sizeof(S) < sizeof(M);
   const S* fc = v.f + static_cast<int64_t>(c) * v.nv + ch.k0;
   const int64_t row = static_cast<int64_t>(c) * ch.stride;
+  S fs[U], gxs[U], gys[U], gzs[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
-    fi[u] = ok[u] ? static_cast<M>(ldg_s(fc + t[u])) : M(0);
-    gix[u] = ok[u] ? static_cast<M>(ldg_s(ch.gx + row + t[u])) : M(0);
-    giy[u] = ok[u] ? static_cast<M>(ldg_s(ch.gy + row + t[u])) : M(0);
-    giz[u] = ok[u] ? static_cast<M>(ldg_s(ch.gz + row + t[u])) : M(0);
+    fs[u] = ok[u] ? ldg_s(fc + t[u]) : S(0);
+    gxs[u] = ok[u] ? ldg_s(ch.gx + row + t[u]) : S(0);
+    gys[u] = ok[u] ? ldg_s(ch.gy + row + t[u]) : S(0);
+    gzs[u] = ok[u] ? ldg_s(ch.gz + row + t[u]) : S(0);
+    fi[u] = static_cast<M>(fs[u]);
     R[u] = M(0);
+  }
+  M gix[U], giy[U], giz[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    gix[u] = static_cast<M>(gxs[u]);
+    giy[u] = static_cast<M>(gys[u]);
+    giz[u] = static_cast<M>(gzs[u]);
   }
   for_entries<NE>(ne, [&](int j) {
     const CsrE<M>& ce = E[j].e;
@@ -581,13 +597,23 @@ __device__ __forceinline__ void residual_tile(const View<S, M>& v, const Chunk<S
         const M a = x[u] * s0 + y[u] * s1 + z[u] * s2;
         const bool up = a >= M(0);
         const bool ld = ok[u] && !up;
-        const M fj = ld ? static_cast<M>(ldg_s(fo + t[u])) : M(0);
-        const M gxj = ld ? static_cast<M>(ldg_s(ch.gx + wj + t[u])) : M(0);
-        const M gyj = ld ? static_cast<M>(ldg_s(ch.gy + wj + t[u])) : M(0);
-        const M gzj = ld ? static_cast<M>(ldg_s(ch.gz + wj + t[u])) : M(0);
-        const M f_up = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
-        const M f_dn = fj + gxj * ce.dn[0] + gyj * ce.dn[1] + gzj * ce.dn[2];
-        R[u] += a * (up ? f_up : f_dn);
+        if constexpr (kLowRecon) {
+          const S fj = ld ? ldg_s(fo + t[u]) : S(0);
+          const S gxj = ld ? ldg_s(ch.gx + wj + t[u]) : S(0);
+          const S gyj = ld ? ldg_s(ch.gy + wj + t[u]) : S(0);
+          const S gzj = ld ? ldg_s(ch.gz + wj + t[u]) : S(0);
+          const S f_up = fs[u] + gxs[u] * E[j].dsf[0] + gys[u] * E[j].dsf[1] + gzs[u] * E[j].dsf[2];
+          const S f_dn = fj + gxj * E[j].dnf[0] + gyj * E[j].dnf[1] + gzj * E[j].dnf[2];
+          R[u] += a * static_cast<M>(up ? f_up : f_dn);
+        } else {
+          const M fj = ld ? static_cast<M>(ldg_s(fo + t[u])) : M(0);
+          const M gxj = ld ? static_cast<M>(ldg_s(ch.gx + wj + t[u])) : M(0);
+          const M gyj = ld ? static_cast<M>(ldg_s(ch.gy + wj + t[u])) : M(0);
+          const M gzj = ld ? static_cast<M>(ldg_s(ch.gz + wj + t[u])) : M(0);
+          const M f_up = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
+          const M f_dn = fj + gxj * ce.dn[0] + gyj * ce.dn[1] + gzj * ce.dn[2];
+          R[u] += a * (up ? f_up : f_dn);
+        }
       }
     } else {
 #pragma unroll
@@ -595,7 +621,10 @@ __device__ __forceinline__ void residual_tile(const View<S, M>& v, const Chunk<S
         const M a = x[u] * s0 + y[u] * s1 + z[u] * s2;
         M ff;
         if (a >= M(0)) {
-          ff = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
+          if constexpr (kLowRecon)
+            ff = static_cast<M>(fs[u] + gxs[u] * E[j].dsf[0] + gys[u] * E[j].dsf[1] + gzs[u] * E[j].dsf[2]);
+          else
+            ff = fi[u] + gix[u] * ce.ds[0] + giy[u] * ce.ds[1] + giz[u] * ce.ds[2];
         } else if (!ok[u]) {
           ff = M(0);
         } else if (kind == kSymmetry) {

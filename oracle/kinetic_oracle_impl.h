@@ -472,10 +472,18 @@ static M N(residual)(const N(State) * s, int k0, int stride, int cell, int t) {
     const M a = x * c->s[0] + y * c->s[1] + z * c->s[2];
     M ff;
     if (a >= (M)0) {
-      ff = fi + gix * c->ds[0] + giy * c->ds[1] + giz * c->ds[2];
+      if (sizeof(S) < sizeof(M)) /* mixed precision: face reconstruction in the storage precision */
+        ff = (M)(s->f[(int64_t)cell * s->nv + p] + s->gx[wi] * (S)c->ds[0] + s->gy[wi] * (S)c->ds[1] +
+                 s->gz[wi] * (S)c->ds[2]);
+      else
+        ff = fi + gix * c->ds[0] + giy * c->ds[1] + giz * c->ds[2];
     } else if (c->other >= 0) {
       const int64_t wj = (int64_t)c->other * stride + t;
-      ff = N(fat)(s, c->other, p) + (M)s->gx[wj] * c->dn[0] + (M)s->gy[wj] * c->dn[1] + (M)s->gz[wj] * c->dn[2];
+      if (sizeof(S) < sizeof(M))
+        ff = (M)(s->f[(int64_t)c->other * s->nv + p] + s->gx[wj] * (S)c->dn[0] + s->gy[wj] * (S)c->dn[1] +
+                 s->gz[wj] * (S)c->dn[2]);
+      else
+        ff = N(fat)(s, c->other, p) + (M)s->gx[wj] * c->dn[0] + (M)s->gy[wj] * c->dn[1] + (M)s->gz[wj] * c->dn[2];
     } else if (kind == KIN_BC_SYMMETRY) {
       const int pm = p ^ s->bf[c->bface].mirror_xor;
       const M fm = N(fat)(s, cell, pm);
