@@ -127,7 +127,7 @@ def build_case(args):
     return setup, host, time.time() - t0
 
 
-def cpu_baseline(args, setup_time_budget=30.0):
+def cpu_baseline(args, steps=None, warmup=1):
     """The reference's own CPU kinetic path (oracle/_ref/libgsisref.so: KineticSolver + OpenMP CpuBackend) on the
     same tube mesh with a reduced velocity grid (a bounded sample); falls back to the C port of oracle/."""
     import numpy as np
@@ -137,7 +137,8 @@ def cpu_baseline(args, setup_time_budget=30.0):
     nv_s = args.cpu_nv
     cores = os.cpu_count() or 1
     mesh = tube.tube_mesh()
-    sample = f"tube 134,528 cells x {nv_s}^3 velocities, {args.cpu_steps} CIS iteration(s), FP64"
+    steps = args.cpu_steps if steps is None else max(1, steps)
+    sample = f"tube 134,528 cells x {nv_s}^3 velocities, {steps} CIS iteration(s), FP64"
     try:
         from oracle import ref
 
@@ -150,11 +151,12 @@ def cpu_baseline(args, setup_time_budget=30.0):
                              kinetic={"precision": args.precision if args.precision != "mixed" else "fp32"})
         case = ref.RefCase(rm, spec)
         case.init_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
-        case.sweep()  # warm-up
-        t0 = time.perf_counter()
-        for _ in range(args.cpu_steps):
+        for _ in range(max(1, warmup)):
             case.sweep()
-        dt = (time.perf_counter() - t0) / args.cpu_steps
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            case.sweep()
+        dt = (time.perf_counter() - t0) / steps
         kind = "reference"
         inner = case.inner_sweeps
         nc = case.setup.n_cells
@@ -165,11 +167,12 @@ def cpu_baseline(args, setup_time_budget=30.0):
         setup, host = tube.tube_case(delta=10.0, nv=nv_s, precision=args.precision)
         sol = KineticSolver(setup, host, OracleBackend(setup))
         sol.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
-        sol.sweep()
-        t0 = time.perf_counter()
-        for _ in range(args.cpu_steps):
+        for _ in range(max(1, warmup)):
             sol.sweep()
-        dt = (time.perf_counter() - t0) / args.cpu_steps
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            sol.sweep()
+        dt = (time.perf_counter() - t0) / steps
         kind = "port"
         inner = host.inner_sweeps
         nc = setup.n_cells
@@ -182,9 +185,9 @@ def cpu_baseline(args, setup_time_budget=30.0):
 def run_reference_arm(args, rank):
     if rank != 0:
         return
-    cb = cpu_baseline(args)
+    cb = cpu_baseline(args, steps=args.steps, warmup=args.warmup)
     line = {"impl": "reference", "metric": "cell_velocity_updates_per_s", "value": cb["value"],
-            "unit": cb["unit"], "n_gpus": args.gpus, "steps": args.cpu_steps, "warmup": 1,
+            "unit": cb["unit"], "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * cb["seconds_per_iteration"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32"}[args.precision],
             "data": "synthetic", "config": workload_config(args),
