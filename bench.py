@@ -101,6 +101,18 @@ class ClockSampler:
                 "samples": len(rows), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(values, ws, device="cuda"):
+    """Element-wise maximum of per-rank timings over all ranks (every rank gets it); identity for one rank."""
+    if ws <= 1:
+        return [float(x) for x in values]
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x) for x in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
@@ -361,12 +373,7 @@ def main():
     bytes_d2h = per_prepare_d2h + inner * nc * 8 + (inner - 1) * 20 * nb * 8
     bytes_h2d = per_prepare_h2d + (inner - 1) * nb * 6 * 8
 
-    if ws > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([t_wall, device_busy], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_wall, device_busy = float(t[0]), float(t[1])
+    t_wall, device_busy = max_over_ranks([t_wall, device_busy], ws)
 
     updates = float(nc) * nv * inner * args.steps
     value = updates * ws / device_busy

@@ -1,0 +1,63 @@
+"""Size-independent properties at the benchmark's full size: the tube of 134,528 cells with 32^3 velocities
+(f 35 GB, work arrays 141 GB in FP64), where the oracle would take hours.
+
+* a uniform rest equilibrium with equal inlet and outlet pressures is a fixed point of the CIS iteration;
+* one CIS iteration is bitwise reproducible, and splitting the velocities into two chunks changes only the summation
+  order of the velocity sums;
+* mixed precision stays within FP32 accuracy of FP64.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(setup, host, iters, **kw):
+    from gsis_sim_b200.backend import B200Backend
+    from gsis_sim_b200.solver import KineticSolver
+
+    with B200Backend(setup, **kw) as be:
+        sol = KineticSolver(setup, host, be)
+        sol.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
+        m0 = sol.moments().copy()
+        info = None
+        for _ in range(iters):
+            info = sol.sweep()
+        return m0, sol.moments().copy(), sol.residual_cell.copy(), info.residual, sol.mass_flow()
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("no CUDA device")
+    return True
+
+
+def test_rest_equilibrium_is_a_fixed_point(gpu):
+    from gsis_sim_b200 import tube
+
+    setup, host = tube.tube_case(delta=10.0, nv=32, precision="fp64", p_out=1.0)
+    m0, m1, _, residual, mdot = _run(setup, host, 2)
+    assert np.max(np.abs(m1[:, :5] - m0[:, :5])) / np.max(np.abs(m0[:, :5])) < 1e-12
+    assert np.max(np.abs(m1[:, 1:4])) < 1e-12
+    assert residual < 1e-12
+    assert abs(mdot[2]) < 1e-12
+
+
+def test_reproducible_and_chunk_independent(gpu):
+    from gsis_sim_b200 import tube
+
+    setup, host = tube.tube_case(delta=10.0, nv=32, precision="fp64")
+    a = _run(setup, host, 1)
+    b = _run(setup, host, 1)
+    c = _run(setup, host, 1, velocity_chunk=setup.nv // 2)
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    assert np.max(np.abs(a[1] - c[1])) / np.max(np.abs(a[1])) < 1e-12
+    assert np.max(np.abs(a[2] - c[2])) / np.max(np.abs(a[2])) < 1e-12
+    # mixed precision after the same iteration: FP32 accuracy on the macroscopic fields
+    sm, hm = tube.tube_case(delta=10.0, nv=32, precision="mixed")
+    d = _run(sm, hm, 1)
+    rel = np.abs(a[1][:, :5] - d[1][:, :5]) / np.maximum(np.abs(a[1][:, :5]), 1e-3)
+    assert np.max(rel) < 1e-4
