@@ -26,6 +26,8 @@ class PolyMesh:
     patch_names: list = field(default_factory=list)
     patch_start: np.ndarray = None
     patch_count: np.ndarray = None
+    patch_kinds: list = field(default_factory=list)  # .pmesh patch kinds (informational: wall, inlet, ...)
+    metadata: dict = field(default_factory=dict)
 
     @property
     def n_faces(self) -> int:
