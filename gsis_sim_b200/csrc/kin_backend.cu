@@ -741,7 +741,7 @@ struct Backend final : KinHandle {
         if (s >= e) continue;
         for (int b = 0; b < n_blocks; ++b) {
           if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
-          const int tile = staged_ne != 0 ? kin::kTileVel : kin::kSweepTile;
+          const int tile = staged_ne != 0 ? 32 * kin::SweepTile<P>::kU : kin::kSweepTile;
           for (int t = s; t < e; t += tile)
             items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + tile, e) - k0, 0));
         }

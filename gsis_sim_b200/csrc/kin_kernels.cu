@@ -837,9 +837,9 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep_pass(View<S, M> v, S
 
 // ---------------------------------------------------------------------------------------------------------
 // staged LU-SGS block pass (k_sweep_tiles): the recurrence of k_sweep_pass, organised for instruction economy.
-//  * One CTA of kTileWarps warps per (direction group, block, tile of kTileVel velocities); a thread carries
-//    kTileU velocities (lane, lane + 32, ...) through every stencil entry, so the per-entry work that does not
-//    depend on the velocity (entry fetch, kind decode, addressing) is shared by kTileU velocities.
+//  * One CTA of kTileThreadsSweep threads per (direction group, block, tile of 32 * kU velocities); a thread carries
+//    SweepTile<M>::kU velocities (lane, lane + 32, ...) through every stencil entry, so the per-entry work that does not
+//    depend on the velocity (entry fetch, kind decode, addressing) is shared by SweepTile<M>::kU velocities.
 //  * The chain's levels are split on the host into sub-levels of at most kStageCells cells and kStageEntries
 //    entries, stored contiguously with each entry's kind for this chain precomputed (periodic, boundary,
 //    in-block lower, in-block upper, other block); the next sub-level is copied into shared memory with
@@ -893,13 +893,13 @@ __device__ __forceinline__ M pos_part(M af) { return af > M(0) ? af : M(0); }
 template <class M>
 __device__ __forceinline__ M neg_part(M af) { return af > M(0) ? M(0) : af; }
 
-// forward value of kTileU velocities of one cell; First: first block pass (no previous Delta f)
+// forward value of SweepTile<M>::kU velocities of one cell; First: first block pass (no previous Delta f)
 template <class S, class M, int NE, bool First>
 __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
-                                                  const StageE<M>* E, int4 p, const int (&t)[kTileU],
-                                                  const bool (&ok)[kTileU], const M (&x)[kTileU],
-                                                  const M (&y)[kTileU], const M (&z)[kTileU]) {
-  M val[NE][kTileU];
+                                                  const StageE<M>* E, int4 p, const int (&t)[SweepTile<M>::kU],
+                                                  const bool (&ok)[SweepTile<M>::kU], const M (&x)[SweepTile<M>::kU],
+                                                  const M (&y)[SweepTile<M>::kU], const M (&z)[SweepTile<M>::kU]) {
+  M val[NE][SweepTile<M>::kU];
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     const uint32_t code = j < p.z ? E[p.y + j].code : 0u;
@@ -908,16 +908,16 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
     const bool load = kind == kKindLower || (!First && kind == kKindOther);
     const S* src = kind == kKindLower ? a.out : a.dprev;
 #pragma unroll
-    for (int u = 0; u < kTileU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(src[row + t[u]]) : M(0);
+    for (int u = 0; u < SweepTile<M>::kU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(src[row + t[u]]) : M(0);
   }
   const int64_t crow = static_cast<int64_t>(p.x) * a.stride;
-  M own[kTileU];
+  M own[SweepTile<M>::kU];
 #pragma unroll
-  for (int u = 0; u < kTileU; ++u) own[u] = ok[u] ? static_cast<M>(__ldcs(a.R + crow + t[u])) : M(0);
+  for (int u = 0; u < SweepTile<M>::kU; ++u) own[u] = ok[u] ? static_cast<M>(__ldcs(a.R + crow + t[u])) : M(0);
   const M diag = v.cp[p.x].diag;
-  M ap[kTileU], lo[kTileU], ext[kTileU];  // ext: am_out (first pass) or Lout (later passes)
+  M ap[SweepTile<M>::kU], lo[SweepTile<M>::kU], ext[SweepTile<M>::kU];  // ext: am_out (first pass) or Lout (later passes)
 #pragma unroll
-  for (int u = 0; u < kTileU; ++u) ap[u] = lo[u] = ext[u] = M(0);
+  for (int u = 0; u < SweepTile<M>::kU; ++u) ap[u] = lo[u] = ext[u] = M(0);
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     if (j >= p.z) break;
@@ -926,7 +926,7 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
     if (kind == kKindPeriodic) continue;
     const M s0 = e.s[0], s1 = e.s[1], s2 = e.s[2];
 #pragma unroll
-    for (int u = 0; u < kTileU; ++u) {
+    for (int u = 0; u < SweepTile<M>::kU; ++u) {
       const M af = x[u] * s0 + y[u] * s1 + z[u] * s2;
       ap[u] += pos_part(af);
       if (kind == kKindLower) lo[u] += neg_part(af) * val[j][u];
@@ -937,7 +937,7 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
     }
   }
 #pragma unroll
-  for (int u = 0; u < kTileU; ++u) {
+  for (int u = 0; u < SweepTile<M>::kU; ++u) {
     if (!ok[u]) continue;
     const M am_out = First ? ext[u] : M(0), Lout = First ? M(0) : ext[u];
     const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out;
@@ -945,33 +945,33 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
   }
 }
 
-// backward value of kTileU velocities of one cell (and f += Delta f in the last pass)
+// backward value of SweepTile<M>::kU velocities of one cell (and f += Delta f in the last pass)
 template <class S, class M, int NE, bool First>
 __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
-                                                   const StageE<M>* E, int4 p, const int (&t)[kTileU],
-                                                   const bool (&ok)[kTileU], const M (&x)[kTileU],
-                                                   const M (&y)[kTileU], const M (&z)[kTileU]) {
-  M val[NE][kTileU];
+                                                   const StageE<M>* E, int4 p, const int (&t)[SweepTile<M>::kU],
+                                                   const bool (&ok)[SweepTile<M>::kU], const M (&x)[SweepTile<M>::kU],
+                                                   const M (&y)[SweepTile<M>::kU], const M (&z)[SweepTile<M>::kU]) {
+  M val[NE][SweepTile<M>::kU];
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     const uint32_t code = j < p.z ? E[p.y + j].code : 0u;
     const bool load = (code >> kKindShift) == kKindUpper;
     const int64_t row = static_cast<int64_t>(code & kIndexMask) * a.stride;
 #pragma unroll
-    for (int u = 0; u < kTileU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(a.out[row + t[u]]) : M(0);
+    for (int u = 0; u < SweepTile<M>::kU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(a.out[row + t[u]]) : M(0);
   }
   const int64_t crow = static_cast<int64_t>(p.x) * a.stride;
   const int64_t frow = static_cast<int64_t>(p.x) * v.nv + a.k0;
-  M own[kTileU], fv[kTileU];
+  M own[SweepTile<M>::kU], fv[SweepTile<M>::kU];
 #pragma unroll
-  for (int u = 0; u < kTileU; ++u) {
+  for (int u = 0; u < SweepTile<M>::kU; ++u) {
     own[u] = ok[u] ? static_cast<M>(a.out[crow + t[u]]) : M(0);
     fv[u] = (ok[u] && a.update_f) ? static_cast<M>(__ldcs(v.f + frow + t[u])) : M(0);
   }
   const M diag = v.cp[p.x].diag;
-  M ap[kTileU], up[kTileU], am_out[kTileU];
+  M ap[SweepTile<M>::kU], up[SweepTile<M>::kU], am_out[SweepTile<M>::kU];
 #pragma unroll
-  for (int u = 0; u < kTileU; ++u) ap[u] = up[u] = am_out[u] = M(0);
+  for (int u = 0; u < SweepTile<M>::kU; ++u) ap[u] = up[u] = am_out[u] = M(0);
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     if (j >= p.z) break;
@@ -980,7 +980,7 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
     if (kind == kKindPeriodic) continue;
     const M s0 = e.s[0], s1 = e.s[1], s2 = e.s[2];
 #pragma unroll
-    for (int u = 0; u < kTileU; ++u) {
+    for (int u = 0; u < SweepTile<M>::kU; ++u) {
       const M af = x[u] * s0 + y[u] * s1 + z[u] * s2;
       ap[u] += pos_part(af);
       if (kind == kKindUpper) up[u] += neg_part(af) * val[j][u];
@@ -988,7 +988,7 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
     }
   }
 #pragma unroll
-  for (int u = 0; u < kTileU; ++u) {
+  for (int u = 0; u < SweepTile<M>::kU; ++u) {
     if (!ok[u]) continue;
     const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out[u];
     const M df = own[u] - up[u] / D;
@@ -997,18 +997,8 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
   }
 }
 
-// resident CTAs per SM of k_sweep_tiles: FP32 arithmetic leaves room for six (measured 9% faster than four)
-template <class M>
-struct SweepOcc {
-  static constexpr int kBlocks = 6;
-};
-template <>
-struct SweepOcc<double> {
-  static constexpr int kBlocks = kTileMinBlocks;
-};
-
 template <class S, class M, int NE, bool First>
-__global__ void __launch_bounds__(kTileThreadsSweep, SweepOcc<M>::kBlocks) k_sweep_tiles(View<S, M> v, SweepArgs<S, M> a) {
+__global__ void __launch_bounds__(kTileThreadsSweep, SweepTile<M>::kBlocks) k_sweep_tiles(View<S, M> v, SweepArgs<S, M> a) {
   constexpr int W = kTileThreadsSweep / 32;
   __shared__ __align__(16) StageBuf<M> sh_buf[2];
   __shared__ int32_t sh_sc[kMaxSubLevels + 1], sh_se[kMaxSubLevels + 1];
@@ -1022,11 +1012,11 @@ __global__ void __launch_bounds__(kTileThreadsSweep, SweepOcc<M>::kBlocks) k_swe
     sh_sc[k] = a.sub_cells[s0 + k];
     sh_se[k] = a.sub_entries[s0 + k];
   }
-  int t[kTileU];
-  bool ok[kTileU];
-  M x[kTileU], y[kTileU], z[kTileU];
+  int t[SweepTile<M>::kU];
+  bool ok[SweepTile<M>::kU];
+  M x[SweepTile<M>::kU], y[SweepTile<M>::kU], z[SweepTile<M>::kU];
 #pragma unroll
-  for (int u = 0; u < kTileU; ++u) {
+  for (int u = 0; u < SweepTile<M>::kU; ++u) {
     t[u] = it.y + lane + 32 * u;
     ok[u] = t[u] < it.z;
     const int q = a.k0 + (ok[u] ? t[u] : it.y);

@@ -27,10 +27,20 @@ struct StageE {
   M s[3];
 };
 
-constexpr int kTileU = 4;                    // velocities per thread of k_sweep_tiles
-constexpr int kTileThreadsSweep = 128;       // threads of one k_sweep_tiles CTA
-constexpr int kTileMinBlocks = 4;            // resident CTAs per SM the FP64 register budget is sized for
-constexpr int kTileVel = 32 * kTileU;        // velocities of one k_sweep_tiles CTA
+constexpr int kTileThreadsSweep = 128;  // threads of one k_sweep_tiles CTA
+
+// k_sweep_tiles shape per arithmetic type: velocities per thread (a CTA covers 32 * kU velocities) and the resident
+// CTAs per SM its register budget is sized for
+template <class M>
+struct SweepTile {
+  static constexpr int kU = 4;
+  static constexpr int kBlocks = 6;
+};
+template <>
+struct SweepTile<double> {
+  static constexpr int kU = 2;
+  static constexpr int kBlocks = 6;
+};
 
 // arguments of one LU-SGS block pass over a velocity chunk
 template <class S, class M>
