@@ -448,13 +448,13 @@ __device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int c
 // registers per velocity, so three CTAs fit)
 template <class M>
 struct TileOcc {
-  static constexpr int kGradient = 3;
+  static constexpr int kGradient = 4;
   static constexpr int kResidual = 3;
-  static constexpr int kGradientU = 4;  // velocities per thread of the gradient
+  static constexpr int kGradientU = 2;  // velocities per thread of the gradient
 };
 template <>
 struct TileOcc<double> {
-  static constexpr int kGradient = 3;
+  static constexpr int kGradient = 4;
   static constexpr int kResidual = 2;
   static constexpr int kGradientU = 2;
 };
