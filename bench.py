@@ -134,8 +134,11 @@ def build_case(args):
     from gsis_sim_b200 import tube
 
     t0 = time.time()
+    from gsis_sim_b200 import kinetic_setup as ks
+
     mesh_kw = None if args.nx == 100 else {"n_x": args.nx}
-    setup, host = tube.tube_case(delta=10.0, nv=args.nv, precision=args.precision, mesh_kw=mesh_kw)
+    grid = ks.VelocityGrid.clustered((args.nv,) * 3, 6.0, 2.0) if args.grid == "clustered" else None
+    setup, host = tube.tube_case(delta=10.0, nv=args.nv, precision=args.precision, mesh_kw=mesh_kw, grid=grid)
     return setup, host, time.time() - t0
 
 
@@ -209,8 +212,10 @@ def run_reference_arm(args, rank):
 
 
 def workload_config(args, cb_nv=None, n_cells=134528):
-    return {"workload": f"kinetic CIS iteration, O-grid tube + reservoir {n_cells} cells, uniform {args.nv}^3 "
-                        f"velocities on [-5,5]^3, delta 10, {args.precision}",
+    grid = (f"uniform {args.nv}^3 velocities on [-5,5]^3" if getattr(args, "grid", "uniform") == "uniform" else
+            f"clustered (sinh, stretch 2) {args.nv}^3 velocities on [-6,6]^3 with quadrature weights")
+    return {"workload": f"kinetic CIS iteration, O-grid tube + reservoir {n_cells} cells, {grid}, delta 10, "
+                        f"{args.precision}",
             "cells": n_cells, "velocities": (cb_nv or args.nv) ** 3, "inner_sweeps": 4, "block_passes": 2,
             "sweep_order": "octant", "equilibrium": "discrete",
             "l2": "no flush: f and the work arrays (tens of GB) exceed the 126 MB L2"}
@@ -304,6 +309,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"])
     ap.add_argument("--nv", type=int, default=32)
+    ap.add_argument("--grid", default="uniform", choices=["uniform", "clustered"],
+                    help="uniform nv^3 on [-5,5]^3 (the parity grid) or sinh-clustered nv^3 on [-6,6]^3 with weights")
     ap.add_argument("--cpu-nv", type=int, default=8)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -83,6 +83,18 @@ class VelocityGrid:
     def uniform(self) -> bool:
         return self.nodes is None and self.weights is None
 
+    @classmethod
+    def clustered(cls, n, vmax: float, stretch: float = 2.0) -> "VelocityGrid":
+        """Nonuniform tensor grid clustered near zero: the midpoint rule in s on (-1, 1) mapped by
+        xi = vmax sinh(c s) / sinh(c) (c = stretch), weights d xi / d s * (2 / n) per axis. Symmetric about zero, so
+        symmetry planes keep exact mirror pairs; an extension of the reference's uniform grids."""
+        nodes, weights = [], []
+        for m in n:
+            sk = -1.0 + (2.0 * np.arange(m) + 1.0) / m
+            nodes.append(vmax * np.sinh(stretch * sk) / np.sinh(stretch))
+            weights.append(vmax * stretch * np.cosh(stretch * sk) / np.sinh(stretch) * (2.0 / m))
+        return cls(n=tuple(n), lo=(-vmax,) * 3, hi=(vmax,) * 3, nodes=tuple(nodes), weights=tuple(weights))
+
     def delta(self, a):
         return (self.hi[a] - self.lo[a]) / self.n[a]
 

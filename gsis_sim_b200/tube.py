@@ -130,14 +130,16 @@ def tube_mesh(R=1.0, L=5.0, n_c=16, n_r=10, n_x=100, res_length=4.0, res_half=2.
     return build_from_cells(pts, cell_faces, names, classify)
 
 
-def tube_case(delta=10.0, nv=32, vmax=5.0, precision="fp64", p_out=0.01, omega=0.81, mesh_kw=None, **params):
+def tube_case(delta=10.0, nv=32, vmax=5.0, precision="fp64", p_out=0.01, omega=0.81, mesh_kw=None, grid=None,
+              **params):
     """The kinetic tube case: inlet p = 1, T = 1; reservoir outlet p = p_out; diffuse walls T = 1; rarefaction delta;
-    uniform nv^3 velocity grid on [-vmax, vmax]^3 (units sqrt(R T0)). Returns (setup, host)."""
+    uniform nv^3 velocity grid on [-vmax, vmax]^3 (units sqrt(R T0)) unless `grid` is given. Returns (setup, host)."""
     mesh = tube_mesh(**(mesh_kw or {}))
     gas = ks.Gas(omega=omega)
     cond = ks.Conditions(L_ref=1.0, T0=273.15, delta_rp=delta)
     bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("wall", "diffuse_wall", T=1.0),
            ks.BC("back", "diffuse_wall", T=1.0), ks.BC("outlet", "pressure_outlet", p=p_out)]
-    grid = ks.VelocityGrid(n=(nv, nv, nv), lo=(-vmax,) * 3, hi=(vmax,) * 3)
+    if grid is None:
+        grid = ks.VelocityGrid(n=(nv, nv, nv), lo=(-vmax,) * 3, hi=(vmax,) * 3)
     kp = ks.KineticParams(precision=precision, **params)
     return ks.build_kinetic_setup(mesh, gas, cond, bcs, grid, kp)
