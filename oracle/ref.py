@@ -232,10 +232,6 @@ class RefCase:
         if rc != 0:
             raise KineticError(self.L.ref_error().decode())
 
-    def _chk(self, rc):
-        if rc != 0:
-            raise KineticError(self.L.ref_error().decode())
-
     def __del__(self):
         if getattr(self, "h", None):
             self.L.ref_case_free(self.h)
