@@ -7,7 +7,7 @@ it. The same descriptor feeds the CUDA library and (in tests) the CPU checkers.
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field, fields
+from dataclasses import dataclass, field
 
 import numpy as np
 

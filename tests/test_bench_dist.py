@@ -3,7 +3,6 @@ reports the element-wise maximum of the ranks' timings."""
 import os
 import socket
 
-import pytest
 
 
 def _free_port():

@@ -3,7 +3,6 @@
 This pins the oracle: every operation of the golden sequence must agree with the reference's own CpuBackend
 (src/kinetic/kinetic_backend_cpu.cpp) within the reference's GPU-vs-CPU tolerances.
 """
-import numpy as np
 import pytest
 
 from tests import common
