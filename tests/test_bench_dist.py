@@ -4,7 +4,6 @@ import os
 import socket
 
 
-
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
