@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-KIN_ABI_VERSION = 1
+KIN_ABI_VERSION = 2
 KIN_OK = 0
 KIN_E_ARG, KIN_E_CUDA, KIN_E_MEMORY, KIN_E_STATE, KIN_E_TIMEOUT = -1, -2, -3, -4, -5
 KIN_NOALLOC_MAX_STATES = 4096
@@ -54,6 +54,7 @@ class KinSetupDesc(C.Structure):
         ("deq_criterion", C.c_double), ("deq_tolerance", C.c_double), ("deq_max_iterations", C.c_int32),
         ("n_maxwell_faces", C.c_int32), ("maxwell_offset", _lp), ("maxwell_specular_fraction", _dp),
         ("grid_to_storage", _ip), ("grid_n", C.c_int32 * 3),
+        ("deq_nv", C.c_int32), ("deq_xi_x", _dp), ("deq_xi_y", _dp), ("deq_xi_z", _dp), ("deq_weights", _dp),
     ]
 
 
@@ -79,12 +80,13 @@ _ARRAY_DTYPES = {
     "bface_patch": np.int32, "bface_geom": np.float64, "volume": np.float64, "vdt": np.float64,
     "block_offsets": np.int32, "sweep_order": np.int32, "sweep_pos": np.int32, "sweep_dir_of": np.uint8,
     "maxwell_offset": np.int64, "maxwell_specular_fraction": np.float64, "grid_to_storage": np.int32,
+    "deq_xi_x": np.float64, "deq_xi_y": np.float64, "deq_xi_z": np.float64, "deq_weights": np.float64,
 }
 _SCALARS = [
     "precision", "device", "n_cells", "nv", "n_bfaces", "n_blocks", "weight", "n_sweep_dirs", "limiter_mode",
     "positivity", "diag_scale", "interface_damping", "block_passes", "negative_check_mode", "velocity_chunk",
     "mu0", "omega", "Pr", "cold_bgk_temperature", "discrete_eq", "deq_fallback_collisionless", "deq_criterion",
-    "deq_tolerance", "deq_max_iterations", "n_maxwell_faces",
+    "deq_tolerance", "deq_max_iterations", "n_maxwell_faces", "deq_nv",
 ]
 _VEC3 = ["deq_lo", "deq_hi", "deq_d", "grid_n"]
 
@@ -164,7 +166,8 @@ class SetupArrays:
             "bface_mirror_xor": nb, "bface_patch": nb, "bface_geom": 7 * nb, "volume": nc, "vdt": nc,
             "block_offsets": d.n_blocks + 1, "sweep_order": nd * nc, "sweep_pos": nd * nc,
             "sweep_dir_of": nv if nd > 0 else 0, "maxwell_offset": nb, "maxwell_specular_fraction": nb,
-            "grid_to_storage": nv,
+            "grid_to_storage": nv, "deq_xi_x": d.deq_nv, "deq_xi_y": d.deq_nv, "deq_xi_z": d.deq_nv,
+            "deq_weights": d.deq_nv,
         }
         for k, n in sizes.items():
             p = getattr(d, k)
@@ -230,6 +233,8 @@ def declare_backend_api(lib, prefix: str, handle_type=C.c_void_p):
         "chunk_width": [h, _ip],
         "discrete_maxwell": [h, _dp, C.c_int64, C.c_double, _dp, _ip],
         "discrete_maxwell_noalloc": [h, _dp, C.c_int64, C.c_double, _dp, _ip],
+        "moment_sums": [h, _dp, C.c_int64],
+        "set_moments": [h, _dp, C.c_int64],
     }
     for name, args in sig.items():
         if not hasattr(lib, prefix + name):

@@ -63,6 +63,17 @@ class KineticBackendABI:
         self._call("compute_moments", abi.as_ptr(out, C.c_double), out.size)
         return out.reshape(self.n_cells, abi.MOMENTS_PER_CELL)
 
+    def moment_sums(self) -> np.ndarray:
+        """The 13 shifted velocity sums per cell over the stored velocities, not finalised (velocity sharding)."""
+        out = np.empty(self.n_cells * 13, dtype=np.float64)
+        self._call("moment_sums", abi.as_ptr(out, C.c_double), out.size)
+        return out.reshape(self.n_cells, 13)
+
+    def set_moments(self, moments) -> None:
+        """Install moments reduced over all velocity shards (they feed update_cell_params) and move the shift."""
+        m = np.ascontiguousarray(moments, dtype=np.float64).ravel()
+        self._call("set_moments", abi.as_ptr(m, C.c_double), m.size)
+
     def scale_distribution(self, s: float) -> None:
         self._call("scale_distribution", C.c_double(s))
 

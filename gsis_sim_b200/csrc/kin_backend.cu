@@ -157,6 +157,8 @@ struct KinHandle {
   virtual void discrete_maxwell(const double* states, int64_t n, double tol, double* out, int32_t* result) = 0;
   virtual void discrete_maxwell_noalloc(const double* states, int64_t n, double tol, double* out,
                                         int32_t* result) = 0;
+  virtual void moment_sums(double* out, int64_t n) = 0;
+  virtual void set_moments(const double* m, int64_t n) = 0;
 };
 
 // Scratch of kin_discrete_maxwell_noalloc: static device memory of this module (one copy per device), laid out as
@@ -230,6 +232,10 @@ struct Backend final : KinHandle {
 
   // device arrays
   DevBuf<M> xi_x, xi_y, xi_z;
+  // full velocity grid of the discrete equilibrium when this handle stores one shard (else unused)
+  DevBuf<M> dq_x, dq_y, dq_z;
+  DevBuf<double> dq_xd, dq_yd, dq_zd, dq_w;
+  int32_t dq_nv = 0;
   DevBuf<double> xid_x, xid_y, xid_z, wts;
   DevBuf<int32_t> csr_off;
   DevBuf<CsrE<M>> csr;
@@ -438,6 +444,21 @@ struct Backend final : KinHandle {
       hw.resize(nv);
       for (int q = 0; q < nv; ++q) hw[q] = d.weights[perm[q]];
       wts.upload(hw.data(), nv, stream);
+    }
+    dq_nv = 0;
+    if (d.deq_nv > 0) {
+      KCHECK(d.deq_xi_x && d.deq_xi_y && d.deq_xi_z, "deq_nv > 0 needs deq_xi_x / y / z");
+      dq_nv = d.deq_nv;
+      const size_t m = static_cast<size_t>(dq_nv);
+      std::vector<M> tx(d.deq_xi_x, d.deq_xi_x + m), ty(d.deq_xi_y, d.deq_xi_y + m), tz(d.deq_xi_z, d.deq_xi_z + m);
+      dq_x.upload(tx.data(), m, stream);
+      dq_y.upload(ty.data(), m, stream);
+      dq_z.upload(tz.data(), m, stream);
+      dq_xd.upload(d.deq_xi_x, m, stream);
+      dq_yd.upload(d.deq_xi_y, m, stream);
+      dq_zd.upload(d.deq_xi_z, m, stream);
+      if (d.deq_weights) dq_w.upload(d.deq_weights, m, stream);
+      KCUDA(cudaStreamSynchronize(stream));
     }
     d_perm.upload(perm.data(), nv, stream);
     d_inv.upload(inv.data(), nv, stream);
@@ -786,6 +807,15 @@ struct Backend final : KinHandle {
     v.specular = specular.p;
     v.specular_first = specular_first.p;
     v.grid_to_pos = grid_to_pos.p;
+    const bool shard = dq_nv > 0;
+    v.dq_x = shard ? dq_x.p : xi_x.p;
+    v.dq_y = shard ? dq_y.p : xi_y.p;
+    v.dq_z = shard ? dq_z.p : xi_z.p;
+    v.dq_xd = shard ? dq_xd.p : xid_x.p;
+    v.dq_yd = shard ? dq_yd.p : xid_y.p;
+    v.dq_zd = shard ? dq_zd.p : xid_z.p;
+    v.dq_w = shard ? dq_w.p : wts.p;
+    v.dq_nv = shard ? dq_nv : nv;
     if constexpr (kSplit) {
       kin::View<S, P>& w = pview;
       w.n_cells = nc;
@@ -812,6 +842,12 @@ struct Backend final : KinHandle {
       w.specular = pspecular.p;
       w.specular_first = pspecular_first.p;
       w.grid_to_pos = grid_to_pos.p;
+      // the FP32 kernels never solve the discrete equilibrium: only the FP64 grid is shared
+      w.dq_xd = v.dq_xd;
+      w.dq_yd = v.dq_yd;
+      w.dq_zd = v.dq_zd;
+      w.dq_w = v.dq_w;
+      w.dq_nv = v.dq_nv;
     }
   }
 
@@ -901,6 +937,31 @@ struct Backend final : KinHandle {
     KCUDA(cudaMemcpyAsync(out, moments.p, moments.bytes(), cudaMemcpyDeviceToHost, stream));
     timer.flush(timings);
     KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void moment_sums(double* out, int64_t n) override {
+    KCHECK(n == 13LL * nc, "length of the moment-sum output does not match");
+    timer.begin(PhaseTimer::kMoments, stream);
+    L::moment_sums(view, shift.p, staging_sums(), stream);
+    launched();
+    timer.end(stream);
+    KCUDA(cudaMemcpyAsync(out, sums.p, sizeof(double) * 13 * nc, cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void set_moments(const double* m, int64_t n) override {
+    KCHECK(n == 15LL * nc, "length of the moments does not match");
+    KCUDA(cudaMemcpyAsync(moments.p, m, moments.bytes(), cudaMemcpyHostToDevice, stream));
+    L::shift_from_moments(moments.p, shift.p, nc, stream);
+    launched();
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  DevBuf<double> sums;
+  double* staging_sums() {
+    if (sums.n != static_cast<size_t>(13) * nc) sums.alloc(static_cast<size_t>(13) * nc);
+    return sums.p;
   }
 
   void scale_distribution(double s) override {
@@ -1256,6 +1317,8 @@ int kin_discrete_maxwell_noalloc(KinHandle* h, const double* states, int64_t n, 
                                  int32_t* result) {
   return guard(h, [&] { h->discrete_maxwell_noalloc(states, n, tolerance, out, result); });
 }
+int kin_moment_sums(KinHandle* h, double* out, int64_t n) { return guard(h, [&] { h->moment_sums(out, n); }); }
+int kin_set_moments(KinHandle* h, const double* m, int64_t n) { return guard(h, [&] { h->set_moments(m, n); }); }
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains) {
   return guard(const_cast<KinHandle*>(h), [&] { h->schedule_info(max_levels, n_chains); });
 }

@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(kCellThreads)
 // ---------------------------------------------------------------------------------------------------------
 // 13 shifted sums in FP64 -> 15 moments (CpuBackend::compute_moments, kinetic_backend_cpu.cpp:92-120)
 // ---------------------------------------------------------------------------------------------------------
-template <class S, class M>
+template <class S, class M, bool Finalize>
 __global__ void __launch_bounds__(kCellThreads)
     k_moments(View<S, M> v, double* __restrict__ shift, double* __restrict__ out) {
   __shared__ double sh[kMomentSums * (kCellThreads / 32)];
@@ -74,6 +74,12 @@ __global__ void __launch_bounds__(kCellThreads)
     acc[12] += fc2 * cz;
   }
   block_sum<kMomentSums, kCellThreads>(acc, sh);
+  if (!Finalize) {  // raw sums of one velocity shard (kin_moment_sums); the shift stays
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < kMomentSums; ++k) out[kMomentSums * static_cast<int64_t>(c) + k] = acc[k];
+    }
+    return;
+  }
   if (threadIdx.x == 0) {
     double* m = out + 15 * static_cast<int64_t>(c);
     finalize_moments(acc, uniform ? v.weight : 1.0, u0x, u0y, u0z, m);
@@ -83,6 +89,13 @@ __global__ void __launch_bounds__(kCellThreads)
       shift[3 * static_cast<int64_t>(c) + 2] = m[3];
     }
   }
+}
+
+// the shift of the next moment sums after moments were installed from outside (kin_set_moments)
+__global__ void k_shift_from_moments(const double* __restrict__ m, double* __restrict__ shift, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n || !(m[15 * static_cast<int64_t>(c)] > 0.0)) return;
+  for (int a = 0; a < 3; ++a) shift[3 * static_cast<int64_t>(c) + a] = m[15 * static_cast<int64_t>(c) + 1 + a];
 }
 
 // f *= s ; moments (rho, p, sigma, q) *= s   (k_scale / k_scale_moments, kinetic_cuda_kernels.cu:207-219)
@@ -1155,7 +1168,7 @@ __global__ void __launch_bounds__(kCellThreads)
   const double* st = states + 5 * static_cast<int64_t>(i);
   Maxwell<double> m;
   double gamma[5];
-  const int r = block_discrete_maxwell_on<double, kCellThreads>(v.xid_x, v.xid_y, v.xid_z, v.wts, v.nv, v.weight, deq,
+  const int r = block_discrete_maxwell_on<double, kCellThreads>(v.dq_xd, v.dq_yd, v.dq_zd, v.dq_w, v.dq_nv, v.weight, deq,
                                                                st[0], st[1], st[2], st[3], st[4], nullptr, m, gamma,
                                                                sh_red, sh_state);
   if (threadIdx.x == 0) {
@@ -1215,7 +1228,17 @@ void Launch<S, M>::set_equilibrium(const View<S, M>& v, const double* states, do
 
 template <class S, class M>
 void Launch<S, M>::moments(const View<S, M>& v, double* shift, double* out, cudaStream_t st) {
-  if (v.n_cells > 0) k_moments<S, M><<<v.n_cells, kCellThreads, 0, st>>>(v, shift, out);
+  if (v.n_cells > 0) k_moments<S, M, true><<<v.n_cells, kCellThreads, 0, st>>>(v, shift, out);
+}
+
+template <class S, class M>
+void Launch<S, M>::moment_sums(const View<S, M>& v, double* shift, double* out, cudaStream_t st) {
+  if (v.n_cells > 0) k_moments<S, M, false><<<v.n_cells, kCellThreads, 0, st>>>(v, shift, out);
+}
+
+template <class S, class M>
+void Launch<S, M>::shift_from_moments(const double* moments, double* shift, int n, cudaStream_t st) {
+  if (n > 0) k_shift_from_moments<<<ceil_div(n, 256), 256, 0, st>>>(moments, shift, n);
 }
 
 template <class S, class M>

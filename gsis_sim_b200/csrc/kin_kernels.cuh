@@ -73,6 +73,16 @@ struct View {
   const int32_t* grid_to_pos;
   int32_t grid_n[3];
   DeqGrid deq;
+  // velocity grid of the discrete equilibrium: the stored velocities, or the full grid when this handle stores one
+  // shard of it (any order: only sums over it are taken)
+  const M* dq_x;
+  const M* dq_y;
+  const M* dq_z;
+  const double* dq_xd;
+  const double* dq_yd;
+  const double* dq_zd;
+  const double* dq_w;  // per-velocity weights, nullptr when uniform
+  int32_t dq_nv;
 };
 
 template <class S>
@@ -315,7 +325,7 @@ template <class S, class M, int B>
 __device__ inline int block_discrete_maxwell(const View<S, M>& v, double rho, double ux, double uy, double uz, double T,
                                              const CellParams<M>* poly, Maxwell<M>& out, double (&gamma)[5],
                                              double* sh_red, double* sh_state) {
-  return block_discrete_maxwell_on<M, B>(v.xi_x, v.xi_y, v.xi_z, v.wts, v.nv, v.weight, v.deq, rho, ux, uy, uz, T,
+  return block_discrete_maxwell_on<M, B>(v.dq_x, v.dq_y, v.dq_z, v.dq_w, v.dq_nv, v.weight, v.deq, rho, ux, uy, uz, T,
                                          poly, out, gamma, sh_red, sh_state);
 }
 

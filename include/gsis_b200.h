@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define KIN_ABI_VERSION 1
+#define KIN_ABI_VERSION 2
 
 /* status codes */
 #define KIN_OK 0
@@ -153,6 +153,15 @@ typedef struct KinSetupDesc {
   const double* maxwell_specular_fraction;   /* n_bfaces */
   const int32_t* grid_to_storage;            /* nv (NULL if no Maxwell walls) */
   int32_t grid_n[3];
+
+  /* velocity sharding (no reference counterpart): when the handle stores only a subset of the velocities (one shard
+     of the grid, the others on other GPUs), the discrete equilibrium is still solved on the full grid given here.
+     deq_nv == 0: the stored velocities are the full grid. */
+  int32_t deq_nv;
+  const double* deq_xi_x;
+  const double* deq_xi_y;
+  const double* deq_xi_z;
+  const double* deq_weights; /* NULL: every point has `weight` */
 } KinSetupDesc;
 
 /* InflowState (src/kinetic/kinetic_backend.hpp:45-50): scale * f_eq(rho, u, T); same memory layout */
@@ -261,6 +270,14 @@ int kin_discrete_maxwell_noalloc(KinHandle* h, const double* states, int64_t n, 
 /* LU-SGS level schedule statistics: number of levels of the longest (direction, block) chain and the total
    number of (direction, block) chains. */
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains);
+
+/* Velocity sharding (no reference counterpart; kin_compute_moments is the unsharded form): the 13 velocity sums of
+   every cell (sum of w f {1, c, c c (6), |c|^2 c}, c = xi - shift, with the handle's current shift) over the
+   velocities this handle stores, not finalised, so that the shards' sums can be added before finalising. */
+int kin_moment_sums(KinHandle* h, double* out, int64_t n);
+/* Velocity sharding: install the finalised moments (15 per cell, reduced over all shards) as the handle's moments
+   (they feed kin_update_cell_params) and move the shift to their velocity, as kin_compute_moments does. */
+int kin_set_moments(KinHandle* h, const double* moments, int64_t n);
 
 #ifdef __cplusplus
 }

@@ -453,8 +453,8 @@ int orc_deq_counts(OrcHandle* h, KinDeqCounts* out) {
   static void deq_states##SF(State##SF* s, const double* st, int64_t n, double tol, double* out, int32_t* res) { \
     _Pragma("omp parallel for schedule(dynamic, 1)")                                                           \
     for (int64_t i = 0; i < n; ++i)                                                                            \
-      res[i] = orc_deq_state_f64(s->xd_x, s->xd_y, s->xd_z, s->w, s->nv, s->weight, s->deq_lo, s->deq_hi,      \
-                                 s->deq_d, s->deq_crit, s->deq_maxit, tol, st + 5 * i, out + 5 * i);           \
+      res[i] = orc_deq_state_f64(s->dq_xd, s->dq_yd, s->dq_zd, s->dq_w, s->dq_nv, s->weight, s->deq_lo,         \
+                                 s->deq_hi, s->deq_d, s->deq_crit, s->deq_maxit, tol, st + 5 * i, out + 5 * i); \
   }
 DEQ_STATES(_f32)
 DEQ_STATES(_f64)
@@ -462,5 +462,16 @@ DEQ_STATES(_mix)
 
 int orc_discrete_maxwell(OrcHandle* h, const double* states, int64_t n, double tol, double* out, int32_t* result) {
   DISPATCH(h, deq_states, states, n, tol, out, result);
+  return KIN_OK;
+}
+
+int orc_moment_sums(OrcHandle* h, double* out, int64_t n) {
+  if (n != 13LL * orc_nc(h)) return orc_fail(h, "length of the moment-sum output does not match");
+  DISPATCH(h, moment_sums, out);
+  return KIN_OK;
+}
+int orc_set_moments(OrcHandle* h, const double* m, int64_t n) {
+  if (n != 15LL * orc_nc(h)) return orc_fail(h, "length of the moments does not match");
+  DISPATCH(h, set_moments, m);
   return KIN_OK;
 }

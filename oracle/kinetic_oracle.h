@@ -36,6 +36,8 @@ int orc_gsis_correction(OrcHandle* h, const double* w_half, const double* w_new,
                         int64_t* replaced);
 int orc_internal_face_mass_flux(OrcHandle* h, const int32_t* cells, const int32_t* entries, int64_t n, double* out);
 int orc_deq_counts(OrcHandle* h, KinDeqCounts* out);
+int orc_moment_sums(OrcHandle* h, double* out, int64_t n);
+int orc_set_moments(OrcHandle* h, const double* m, int64_t n);
 int orc_discrete_maxwell(OrcHandle* h, const double* states, int64_t n, double tolerance, double* out,
                          int32_t* result);
 

@@ -41,6 +41,10 @@ typedef struct {
   S *gx, *gy, *gz, *r;
   int32_t* deq_flags;
   int deq_valid;
+  /* velocity grid of the discrete equilibrium: the stored velocities, or the full grid of a velocity shard */
+  M *dq_x, *dq_y, *dq_z;
+  double *dq_xd, *dq_yd, *dq_zd, *dq_w;
+  int dq_nv, dq_own;
 } N(State);
 
 static inline M N(mexp)(M x) { return (sizeof(M) == sizeof(float)) ? (M)expf((float)x) : (M)exp((double)x); }
@@ -231,7 +235,7 @@ static int N(deq_seq)(const N(State) * s, double rho, double ux, double uy, doub
   double beta[5];
   orc_deq_initial_beta(rho, T, beta);
   const M fux = (M)ux, fuy = (M)uy, fuz = (M)uz;
-  const double w = s->w ? 1.0 : s->weight;
+  const double w = s->dq_w ? 1.0 : s->weight;
   double rel_prev = 1e300;
   for (int it = 0; it < s->deq_maxit; ++it) {
     N(Mx) m;
@@ -245,12 +249,12 @@ static int N(deq_seq)(const N(State) * s, double rho, double ux, double uy, doub
       m.B = (M)B;
     }
     double sums[20] = {0};
-    for (int p = 0; p < s->nv; ++p) {
-      const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
+    for (int p = 0; p < s->dq_nv; ++p) {
+      const M x = s->dq_x[p], y = s->dq_y[p], z = s->dq_z[p];
       const M cx = x - fux, cy = y - fuy, cz = z - fuz;
       M e = N(maxw)(&m, x, y, z);
       const M pm = poly ? N(spoly)(poly, cx, cy, cz, cx * cx + cy * cy + cz * cz) : (M)0;
-      if (s->w) e *= (M)s->w[p];
+      if (s->dq_w) e *= (M)s->dq_w[p];
       const M h = (M)0.5 * (cx * cx + cy * cy + cz * cz);
       M t[20];
       t[0] = e; t[1] = e * cx; t[2] = e * cy; t[3] = e * cz; t[4] = e * h;
@@ -327,6 +331,36 @@ static void N(compute_moments)(N(State) * s, double* out) {
     }
   }
   memcpy(out, s->moments, sizeof(double) * 15 * (size_t)s->nc);
+}
+
+/* the 13 shifted sums of one velocity shard, not finalised (velocity sharding; no reference counterpart) */
+static void N(moment_sums)(N(State) * s, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < s->nc; ++c) {
+    const double u0x = s->shift[3 * c], u0y = s->shift[3 * c + 1], u0z = s->shift[3 * c + 2];
+    double sums[13] = {0};
+    for (int p = 0; p < s->nv; ++p) {
+      double f = (double)s->f[(int64_t)c * s->nv + p];
+      if (s->w) f *= s->w[p];
+      const double cx = s->xd_x[p] - u0x, cy = s->xd_y[p] - u0y, cz = s->xd_z[p] - u0z;
+      const double t1 = f * cx, t2 = f * cy, t3 = f * cz, fc2 = f * (cx * cx + cy * cy + cz * cz);
+      sums[0] += f; sums[1] += t1; sums[2] += t2; sums[3] += t3;
+      sums[4] += t1 * cx; sums[5] += t2 * cy; sums[6] += t3 * cz;
+      sums[7] += t1 * cy; sums[8] += t2 * cz; sums[9] += t1 * cz;
+      sums[10] += fc2 * cx; sums[11] += fc2 * cy; sums[12] += fc2 * cz;
+    }
+    for (int k = 0; k < 13; ++k) out[13 * (int64_t)c + k] = sums[k];
+  }
+}
+
+/* install moments reduced over all shards and move the shift as compute_moments does */
+static void N(set_moments)(N(State) * s, const double* m) {
+  memcpy(s->moments, m, sizeof(double) * 15 * (size_t)s->nc);
+  for (int c = 0; c < s->nc; ++c) {
+    if (m[15 * (int64_t)c] > 0.0) {
+      for (int a = 0; a < 3; ++a) s->shift[3 * c + a] = m[15 * (int64_t)c + 1 + a];
+    }
+  }
 }
 
 static void N(scale)(N(State) * s, double sc) {
@@ -763,6 +797,33 @@ static N(State) * N(create)(const KinSetupDesc* d) {
     s->xi_z[p] = (M)d->xi_z[p];
   }
   s->w = d->weights ? orc_dup_d(d->weights, nv) : NULL;
+  if (d->deq_nv > 0) {
+    const int m = d->deq_nv;
+    s->dq_own = 1;
+    s->dq_nv = m;
+    s->dq_xd = orc_dup_d(d->deq_xi_x, m);
+    s->dq_yd = orc_dup_d(d->deq_xi_y, m);
+    s->dq_zd = orc_dup_d(d->deq_xi_z, m);
+    s->dq_w = d->deq_weights ? orc_dup_d(d->deq_weights, m) : NULL;
+    s->dq_x = (M*)malloc(sizeof(M) * m);
+    s->dq_y = (M*)malloc(sizeof(M) * m);
+    s->dq_z = (M*)malloc(sizeof(M) * m);
+    for (int p = 0; p < m; ++p) {
+      s->dq_x[p] = (M)d->deq_xi_x[p];
+      s->dq_y[p] = (M)d->deq_xi_y[p];
+      s->dq_z[p] = (M)d->deq_xi_z[p];
+    }
+  } else {
+    s->dq_own = 0;
+    s->dq_nv = nv;
+    s->dq_x = s->xi_x;
+    s->dq_y = s->xi_y;
+    s->dq_z = s->xi_z;
+    s->dq_xd = s->xd_x;
+    s->dq_yd = s->xd_y;
+    s->dq_zd = s->xd_z;
+    s->dq_w = s->w;
+  }
   s->csr_off = orc_dup_i(d->csr_offsets, nc + 1);
   const int n_csr = d->csr_offsets[nc];
   s->csr = (N(Csr)*)malloc(sizeof(N(Csr)) * (n_csr > 0 ? n_csr : 1));
@@ -822,6 +883,10 @@ static N(State) * N(create)(const KinSetupDesc* d) {
 }
 
 static void N(destroy)(N(State) * s) {
+  if (s->dq_own) {
+    void* own[] = {s->dq_x, s->dq_y, s->dq_z, s->dq_xd, s->dq_yd, s->dq_zd, s->dq_w};
+    for (size_t i = 0; i < sizeof(own) / sizeof(own[0]); ++i) free(own[i]);
+  }
   void* ptrs[] = {s->xi_x, s->xi_y, s->xi_z, s->xd_x, s->xd_y, s->xd_z, s->w, s->csr_off, s->csr, s->eps2, s->bf,
                   s->volume, s->vdt, s->block_off, s->order, s->pos, s->dir_of, s->mw_off, s->mw_frac, s->g2s,
                   s->spec, s->spec_first, s->in, s->cp, s->f, s->moments, s->shift, s->gx, s->gy, s->gz, s->r,
