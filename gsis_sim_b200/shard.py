@@ -174,6 +174,13 @@ class ShardedBackend:
     def gsis_correction(self, w_half, w_new):
         raise NotImplementedError("the GSIS correction's negativity rules are not sharded")
 
+    def launch_count(self):
+        return sum(be.launch_count() for be in self.backends)
+
+    def close(self):
+        for be in self.backends:
+            be.close()
+
     def take_timings(self):
         out = {}
         for be in self.backends:
