@@ -372,3 +372,20 @@ def case_setup(cfg: CaseConfig, precision: str | None = None, mesh=None):
     vg = cfg.velocity_grid
     grid = ks.VelocityGrid(n=tuple(vg["n"]), lo=tuple(vg["lo"]), hi=tuple(vg["hi"]))
     return ks.build_kinetic_setup(mesh, cfg.gas, cfg.conditions, bcs, grid, kinetic_params(cfg, precision))
+
+
+def output_sections(cfg: CaseConfig):
+    """parse_output_sections (src/kinetic/kinetic_output.cpp:70-76): the section cuts of [output]
+    (`mass_flow_sections`, a string of positions in L_ref units; `mass_flow_section_axis`, "x" by default). Any other
+    key of [output] is an error, as the reference's ModuleSection::finish makes it; an empty or missing string gives
+    no sections."""
+    from . import section as sec
+
+    out = cfg.output or {}
+    for k, v in out.items():
+        _check(k in ("mass_flow_sections", "mass_flow_section_axis"), f"[output] has unknown key {k}")
+        _check(isinstance(v, str), f"output.{k} must be a string")
+    try:
+        return sec.parse_section_spec(out.get("mass_flow_sections", ""), out.get("mass_flow_section_axis", "x"))
+    except sec.SectionError as e:
+        raise CaseError(str(e)) from e

@@ -520,3 +520,44 @@ class KineticSolver:
         mdot_in = -sum(pm[p] for p in range(len(pm)) if self.ptype[p] in (T_PRESSURE_INLET, T_MASS_FLOW_INLET))
         mdot_out = sum(pm[p] for p in range(len(pm)) if self.ptype[p] in (T_PRESSURE_OUTLET, T_VACUUM))
         return mdot_in * f, mdot_out * f, 0.5 * (mdot_in + mdot_out) * f
+
+    # ---- section cuts ------------------------------------------------------------------------------------------
+    def section_cuts(self, spec):
+        """section_cuts (src/kinetic/kinetic_solver.cpp:687-690): the cuts of `spec` on the internal (renumbered)
+        mesh, with the (cell, CSR entry) pairs the backend reads (build_sections, kinetic_solver.cpp:56-79).
+        Cached until the spec changes."""
+        from . import section as sec
+
+        if getattr(self, "_section_spec", None) == spec:
+            return self._section_cuts
+        h = self.h
+        if getattr(self, "_face_entry", None) is None:
+            self._face_neighbour, self._face_entry = sec.owner_entries(
+                self.s["csr_offsets"], self.s["csr_other"], h.csr_faces, h.owner, self.ni)
+        cuts = sec.build_section_cuts(h.owner, self._face_neighbour, h.cell_center, h.face_center, h.face_normal,
+                                      h.face_area, h.length_scale, spec)
+        faces = np.concatenate([c.faces for c in cuts]) if cuts else np.zeros(0, np.int64)
+        self._section_cells = np.asarray(h.owner)[faces].astype(np.int32)
+        self._section_entries = self._face_entry[faces].astype(np.int32)
+        self._section_spec = sec.SectionSpec(spec.axis, list(spec.positions))
+        self._section_cuts = cuts
+        return cuts
+
+    def section_mass_flow(self, spec) -> np.ndarray:
+        """section_mass_flow (src/kinetic/kinetic_solver.cpp:669-685): nondimensional mass flow through each cut of
+        `spec` (+axis direction) from the current f: prepare, the backend's discrete internal-face flux on the cut
+        faces, summed with the cut signs."""
+        if spec.empty():
+            return np.zeros(0)
+        self.prepare()
+        cuts = self.section_cuts(spec)
+        flux = self.backend.internal_face_mass_flux(self._section_cells, self._section_entries)
+        out = np.zeros(len(cuts))
+        k = 0
+        for i, c in enumerate(cuts):
+            s = 0.0
+            for j in range(len(c.faces)):
+                s += float(c.sign[j]) * flux[k]
+                k += 1
+            out[i] = s
+        return out

@@ -9,7 +9,8 @@ Each fixture holds
     sequence (set_equilibrium, compute_moments, update_cell_params, set_inflow, boundary_sums, 2 x sweep,
     gsis_correction, internal_face_mass_flux);
   * `solver.*`: the reference KineticSolver (src/kinetic/kinetic_solver.cpp) after a few CIS iterations from a
-    uniform state: residual history, moments, boundary fluxes and f (original numbering).
+    uniform state: residual history, moments, boundary fluxes, f (original numbering) and section mass flows
+    (KineticSolver::section_mass_flow, src/kinetic/kinetic_solver.cpp:669-685) at fixed x and y positions.
 The cases are the reference GPU tests' cases (tests/kinetic/test_kinetic_gpu.cpp:50-91, 160-173, 261-273) with a
 smaller velocity grid so that every fixture stays small.
 """
@@ -30,6 +31,8 @@ from oracle import ref  # noqa: E402
 MIXED_PATCHES = ["inlet", "outlet", "wall", "wall", "sym", "sym"]
 MIXED_BCS = [("inlet", "pressure_inlet", dict(T=1.0, p=1.1)), ("outlet", "pressure_outlet", dict(p=0.3)),
              ("wall", "diffuse_wall", dict(T=1.0, u=(0.1, 0.0, 0.05))), ("sym", "symmetry", {})]
+SECTION_X = [0.0, 0.13, 0.5, 0.5, 0.71, 0.99, 3.0]
+SECTION_Y = [0.3, 0.45]
 OLD_CIS = dict(sweep_order="block", inner_sweeps=1, inner_wall_update=False, block_passes=1, equilibrium="continuous")
 
 # name -> (mesh kwargs, bcs, Kn, nv, kinetic, init (rho, u, T), iterations)
@@ -163,6 +166,11 @@ def run_case(name, mesh_kw, bcs, Kn, nv, kinetic, init, iterations) -> dict:
     fp, fm, fs = case.boundary_fluxes()
     out["solver.F_plus"], out["solver.F_minus"], out["solver.face_state"] = fp, fm, fs
     out["solver.f"] = case.distribution()
+    # section mass flows (KineticSolver::section_mass_flow): x cuts across the box, one outside it, one y cut
+    out["solver.section_x"] = np.array(SECTION_X)
+    out["solver.section_flow_x"] = case.section_mass_flow(SECTION_X, axis=0)
+    out["solver.section_y"] = np.array(SECTION_Y)
+    out["solver.section_flow_y"] = case.section_mass_flow(SECTION_Y, axis=1)
     out["meta.name"] = np.array(name)
     return out
 

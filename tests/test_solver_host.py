@@ -8,6 +8,7 @@ import pytest
 
 from tests import common
 from gsis_sim_b200.kinetic_setup import HostSetup
+from gsis_sim_b200.section import SectionSpec
 from gsis_sim_b200.solver import KineticSolver
 
 
@@ -35,6 +36,15 @@ def check_solver(sol, infos, z, tol):
     assert common.max_rel(fm, z["solver.F_minus"]) < 10 * tol
     assert common.max_rel(sol.prepare().patch_mass_flow, z["solver.patch_mass_flow"]) < 100 * tol
     assert common.max_rel(sol.distribution(), z["solver.f"]) < tol
+    # section mass flows (KineticSolver::section_mass_flow); the empty cuts (x = 0 before every cell centre,
+    # x = 3 behind them) must give exactly 0
+    for ax, key in ((0, "x"), (1, "y")):
+        spec = SectionSpec(ax, list(z[f"solver.section_{key}"]))
+        flows = sol.section_mass_flow(spec)
+        assert common.max_rel(flows, z[f"solver.section_flow_{key}"]) < 100 * tol
+        for c, q in zip(sol.section_cuts(spec), flows):
+            if len(c.faces) == 0:
+                assert q == 0.0 and c.face_position == c.position
 
 
 @pytest.mark.parametrize("name", common.golden_names())
