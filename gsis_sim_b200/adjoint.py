@@ -1,0 +1,301 @@
+"""Discrete adjoint of the converged CIS fixed point: dM_dot / d(mu_hat0, delta, T_w per wall face) on the B200 backend.
+
+There is no reference counterpart; the steady problem differentiated is the one the reference's CIS iteration
+converges to (src/kinetic/kinetic_solver.cpp prepare + sweep, src/kinetic/kinetic_kernels.hpp):
+
+  F(x; p) = ( R(f, rho_Gamma)                 residual_value with the limited LSQ gradient, Shakhov target of the
+                                              cell moments, inflow of walls / pressure faces ("cell" reconstruction)
+              rho_Gamma - Phi(f, rho_Gamma) ) zero net mass flux of every diffuse wall face
+  J = M_dot = 1/2 (mdot_in + mdot_out) sqrt(2/pi)   (tube_mass_flow_json, src/kinetic/kinetic_output.cpp:273-284)
+
+The adjoint y = (lambda, nu) solves O(y) = y^T dF/dx - dJ/dx = 0 by the preconditioned fixed-point iteration
+  lambda <- lambda - P^-T O_f(y),   nu <- nu - O_nu(y)
+where P^-T is the forward LU-SGS block passes run on velocity-reversed storage (the transposed sweep; the device does
+it, kin_adjoint_update). Then dJ/dp = dJ/dp|_x - y^T dF/dp. The transposed transport, the per-cell sums against the
+Shakhov target and the per-face sums against the inflow Maxwellians run on the device (csrc/kin_adjoint.cu); this
+module finishes the per-cell / per-face algebra: the moments -> cell parameter chain, the pressure-face chain
+(App. A.2 acoustic correction), the wall-density equations and the parameter gradients.
+
+Scope (`check_scope`): FP64 backend with one velocity chunk; continuous equilibrium (kinetic.equilibrium =
+"continuous") or every state resolved by the velocity grid; diffuse walls, pressure inlets / outlets with
+pressure_boundary_reconstruction = "cell", vacuum, symmetry, periodic faces; no Maxwell walls, mass-flow inlets,
+positivity limiter or closed-domain scaling.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .kinetic_setup import BOUNDARY_TYPES
+
+C_J = 0.5 * math.sqrt(2.0 / math.pi)
+_INLETS = (BOUNDARY_TYPES.index("pressure_inlet"), BOUNDARY_TYPES.index("mass_flow_inlet"))
+_OUTLETS = (BOUNDARY_TYPES.index("pressure_outlet"), BOUNDARY_TYPES.index("vacuum"))
+
+
+class AdjointScopeError(ValueError):
+    pass
+
+
+def reversed_velocities(xi: np.ndarray) -> np.ndarray:
+    """rev[p] = index of -xi_p in the same list (a velocity grid symmetric about 0). Raises AdjointScopeError."""
+    xi = np.asarray(xi, float)
+    scale = max(float(np.abs(xi).max()), 1e-300)
+    key = np.round(xi / scale * 2.0 ** 40).astype(np.int64)
+    index = {tuple(k): i for i, k in enumerate(key.tolist())}
+    rev = np.array([index.get(tuple((-k).tolist()), -1) for k in key], np.int32)
+    if np.any(rev < 0):
+        raise AdjointScopeError("the velocity grid is not symmetric about 0 (no reversed velocity)")
+    return rev
+
+
+def reverse_entries(csr_offsets, csr_other, csr_faces) -> np.ndarray:
+    """For every internal CSR entry (cell j -> i through face f) the entry of cell i that points back to j through f;
+    -1 for boundary entries."""
+    offs = np.asarray(csr_offsets, np.int64)
+    other = np.asarray(csr_other, np.int64)
+    faces = np.asarray(csr_faces, np.int64)
+    row = np.repeat(np.arange(len(offs) - 1), np.diff(offs))
+    out = np.full(len(other), -1, np.int32)
+    internal = np.flatnonzero(other >= 0)
+    # key (face, cell of the row) -> entry
+    key = {(int(faces[e]), int(row[e])): int(e) for e in internal}
+    for e in internal.tolist():
+        back = key.get((int(faces[e]), int(other[e])))
+        if back is None:
+            raise AdjointScopeError(f"CSR entry {e} has no reverse entry")
+        out[e] = back
+    return out
+
+
+def moment_expansion_coefficients(m: np.ndarray, rho_b, u_b, T_b, q_b) -> np.ndarray:
+    """Per cell the coefficients (a0, a (3), a2, b (3)) of d(rho_b rho + u_b.u + T_b T + q_b.q)/d f_q
+    = w_q (a0 + a.c + a2 c^2 + b.c c^2), c = xi_q - u, for the moments of finalize_moments
+    (rho = sum w f, u = sum w xi f / rho, T = sum w c^2 f / (3 rho), q = 1/2 sum w c c^2 f); m: (n, 15) moments."""
+    rho, T, p = m[:, 0], m[:, 4], m[:, 5]
+    s = m[:, 6:12]
+    P = np.empty((len(m), 3, 3))
+    P[:, 0, 0], P[:, 1, 1], P[:, 2, 2] = s[:, 0] + p, s[:, 1] + p, s[:, 2] + p
+    P[:, 0, 1] = P[:, 1, 0] = s[:, 3]
+    P[:, 1, 2] = P[:, 2, 1] = s[:, 4]
+    P[:, 0, 2] = P[:, 2, 0] = s[:, 5]
+    Pq = np.einsum("nab,na->nb", P, q_b)
+    out = np.empty((len(m), 8))
+    out[:, 0] = rho_b - T_b * T / rho
+    out[:, 1:4] = (u_b - 1.5 * p[:, None] * q_b - Pq) / rho[:, None]
+    out[:, 4] = T_b / (3.0 * rho)
+    out[:, 5:8] = 0.5 * q_b
+    return out
+
+
+def pressure_face_adjoint(p_o, u_o, T_o, n, p_patch, inlet, zero_tan, gamma, rho_bar, u_bar, T_bar):
+    """Adjoint of the pressure-face state W_b = (rho_b, u_b, T_b) of the "cell" reconstruction (update_pressure_inflow,
+    src/kinetic/kinetic_solver.cpp:172-260) with respect to the owner cell's (p, u, T): returns (p_bar, u_bar, T_bar)
+    of the owners. u_b = u_o + du n (or (u_o.n + du) n with zero tangential velocity), du = (p_o - p_b) / (rho_o c_s),
+    rho_o = p_o / T_o, c_s = sqrt(gamma T_o); T_b = T_patch at inlets, T_o at outlets; rho_b = p_b / T_b."""
+    sg = math.sqrt(gamma)
+    sT = np.sqrt(T_o)
+    dbar = np.einsum("na,na->n", u_bar, n)
+    uo_bar = np.where(zero_tan[:, None], dbar[:, None] * n, u_bar)
+    p_bar = dbar * sT / sg * p_patch / (p_o * p_o)
+    T_out = dbar * (p_o - p_patch) / (p_o * sg) * 0.5 / sT
+    T_b = np.where(inlet, 0.0, 1.0)  # outlet: T_b = T_o
+    T_out = T_out + T_b * (T_bar - rho_bar * p_patch / (T_o * T_o))
+    return p_bar, uo_bar, T_out
+
+
+def collision_moment_adjoint(m, volume, mu0, omega, cell_sums):
+    """Adjoints of the cell moments (rho, u, T, q) from the collision term -coll (f^S - f) of the residual
+    (make_cell_params, src/kinetic/kinetic_kernels.hpp:451-471: coll = V p / (mu0 T^omega), p = rho T), given the
+    per-cell sums of k_adj_cell: Lambda0 = sum lambda (f^S - f), Lambda_theta = sum lambda d f^S / d theta.
+    Returns (rho_bar, u_bar, T_bar, q_bar, coll)."""
+    rho, T, p = m[:, 0], m[:, 4], m[:, 5]
+    coll = volume * p / (mu0 * T ** omega)
+    L0, Lr, Lu, LT, Lq = cell_sums[:, 0], cell_sums[:, 1], cell_sums[:, 2:5], cell_sums[:, 5], cell_sums[:, 6:9]
+    rho_b = -(coll / rho) * L0 - coll * Lr
+    T_b = -((1.0 - omega) * coll / T) * L0 - coll * LT
+    u_b = -coll[:, None] * Lu
+    q_b = -coll[:, None] * Lq
+    return rho_b, u_b, T_b, q_b, coll
+
+
+@dataclass
+class AdjointResult:
+    J: float
+    dJ_dmu0: float
+    dJ_dTw: np.ndarray       # per boundary face (internal numbering), zero off the diffuse walls
+    iterations: int
+    residual: float
+    history: list
+
+    def dJ_ddelta(self, mu0: float, delta: float) -> float:
+        """dJ/d delta when mu_hat0 = 1 / (sqrt(2) delta)."""
+        return -self.dJ_dmu0 * mu0 / delta
+
+
+class KineticAdjoint:
+    """Adjoint of M_dot at the converged state of a KineticSolver whose backend is a B200Backend (FP64)."""
+
+    def __init__(self, solver):
+        self.sol = solver
+        s, h = solver.s, solver.h
+        self.check_scope()
+        solver.prepare()
+        self.nc, self.nb, self.nv = solver.nc, solver.nb, solver.nv
+        xi = np.stack([np.asarray(s["xi_x"]), np.asarray(s["xi_y"]), np.asarray(s["xi_z"])], 1)
+        self.rev_v = reversed_velocities(xi)
+        self.rev_e = reverse_entries(s["csr_offsets"], s["csr_other"], h.csr_faces)
+        solver.backend.adjoint_begin(self.rev_v, self.rev_e)
+        bk = solver.bkind
+        self.wall = np.flatnonzero(bk == abi.BC_DIFFUSE_WALL)
+        self.pres = np.flatnonzero(bk == abi.BC_PRESSURE)
+        ptype = solver.ptype[solver.bpatch] if self.nb else np.zeros(0, int)
+        self.sgn = np.where(np.isin(ptype, _INLETS), -1.0, np.where(np.isin(ptype, _OUTLETS), 1.0, 0.0))
+        self.sgn[(bk != abi.BC_PRESSURE) & (bk != abi.BC_VACUUM)] = 0.0
+        self.nu = np.zeros(len(self.wall))
+        self.history = []
+
+    # ---- scope ---------------------------------------------------------------------------------------------------
+    def check_scope(self):
+        sol = self.sol
+        s, h = sol.s, sol.h
+        if int(s["precision"]) != abi.KIN_PREC_FP64:
+            raise AdjointScopeError("the adjoint needs precision = fp64")
+        if int(s["positivity"]) != 0:
+            raise AdjointScopeError("positivity limiter")
+        if h.closed_domain:
+            raise AdjointScopeError("closed-domain mass scaling")
+        if np.any(sol.bkind == abi.BC_MAXWELL_WALL):
+            raise AdjointScopeError("Maxwell walls (accommodation < 1)")
+        if np.any(sol.ptype == BOUNDARY_TYPES.index("mass_flow_inlet")):
+            raise AdjointScopeError("mass-flow inlets")
+        if np.any(sol.bkind == abi.BC_PRESSURE) and h.pressure_boundary_reconstruction != "cell":
+            raise AdjointScopeError('pressure boundaries need pressure_boundary_reconstruction = "cell"')
+        if float(s["cold_bgk_temperature"]) > 0.0:
+            raise AdjointScopeError("cold-BGK switch")
+        if sol.discrete_eq:
+            sol.prepare()
+            m = sol.moments_
+            st = np.stack([m[:, 0], m[:, 1], m[:, 2], m[:, 3], m[:, 4]], 1)
+            used = (sol.bkind == abi.BC_DIFFUSE_WALL) | (sol.bkind == abi.BC_PRESSURE)
+            if not np.all(sol._deq_resolved(st)) or (np.any(used) and
+                                                     not np.all(sol._deq_resolved(sol.inflow[used][:, 1:6]))):
+                raise AdjointScopeError('a state is not resolved by the velocity grid: use kinetic.equilibrium = '
+                                        '"continuous" or a wider / finer velocity grid')
+
+    # ---- one evaluation of O(y) ----------------------------------------------------------------------------------
+    def _mu(self):
+        sol = self.sol
+        mu = np.zeros(self.nb)
+        sm0, sm5 = sol.bsums[:, 0], sol.bsums[:, 5]
+        w = self.wall
+        with np.errstate(divide="ignore", invalid="ignore"):
+            pos = (sm5[w] < 0) & (-sm0[w] / sm5[w] > 0)
+            mu[w] = np.where(pos, self.nu / (sol.barea[w] * sm5[w]), 0.0)
+        j = self.sgn != 0
+        mu[j] = -C_J * self.sgn[j]
+        return mu
+
+    def _reduce(self):
+        cell, face = self.sol.backend.adjoint_reduce(self._mu())
+        return cell.reshape(self.nc, 9), face.reshape(max(self.nb, 0), 7)
+
+    def _coefficients(self, cell, face):
+        sol = self.sol
+        m = sol.moments_
+        rho, u, T, p = m[:, 0], m[:, 1:4], m[:, 4], m[:, 5]
+        rho_b, u_b, T_b, q_b, coll = collision_moment_adjoint(m, sol.volume, float(sol.s["mu0"]),
+                                                              float(sol.s["omega"]), cell)
+        if len(self.pres):
+            b = self.pres
+            inf = sol.inflow[b]
+            rb, Tb = inf[:, 1], inf[:, 5]
+            S = face[b]
+            rho_bar = S[:, 0] / rb
+            u_bar = S[:, 1:4] / Tb[:, None]
+            T_bar = S[:, 4] / (2.0 * Tb * Tb) - 1.5 * S[:, 0] / Tb
+            o = sol.bowner[b]
+            h = sol.h
+            n = h.face_normal[sol.bf_global[b]]
+            patch = sol.bpatch[b]
+            inlet = np.isin(sol.ptype[patch], _INLETS)
+            p_bar, uo_bar, To_bar = pressure_face_adjoint(p[o], u[o], T[o], n, h.patch_dbl[patch, 1], inlet,
+                                                          h.patch_dbl[patch, 6] > 0.5, h.gamma, rho_bar, u_bar, T_bar)
+            # p = rho T
+            np.add.at(rho_b, o, p_bar * T[o])
+            np.add.at(T_b, o, p_bar * rho[o] + To_bar)
+            np.add.at(u_b, o, uo_bar)
+        return moment_expansion_coefficients(m, rho_b, u_b, T_b, q_b), coll
+
+    def operator(self, lam=None, nu=None, with_objective=True):
+        """O(y) (or y^T dF/dx without the objective term) for the given lambda (storage order) and nu; returns
+        (O_f (nc, nv), O_nu (n_wall,))."""
+        be = self.sol.backend
+        if lam is not None:
+            be.adjoint_set(np.asarray(lam, float))
+        if nu is not None:
+            self.nu = np.asarray(nu, float).copy()
+        sgn = self.sgn
+        if not with_objective:
+            self.sgn = np.zeros_like(sgn)
+        try:
+            cell, face = self._reduce()
+            coef, _ = self._coefficients(cell, face)
+            _, op = be.adjoint_update(coef, run_passes=False, want_operator=True)
+        finally:
+            self.sgn = sgn
+        return op.reshape(self.nc, self.nv), face[self.wall, 0] + self.nu
+
+    # ---- the solve -----------------------------------------------------------------------------------------------
+    def solve(self, tol: float = 1e-10, max_iterations: int = 5000, callback=None) -> AdjointResult:
+        """Iterate to ||O_f||_2 / ||dJ/df||_2 < tol and the same for the wall equations; return the gradients."""
+        be = self.sol.backend
+        ref = None
+        it = 0
+        res = math.inf
+        for it in range(1, max_iterations + 1):
+            cell, face = self._reduce()
+            coef, _ = self._coefficients(cell, face)
+            res_cell, _ = be.adjoint_update(coef, run_passes=True)
+            nu_new = -face[self.wall, 0]
+            dnu = float(np.sqrt(np.sum((nu_new - self.nu) ** 2)))
+            self.nu = nu_new
+            r = math.sqrt(float(np.sum(res_cell)))
+            if ref is None:
+                ref = max(r, 1e-300)
+            res = max(r / ref, dnu / max(float(np.sqrt(np.sum(nu_new ** 2))), 1e-300) if len(nu_new) else 0.0)
+            self.history.append(r)
+            if callback is not None:
+                callback(it, r)
+            if r / ref < tol and (len(nu_new) == 0 or dnu <= tol * max(float(np.abs(nu_new).max()), 1e-300)):
+                break
+        return self.gradients(it, res)
+
+    def gradients(self, iterations: int = 0, residual: float = 0.0) -> AdjointResult:
+        sol = self.sol
+        cell, face = self._reduce()
+        _, coll = self._coefficients(cell, face)
+        mu0 = float(sol.s["mu0"])
+        dmu = -float(np.sum(coll / mu0 * cell[:, 0]))
+        dTw = np.zeros(self.nb)
+        w = self.wall
+        if len(w):
+            T = sol.inflow[w, 5]
+            S = face[w]
+            rg = sol.inflow[w, 0]
+            sm0, sm5 = sol.bsums[w, 0], sol.bsums[w, 5]
+            dR = rg * (S[:, 4] / (2.0 * T * T) - 1.5 * S[:, 0] / T)
+            D5 = S[:, 5] / (2.0 * T * T) - 1.5 * S[:, 6] / T
+            with np.errstate(divide="ignore", invalid="ignore"):
+                pos = (sm5 < 0) & (-sm0 / sm5 > 0)
+                dPhi = np.where(pos, sm0 / (sm5 * sm5) * D5, 0.0)
+            dTw[w] = -(dR - self.nu * dPhi)
+        J = sol.mass_flow()[2]
+        return AdjointResult(J=J, dJ_dmu0=dmu, dJ_dTw=dTw, iterations=iterations, residual=residual,
+                             history=list(self.history))
+
+    def close(self):
+        self.sol.backend.adjoint_end()

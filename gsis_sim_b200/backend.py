@@ -74,6 +74,42 @@ class KineticBackendABI:
         m = np.ascontiguousarray(moments, dtype=np.float64).ravel()
         self._call("set_moments", abi.as_ptr(m, C.c_double), m.size)
 
+    # --- discrete adjoint (gsis_sim_b200.adjoint drives these) -----------------------------------------------
+    def adjoint_begin(self, rev_velocity, rev_entry) -> None:
+        rv = np.ascontiguousarray(rev_velocity, dtype=np.int32)
+        re = np.ascontiguousarray(rev_entry, dtype=np.int32)
+        self._adj_keep = (rv, re)
+        self._call("adjoint_begin", abi.as_ptr(rv, C.c_int32), abi.as_ptr(re, C.c_int32), re.size)
+
+    def adjoint_set(self, lam) -> None:
+        a = np.ascontiguousarray(lam, dtype=np.float64).ravel()
+        self._call("adjoint_set", abi.as_ptr(a, C.c_double), a.size)
+
+    def adjoint_get(self) -> np.ndarray:
+        out = np.empty(self.n_cells * self.nv, dtype=np.float64)
+        self._call("adjoint_get", abi.as_ptr(out, C.c_double), out.size)
+        return out.reshape(self.n_cells, self.nv)
+
+    def adjoint_reduce(self, mu):
+        m = np.ascontiguousarray(mu, dtype=np.float64)
+        cell = np.empty(self.n_cells * 9, dtype=np.float64)
+        face = np.empty(max(self.n_bfaces, 1) * 7, dtype=np.float64)
+        self._call("adjoint_reduce", abi.as_ptr(m, C.c_double), m.size, abi.as_ptr(cell, C.c_double), cell.size,
+                   abi.as_ptr(face, C.c_double), self.n_bfaces * 7)
+        return cell, face[:self.n_bfaces * 7]
+
+    def adjoint_update(self, coef, run_passes: bool = True, want_operator: bool = False):
+        c = np.ascontiguousarray(coef, dtype=np.float64).ravel()
+        res = np.empty(self.n_cells, dtype=np.float64)
+        op = np.empty(self.n_cells * self.nv, dtype=np.float64) if want_operator else None
+        self._call("adjoint_update", abi.as_ptr(c, C.c_double), c.size, abi.as_ptr(res, C.c_double), res.size,
+                   C.c_int32(1 if run_passes else 0), abi.as_ptr(op, C.c_double) if op is not None else None,
+                   op.size if op is not None else 0)
+        return res, op
+
+    def adjoint_end(self) -> None:
+        self._call("adjoint_end")
+
     def scale_distribution(self, s: float) -> None:
         self._call("scale_distribution", C.c_double(s))
 

@@ -1,0 +1,52 @@
+// Discrete adjoint of the converged CIS fixed point (FP64): launch interface of kin_adjoint.cu.
+//
+// The steady discrete problem of the kinetic solver (residual_value with the limited LSQ gradient, the Shakhov target
+// of the cell moments and the boundary inflow, src/kinetic/kinetic_kernels.hpp) together with the zero-net-flux
+// equation of every diffuse-wall density rho_Gamma (process_boundary_sums, src/kinetic/kinetic_solver.cpp:280-335) is
+// F(f, rho_Gamma; p) = 0. For the adjoint y = (lambda, nu) of the objective J (the tube mass flow M_dot) the kernels
+// here evaluate the operator O(y) = y^T dF/dx - dJ/dx in pieces:
+//   k_adj_cell       per cell: the velocity sums Lambda of lambda against the Shakhov target and its derivatives
+//                    (moments -> cell parameters part, finished on the host)
+//   k_adj_transport  per (cell, velocity): the transposed upwind flux and limited-gradient terms that land on the
+//                    cell itself, plus the seeds the neighbours gather (gradient seed G_bar, limiter extremum seeds)
+//   k_adj_faces      per boundary face: the seeds on the inflow values (wall density, pressure-face state) summed
+//                    against the inflow Maxwellian and its derivatives
+//   k_adj_gather     per (cell, velocity): the neighbour and mirror gathers, the collision diagonal and the moment
+//                    expansion w (a0 + a.c + a2 c^2 + b.c c^2), written at the position of the reversed velocity
+// The LU-SGS passes of the forward solver, run on velocity-reversed storage, are the transposed preconditioner.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kin_kernels.cuh"
+
+namespace kin {
+
+constexpr int kAdjCellSums = 9;   // Lambda0, Lambda_rho, Lambda_u (3), Lambda_T, Lambda_q (3)
+constexpr int kAdjFaceSums = 7;   // S0, S1 (3), S2, S5, S6 (k_adj_faces)
+constexpr int kAdjCoefs = 8;      // a0, a (3), a2, b (3)
+
+struct AdjView {
+  const double* lam;       // [cell][p]: the adjoint of velocity rev[p] (velocity-reversed storage)
+  const int32_t* rev;      // position of -xi for every position
+  const int32_t* rev_entry;  // for an internal CSR entry (cell j -> i): the entry of cell i that points back to j
+  double* gbx;             // gradient seeds G_bar [cell][q]
+  double* gby;
+  double* gbz;
+  double* hmax;            // seed on the stencil maximum / minimum of the limiter when it is a stencil entry
+  double* hmin;
+  int8_t* imax;            // that entry (offset within the cell's CSR row), -1 none
+  int8_t* imin;
+  double* lfb;             // seeds that land on f[cell][q] itself
+  const double* mu;        // per boundary face: seed weight of the outgoing face values (nu and objective terms)
+  const double* coef;      // per cell: moment expansion coefficients (kAdjCoefs)
+  const double* moments;   // per cell: the 15 moments of the forward state
+  double* out;             // O_f(y) at the reversed position [cell][rev[q]]
+};
+
+void adj_cell_sums(const View<double, double>& v, const AdjView& a, double* out, cudaStream_t st);
+void adj_transport(const View<double, double>& v, const AdjView& a, cudaStream_t st);
+void adj_face_sums(const View<double, double>& v, const AdjView& a, double* out, cudaStream_t st);
+void adj_gather(const View<double, double>& v, const AdjView& a, double* res_cell, cudaStream_t st);
+
+}  // namespace kin

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "gsis_b200.h"
+#include "kin_adjoint.h"
 #include "kin_launch.h"
 
 namespace {
@@ -159,6 +160,15 @@ struct KinHandle {
                                         int32_t* result) = 0;
   virtual void moment_sums(double* out, int64_t n) = 0;
   virtual void set_moments(const double* m, int64_t n) = 0;
+  // discrete adjoint (FP64 handles with one velocity chunk)
+  virtual void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries) = 0;
+  virtual void adjoint_set(const double* lam, int64_t n) = 0;
+  virtual void adjoint_get(double* lam, int64_t n) = 0;
+  virtual void adjoint_reduce(const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell, double* face_sums,
+                              int64_t n_face) = 0;
+  virtual void adjoint_update(const double* coef, int64_t n_coef, double* res_cell, int64_t n_res, int32_t run_passes,
+                              double* op_out, int64_t n_op) = 0;
+  virtual void adjoint_end() = 0;
 };
 
 // Scratch of kin_discrete_maxwell_noalloc: static device memory of this module (one copy per device), laid out as
@@ -268,6 +278,12 @@ struct Backend final : KinHandle {
   DevBuf<int32_t> flags, face_cells, face_entries;
   DevBuf<double> face_out;
   DevBuf<S> f, gx, gy, gz, r;
+
+  // discrete adjoint: lambda in velocity-reversed storage, seeds of the transposed gradient
+  bool adj_on = false;
+  DevBuf<double> adj_lam, adj_lfb, adj_hmax, adj_hmin, adj_mu, adj_coef, adj_cell, adj_face, adj_res;
+  DevBuf<int8_t> adj_imax, adj_imin;
+  DevBuf<int32_t> adj_rev, adj_rev_entry, adj_perm2, adj_inv2;
 
   bool inflow_set = false;
   bool deq_valid = false;
@@ -1200,6 +1216,198 @@ struct Backend final : KinHandle {
     *ml = max_levels;
     *nch = n_chains;
   }
+
+  // ---- discrete adjoint ------------------------------------------------------------------------------------
+  // lambda is stored at the position of the reversed velocity, so that the forward LU-SGS passes (which at
+  // position p use xi_p and the sweep direction of p) act on the adjoint of -xi_p as the transposed preconditioner:
+  // the in-block lower / upper couplings of velocity -xi are the transposes of the upper / lower ones of xi.
+  void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries) override {
+    if constexpr (!std::is_same<S, double>::value || !std::is_same<M, double>::value) {
+      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
+    } else {
+      KCHECK(chunk == nv, "the adjoint needs one velocity chunk (velocity_chunk = 0 with enough device memory)");
+      KCHECK(n_maxwell == 0, "the adjoint does not cover Maxwell walls");
+      KCHECK(rev_velocity != nullptr && rev_entry != nullptr, "missing adjoint maps");
+      std::vector<int32_t> hcsr(static_cast<size_t>(nc) + 1);
+      KCUDA(cudaMemcpy(hcsr.data(), csr_off.p, hcsr.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      KCHECK(n_entries == hcsr[nc], "length of the reverse CSR entry map does not match");
+      std::vector<int32_t> rev(nv), perm2(nv), inv2(nv);
+      for (int q = 0; q < nv; ++q) {
+        const int s = rev_velocity[perm[q]];
+        KCHECK(s >= 0 && s < nv, "reversed velocity out of range");
+        rev[q] = inv[s];
+      }
+      for (int q = 0; q < nv; ++q) KCHECK(rev[rev[q]] == q, "the velocity reversal is not an involution");
+      for (int p = 0; p < nv; ++p) perm2[p] = perm[rev[p]];
+      for (int s = 0; s < nv; ++s) inv2[s] = rev[inv[s]];
+      for (int64_t e = 0; e < n_entries; ++e) KCHECK(rev_entry[e] >= -1 && rev_entry[e] < n_entries, "reverse entry out of range");
+      const size_t nf = static_cast<size_t>(nc) * nv;
+      adj_rev.upload(rev.data(), nv, stream);
+      adj_perm2.upload(perm2.data(), nv, stream);
+      adj_inv2.upload(inv2.data(), nv, stream);
+      adj_rev_entry.upload(rev_entry, static_cast<size_t>(n_entries), stream);
+      adj_lam.alloc(nf);
+      KCUDA(cudaMemsetAsync(adj_lam.p, 0, adj_lam.bytes(), stream));
+      adj_lfb.alloc(nf);
+      adj_hmax.alloc(nf);
+      adj_hmin.alloc(nf);
+      adj_imax.alloc(nf);
+      adj_imin.alloc(nf);
+      adj_mu.alloc(static_cast<size_t>(std::max(nb, 1)));
+      KCUDA(cudaMemsetAsync(adj_mu.p, 0, adj_mu.bytes(), stream));
+      adj_coef.alloc(static_cast<size_t>(nc) * kin::kAdjCoefs);
+      KCUDA(cudaMemsetAsync(adj_coef.p, 0, adj_coef.bytes(), stream));
+      adj_cell.alloc(static_cast<size_t>(nc) * kin::kAdjCellSums);
+      adj_face.alloc(static_cast<size_t>(std::max(nb, 1)) * kin::kAdjFaceSums);
+      adj_res.alloc(static_cast<size_t>(nc));
+      KCUDA(cudaStreamSynchronize(stream));
+      adj_on = true;
+    }
+  }
+
+  kin::AdjView adj_view() {
+    kin::AdjView a{};
+    a.lam = adj_lam.p;
+    a.rev = adj_rev.p;
+    a.rev_entry = adj_rev_entry.p;
+    a.gbx = reinterpret_cast<double*>(gx.p);
+    a.gby = reinterpret_cast<double*>(gy.p);
+    a.gbz = reinterpret_cast<double*>(gz.p);
+    a.hmax = adj_hmax.p;
+    a.hmin = adj_hmin.p;
+    a.imax = adj_imax.p;
+    a.imin = adj_imin.p;
+    a.lfb = adj_lfb.p;
+    a.mu = adj_mu.p;
+    a.coef = adj_coef.p;
+    a.moments = moments.p;
+    a.out = reinterpret_cast<double*>(r.p);
+    return a;
+  }
+
+  void adjoint_set(const double* h, int64_t n) override {
+    KCHECK(adj_on, "adjoint_begin first");
+    KCHECK(n == static_cast<int64_t>(nc) * nv, "length of lambda does not match");
+    for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
+      const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
+      KCUDA(cudaMemcpyAsync(staging.p, h + c0 * nv, sizeof(double) * cnt * nv, cudaMemcpyHostToDevice, stream));
+      kin::Launch<double, double>::import_f(staging.p, adj_lam.p, adj_perm2.p, c0, cnt, nv, stream);
+      launched();
+    }
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void adjoint_get(double* h, int64_t n) override {
+    KCHECK(adj_on, "adjoint_begin first");
+    KCHECK(n == static_cast<int64_t>(nc) * nv, "length of lambda does not match");
+    for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
+      const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
+      kin::Launch<double, double>::export_f(adj_lam.p, staging.p, adj_inv2.p, c0, cnt, nv, stream);
+      launched();
+      KCUDA(cudaMemcpyAsync(h + c0 * nv, staging.p, sizeof(double) * cnt * nv, cudaMemcpyDeviceToHost, stream));
+    }
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void adjoint_reduce(const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell, double* face_sums,
+                      int64_t n_face) override {
+    if constexpr (std::is_same<S, double>::value && std::is_same<M, double>::value) {
+      KCHECK(adj_on, "adjoint_begin first");
+      KCHECK(n_mu == nb && n_cell == static_cast<int64_t>(nc) * kin::kAdjCellSums &&
+                 n_face == static_cast<int64_t>(nb) * kin::kAdjFaceSums,
+             "adjoint_reduce: array lengths do not match");
+      if (nb > 0) KCUDA(cudaMemcpyAsync(adj_mu.p, mu, sizeof(double) * nb, cudaMemcpyHostToDevice, stream));
+      const kin::AdjView a = adj_view();
+      kin::adj_cell_sums(view, a, adj_cell.p, stream);
+      kin::adj_transport(view, a, stream);
+      kin::adj_face_sums(view, a, adj_face.p, stream);
+      launched(nb > 0 ? 3 : 2);
+      KCUDA(cudaGetLastError());
+      KCUDA(cudaMemcpyAsync(cell_sums, adj_cell.p, sizeof(double) * n_cell, cudaMemcpyDeviceToHost, stream));
+      if (nb > 0)
+        KCUDA(cudaMemcpyAsync(face_sums, adj_face.p, sizeof(double) * n_face, cudaMemcpyDeviceToHost, stream));
+      KCUDA(cudaStreamSynchronize(stream));
+    } else {
+      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
+    }
+  }
+
+  void adjoint_update(const double* coef, int64_t n_coef, double* res_cell, int64_t n_res, int32_t run_passes,
+                      double* op_out, int64_t n_op) override {
+    if constexpr (std::is_same<S, double>::value && std::is_same<M, double>::value) {
+      KCHECK(adj_on, "adjoint_begin first");
+      KCHECK(n_coef == static_cast<int64_t>(nc) * kin::kAdjCoefs && n_res == nc, "adjoint_update: array lengths");
+      KCHECK(op_out == nullptr || n_op == static_cast<int64_t>(nc) * nv, "adjoint_update: operator output length");
+      KCUDA(cudaMemcpyAsync(adj_coef.p, coef, sizeof(double) * n_coef, cudaMemcpyHostToDevice, stream));
+      kin::adj_gather(view, adj_view(), adj_res.p, stream);
+      launched();
+      KCUDA(cudaGetLastError());
+      if (op_out != nullptr) {
+        for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
+          const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
+          kin::Launch<double, double>::export_f(reinterpret_cast<const double*>(r.p), staging.p, adj_inv2.p, c0, cnt,
+                                                nv, stream);
+          launched();
+          KCUDA(cudaMemcpyAsync(op_out + c0 * nv, staging.p, sizeof(double) * cnt * nv, cudaMemcpyDeviceToHost,
+                                stream));
+        }
+      }
+      if (run_passes) {
+        // the forward block passes on lambda (reversed storage) with R = O_f(y): lambda += -P^-T O_f(y)
+        kin::View<S, P> av = sweep_view();
+        av.f = adj_lam.p;
+        const auto& cp = chunks.front();
+        S* prev = nullptr;
+        for (int pass = 0; pass < block_passes; ++pass) {
+          S* out = (pass % 2 == 0) ? gz.p : gy.p;
+          kin::SweepArgs<S, P> sa{};
+          sa.items = cp->items.p;
+          sa.n_items = cp->n_items;
+          sa.n_blocks = n_blocks;
+          sa.block_offsets = block_offsets.p;
+          sa.prog = prog.p;
+          sa.chain_start = chain_start.p;
+          sa.lev_bounds = lev_bounds.p;
+          sa.lev_start = lev_start.p;
+          sa.lev_count = lev_count.p;
+          sa.se = sweep_entries.p;
+          sa.staged_ne = staged_ne;
+          sa.sprog = sprog.p;
+          sa.sse = sse.p;
+          sa.sub_cells = sub_cells.p;
+          sa.sub_entries = sub_entries.p;
+          sa.sub_start = sub_start.p;
+          sa.sub_count = sub_count.p;
+          sa.R = r.p;
+          sa.dprev = prev;
+          sa.out = out;
+          sa.update_f = pass + 1 == block_passes ? 1 : 0;
+          sa.k0 = cp->k0;
+          sa.stride = chunk;
+          LP::sweep_pass(av, sa, stream);
+          launched();
+          prev = out;
+        }
+        KCUDA(cudaGetLastError());
+      }
+      KCUDA(cudaMemcpyAsync(res_cell, adj_res.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, stream));
+      KCUDA(cudaStreamSynchronize(stream));
+    } else {
+      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
+    }
+  }
+
+  void adjoint_end() override {
+    for (auto* b : {&adj_lam, &adj_lfb, &adj_hmax, &adj_hmin, &adj_mu, &adj_coef, &adj_cell, &adj_face, &adj_res})
+      b->release();
+    adj_imax.release();
+    adj_imin.release();
+    adj_rev.release();
+    adj_rev_entry.release();
+    adj_perm2.release();
+    adj_inv2.release();
+    adj_on = false;
+  }
 };
 
 template <class Fn>
@@ -1318,6 +1526,20 @@ int kin_discrete_maxwell_noalloc(KinHandle* h, const double* states, int64_t n, 
   return guard(h, [&] { h->discrete_maxwell_noalloc(states, n, tolerance, out, result); });
 }
 int kin_moment_sums(KinHandle* h, double* out, int64_t n) { return guard(h, [&] { h->moment_sums(out, n); }); }
+int kin_adjoint_begin(KinHandle* h, const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries) {
+  return guard(h, [&] { h->adjoint_begin(rev_velocity, rev_entry, n_entries); });
+}
+int kin_adjoint_set(KinHandle* h, const double* lam, int64_t n) { return guard(h, [&] { h->adjoint_set(lam, n); }); }
+int kin_adjoint_get(KinHandle* h, double* lam, int64_t n) { return guard(h, [&] { h->adjoint_get(lam, n); }); }
+int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,
+                       double* face_sums, int64_t n_face) {
+  return guard(h, [&] { h->adjoint_reduce(mu, n_mu, cell_sums, n_cell, face_sums, n_face); });
+}
+int kin_adjoint_update(KinHandle* h, const double* coef, int64_t n_coef, double* res_cell, int64_t n_res,
+                       int32_t run_passes, double* op_out, int64_t n_op) {
+  return guard(h, [&] { h->adjoint_update(coef, n_coef, res_cell, n_res, run_passes, op_out, n_op); });
+}
+int kin_adjoint_end(KinHandle* h) { return guard(h, [&] { h->adjoint_end(); }); }
 int kin_set_moments(KinHandle* h, const double* m, int64_t n) { return guard(h, [&] { h->set_moments(m, n); }); }
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains) {
   return guard(const_cast<KinHandle*>(h), [&] { h->schedule_info(max_levels, n_chains); });

@@ -279,6 +279,36 @@ int kin_moment_sums(KinHandle* h, double* out, int64_t n);
    (they feed kin_update_cell_params) and move the shift to their velocity, as kin_compute_moments does. */
 int kin_set_moments(KinHandle* h, const double* moments, int64_t n);
 
+/* ---- discrete adjoint of the converged fixed point (no reference counterpart; FP64 handles, one velocity chunk,
+   continuous equilibrium, no Maxwell walls) ----------------------------------------------------------------------
+   The adjoint y = (lambda [cell][velocity], nu [diffuse wall face]) of an objective J solves O(y) = 0 with
+   O(y) = y^T dF/dx - dJ/dx, F = (steady residual R of residual_value, rho_Gamma - Phi of the wall densities). The
+   handle evaluates O in pieces; the host finishes the per-cell and per-face algebra (gsis_sim_b200/adjoint.py).
+   Prerequisites: the forward state installed (f, moments, cell parameters and inflow of the last prepare).
+
+   kin_adjoint_begin: allocate the adjoint arrays, lambda = 0. rev_velocity[p] = storage position of -xi_p (a
+   symmetric grid); rev_entry[e] = for an internal CSR entry of cell j pointing at cell i, the entry of cell i that
+   points back at j (-1 for boundary entries). */
+int kin_adjoint_begin(KinHandle* h, const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries);
+/* lambda in the storage order of kin_set_distribution (n = n_cells * nv). */
+int kin_adjoint_set(KinHandle* h, const double* lambda, int64_t n);
+int kin_adjoint_get(KinHandle* h, double* lambda, int64_t n);
+/* Transposed transport and the per-cell / per-face sums. mu[b] (n_bfaces): weight of the seed w_q a_q mu[b] on the
+   outgoing face values of boundary face b (diffuse walls: nu_b / (area_b sm5_b); inlet / outlet faces: the objective's
+   -dJ/d(patch flow) factor), also applied to the incoming values of pressure faces. Outputs, per cell (9): the sums of
+   lambda against f^S - f and d f^S / d(rho, u, T, q); per boundary face (7): S0, S1 (3), S2 of the seeds on the
+   incoming inflow values against the inflow Maxwellian (M, M c, M c^2) and S5, S6 = sum_in w an M {c^2, 1}. */
+int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,
+                       double* face_sums, int64_t n_face);
+/* Finish O_f(y) with the per-cell moment-expansion coefficients coef (8 per cell: a0, a (3), a2, b (3); the term
+   w_q (a0 + a.c + a2 c^2 + b.c c^2), c = xi_q - u_cell), return sum_q O_f^2 per cell in res_cell and, if op_out is not
+   NULL, O_f(y) itself (storage order); with run_passes != 0 then update lambda by the LU-SGS block passes of the
+   reversed velocities (the transposed preconditioner): lambda -= P^-T O_f(y). */
+int kin_adjoint_update(KinHandle* h, const double* coef, int64_t n_coef, double* res_cell, int64_t n_res,
+                       int32_t run_passes, double* op_out, int64_t n_op);
+/* Free the adjoint arrays. */
+int kin_adjoint_end(KinHandle* h);
+
 #ifdef __cplusplus
 }
 #endif

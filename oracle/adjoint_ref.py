@@ -1,0 +1,345 @@
+"""CPU reference of the discrete adjoint of the converged CIS fixed point (TEST INFRASTRUCTURE: used only by tests/
+as the checker of the B200 adjoint; never by the product).
+
+The steady discrete problem that the CIS iteration of the reference converges to (src/kinetic/kinetic_solver.cpp
+prepare + sweep, src/kinetic/kinetic_kernels.hpp) is written here as one differentiable map in torch (float64, CPU),
+and its transposed Jacobian is taken by autograd:
+
+  unknowns   x = (f [cell][velocity], rho_Gamma [diffuse wall face])
+  equations  R(f, rho_Gamma; p) = 0       the residual of residual_value (kinetic_kernels.hpp:238-278) with the
+                                          limited LSQ gradient (:161-201), the Shakhov target of the cell moments
+                                          (make_cell_params :451-471) and the inflow of the boundary faces
+             rho_Gamma - Phi(f, rho_Gamma) = 0   zero net mass flux of each diffuse wall face
+                                          (process_boundary_sums, kinetic_solver.cpp:280-335)
+  objective  J = M_dot = 1/2 (mdot_in + mdot_out) sqrt(2/pi) from the patch flows of the boundary sums
+  parameters p = (mu_hat0, T_w per boundary face); delta enters only through mu_hat0 = 1 / (sqrt(2) delta)
+
+The adjoint y solves (dF/dx)^T y = dJ/dx (GMRES over autograd vector-Jacobian products) and
+dJ/dp = dJ/dp|_x - y^T dF/dp.
+
+Scope (the same as the B200 adjoint; `check_scope` raises outside it): diffuse walls, pressure inlets / outlets with
+the "cell" boundary reconstruction (W_b from the owner cell, App. A.2 acoustic correction), vacuum, symmetry and
+periodic faces; Venkatakrishnan limiter (absolute or relative epsilon) or none; no positivity limiter, no closed-domain
+scaling, no mass-flow inlets, no Maxwell walls; every cell and inflow state resolved by the velocity grid (the
+discrete-equilibrium Newton inactive, deq_resolved of src/kinetic/discrete_equilibrium.hpp:35-48).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+BC_DIFFUSE_WALL, BC_PRESSURE, BC_VACUUM, BC_SYMMETRY, BC_PERIODIC, BC_MAXWELL_WALL = 0, 1, 2, 3, 4, 5
+LIMITER_NONE, LIMITER_ABS, LIMITER_REL = 0, 1, 2
+# BoundaryType indices (gsis_sim_b200.kinetic_setup.BOUNDARY_TYPES)
+T_INLETS = ("pressure_inlet", "mass_flow_inlet")
+T_OUTLETS = ("pressure_outlet", "vacuum")
+
+
+class ScopeError(ValueError):
+    pass
+
+
+def _t(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype)
+
+
+class SteadyMap:
+    """The steady map F(x; p) and objective J(x; p) of one kinetic set-up (internal numbering, storage order)."""
+
+    def __init__(self, setup, host):
+        from gsis_sim_b200.kinetic_setup import BOUNDARY_TYPES
+
+        s = setup
+        self.nc, self.nv, self.nb = s.n_cells, s.nv, s.n_bfaces
+        nc, nv = self.nc, self.nv
+        self.xi = torch.stack([_t(s["xi_x"]), _t(s["xi_y"]), _t(s["xi_z"])], 1)  # (nv, 3)
+        w = s.arrays.get("weights") if hasattr(s, "arrays") else None
+        self.w = _t(w) if w is not None else torch.full((nv,), float(s["weight"]), dtype=torch.float64)
+        off = np.asarray(s["csr_offsets"], np.int64)
+        cnt = np.diff(off)
+        E = int(cnt.max())
+        self.E = E
+        ent = off[:-1, None] + np.arange(E)[None, :]
+        mask = np.arange(E)[None, :] < cnt[:, None]
+        ent = np.where(mask, ent, 0)
+        geom = np.asarray(s["csr_geom"], float).reshape(-1, 12)[ent]  # (nc, E, 12)
+        other = np.where(mask, np.asarray(s["csr_other"])[ent], -1)
+        bface = np.where(mask, np.asarray(s["csr_bface"])[ent], -1)
+        bkind = np.asarray(s["bface_kind"])
+        kind = np.where(bface >= 0, bkind[np.maximum(bface, 0)], -1)
+        self.mask = torch.as_tensor(mask)
+        self.internal = torch.as_tensor(mask & (other >= 0))
+        self.other = torch.as_tensor(np.maximum(other, 0))
+        self.bface = torch.as_tensor(np.maximum(bface, 0))
+        self.kind = torch.as_tensor(np.where(mask, kind, -2))
+        self.S, self.ds, self.dn, self.c = (_t(geom[..., 3 * k:3 * k + 3]) for k in range(4))
+        self.eps2 = _t(s["eps2"])
+        self.limiter = int(s["limiter_mode"])
+        mx = np.asarray(s["bface_mirror_xor"])
+        q = np.arange(nv)
+        self.mirror = torch.as_tensor(np.where((kind == BC_SYMMETRY)[..., None], q[None, None, :] ^
+                                               mx[np.maximum(bface, 0)][..., None], q[None, None, :]))
+        bg = np.asarray(s["bface_geom"], float).reshape(-1, 7)
+        self.bn, self.barea, self.bd = _t(bg[:, 0:3]), _t(bg[:, 3]), _t(bg[:, 4:7])
+        self.bowner = torch.as_tensor(np.asarray(s["bface_owner"], np.int64))
+        self.bkind = torch.as_tensor(bkind)
+        self.bpatch = np.asarray(s["bface_patch"])
+        self.volume = _t(s["volume"])
+        self.omega, self.Pr = float(s["omega"]), float(s["Pr"])
+        self.mu0 = float(s["mu0"])
+        self.cold = float(s["cold_bgk_temperature"])
+        self.gamma = host.gamma
+        pd = np.asarray(host.patch_dbl, float)
+        ptype = np.asarray(host.patch_int)[:, 3]
+        self.ptype_names = [BOUNDARY_TYPES[t] for t in ptype]
+        bp = self.bpatch
+        self.T_patch = _t(pd[bp, 0])
+        self.p_patch = _t(pd[bp, 1])
+        self.u_patch = _t(pd[bp, 2:5])
+        self.zero_tan = torch.as_tensor(pd[bp, 6] > 0.5)
+        self.inlet_face = torch.as_tensor(np.array([self.ptype_names[p] in T_INLETS for p in bp], bool))
+        self.outlet_face = torch.as_tensor(np.array([self.ptype_names[p] in T_OUTLETS for p in bp], bool))
+        self.wall = self.bkind == BC_DIFFUSE_WALL
+        self.wall_idx = torch.nonzero(self.wall).ravel()
+        self.setup, self.host = setup, host
+
+    # ---- scope ---------------------------------------------------------------------------------------------------
+    def check_scope(self, solver=None):
+        s, h = self.setup, self.host
+        if int(s["positivity"]) != 0:
+            raise ScopeError("positivity limiter")
+        if h.closed_domain:
+            raise ScopeError("closed-domain mass scaling")
+        if torch.any(self.bkind == BC_MAXWELL_WALL):
+            raise ScopeError("Maxwell walls (alpha < 1)")
+        if "mass_flow_inlet" in self.ptype_names:
+            raise ScopeError("mass-flow inlets")
+        if torch.any(self.bkind == BC_PRESSURE) and h.pressure_boundary_reconstruction != "cell":
+            raise ScopeError('pressure boundaries need pressure_boundary_reconstruction = "cell"')
+        if solver is not None and solver.discrete_eq:
+            m = solver.moments_
+            st = np.stack([m[:, 0], m[:, 1], m[:, 2], m[:, 3], m[:, 4]], 1)
+            if not np.all(solver._deq_resolved(st)):
+                raise ScopeError("a cell state is not resolved by the velocity grid (discrete equilibrium active)")
+            used = (solver.bkind == BC_DIFFUSE_WALL) | (solver.bkind == BC_PRESSURE)
+            if np.any(used) and not np.all(solver._deq_resolved(solver.inflow[used][:, 1:6])):
+                raise ScopeError("an inflow state is not resolved by the velocity grid")
+
+    # ---- pieces --------------------------------------------------------------------------------------------------
+    def moments(self, f):
+        w = self.w
+        rho = f @ w
+        u = (f * w) @ self.xi / rho[:, None]
+        c = self.xi[None, :, :] - u[:, None, :]
+        c2 = (c * c).sum(-1)
+        p = ((f * w) * c2).sum(1) / 3.0
+        T = p / rho
+        q = 0.5 * ((f * w * c2)[..., None] * c).sum(1)
+        return rho, u, T, p, q
+
+    def maxwell(self, rho, u, T):
+        """rho, T: (n,), u: (n, 3) -> (n, nv)."""
+        c = self.xi[None, :, :] - u[:, None, :]
+        tp = 2.0 * math.pi * T
+        return (rho / (tp * torch.sqrt(tp)))[:, None] * torch.exp(-(c * c).sum(-1) / (2.0 * T)[:, None])
+
+    def target(self, f, mu0):
+        rho, u, T, p, q = self.moments(f)
+        c = self.xi[None, :, :] - u[:, None, :]
+        c2 = (c * c).sum(-1)
+        coef = torch.where(T < self.cold, torch.zeros_like(T), (1.0 - self.Pr) / (5.0 * (rho * T) * T))
+        poly = coef[:, None] * (c * q[:, None, :]).sum(-1) * (c2 / T[:, None] - 5.0)
+        fS = self.maxwell(rho, u, T) * (1.0 + poly)
+        coll = self.volume * p / (mu0 * T ** self.omega)
+        return coll, fS, (rho, u, T, p, q)
+
+    def inflow(self, mom, rho_gamma, Tw):
+        """(scale (nb,), Maxwellian values (nb, nv)) of every boundary face; walls at rest-frame density 1 with the
+        wall velocity and temperature Tw, pressure faces W_b of the owner cell (App. A.2, kinetic_solver.cpp:172-260,
+        "cell" reconstruction)."""
+        rho, u, T, p, q = mom
+        nb = self.nb
+        own = self.bowner
+        # pressure: (p_ib, u_ib, T_ib) = owner state
+        p_ib, u_ib, T_ib = p[own], u[own], T[own]
+        rho_ib = p_ib / T_ib
+        cs = torch.sqrt(self.gamma * T_ib)
+        T_b = torch.where(self.inlet_face, self.T_patch, T_ib)
+        du = (p_ib - self.p_patch) / (rho_ib * cs)
+        un = (u_ib * self.bn).sum(1)
+        u_p = torch.where(self.zero_tan[:, None], (un + du)[:, None] * self.bn, u_ib + du[:, None] * self.bn)
+        rho_p = self.p_patch / T_b
+        wall = self.wall
+        rho_s = torch.where(wall, torch.ones(nb, dtype=torch.float64), rho_p)
+        u_s = torch.where(wall[:, None], self.u_patch, u_p)
+        T_s = torch.where(wall, Tw, T_b)
+        pres = self.bkind == BC_PRESSURE
+        use = wall | pres
+        safe_T = torch.where(use, T_s, torch.ones_like(T_s))
+        safe_rho = torch.where(use, rho_s, torch.ones_like(rho_s))
+        M = self.maxwell(safe_rho, u_s, safe_T)
+        rg = torch.zeros(nb, dtype=torch.float64)
+        if len(self.wall_idx):
+            rg = rg.index_put((self.wall_idx,), rho_gamma)
+        scale = torch.where(wall, rg, torch.where(pres, torch.ones(nb, dtype=torch.float64),
+                                                  torch.zeros(nb, dtype=torch.float64)))
+        return scale, M
+
+    def _entry_f(self, f, scale, M):
+        """f at the stencil entries (nc, E, nv) and the inflow values of boundary entries."""
+        fi = f[:, None, :].expand(-1, self.E, -1)
+        fo = f[self.other]  # (nc, E, nv)
+        b = self.bface
+        a = (self.S @ self.xi.T)  # (nc, E, nv)
+        infl = scale[b][..., None] * M[b]
+        fm = torch.gather(fi, 2, self.mirror)
+        k = self.kind[..., None]
+        bval = torch.where(k == BC_PERIODIC, fi,
+                           torch.where(k == BC_SYMMETRY, 0.5 * (fi + fm),
+                                       torch.where(a >= 0, fi, torch.where(k == BC_VACUUM, torch.zeros_like(fi), infl))))
+        fk = torch.where(self.internal[..., None], fo, bval)
+        fk = torch.where(self.mask[..., None], fk, fi)
+        return fk, a, infl
+
+    def gradient(self, f, fk):
+        """limited_gradient (kinetic_kernels.hpp:161-201) at every (cell, velocity): (nc, nv, 3)."""
+        fi = f[:, None, :]
+        d = torch.where(self.mask[..., None], fk - fi, torch.zeros_like(fk))
+        G = torch.einsum("cek,cev->cvk", self.c, d)
+        if self.limiter == LIMITER_NONE:
+            return G
+        fmax = torch.maximum(f, fk.amax(1))
+        fmin = torch.minimum(f, fk.amin(1))
+        eps2 = self.eps2[:, None].expand(-1, self.nv)
+        if self.limiter == LIMITER_REL:
+            sc = torch.maximum(fmax.abs(), fmin.abs())
+            eps2 = eps2 * sc * sc
+        proj = torch.einsum("cvk,cek->cev", G, self.ds)
+        dmax = (fmax - f)[:, None, :]
+        dmin = (fmin - f)[:, None, :]
+        d1 = torch.where(proj > 0, dmax, dmin)
+        e2 = eps2[:, None, :]
+        num = (d1 * d1 + e2) + 2.0 * d1 * proj
+        den = d1 * d1 + 2.0 * proj * proj + d1 * proj + e2
+        ok = (proj != 0) & (den > 0)
+        v = torch.clamp(num / torch.where(ok, den, torch.ones_like(den)), 0.0, 1.0)
+        v = torch.where(proj == 0, torch.ones_like(v), torch.where(den > 0, v, torch.zeros_like(v)))
+        active = (self.mask & (self.kind != BC_PERIODIC))[..., None]
+        v = torch.where(active, v, torch.ones_like(v))
+        phi = torch.clamp(v.amin(1), max=1.0)
+        return phi[..., None] * G
+
+    def residual(self, f, g, fk, a, infl, coll, fS):
+        """residual_value (kinetic_kernels.hpp:238-278) at every (cell, velocity)."""
+        gi = g[:, None, :, :]  # (nc, 1, nv, 3)
+        own_face = f[:, None, :] + (gi * self.ds[:, :, None, :]).sum(-1)
+        go = g[self.other]  # (nc, E, nv, 3)
+        nb_face = f[self.other] + (go * self.dn[:, :, None, :]).sum(-1)
+        gm = torch.gather(g[:, None, :, :].expand(-1, self.E, -1, -1), 2,
+                          self.mirror[..., None].expand(-1, -1, -1, 3))
+        fmr = torch.gather(f[:, None, :].expand(-1, self.E, -1), 2, self.mirror)
+        sym_face = fmr + (gm * self.ds[:, :, None, :]).sum(-1)
+        k = self.kind[..., None]
+        ff = torch.where(a >= 0, own_face,
+                         torch.where(self.internal[..., None], nb_face,
+                                     torch.where(k == BC_SYMMETRY, sym_face,
+                                                 torch.where(k == BC_VACUUM, torch.zeros_like(infl), infl))))
+        use = (self.mask & (self.kind != BC_PERIODIC))[..., None]
+        R = torch.where(use, a * ff, torch.zeros_like(ff)).sum(1)
+        return R - coll[:, None] * (fS - f)
+
+    def boundary_sums(self, f, g, M):
+        """sm0 = sum_{an >= 0} w an f_b (reconstructed) and sm5 = sum_{an < 0} w an M_b per face
+        (k_boundary_sums, kinetic_cuda_kernels.cu:275-323; the other 18 sums are not needed here)."""
+        own = self.bowner
+        an = self.bn @ self.xi.T  # (nb, nv)
+        fb = f[own] + (g[own] * self.bd[:, None, :]).sum(-1)
+        out = an >= 0
+        sm0 = torch.where(out, self.w * an * fb, torch.zeros_like(fb)).sum(1)
+        sm5 = torch.where(out, torch.zeros_like(fb), self.w * an * M).sum(1)
+        return sm0, sm5
+
+    # ---- the map -------------------------------------------------------------------------------------------------
+    def evaluate(self, f, rho_gamma, mu0, Tw):
+        """(R (nc, nv), wall equations rho_Gamma - Phi (n_wall,), J = M_dot)."""
+        coll, fS, mom = self.target(f, mu0)
+        scale, M = self.inflow(mom, rho_gamma, Tw)
+        fk, a, infl = self._entry_f(f, scale, M)
+        g = self.gradient(f, fk)
+        R = self.residual(f, g, fk, a, infl, coll, fS)
+        sm0, sm5 = self.boundary_sums(f, g, M)
+        wi = self.wall_idx
+        phi = torch.clamp(-sm0[wi] / sm5[wi], min=0.0)
+        Fw = rho_gamma - phi
+        in_scale = scale  # pressure 1, vacuum 0, walls rho_Gamma
+        flow = self.barea * (sm0 + in_scale * sm5)
+        mdot_in = -flow[self.inlet_face].sum()
+        mdot_out = flow[self.outlet_face].sum()
+        J = 0.5 * (mdot_in + mdot_out) * math.sqrt(2.0 / math.pi)
+        return R, Fw, J
+
+    def params_of(self, solver=None):
+        Tw = self.T_patch.clone()
+        return torch.tensor(self.mu0, dtype=torch.float64), Tw
+
+
+def state_of(solver):
+    """(f, rho_Gamma of the wall faces) of a KineticSolver (internal numbering, storage order)."""
+    f = torch.as_tensor(np.asarray(solver.backend.get_distribution(), float))
+    wall = np.flatnonzero(solver.bkind == BC_DIFFUSE_WALL)
+    return f, torch.as_tensor(solver.inflow[wall, 0].copy())
+
+
+def adjoint_gradient(sm: SteadyMap, f, rho_gamma, tol=1e-12, maxiter=4000):
+    """dJ/d(mu_hat0) and dJ/dT_w (per boundary face; zero off the walls) at the fixed point (f, rho_Gamma), with the
+    adjoint solved by GMRES. Returns (dJ_dmu0, dJ_dTw (nb,), info) with info = (J, ||F||, gmres iterations)."""
+    from scipy.sparse.linalg import LinearOperator, gmres
+
+    mu0, Tw = sm.params_of()
+    f = f.clone().requires_grad_(True)
+    rg = rho_gamma.clone().requires_grad_(True)
+    mu0 = mu0.clone().requires_grad_(True)
+    Tw = Tw.clone().requires_grad_(True)
+    R, Fw, J = sm.evaluate(f, rg, mu0, Tw)
+    nf, nw = f.numel(), rg.numel()
+    gJ = torch.autograd.grad(J, (f, rg, mu0, Tw), allow_unused=True, retain_graph=True)
+    gJ = [torch.zeros_like(t) if g is None else g for g, t in zip(gJ, (f, rg, mu0, Tw))]
+    rhs = torch.cat([gJ[0].ravel(), gJ[1].ravel()]).numpy()
+
+    def vjp(y):
+        yt = torch.as_tensor(y)
+        yR, yW = yt[:nf].view_as(R), yt[nf:]
+        gf, gr = torch.autograd.grad((R, Fw), (f, rg), grad_outputs=(yR, yW), retain_graph=True, allow_unused=True)
+        gr = torch.zeros_like(rg) if gr is None else gr
+        return torch.cat([gf.ravel(), gr.ravel()]).numpy()
+
+    n = nf + nw
+    it = [0]
+
+    def cb(_):
+        it[0] += 1
+
+    op = LinearOperator((n, n), matvec=vjp, dtype=np.float64)
+    y, code = gmres(op, rhs, rtol=tol, atol=0.0, restart=400, maxiter=maxiter, callback=cb, callback_type="pr_norm")
+    if code != 0:
+        raise RuntimeError(f"adjoint GMRES did not converge (code {code})")
+    yt = torch.as_tensor(y)
+    gp = torch.autograd.grad((R, Fw), (mu0, Tw), grad_outputs=(yt[:nf].view_as(R), yt[nf:]), allow_unused=True)
+    gp = [torch.zeros_like(t) if g is None else g for g, t in zip(gp, (mu0, Tw))]
+    dmu = float(gJ[2] - gp[0])
+    dTw = (gJ[3] - gp[1]).detach().numpy()
+    fres = float(torch.sqrt((R.detach() ** 2).sum() + (Fw.detach() ** 2).sum()))
+    return dmu, dTw, (float(J.detach()), fres, it[0], y)
+
+
+def transposed_jacobian_product(sm: SteadyMap, f, rho_gamma, y_f, y_w):
+    """(dF/dx)^T y at (f, rho_Gamma): the adjoint residual operator the B200 kernels compute. Returns (x_f, x_w)."""
+    mu0, Tw = sm.params_of()
+    f = f.clone().requires_grad_(True)
+    rg = rho_gamma.clone().requires_grad_(True)
+    R, Fw, J = sm.evaluate(f, rg, mu0, Tw)
+    gf, gr = torch.autograd.grad((R, Fw), (f, rg), grad_outputs=(torch.as_tensor(y_f), torch.as_tensor(y_w)),
+                                 allow_unused=True)
+    return gf.numpy(), (torch.zeros_like(rg) if gr is None else gr).numpy()

@@ -1,0 +1,203 @@
+"""Discrete adjoint of the converged CIS fixed point (CPU part).
+
+* The reference adjoint (oracle/adjoint_ref.py: the steady map in torch, transposed by autograd) is pinned against
+  central finite differences of the converged CPU-oracle forward solver: dM_dot/d mu_hat0 and dM_dot/dT_w.
+* The host algebra of gsis_sim_b200/adjoint.py (moments -> Shakhov target -> collision term chain, pressure-face
+  chain, index maps) against torch autograd of the same forward formulas.
+The device kernels are checked against the reference adjoint in tests/test_gpu_adjoint.py."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from gsis_sim_b200 import adjoint as adj
+from gsis_sim_b200 import kinetic_setup as ks
+from gsis_sim_b200.mesh import box_mesh
+from gsis_sim_b200.solver import KineticSolver
+
+
+def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="periodic_slab", limiter="venkatakrishnan",
+                 eps="relative"):
+    """Pressure-driven channel (inlet p 1, outlet p 0.5, diffuse walls) in the adjoint's scope."""
+    m = box_mesh(n, (0, 0, 0), (2.0, 1.0, 1.0 / 3), ("inlet", "outlet", "wall", "wall", "side", "side"))
+    bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "pressure_outlet", p=0.5),
+           ks.BC("wall", "diffuse_wall", T=Tw), ks.BC("side", side)]
+    kp = ks.KineticParams(precision="fp64", pressure_boundary_reconstruction="cell", limiter=limiter,
+                          limiter_eps=eps, sweep_blocks=1, equilibrium="continuous")
+    setup, host = ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, Kn=0.3), bcs,
+                                         ks.VelocityGrid(n=nv), kp)
+    if mu_scale != 1.0:
+        setup["mu0"] = setup["mu0"] * mu_scale
+    return setup, host
+
+
+def converge(backend, setup, host, tol=1e-13, iters=3000):
+    sol = KineticSolver(setup, host, backend)
+    sol.initialize_uniform(0.75, (0.0, 0.0, 0.0), 1.0)
+    r = 1.0
+    for _ in range(iters):
+        r = sol.sweep().residual
+        if r < tol:
+            break
+    assert r < 1e-12
+    return sol
+
+
+def _oracle_solution(**kw):
+    from oracle.kinetic_oracle import OracleBackend
+
+    setup, host = channel_case(**kw)
+    return converge(OracleBackend(setup), setup, host), setup, host
+
+
+@pytest.mark.timeout(600)
+def test_reference_adjoint_matches_finite_differences():
+    from oracle import adjoint_ref as ar
+
+    sol, setup, host = _oracle_solution()
+    sm = ar.SteadyMap(setup, host)
+    sm.check_scope(sol)
+    f, rg = ar.state_of(sol)
+    mu0, Tw = sm.params_of()
+    R, Fw, J = sm.evaluate(f, rg, mu0, Tw)
+    # the torch map is the fixed point the oracle converged to
+    assert float(R.abs().max()) < 1e-13 and float(Fw.abs().max()) < 1e-13
+    assert abs(float(J) - sol.mass_flow()[2]) < 1e-14
+    dmu, dTw, info = ar.adjoint_gradient(sm, f, rg)
+    h = 1e-5
+    Jp = _oracle_solution(mu_scale=1 + h)[0].mass_flow()[2]
+    Jm = _oracle_solution(mu_scale=1 - h)[0].mass_flow()[2]
+    fd_mu = (Jp - Jm) / (2 * h * sm.mu0)
+    assert abs(dmu - fd_mu) <= 1e-6 * abs(fd_mu)
+    Jp = _oracle_solution(Tw=1 + h)[0].mass_flow()[2]
+    Jm = _oracle_solution(Tw=1 - h)[0].mass_flow()[2]
+    fd_T = (Jp - Jm) / (2 * h)
+    assert abs(dTw.sum() - fd_T) <= 1e-6 * abs(fd_T)
+    assert np.all(dTw[sm.bkind.numpy() != ar.BC_DIFFUSE_WALL] == 0.0)
+
+
+def _maxwellian_f(rng, nc, xi, w):
+    rho = 0.5 + rng.random(nc)
+    u = 0.3 * rng.standard_normal((nc, 3))
+    T = 0.8 + 0.4 * rng.random(nc)
+    c = xi[None] - u[:, None]
+    f = rho[:, None] / (2 * np.pi * T[:, None]) ** 1.5 * np.exp(-(c * c).sum(-1) / (2 * T[:, None]))
+    return f * (1 + 0.1 * rng.standard_normal(f.shape) * np.exp(-0.1 * (c * c).sum(-1)))
+
+
+def _moments(f, xi, w):
+    rho = f @ w
+    u = (f * w) @ xi / rho[:, None]
+    c = xi[None] - u[:, None]
+    c2 = (c * c).sum(-1)
+    p = (f * w * c2).sum(1) / 3
+    P = np.einsum("nq,nqa,nqb->nab", f * w, c, c)
+    q = 0.5 * np.einsum("nq,nqa->na", f * w * c2, c)
+    m = np.zeros((len(f), 15))
+    m[:, 0], m[:, 1:4], m[:, 4], m[:, 5] = rho, u, p / rho, p
+    m[:, 6], m[:, 7], m[:, 8] = P[:, 0, 0] - p, P[:, 1, 1] - p, P[:, 2, 2] - p
+    m[:, 9], m[:, 10], m[:, 11] = P[:, 0, 1], P[:, 1, 2], P[:, 0, 2]
+    m[:, 12:15] = q
+    return m
+
+
+def test_collision_chain_matches_autograd():
+    """lambda^T d[-coll (f^S(f) - f)]/df through the k_adj_cell sums, collision_moment_adjoint and the moment
+    expansion equals torch autograd of the same forward formulas."""
+    rng = np.random.default_rng(7)
+    g = np.linspace(-4.5, 4.5, 8)
+    xi = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    w = np.full(len(xi), (g[1] - g[0]) ** 3)
+    nc = 5
+    f = _maxwellian_f(rng, nc, xi, w)
+    lam = rng.standard_normal(f.shape)
+    vol, mu0, omega, Pr = 0.3 + rng.random(nc), 0.07, 0.81, 2.0 / 3.0
+    # forward in torch
+    ft = torch.tensor(f, requires_grad=True)
+    xt, wt = torch.tensor(xi), torch.tensor(w)
+    rho = ft @ wt
+    u = (ft * wt) @ xt / rho[:, None]
+    c = xt[None] - u[:, None]
+    c2 = (c * c).sum(-1)
+    p = (ft * wt * c2).sum(1) / 3
+    T = p / rho
+    q = 0.5 * ((ft * wt * c2)[..., None] * c).sum(1)
+    kap = (1 - Pr) / (5 * rho * T * T)
+    M = rho[:, None] / (2 * np.pi * T[:, None]) ** 1.5 * torch.exp(-c2 / (2 * T[:, None]))
+    fS = M * (1 + kap[:, None] * (c * q[:, None]).sum(-1) * (c2 / T[:, None] - 5))
+    coll = torch.tensor(vol) * p / (mu0 * T ** omega)
+    R = -coll[:, None] * (fS - ft)
+    (g_ref,) = torch.autograd.grad(R, ft, grad_outputs=torch.tensor(lam))
+    # the same through the adjoint pieces (k_adj_cell sums restated in numpy)
+    m = _moments(f, xi, w)
+    rho_n, u_n, T_n = m[:, 0], m[:, 1:4], m[:, 4]
+    q_n = m[:, 12:15]
+    cc = xi[None] - u_n[:, None]
+    c2n = (cc * cc).sum(-1)
+    kn = (1 - Pr) / (5 * rho_n * T_n * T_n)
+    Mn = rho_n[:, None] / (2 * np.pi * T_n[:, None]) ** 1.5 * np.exp(-c2n / (2 * T_n[:, None]))
+    cq = (cc * q_n[:, None]).sum(-1)
+    h = c2n / T_n[:, None] - 5
+    P = kn[:, None] * cq * h
+    lm = lam * Mn
+    Tt, kk = T_n[:, None], kn[:, None]
+    sums = np.zeros((nc, 9))
+    sums[:, 0] = (lam * (Mn * (1 + P) - f)).sum(1)
+    sums[:, 1] = (lm / rho_n[:, None]).sum(1)
+    for a in range(3):
+        sums[:, 2 + a] = (lm * (cc[..., a] / Tt * (1 + P) + kk * (-q_n[:, a:a + 1] * h - 2 * cq * cc[..., a] / Tt))).sum(1)
+        sums[:, 6 + a] = (lm * kk * cc[..., a] * h).sum(1)
+    sums[:, 5] = (lm * ((c2n / (2 * Tt * Tt) - 1.5 / Tt) * (1 + P) + cq * (-2 * kk / Tt * h - kk * c2n / (Tt * Tt)))).sum(1)
+    rb, ub, Tb, qb, colln = adj.collision_moment_adjoint(m, vol, mu0, omega, sums)
+    coef = adj.moment_expansion_coefficients(m, rb, ub, Tb, qb)
+    fb = colln[:, None] * lam + w * (coef[:, 0:1] + (cc * coef[:, None, 1:4]).sum(-1) + coef[:, 4:5] * c2n +
+                                    (cc * coef[:, None, 5:8]).sum(-1) * c2n)
+    assert np.max(np.abs(fb - g_ref.numpy())) <= 1e-11 * np.max(np.abs(g_ref.numpy()))
+
+
+def test_pressure_face_adjoint_matches_autograd():
+    rng = np.random.default_rng(3)
+    n_f = 6
+    p_o = torch.tensor(0.5 + rng.random(n_f), requires_grad=True)
+    u_o = torch.tensor(0.2 * rng.standard_normal((n_f, 3)), requires_grad=True)
+    T_o = torch.tensor(0.8 + 0.4 * rng.random(n_f), requires_grad=True)
+    nrm = rng.standard_normal((n_f, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    p_pat = 0.3 + rng.random(n_f)
+    T_pat = 0.9 + 0.2 * rng.random(n_f)
+    inlet = np.array([True, False, True, False, True, False])
+    zt = np.array([False, False, True, True, False, True])
+    gamma = 5.0 / 3.0
+    nt = torch.tensor(nrm)
+    rho_ib = p_o / T_o
+    du = (p_o - torch.tensor(p_pat)) / (rho_ib * torch.sqrt(gamma * T_o))
+    un = (u_o * nt).sum(1)
+    u_b = torch.where(torch.tensor(zt)[:, None], (un + du)[:, None] * nt, u_o + du[:, None] * nt)
+    T_b = torch.where(torch.tensor(inlet), torch.tensor(T_pat), T_o)
+    rho_b = torch.tensor(p_pat) / T_b
+    rbar, ubar, Tbar = rng.standard_normal(n_f), rng.standard_normal((n_f, 3)), rng.standard_normal(n_f)
+    L = (rho_b * torch.tensor(rbar)).sum() + (u_b * torch.tensor(ubar)).sum() + (T_b * torch.tensor(Tbar)).sum()
+    gp, gu, gT = torch.autograd.grad(L, (p_o, u_o, T_o))
+    pb, ub, Tb = adj.pressure_face_adjoint(p_o.detach().numpy(), u_o.detach().numpy(), T_o.detach().numpy(), nrm,
+                                           p_pat, inlet, zt, gamma, rbar, ubar, Tbar)
+    assert np.allclose(pb, gp.numpy(), rtol=1e-12, atol=1e-14)
+    assert np.allclose(ub, gu.numpy(), rtol=1e-12, atol=1e-14)
+    assert np.allclose(Tb, gT.numpy(), rtol=1e-12, atol=1e-14)
+
+
+def test_index_maps():
+    setup, host = channel_case()
+    xi = np.stack([setup["xi_x"], setup["xi_y"], setup["xi_z"]], 1)
+    rev = adj.reversed_velocities(xi)
+    assert np.array_equal(xi[rev], -xi) and np.array_equal(rev[rev], np.arange(len(xi)))
+    re = adj.reverse_entries(setup["csr_offsets"], setup["csr_other"], host.csr_faces)
+    offs, other = np.asarray(setup["csr_offsets"]), np.asarray(setup["csr_other"])
+    row = np.repeat(np.arange(len(offs) - 1), np.diff(offs))
+    internal = other >= 0
+    assert np.all(re[~internal] == -1)
+    e = np.flatnonzero(internal)
+    assert np.array_equal(row[re[e]], other[e]) and np.array_equal(other[re[e]], row[e])
+    assert np.array_equal(re[re[e]], e)
+    with pytest.raises(adj.AdjointScopeError):
+        adj.reversed_velocities(xi + 0.1)

@@ -1,0 +1,90 @@
+"""Discrete adjoint on the B200 (csrc/kin_adjoint.cu + gsis_sim_b200/adjoint.py) against the reference adjoint of
+oracle/adjoint_ref.py (the steady map transposed by torch autograd, itself pinned against finite differences in
+tests/test_adjoint.py), at the fixed point the B200 forward solver converged to:
+* the operator y^T dF/dx (and the objective term dJ/dx) for random adjoint states, to 1e-10;
+* the converged adjoint's dM_dot/d mu_hat0 and dM_dot/dT_w, to 1e-8 against the reference adjoint and to 1e-5
+  against central finite differences of the B200 forward solver."""
+import numpy as np
+import pytest
+import torch
+
+from tests.test_adjoint import channel_case, converge
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_solution(**kw):
+    from gsis_sim_b200.backend import B200Backend
+
+    setup, host = channel_case(**kw)
+    be = B200Backend(setup)
+    return converge(be, setup, host), setup, host
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(side="symmetry"), dict(limiter="none"), dict(eps="absolute"),
+                                dict(n=(6, 4, 2), side="symmetry")])
+def test_gpu_adjoint_operator_matches_reference(kw):
+    from gsis_sim_b200.adjoint import KineticAdjoint
+    from oracle import adjoint_ref as ar
+
+    assert torch.cuda.is_available()
+    sol, setup, host = _gpu_solution(**kw)
+    try:
+        ka = KineticAdjoint(sol)
+        sm = ar.SteadyMap(setup, host)
+        f, rg = ar.state_of(sol)
+        rng = np.random.default_rng(11)
+        lam = rng.standard_normal((sol.nc, sol.nv))
+        nu = rng.standard_normal(len(ka.wall))
+        op_f, op_w = ka.operator(lam, nu, with_objective=False)
+        ref_f, ref_w = ar.transposed_jacobian_product(sm, f, rg, lam, nu)
+        scale = np.max(np.abs(ref_f))
+        assert np.max(np.abs(op_f - ref_f)) <= 1e-10 * scale
+        assert np.max(np.abs(op_w - ref_w)) <= 1e-10 * max(np.max(np.abs(ref_w)), 1e-300)
+        # the objective term: O(y) - y^T dF/dx = -dJ/dx
+        mu0, Tw = sm.params_of()
+        ft = f.clone().requires_grad_(True)
+        rt = rg.clone().requires_grad_(True)
+        _, _, J = sm.evaluate(ft, rt, mu0, Tw)
+        gJ = torch.autograd.grad(J, (ft, rt), allow_unused=True)
+        gJf = gJ[0].numpy()
+        gJw = np.zeros(len(nu)) if gJ[1] is None else gJ[1].numpy()
+        opJ_f, opJ_w = ka.operator(lam, nu, with_objective=True)
+        assert np.max(np.abs((opJ_f - op_f) + gJf)) <= 1e-10 * max(np.max(np.abs(gJf)), scale)
+        assert np.max(np.abs((opJ_w - op_w) + gJw)) <= 1e-10 * max(np.max(np.abs(ref_w)), 1e-300)
+        ka.close()
+    finally:
+        sol.backend.close()
+
+
+@pytest.mark.timeout(900)
+def test_gpu_adjoint_gradients_match_reference_and_finite_differences():
+    from gsis_sim_b200.adjoint import KineticAdjoint
+    from oracle import adjoint_ref as ar
+
+    sol, setup, host = _gpu_solution()
+    try:
+        ka = KineticAdjoint(sol)
+        res = ka.solve(tol=1e-12, max_iterations=4000)
+        assert res.residual < 1e-10
+        sm = ar.SteadyMap(setup, host)
+        f, rg = ar.state_of(sol)
+        dmu, dTw, _ = ar.adjoint_gradient(sm, f, rg)
+        assert abs(res.dJ_dmu0 - dmu) <= 1e-8 * abs(dmu)
+        assert np.max(np.abs(res.dJ_dTw - dTw)) <= 1e-8 * np.max(np.abs(dTw))
+        ka.close()
+    finally:
+        sol.backend.close()
+    h = 1e-5
+    Jp = _gpu_solution(mu_scale=1 + h)
+    Jm = _gpu_solution(mu_scale=1 - h)
+    fd_mu = (Jp[0].mass_flow()[2] - Jm[0].mass_flow()[2]) / (2 * h * float(setup["mu0"]))
+    for s in (Jp, Jm):
+        s[0].backend.close()
+    assert abs(res.dJ_dmu0 - fd_mu) <= 1e-5 * abs(fd_mu)
+    Tp = _gpu_solution(Tw=1 + h)
+    Tm = _gpu_solution(Tw=1 - h)
+    fd_T = (Tp[0].mass_flow()[2] - Tm[0].mass_flow()[2]) / (2 * h)
+    for s in (Tp, Tm):
+        s[0].backend.close()
+    assert abs(res.dJ_dTw.sum() - fd_T) <= 1e-5 * abs(fd_T)
