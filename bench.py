@@ -300,6 +300,107 @@ def run_time_to_mdot(args, local):
     print(json.dumps(line), flush=True)
 
 
+def channel_case(delta=5.0, Tw=1.0, nv=24, n=(64, 32, 1)):
+    """Pressure-driven channel: box n[0] x n[1] x 1 on x in [0, 4], y in [0, 1], one cell thick with periodic sides;
+    inlet p 1, outlet p 0.5, T 1; diffuse walls T_w; nv^3 uniform velocities on [-5, 5]^3; FP64 with the continuous
+    equilibrium and the "cell" pressure-boundary reconstruction (the adjoint's scope)."""
+    from gsis_sim_b200 import kinetic_setup as ks
+    from gsis_sim_b200.mesh import box_mesh
+
+    m = box_mesh(n, (0.0, 0.0, 0.0), (4.0, 1.0, 1.0 / n[1]), ("inlet", "outlet", "wall", "wall", "side", "side"))
+    bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "pressure_outlet", p=0.5),
+           ks.BC("wall", "diffuse_wall", T=Tw), ks.BC("side", "periodic_slab")]
+    kp = ks.KineticParams(precision="fp64", equilibrium="continuous", pressure_boundary_reconstruction="cell")
+    return ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, delta_rp=delta), bcs,
+                                  ks.VelocityGrid(n=(nv, nv, nv)), kp)
+
+
+def converge_channel(setup, host, local, tol, max_iters):
+    """Plain CIS from rest to a residual below tol; returns (solver, wall seconds, iterations)."""
+    import torch
+
+    from gsis_sim_b200.backend import B200Backend
+    from gsis_sim_b200.solver import KineticSolver
+
+    be = B200Backend(setup, device=local)
+    sol = KineticSolver(setup, host, be)
+    sol.initialize_uniform(0.75, (0.0, 0.0, 0.0), 1.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    it = 0
+    for it in range(1, max_iters + 1):
+        if sol.sweep().residual < tol:
+            break
+    sol.prepare()
+    torch.cuda.synchronize()
+    return sol, time.perf_counter() - t0, it
+
+
+def run_adjoint(args, local):
+    """Adjoint / forward wall-time ratio on the channel (or, --adjoint-case tube, on the tube mesh): the forward CIS
+    solve from rest to residual --fwd-tol, then
+    the adjoint solve of dM_dot/d(delta, T_w) to --adj-tol (both through the public host loops, wall clock). With
+    --adjoint-fd also the central finite difference of M_dot in delta (two more forward solves)."""
+    import numpy as np
+    import torch
+
+    from gsis_sim_b200.adjoint import KineticAdjoint
+
+    torch.cuda.set_device(local)
+    if args.adjoint_case == "tube":
+        from gsis_sim_b200 import tube
+
+        delta = 10.0
+
+        def make(d):
+            return tube.tube_case(delta=d, nv=args.adj_nv, precision="fp64", equilibrium="continuous",
+                                  pressure_boundary_reconstruction="cell")
+
+        workload = (f"kinetic CIS, O-grid tube + reservoir 134528 cells, inlet p 1 / outlet p 0.01, diffuse walls, "
+                    f"{args.adj_nv}^3 velocities on [-5,5]^3, delta 10, continuous equilibrium")
+    else:
+        delta = 5.0
+
+        def make(d):
+            return channel_case(delta=d, nv=args.adj_nv)
+
+        workload = (f"kinetic CIS, channel 64x32x1 cells x in [0,4], inlet p 1 / outlet p 0.5, diffuse walls, "
+                    f"{args.adj_nv}^3 velocities on [-5,5]^3, delta 5, continuous equilibrium")
+    setup, host = make(delta)
+    sol, t_fwd, it_fwd = converge_channel(setup, host, local, args.fwd_tol, args.max_iters)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ka = KineticAdjoint(sol)
+    res = ka.solve(tol=args.adj_tol, max_iterations=args.max_iters)
+    torch.cuda.synchronize()
+    t_adj = time.perf_counter() - t0
+    mu0 = float(setup["mu0"])
+    dJ_ddelta = res.dJ_ddelta(mu0, delta)
+    ka.close()
+    sol.backend.close()
+    line = {"metric": "adjoint / forward wall-time ratio (dM_dot / d(delta, T_w per wall face))",
+            "value": t_adj / t_fwd, "unit": "x", "higher_is_better": False,
+            "forward_seconds": t_fwd, "forward_iterations": it_fwd, "adjoint_seconds": t_adj,
+            "adjoint_iterations": res.iterations, "adjoint_residual": res.residual, "M_dot": res.J,
+            "dM_dot_d_delta": dJ_ddelta, "dM_dot_dT_w_sum": float(np.sum(res.dJ_dTw)),
+            "dM_dot_dT_w_max_abs": float(np.max(np.abs(res.dJ_dTw))),
+            "n_wall_faces": int(np.count_nonzero(res.dJ_dTw)), "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload, "cells": setup.n_cells, "velocities": setup.nv,
+                       "forward_tol": args.fwd_tol, "adjoint_tol": args.adj_tol}}
+    if args.adjoint_fd:
+        h = 1e-5
+        Js = []
+        for sgn in (1, -1):
+            sp, hp = make(delta * (1 + sgn * h))
+            sp_sol = converge_channel(sp, hp, local, args.fwd_tol, args.max_iters)[0]
+            Js.append(sp_sol.mass_flow()[2])
+            sp_sol.backend.close()
+        fd = (Js[0] - Js[1]) / (2 * h * delta)
+        line["dM_dot_d_delta_fd"] = fd
+        line["fd_rel_error"] = abs(dJ_ddelta - fd) / abs(fd)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -323,6 +424,13 @@ def main():
     ap.add_argument("--mdot-tol", type=float, default=1e-4)
     ap.add_argument("--max-iters", type=int, default=2000)
     ap.add_argument("--history", default=None, help="write per-iteration (wall s, M_dot, residual) to <prefix>_<prec>.txt")
+    # third headline metric: adjoint / forward wall-time ratio on the channel
+    ap.add_argument("--adjoint", action="store_true")
+    ap.add_argument("--adjoint-fd", action="store_true", help="with --adjoint: also the finite difference in delta")
+    ap.add_argument("--adj-nv", type=int, default=24)
+    ap.add_argument("--adjoint-case", default="channel", choices=["channel", "tube"])
+    ap.add_argument("--fwd-tol", type=float, default=1e-10)
+    ap.add_argument("--adj-tol", type=float, default=1e-10)
     args = ap.parse_args()
 
     rank, ws, local = dist_init() if args.gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1 else (0, 1, 0)
@@ -332,6 +440,10 @@ def main():
     if args.time_to_mdot:
         if rank == 0:
             run_time_to_mdot(args, local)
+        return
+    if args.adjoint:
+        if rank == 0:
+            run_adjoint(args, local)
         return
 
     import numpy as np

@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_gather(View<double, double>
       if (c.other >= 0) {
         const int n = c.other;
         const int eb = a.rev_entry[e];
+        if (eb < 0) continue;
         const CsrE<double>& cn = v.csr[eb];
         const int k = eb - v.csr_off[n];
         const int64_t j = static_cast<int64_t>(n) * nv + q;

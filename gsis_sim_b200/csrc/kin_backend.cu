@@ -1227,6 +1227,7 @@ struct Backend final : KinHandle {
     } else {
       KCHECK(chunk == nv, "the adjoint needs one velocity chunk (velocity_chunk = 0 with enough device memory)");
       KCHECK(n_maxwell == 0, "the adjoint does not cover Maxwell walls");
+      KCHECK(max_entries <= 127, "the adjoint stores stencil entry offsets in 8 bits (at most 127 faces per cell)");
       KCHECK(rev_velocity != nullptr && rev_entry != nullptr, "missing adjoint maps");
       std::vector<int32_t> hcsr(static_cast<size_t>(nc) + 1);
       KCUDA(cudaMemcpy(hcsr.data(), csr_off.p, hcsr.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));

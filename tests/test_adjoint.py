@@ -18,11 +18,22 @@ from gsis_sim_b200.solver import KineticSolver
 
 
 def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="periodic_slab", limiter="venkatakrishnan",
-                 eps="relative"):
-    """Pressure-driven channel (inlet p 1, outlet p 0.5, diffuse walls) in the adjoint's scope."""
-    m = box_mesh(n, (0, 0, 0), (2.0, 1.0, 1.0 / 3), ("inlet", "outlet", "wall", "wall", "side", "side"))
+                 eps="relative", half=False, quarter=False):
+    """Pressure-driven channel (inlet p 1, outlet p 0.5, diffuse walls) in the adjoint's scope; `half`: symmetry
+    plane at y = 0 instead of the lower wall; `quarter`: a duct quarter, symmetry planes at y = 0 and z = 0, walls at
+    y = 1 and z = 0.7 (a flow that varies in y and z)."""
+    lower = "sym" if (half or quarter) else "wall"
+    sides = ("symz", "wall") if quarter else ("side", "side")
+    hz = 0.7 if quarter else 1.0 / 3  # quarter: not square, so no y <-> z mirror symmetry (no limiter ties)
+    m = box_mesh(n, (0, 0, 0), (2.0, 1.0, hz), ("inlet", "outlet", lower, "wall", *sides))
     bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "pressure_outlet", p=0.5),
-           ks.BC("wall", "diffuse_wall", T=Tw), ks.BC("side", side)]
+           ks.BC("wall", "diffuse_wall", T=Tw)]
+    if not quarter:
+        bcs.append(ks.BC("side", side))
+    if half or quarter:
+        bcs.append(ks.BC("sym", "symmetry"))
+    if quarter:
+        bcs.append(ks.BC("symz", "symmetry"))
     kp = ks.KineticParams(precision="fp64", pressure_boundary_reconstruction="cell", limiter=limiter,
                           limiter_eps=eps, sweep_blocks=1, equilibrium="continuous")
     setup, host = ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, Kn=0.3), bcs,

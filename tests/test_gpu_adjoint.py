@@ -21,8 +21,13 @@ def _gpu_solution(**kw):
     return converge(be, setup, host), setup, host
 
 
-@pytest.mark.parametrize("kw", [dict(), dict(side="symmetry"), dict(limiter="none"), dict(eps="absolute"),
-                                dict(n=(6, 4, 2), side="symmetry")])
+# States with exact ties in the limiter's stencil extrema are left out of the operator comparison: a channel between
+# two symmetry planes z = const does not vary in z and is mirror-symmetric in xi_z to the last bit, so neighbour and
+# symmetry-face values equal the cell's own. There the max / min has no derivative, the kernels take the first
+# extremum (the cell's own value) and autograd splits the seed; both agree on every mirror-symmetric direction, which
+# the gradient test covers (side="symmetry").
+@pytest.mark.parametrize("kw", [dict(), dict(half=True), dict(limiter="none"), dict(eps="absolute"),
+                                dict(n=(5, 3, 3), quarter=True), dict(n=(5, 3, 3), quarter=True, limiter="none")])
 def test_gpu_adjoint_operator_matches_reference(kw):
     from gsis_sim_b200.adjoint import KineticAdjoint
     from oracle import adjoint_ref as ar
@@ -58,11 +63,12 @@ def test_gpu_adjoint_operator_matches_reference(kw):
 
 
 @pytest.mark.timeout(900)
-def test_gpu_adjoint_gradients_match_reference_and_finite_differences():
+@pytest.mark.parametrize("kw", [dict(), dict(side="symmetry")])
+def test_gpu_adjoint_gradients_match_reference_and_finite_differences(kw):
     from gsis_sim_b200.adjoint import KineticAdjoint
     from oracle import adjoint_ref as ar
 
-    sol, setup, host = _gpu_solution()
+    sol, setup, host = _gpu_solution(**kw)
     try:
         ka = KineticAdjoint(sol)
         res = ka.solve(tol=1e-12, max_iterations=4000)
@@ -76,14 +82,14 @@ def test_gpu_adjoint_gradients_match_reference_and_finite_differences():
     finally:
         sol.backend.close()
     h = 1e-5
-    Jp = _gpu_solution(mu_scale=1 + h)
-    Jm = _gpu_solution(mu_scale=1 - h)
+    Jp = _gpu_solution(mu_scale=1 + h, **kw)
+    Jm = _gpu_solution(mu_scale=1 - h, **kw)
     fd_mu = (Jp[0].mass_flow()[2] - Jm[0].mass_flow()[2]) / (2 * h * float(setup["mu0"]))
     for s in (Jp, Jm):
         s[0].backend.close()
     assert abs(res.dJ_dmu0 - fd_mu) <= 1e-5 * abs(fd_mu)
-    Tp = _gpu_solution(Tw=1 + h)
-    Tm = _gpu_solution(Tw=1 - h)
+    Tp = _gpu_solution(Tw=1 + h, **kw)
+    Tm = _gpu_solution(Tw=1 - h, **kw)
     fd_T = (Tp[0].mass_flow()[2] - Tm[0].mass_flow()[2]) / (2 * h)
     for s in (Tp, Tm):
         s[0].backend.close()
