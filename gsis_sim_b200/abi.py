@@ -235,7 +235,7 @@ def declare_backend_api(lib, prefix: str, handle_type=C.c_void_p):
         "discrete_maxwell_noalloc": [h, _dp, C.c_int64, C.c_double, _dp, _ip],
         "moment_sums": [h, _dp, C.c_int64],
         "set_moments": [h, _dp, C.c_int64],
-        "adjoint_begin": [h, _ip, _ip, C.c_int64],
+        "adjoint_begin": [h, _ip, _ip, C.c_int64, _ip, _ip],
         "adjoint_set": [h, _dp, C.c_int64],
         "adjoint_get": [h, _dp, C.c_int64],
         "adjoint_reduce": [h, _dp, C.c_int64, _dp, C.c_int64, _dp, C.c_int64],

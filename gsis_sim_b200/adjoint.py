@@ -1,4 +1,5 @@
-"""Discrete adjoint of the converged CIS fixed point: dM_dot / d(mu_hat0, delta, T_w per wall face) on the B200 backend.
+"""Discrete adjoint of the converged CIS fixed point: dM_dot / d(mu_hat0, delta, T_w per wall face, accommodation per
+wall face at alpha = 1) on the B200 backend.
 
 There is no reference counterpart; the steady problem differentiated is the one the reference's CIS iteration
 converges to (src/kinetic/kinetic_solver.cpp prepare + sweep, src/kinetic/kinetic_kernels.hpp):
@@ -50,6 +51,29 @@ def reversed_velocities(xi: np.ndarray) -> np.ndarray:
     if np.any(rev < 0):
         raise AdjointScopeError("the velocity grid is not symmetric about 0 (no reversed velocity)")
     return rev
+
+
+def flipped_velocities(xi: np.ndarray) -> np.ndarray:
+    """(3, nv): for each axis a, the index of xi with component a negated. Raises AdjointScopeError."""
+    xi = np.asarray(xi, float)
+    scale = max(float(np.abs(xi).max()), 1e-300)
+    key = np.round(xi / scale * 2.0 ** 40).astype(np.int64)
+    index = {tuple(k): i for i, k in enumerate(key.tolist())}
+    out = np.empty((3, len(xi)), np.int32)
+    for a in range(3):
+        sgn = np.ones(3, np.int64)
+        sgn[a] = -1
+        out[a] = [index.get(tuple((k * sgn).tolist()), -1) for k in key]
+    if np.any(out < 0):
+        raise AdjointScopeError("the velocity grid is not symmetric in every axis")
+    return out
+
+
+def face_axes(normals: np.ndarray, tol: float = 1e-10) -> np.ndarray:
+    """The axis each unit normal is aligned with, -1 if none."""
+    n = np.abs(np.asarray(normals, float))
+    ax = np.argmax(n, axis=1).astype(np.int32)
+    return np.where(np.abs(n[np.arange(len(n)), ax] - 1.0) < tol, ax, -1).astype(np.int32)
 
 
 def reverse_entries(csr_offsets, csr_other, csr_faces) -> np.ndarray:
@@ -127,6 +151,8 @@ class AdjointResult:
     J: float
     dJ_dmu0: float
     dJ_dTw: np.ndarray       # per boundary face (internal numbering), zero off the diffuse walls
+    dJ_dalpha: np.ndarray    # per boundary face: the accommodation derivative at alpha = 1 (from below) of the
+    #                          axis-aligned diffuse walls, NaN for other wall faces, zero off the walls
     iterations: int
     residual: float
     history: list
@@ -148,7 +174,10 @@ class KineticAdjoint:
         xi = np.stack([np.asarray(s["xi_x"]), np.asarray(s["xi_y"]), np.asarray(s["xi_z"])], 1)
         self.rev_v = reversed_velocities(xi)
         self.rev_e = reverse_entries(s["csr_offsets"], s["csr_other"], h.csr_faces)
-        solver.backend.adjoint_begin(self.rev_v, self.rev_e)
+        self.flip = flipped_velocities(xi)
+        self.axis = face_axes(np.asarray(s["bface_geom"], float).reshape(-1, 7)[:, 0:3]) if solver.nb else \
+            np.zeros(0, np.int32)
+        solver.backend.adjoint_begin(self.rev_v, self.rev_e, self.flip.ravel(), self.axis)
         bk = solver.bkind
         self.wall = np.flatnonzero(bk == abi.BC_DIFFUSE_WALL)
         self.pres = np.flatnonzero(bk == abi.BC_PRESSURE)
@@ -201,7 +230,7 @@ class KineticAdjoint:
 
     def _reduce(self):
         cell, face = self.sol.backend.adjoint_reduce(self._mu())
-        return cell.reshape(self.nc, 9), face.reshape(max(self.nb, 0), 7)
+        return cell.reshape(self.nc, 9), face.reshape(max(self.nb, 0), 10)
 
     def _coefficients(self, cell, face):
         sol = self.sol
@@ -250,9 +279,17 @@ class KineticAdjoint:
         return op.reshape(self.nc, self.nv), face[self.wall, 0] + self.nu
 
     # ---- the solve -----------------------------------------------------------------------------------------------
-    def solve(self, tol: float = 1e-10, max_iterations: int = 5000, callback=None) -> AdjointResult:
-        """Iterate to ||O_f||_2 / ||dJ/df||_2 < tol and the same for the wall equations; return the gradients."""
+    def solve(self, tol: float = 1e-10, max_iterations: int = 5000, inner: int | None = None,
+              callback=None) -> AdjointResult:
+        """Iterate to ||O_f||_2 / ||O_f(0)||_2 < tol (and the wall densities settled to tol); return the gradients.
+
+        Mirrors the forward CIS iteration: per outer iteration the coupling terms (moment expansion of the cell
+        parameters, pressure-face chain) are evaluated once and frozen for `inner` transposed transport sweeps
+        (default: the set-up's inner_sweeps), with the wall adjoint refreshed after each sweep as the forward
+        refreshes rho_Gamma. The outer iteration then has the spectrum of the forward's. `max_iterations` counts
+        outer iterations; the residual is that of the first sweep of each outer iteration (fresh coupling)."""
         be = self.sol.backend
+        inner = max(1, int(self.sol.h.inner_sweeps if inner is None else inner))
         ref = None
         it = 0
         res = math.inf
@@ -270,8 +307,14 @@ class KineticAdjoint:
             self.history.append(r)
             if callback is not None:
                 callback(it, r)
+            if not math.isfinite(r):
+                raise FloatingPointError(f"adjoint iteration diverged at outer iteration {it}")
             if r / ref < tol and (len(nu_new) == 0 or dnu <= tol * max(float(np.abs(nu_new).max()), 1e-300)):
                 break
+            for _ in range(1, inner):
+                _, face = self._reduce()
+                be.adjoint_update(coef, run_passes=True)
+                self.nu = -face[self.wall, 0]
         return self.gradients(it, res)
 
     def gradients(self, iterations: int = 0, residual: float = 0.0) -> AdjointResult:
@@ -293,8 +336,16 @@ class KineticAdjoint:
                 pos = (sm5 < 0) & (-sm0 / sm5 > 0)
                 dPhi = np.where(pos, sm0 / (sm5 * sm5) * D5, 0.0)
             dTw[w] = -(dR - self.nu * dPhi)
+        # accommodation at alpha = 1: the inflow rho M + (1 - alpha) f_spec of a Maxwell wall and its zero-net-flux
+        # density rho = -(sm0 + (1 - alpha) S_spec) / sm5; dJ/dalpha = A1 + A2 + nu S_spec / sm5
+        dA = np.zeros(self.nb)
+        if len(w):
+            S = face[w]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                nu_t = np.where(pos, self.nu * S[:, 9] / sm5, 0.0)
+            dA[w] = np.where(self.axis[w] >= 0, S[:, 7] + S[:, 8] + nu_t, np.nan)
         J = sol.mass_flow()[2]
-        return AdjointResult(J=J, dJ_dmu0=dmu, dJ_dTw=dTw, iterations=iterations, residual=residual,
+        return AdjointResult(J=J, dJ_dmu0=dmu, dJ_dTw=dTw, dJ_dalpha=dA, iterations=iterations, residual=residual,
                              history=list(self.history))
 
     def close(self):

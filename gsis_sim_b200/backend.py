@@ -15,6 +15,9 @@ from . import abi
 from ._lib import load_library
 
 
+ADJ_FACE_SUMS = 10  # per boundary face sums of kin_adjoint_reduce
+
+
 class KineticError(RuntimeError):
     """A backend call failed (the reference raises gsis::Error in the same places)."""
 
@@ -75,11 +78,14 @@ class KineticBackendABI:
         self._call("set_moments", abi.as_ptr(m, C.c_double), m.size)
 
     # --- discrete adjoint (gsis_sim_b200.adjoint drives these) -----------------------------------------------
-    def adjoint_begin(self, rev_velocity, rev_entry) -> None:
+    def adjoint_begin(self, rev_velocity, rev_entry, flip_velocity=None, face_axis=None) -> None:
         rv = np.ascontiguousarray(rev_velocity, dtype=np.int32)
         re = np.ascontiguousarray(rev_entry, dtype=np.int32)
-        self._adj_keep = (rv, re)
-        self._call("adjoint_begin", abi.as_ptr(rv, C.c_int32), abi.as_ptr(re, C.c_int32), re.size)
+        fl = None if flip_velocity is None else np.ascontiguousarray(flip_velocity, dtype=np.int32)
+        fa = None if face_axis is None else np.ascontiguousarray(face_axis, dtype=np.int32)
+        self._adj_keep = (rv, re, fl, fa)
+        self._call("adjoint_begin", abi.as_ptr(rv, C.c_int32), abi.as_ptr(re, C.c_int32), re.size,
+                   None if fl is None else abi.as_ptr(fl, C.c_int32), None if fa is None else abi.as_ptr(fa, C.c_int32))
 
     def adjoint_set(self, lam) -> None:
         a = np.ascontiguousarray(lam, dtype=np.float64).ravel()
@@ -93,10 +99,10 @@ class KineticBackendABI:
     def adjoint_reduce(self, mu):
         m = np.ascontiguousarray(mu, dtype=np.float64)
         cell = np.empty(self.n_cells * 9, dtype=np.float64)
-        face = np.empty(max(self.n_bfaces, 1) * 7, dtype=np.float64)
+        face = np.empty(max(self.n_bfaces, 1) * ADJ_FACE_SUMS, dtype=np.float64)
         self._call("adjoint_reduce", abi.as_ptr(m, C.c_double), m.size, abi.as_ptr(cell, C.c_double), cell.size,
-                   abi.as_ptr(face, C.c_double), self.n_bfaces * 7)
-        return cell, face[:self.n_bfaces * 7]
+                   abi.as_ptr(face, C.c_double), self.n_bfaces * ADJ_FACE_SUMS)
+        return cell, face[:self.n_bfaces * ADJ_FACE_SUMS]
 
     def adjoint_update(self, coef, run_passes: bool = True, want_operator: bool = False):
         c = np.ascontiguousarray(coef, dtype=np.float64).ravel()

@@ -220,7 +220,12 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_transport(View<double, doub
 
 // k_adj_faces: per wall / pressure face, the seeds on the incoming inflow values (residual term, gradient entry and
 // limiter extremum) summed against the inflow Maxwellian m: S0 = sum s M, S1 = sum s M c, S2 = sum s M c^2 with
-// c = xi - u_b; for the wall-temperature derivative of sm5 also S5 = sum_in w an M c^2, S6 = sum_in w an M.
+// c = xi - u_b; for the wall-temperature derivative of sm5 also S5 = sum_in w an M c^2, S6 = sum_in w an M. For a
+// diffuse wall aligned with an axis, the partially specular inflow rho M + (1 - alpha) f_spec of a Maxwell wall
+// (maxwell_inflow / reflected_value, src/kinetic/kinetic_kernels.hpp:86-133) gives the accommodation derivative at
+// alpha = 1 from A1 = sum_in a lambda f_spec (f_spec: the owner's reconstructed face value at the reflected
+// velocity), A2 = sum_in s_grad f_o(reflected) (the first-order specular value of the gradient) and
+// S_spec = sum_in w an f_spec.
 __global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<double, double> v, AdjView a, double* __restrict__ out) {
   __shared__ double sh[kAdjFaceSums * (kAdjThreads / 32)];
   const int b = blockIdx.x;
@@ -259,6 +264,18 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<double, double> 
       const double wa = wq * ae / bf.area * M;
       s[5] += wa * c2;
       s[6] += wa;
+      if (bf.kind == kDiffuseWall && a.face_axis != nullptr && a.face_axis[b] >= 0) {
+        const int r = a.flip[a.face_axis[b] * nv + q];
+        const double xr = v.xi_x[r], yr = v.xi_y[r], zr = v.xi_z[r];
+        const double fr = f_at(v, o, r);
+        double gx, gy, gz;
+        limited_gradient(v, o, r, xr, yr, zr, fr, gx, gy, gz);
+        const double fspec = fr + gx * bf.d[0] + gy * bf.d[1] + gz * bf.d[2];
+        const double sgrad = seed - ae * (lam_at(a, nv, o, q) + wq * mu);
+        s[7] += ae * lam_at(a, nv, o, q) * fspec;
+        s[8] += sgrad * fr;
+        s[9] += wq * ae / bf.area * fspec;
+      }
     }
   }
   block_sum<kAdjFaceSums, kAdjThreads>(s, sh);

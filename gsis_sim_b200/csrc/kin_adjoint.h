@@ -23,7 +23,7 @@
 namespace kin {
 
 constexpr int kAdjCellSums = 9;   // Lambda0, Lambda_rho, Lambda_u (3), Lambda_T, Lambda_q (3)
-constexpr int kAdjFaceSums = 7;   // S0, S1 (3), S2, S5, S6 (k_adj_faces)
+constexpr int kAdjFaceSums = 10;  // S0, S1 (3), S2, S5, S6, A1, A2, S_spec (k_adj_faces)
 constexpr int kAdjCoefs = 8;      // a0, a (3), a2, b (3)
 
 struct AdjView {
@@ -39,6 +39,8 @@ struct AdjView {
   int8_t* imin;
   double* lfb;             // seeds that land on f[cell][q] itself
   const double* mu;        // per boundary face: seed weight of the outgoing face values (nu and objective terms)
+  const int32_t* flip;     // [axis][q]: position of xi with component `axis` negated (3 x nv)
+  const int32_t* face_axis;  // per boundary face: the axis its normal is aligned with, -1 if none
   const double* coef;      // per cell: moment expansion coefficients (kAdjCoefs)
   const double* moments;   // per cell: the 15 moments of the forward state
   double* out;             // O_f(y) at the reversed position [cell][rev[q]]

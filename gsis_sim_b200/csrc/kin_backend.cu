@@ -161,7 +161,8 @@ struct KinHandle {
   virtual void moment_sums(double* out, int64_t n) = 0;
   virtual void set_moments(const double* m, int64_t n) = 0;
   // discrete adjoint (FP64 handles with one velocity chunk)
-  virtual void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries) = 0;
+  virtual void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries,
+                             const int32_t* flip_velocity, const int32_t* face_axis) = 0;
   virtual void adjoint_set(const double* lam, int64_t n) = 0;
   virtual void adjoint_get(double* lam, int64_t n) = 0;
   virtual void adjoint_reduce(const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell, double* face_sums,
@@ -283,7 +284,7 @@ struct Backend final : KinHandle {
   bool adj_on = false;
   DevBuf<double> adj_lam, adj_lfb, adj_hmax, adj_hmin, adj_mu, adj_coef, adj_cell, adj_face, adj_res;
   DevBuf<int8_t> adj_imax, adj_imin;
-  DevBuf<int32_t> adj_rev, adj_rev_entry, adj_perm2, adj_inv2;
+  DevBuf<int32_t> adj_rev, adj_rev_entry, adj_perm2, adj_inv2, adj_flip, adj_face_axis;
 
   bool inflow_set = false;
   bool deq_valid = false;
@@ -1221,7 +1222,8 @@ struct Backend final : KinHandle {
   // lambda is stored at the position of the reversed velocity, so that the forward LU-SGS passes (which at
   // position p use xi_p and the sweep direction of p) act on the adjoint of -xi_p as the transposed preconditioner:
   // the in-block lower / upper couplings of velocity -xi are the transposes of the upper / lower ones of xi.
-  void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries) override {
+  void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries,
+                     const int32_t* flip_velocity, const int32_t* face_axis) override {
     if constexpr (!std::is_same<S, double>::value || !std::is_same<M, double>::value) {
       throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
     } else {
@@ -1247,6 +1249,20 @@ struct Backend final : KinHandle {
       adj_perm2.upload(perm2.data(), nv, stream);
       adj_inv2.upload(inv2.data(), nv, stream);
       adj_rev_entry.upload(rev_entry, static_cast<size_t>(n_entries), stream);
+      adj_flip.release();
+      adj_face_axis.release();
+      if (flip_velocity != nullptr && face_axis != nullptr && nb > 0) {
+        std::vector<int32_t> flip(3 * static_cast<size_t>(nv));
+        for (int ax = 0; ax < 3; ++ax)
+          for (int q = 0; q < nv; ++q) {
+            const int s2 = flip_velocity[ax * nv + perm[q]];
+            KCHECK(s2 >= 0 && s2 < nv, "flipped velocity out of range");
+            flip[static_cast<size_t>(ax) * nv + q] = inv[s2];
+          }
+        for (int b = 0; b < nb; ++b) KCHECK(face_axis[b] >= -1 && face_axis[b] <= 2, "face axis out of range");
+        adj_flip.upload(flip.data(), flip.size(), stream);
+        adj_face_axis.upload(face_axis, static_cast<size_t>(nb), stream);
+      }
       adj_lam.alloc(nf);
       KCUDA(cudaMemsetAsync(adj_lam.p, 0, adj_lam.bytes(), stream));
       adj_lfb.alloc(nf);
@@ -1280,6 +1296,8 @@ struct Backend final : KinHandle {
     a.imin = adj_imin.p;
     a.lfb = adj_lfb.p;
     a.mu = adj_mu.p;
+    a.flip = adj_flip.p;
+    a.face_axis = adj_face_axis.p;
     a.coef = adj_coef.p;
     a.moments = moments.p;
     a.out = reinterpret_cast<double*>(r.p);
@@ -1407,6 +1425,8 @@ struct Backend final : KinHandle {
     adj_rev_entry.release();
     adj_perm2.release();
     adj_inv2.release();
+    adj_flip.release();
+    adj_face_axis.release();
     adj_on = false;
   }
 };
@@ -1527,8 +1547,9 @@ int kin_discrete_maxwell_noalloc(KinHandle* h, const double* states, int64_t n, 
   return guard(h, [&] { h->discrete_maxwell_noalloc(states, n, tolerance, out, result); });
 }
 int kin_moment_sums(KinHandle* h, double* out, int64_t n) { return guard(h, [&] { h->moment_sums(out, n); }); }
-int kin_adjoint_begin(KinHandle* h, const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries) {
-  return guard(h, [&] { h->adjoint_begin(rev_velocity, rev_entry, n_entries); });
+int kin_adjoint_begin(KinHandle* h, const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries,
+                      const int32_t* flip_velocity, const int32_t* face_axis) {
+  return guard(h, [&] { h->adjoint_begin(rev_velocity, rev_entry, n_entries, flip_velocity, face_axis); });
 }
 int kin_adjoint_set(KinHandle* h, const double* lam, int64_t n) { return guard(h, [&] { h->adjoint_set(lam, n); }); }
 int kin_adjoint_get(KinHandle* h, double* lam, int64_t n) { return guard(h, [&] { h->adjoint_get(lam, n); }); }

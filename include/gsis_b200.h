@@ -288,16 +288,22 @@ int kin_set_moments(KinHandle* h, const double* moments, int64_t n);
 
    kin_adjoint_begin: allocate the adjoint arrays, lambda = 0. rev_velocity[p] = storage position of -xi_p (a
    symmetric grid); rev_entry[e] = for an internal CSR entry of cell j pointing at cell i, the entry of cell i that
-   points back at j (-1 for boundary entries). */
-int kin_adjoint_begin(KinHandle* h, const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries);
+   points back at j (-1 for boundary entries). Optional (NULL: no accommodation sums): flip_velocity[a * nv + p] =
+   storage position of xi_p with component a negated, face_axis[b] = the axis boundary face b's normal is aligned with
+   (-1 none); they give the specular sums of axis-aligned diffuse walls. */
+int kin_adjoint_begin(KinHandle* h, const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries,
+                      const int32_t* flip_velocity, const int32_t* face_axis);
 /* lambda in the storage order of kin_set_distribution (n = n_cells * nv). */
 int kin_adjoint_set(KinHandle* h, const double* lambda, int64_t n);
 int kin_adjoint_get(KinHandle* h, double* lambda, int64_t n);
 /* Transposed transport and the per-cell / per-face sums. mu[b] (n_bfaces): weight of the seed w_q a_q mu[b] on the
    outgoing face values of boundary face b (diffuse walls: nu_b / (area_b sm5_b); inlet / outlet faces: the objective's
    -dJ/d(patch flow) factor), also applied to the incoming values of pressure faces. Outputs, per cell (9): the sums of
-   lambda against f^S - f and d f^S / d(rho, u, T, q); per boundary face (7): S0, S1 (3), S2 of the seeds on the
-   incoming inflow values against the inflow Maxwellian (M, M c, M c^2) and S5, S6 = sum_in w an M {c^2, 1}. */
+   lambda against f^S - f and d f^S / d(rho, u, T, q); per boundary face: S0, S1 (3), S2 of the seeds on the
+   incoming inflow values against the inflow Maxwellian (M, M c, M c^2) and S5, S6 = sum_in w an M {c^2, 1}; per
+   boundary face also (10 in all) A1 = sum_in a lambda f_spec, A2 = sum_in s_grad f_owner(reflected velocity),
+   S_spec = sum_in w an f_spec (axis-aligned diffuse walls, f_spec = the owner's reconstructed face value at the
+   reflected velocity; zero elsewhere). */
 int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,
                        double* face_sums, int64_t n_face);
 /* Finish O_f(y) with the per-cell moment-expansion coefficients coef (8 per cell: a0, a (3), a2, b (3); the term

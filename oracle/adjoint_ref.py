@@ -12,7 +12,9 @@ and its transposed Jacobian is taken by autograd:
              rho_Gamma - Phi(f, rho_Gamma) = 0   zero net mass flux of each diffuse wall face
                                           (process_boundary_sums, kinetic_solver.cpp:280-335)
   objective  J = M_dot = 1/2 (mdot_in + mdot_out) sqrt(2/pi) from the patch flows of the boundary sums
-  parameters p = (mu_hat0, T_w per boundary face); delta enters only through mu_hat0 = 1 / (sqrt(2) delta)
+  parameters p = (mu_hat0, T_w per boundary face, accommodation alpha per wall face at 1: the partially specular
+             inflow rho M + (1 - alpha) f_spec of axis-aligned walls, maxwell_inflow / reflected_value,
+             kinetic_kernels.hpp:86-133); delta enters only through mu_hat0 = 1 / (sqrt(2) delta)
 
 The adjoint y solves (dF/dx)^T y = dJ/dx (GMRES over autograd vector-Jacobian products) and
 dJ/dp = dJ/dp|_x - y^T dF/dp.
@@ -103,6 +105,22 @@ class SteadyMap:
         self.outlet_face = torch.as_tensor(np.array([self.ptype_names[p] in T_OUTLETS for p in bp], bool))
         self.wall = self.bkind == BC_DIFFUSE_WALL
         self.wall_idx = torch.nonzero(self.wall).ravel()
+        # specular reflection of axis-aligned walls (the accommodation derivative at alpha = 1): the velocity with the
+        # normal component negated, per boundary face and per stencil entry
+        xi = np.stack([np.asarray(s["xi_x"]), np.asarray(s["xi_y"]), np.asarray(s["xi_z"])], 1)
+        key = {tuple(np.round(x * 2.0 ** 30).astype(np.int64).tolist()): i for i, x in enumerate(xi)}
+        flips = []
+        for a in range(3):
+            sg = np.ones(3)
+            sg[a] = -1.0
+            flips.append([key.get(tuple(np.round(x * sg * 2.0 ** 30).astype(np.int64).tolist()), -1) for x in xi])
+        flips = np.array(flips)
+        an = np.abs(bg[:, 0:3])
+        axis = np.argmax(an, 1)
+        aligned = np.abs(an[np.arange(len(an)), axis] - 1.0) < 1e-10
+        self.bflip = torch.as_tensor(np.where(aligned[:, None], flips[axis], q[None, :]))  # (nb, nv)
+        self.baligned = torch.as_tensor(aligned)
+        self.eflip = self.bflip[self.bface]  # (nc, E, nv)
         self.setup, self.host = setup, host
 
     # ---- scope ---------------------------------------------------------------------------------------------------
@@ -187,13 +205,17 @@ class SteadyMap:
                                                   torch.zeros(nb, dtype=torch.float64)))
         return scale, M
 
-    def _entry_f(self, f, scale, M):
-        """f at the stencil entries (nc, E, nv) and the inflow values of boundary entries."""
+    def _entry_f(self, f, scale, M, alpha):
+        """f at the stencil entries (nc, E, nv) and the inflow values of boundary entries (first order: the specular
+        part of a wall with alpha < 1 is the cell's own value at the reflected velocity)."""
         fi = f[:, None, :].expand(-1, self.E, -1)
         fo = f[self.other]  # (nc, E, nv)
         b = self.bface
         a = (self.S @ self.xi.T)  # (nc, E, nv)
         infl = scale[b][..., None] * M[b]
+        wall_e = (self.kind == BC_DIFFUSE_WALL)[..., None]
+        infl = infl + torch.where(wall_e, (1.0 - alpha[b])[..., None] * torch.gather(fi, 2, self.eflip),
+                                  torch.zeros_like(infl))
         fm = torch.gather(fi, 2, self.mirror)
         k = self.kind[..., None]
         bval = torch.where(k == BC_PERIODIC, fi,
@@ -231,8 +253,17 @@ class SteadyMap:
         phi = torch.clamp(v.amin(1), max=1.0)
         return phi[..., None] * G
 
-    def residual(self, f, g, fk, a, infl, coll, fS):
-        """residual_value (kinetic_kernels.hpp:238-278) at every (cell, velocity)."""
+    def residual(self, f, g, fk, a, infl, coll, fS, alpha=None, scale=None, M=None):
+        """residual_value (kinetic_kernels.hpp:238-278) at every (cell, velocity). The incoming value of a wall is
+        rho M + (1 - alpha) f_spec with f_spec the cell's reconstructed face value at the reflected velocity."""
+        if alpha is not None:
+            b = self.bface
+            gi4 = g[:, None, :, :].expand(-1, self.E, -1, -1)
+            gr = torch.gather(gi4, 2, self.eflip[..., None].expand(-1, -1, -1, 3))
+            fr = torch.gather(f[:, None, :].expand(-1, self.E, -1), 2, self.eflip)
+            spec = fr + (gr * self.ds[:, :, None, :]).sum(-1)
+            wall_e = (self.kind == BC_DIFFUSE_WALL)[..., None]
+            infl = torch.where(wall_e, scale[b][..., None] * M[b] + (1.0 - alpha[b])[..., None] * spec, infl)
         gi = g[:, None, :, :]  # (nc, 1, nv, 3)
         own_face = f[:, None, :] + (gi * self.ds[:, :, None, :]).sum(-1)
         go = g[self.other]  # (nc, E, nv, 3)
@@ -252,26 +283,34 @@ class SteadyMap:
 
     def boundary_sums(self, f, g, M):
         """sm0 = sum_{an >= 0} w an f_b (reconstructed) and sm5 = sum_{an < 0} w an M_b per face
-        (k_boundary_sums, kinetic_cuda_kernels.cu:275-323; the other 18 sums are not needed here)."""
+        (k_boundary_sums, kinetic_cuda_kernels.cu:275-323; the other 18 sums are not needed here), and
+        S_spec = sum_{an < 0} w an f_spec (reconstructed at the reflected velocity)."""
         own = self.bowner
         an = self.bn @ self.xi.T  # (nb, nv)
         fb = f[own] + (g[own] * self.bd[:, None, :]).sum(-1)
         out = an >= 0
         sm0 = torch.where(out, self.w * an * fb, torch.zeros_like(fb)).sum(1)
         sm5 = torch.where(out, torch.zeros_like(fb), self.w * an * M).sum(1)
-        return sm0, sm5
+        fr = torch.gather(f[own], 1, self.bflip)
+        gr = torch.gather(g[own], 1, self.bflip[..., None].expand(-1, -1, 3))
+        spec = fr + (gr * self.bd[:, None, :]).sum(-1)
+        sspec = torch.where(out, torch.zeros_like(fb), self.w * an * spec).sum(1)
+        return sm0, sm5, sspec
 
     # ---- the map -------------------------------------------------------------------------------------------------
-    def evaluate(self, f, rho_gamma, mu0, Tw):
-        """(R (nc, nv), wall equations rho_Gamma - Phi (n_wall,), J = M_dot)."""
+    def evaluate(self, f, rho_gamma, mu0, Tw, alpha=None):
+        """(R (nc, nv), wall equations rho_Gamma - Phi (n_wall,), J = M_dot). alpha (per boundary face, walls only;
+        default 1): the accommodation, with the specular part of axis-aligned walls (a Maxwell wall)."""
+        if alpha is None:
+            alpha = torch.ones(self.nb, dtype=torch.float64)
         coll, fS, mom = self.target(f, mu0)
         scale, M = self.inflow(mom, rho_gamma, Tw)
-        fk, a, infl = self._entry_f(f, scale, M)
+        fk, a, infl = self._entry_f(f, scale, M, alpha)
         g = self.gradient(f, fk)
-        R = self.residual(f, g, fk, a, infl, coll, fS)
-        sm0, sm5 = self.boundary_sums(f, g, M)
+        R = self.residual(f, g, fk, a, infl, coll, fS, alpha, scale, M)
+        sm0, sm5, sspec = self.boundary_sums(f, g, M)
         wi = self.wall_idx
-        phi = torch.clamp(-sm0[wi] / sm5[wi], min=0.0)
+        phi = torch.clamp(-(sm0[wi] + (1.0 - alpha[wi]) * sspec[wi]) / sm5[wi], min=0.0)
         Fw = rho_gamma - phi
         in_scale = scale  # pressure 1, vacuum 0, walls rho_Gamma
         flow = self.barea * (sm0 + in_scale * sm5)
@@ -293,8 +332,9 @@ def state_of(solver):
 
 
 def adjoint_gradient(sm: SteadyMap, f, rho_gamma, tol=1e-12, maxiter=4000):
-    """dJ/d(mu_hat0) and dJ/dT_w (per boundary face; zero off the walls) at the fixed point (f, rho_Gamma), with the
-    adjoint solved by GMRES. Returns (dJ_dmu0, dJ_dTw (nb,), info) with info = (J, ||F||, gmres iterations)."""
+    """dJ/d(mu_hat0), dJ/dT_w and dJ/dalpha (per boundary face; alpha at 1, the derivative from below) at the fixed
+    point (f, rho_Gamma), with the adjoint solved by GMRES. Returns (dJ_dmu0, dJ_dTw (nb,), info) with
+    info = (J, ||F||, gmres iterations, y, dJ_dalpha (nb,))."""
     from scipy.sparse.linalg import LinearOperator, gmres
 
     mu0, Tw = sm.params_of()
@@ -302,10 +342,12 @@ def adjoint_gradient(sm: SteadyMap, f, rho_gamma, tol=1e-12, maxiter=4000):
     rg = rho_gamma.clone().requires_grad_(True)
     mu0 = mu0.clone().requires_grad_(True)
     Tw = Tw.clone().requires_grad_(True)
-    R, Fw, J = sm.evaluate(f, rg, mu0, Tw)
+    alpha = torch.ones(sm.nb, dtype=torch.float64, requires_grad=True)
+    R, Fw, J = sm.evaluate(f, rg, mu0, Tw, alpha)
     nf, nw = f.numel(), rg.numel()
-    gJ = torch.autograd.grad(J, (f, rg, mu0, Tw), allow_unused=True, retain_graph=True)
-    gJ = [torch.zeros_like(t) if g is None else g for g, t in zip(gJ, (f, rg, mu0, Tw))]
+    # J depends on alpha explicitly too: the limited gradient of an inlet / outlet owner that also has a wall face
+    gJ = torch.autograd.grad(J, (f, rg, mu0, Tw, alpha), allow_unused=True, retain_graph=True)
+    gJ = [torch.zeros_like(t) if g is None else g for g, t in zip(gJ, (f, rg, mu0, Tw, alpha))]
     rhs = torch.cat([gJ[0].ravel(), gJ[1].ravel()]).numpy()
 
     def vjp(y):
@@ -326,12 +368,14 @@ def adjoint_gradient(sm: SteadyMap, f, rho_gamma, tol=1e-12, maxiter=4000):
     if code != 0:
         raise RuntimeError(f"adjoint GMRES did not converge (code {code})")
     yt = torch.as_tensor(y)
-    gp = torch.autograd.grad((R, Fw), (mu0, Tw), grad_outputs=(yt[:nf].view_as(R), yt[nf:]), allow_unused=True)
-    gp = [torch.zeros_like(t) if g is None else g for g, t in zip(gp, (mu0, Tw))]
+    gp = torch.autograd.grad((R, Fw), (mu0, Tw, alpha), grad_outputs=(yt[:nf].view_as(R), yt[nf:]),
+                             allow_unused=True)
+    gp = [torch.zeros_like(t) if g is None else g for g, t in zip(gp, (mu0, Tw, alpha))]
     dmu = float(gJ[2] - gp[0])
     dTw = (gJ[3] - gp[1]).detach().numpy()
+    dal = (gJ[4] - gp[2]).detach().numpy()
     fres = float(torch.sqrt((R.detach() ** 2).sum() + (Fw.detach() ** 2).sum()))
-    return dmu, dTw, (float(J.detach()), fres, it[0], y)
+    return dmu, dTw, (float(J.detach()), fres, it[0], y, dal)
 
 
 def transposed_jacobian_product(sm: SteadyMap, f, rho_gamma, y_f, y_w):

@@ -1,7 +1,8 @@
 """Discrete adjoint of the converged CIS fixed point (CPU part).
 
 * The reference adjoint (oracle/adjoint_ref.py: the steady map in torch, transposed by autograd) is pinned against
-  central finite differences of the converged CPU-oracle forward solver: dM_dot/d mu_hat0 and dM_dot/dT_w.
+  finite differences of the converged CPU-oracle forward solver: dM_dot/d mu_hat0 and dM_dot/dT_w (central) and
+  dM_dot/d alpha at alpha = 1 (one-sided from below, through Maxwell-wall solves).
 * The host algebra of gsis_sim_b200/adjoint.py (moments -> Shakhov target -> collision term chain, pressure-face
   chain, index maps) against torch autograd of the same forward formulas.
 The device kernels are checked against the reference adjoint in tests/test_gpu_adjoint.py."""
@@ -18,7 +19,7 @@ from gsis_sim_b200.solver import KineticSolver
 
 
 def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="periodic_slab", limiter="venkatakrishnan",
-                 eps="relative", half=False, quarter=False):
+                 eps="relative", half=False, quarter=False, alpha=1.0):
     """Pressure-driven channel (inlet p 1, outlet p 0.5, diffuse walls) in the adjoint's scope; `half`: symmetry
     plane at y = 0 instead of the lower wall; `quarter`: a duct quarter, symmetry planes at y = 0 and z = 0, walls at
     y = 1 and z = 0.7 (a flow that varies in y and z)."""
@@ -27,7 +28,7 @@ def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="perio
     hz = 0.7 if quarter else 1.0 / 3  # quarter: not square, so no y <-> z mirror symmetry (no limiter ties)
     m = box_mesh(n, (0, 0, 0), (2.0, 1.0, hz), ("inlet", "outlet", lower, "wall", *sides))
     bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "pressure_outlet", p=0.5),
-           ks.BC("wall", "diffuse_wall", T=Tw)]
+           ks.BC("wall", "diffuse_wall", T=Tw, alpha=alpha)]
     if not quarter:
         bcs.append(ks.BC("side", side))
     if half or quarter:
@@ -86,6 +87,13 @@ def test_reference_adjoint_matches_finite_differences():
     fd_T = (Jp - Jm) / (2 * h)
     assert abs(dTw.sum() - fd_T) <= 1e-6 * abs(fd_T)
     assert np.all(dTw[sm.bkind.numpy() != ar.BC_DIFFUSE_WALL] == 0.0)
+    # accommodation at alpha = 1, from below (alpha <= 1): second-order one-sided difference of Maxwell-wall solves
+    ha = 1e-4
+    J1 = _oracle_solution(alpha=1 - ha)[0].mass_flow()[2]
+    J2 = _oracle_solution(alpha=1 - 2 * ha)[0].mass_flow()[2]
+    fd_a = (3 * sol.mass_flow()[2] - 4 * J1 + J2) / (2 * ha)
+    dal = info[4]
+    assert abs(dal.sum() - fd_a) <= 1e-6 * abs(fd_a)
 
 
 def _maxwellian_f(rng, nc, xi, w):

@@ -2,8 +2,9 @@
 oracle/adjoint_ref.py (the steady map transposed by torch autograd, itself pinned against finite differences in
 tests/test_adjoint.py), at the fixed point the B200 forward solver converged to:
 * the operator y^T dF/dx (and the objective term dJ/dx) for random adjoint states, to 1e-10;
-* the converged adjoint's dM_dot/d mu_hat0 and dM_dot/dT_w, to 1e-8 against the reference adjoint and to 1e-5
-  against central finite differences of the B200 forward solver."""
+* the converged adjoint's dM_dot/d mu_hat0, dM_dot/dT_w and dM_dot/d alpha (at alpha = 1), to 1e-8 against the
+  reference adjoint and to 1e-5 against finite differences of the B200 forward solver (alpha: one-sided, through
+  Maxwell-wall solves)."""
 import numpy as np
 import pytest
 import torch
@@ -75,9 +76,11 @@ def test_gpu_adjoint_gradients_match_reference_and_finite_differences(kw):
         assert res.residual < 1e-10
         sm = ar.SteadyMap(setup, host)
         f, rg = ar.state_of(sol)
-        dmu, dTw, _ = ar.adjoint_gradient(sm, f, rg)
+        dmu, dTw, info = ar.adjoint_gradient(sm, f, rg)
         assert abs(res.dJ_dmu0 - dmu) <= 1e-8 * abs(dmu)
         assert np.max(np.abs(res.dJ_dTw - dTw)) <= 1e-8 * np.max(np.abs(dTw))
+        walls = np.flatnonzero(sol.bkind == 0)
+        assert np.max(np.abs(res.dJ_dalpha[walls] - info[4][walls])) <= 1e-8 * np.max(np.abs(info[4]))
         ka.close()
     finally:
         sol.backend.close()
@@ -94,3 +97,12 @@ def test_gpu_adjoint_gradients_match_reference_and_finite_differences(kw):
     for s in (Tp, Tm):
         s[0].backend.close()
     assert abs(res.dJ_dTw.sum() - fd_T) <= 1e-5 * abs(fd_T)
+    # accommodation at alpha = 1 from below: Maxwell-wall solves on the B200
+    ha = 1e-4
+    A1 = _gpu_solution(alpha=1 - ha, **kw)
+    A2 = _gpu_solution(alpha=1 - 2 * ha, **kw)
+    J0 = res.J
+    fd_a = (3 * J0 - 4 * A1[0].mass_flow()[2] + A2[0].mass_flow()[2]) / (2 * ha)
+    for s in (A1, A2):
+        s[0].backend.close()
+    assert abs(np.nansum(res.dJ_dalpha) - fd_a) <= 1e-5 * abs(fd_a)
