@@ -285,21 +285,27 @@ class KineticAdjoint:
 
         Mirrors the forward CIS iteration: per outer iteration the coupling terms (moment expansion of the cell
         parameters, pressure-face chain) are evaluated once and frozen for `inner` transposed transport sweeps
-        (default: the set-up's inner_sweeps), with the wall adjoint refreshed after each sweep as the forward
-        refreshes rho_Gamma. The outer iteration then has the spectrum of the forward's. `max_iterations` counts
+        (default: the set-up's inner_sweeps); before every sweep the wall adjoint is recomputed from the current
+        lambda, as the forward recomputes rho_Gamma from the current f. The outer iteration then has the spectrum of the forward's. `max_iterations` counts
         outer iterations; the residual is that of the first sweep of each outer iteration (fresh coupling)."""
         be = self.sol.backend
         inner = max(1, int(self.sol.h.inner_sweeps if inner is None else inner))
+        walls = len(self.wall) > 0
         ref = None
         it = 0
         res = math.inf
         for it in range(1, max_iterations + 1):
+            # wall adjoint first, from the current lambda (the transpose of the forward's rho_Gamma = Phi(f) before
+            # each sweep; a one-sweep lag on these strongly coupled unknowns can make the iteration unstable)
+            nu_old = self.nu
+            if walls:
+                _, face = self._reduce()
+                self.nu = -face[self.wall, 0]
             cell, face = self._reduce()
             coef, _ = self._coefficients(cell, face)
             res_cell, _ = be.adjoint_update(coef, run_passes=True)
-            nu_new = -face[self.wall, 0]
-            dnu = float(np.sqrt(np.sum((nu_new - self.nu) ** 2)))
-            self.nu = nu_new
+            nu_new = self.nu
+            dnu = float(np.sqrt(np.sum((nu_new - nu_old) ** 2)))
             r = math.sqrt(float(np.sum(res_cell)))
             if ref is None:
                 ref = max(r, 1e-300)
@@ -312,9 +318,11 @@ class KineticAdjoint:
             if r / ref < tol and (len(nu_new) == 0 or dnu <= tol * max(float(np.abs(nu_new).max()), 1e-300)):
                 break
             for _ in range(1, inner):
-                _, face = self._reduce()
+                if walls:
+                    _, face = self._reduce()
+                    self.nu = -face[self.wall, 0]
+                self._reduce()
                 be.adjoint_update(coef, run_passes=True)
-                self.nu = -face[self.wall, 0]
         return self.gradients(it, res)
 
     def gradients(self, iterations: int = 0, residual: float = 0.0) -> AdjointResult:
