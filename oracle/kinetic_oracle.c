@@ -470,6 +470,11 @@ int orc_moment_sums(OrcHandle* h, double* out, int64_t n) {
   DISPATCH(h, moment_sums, out);
   return KIN_OK;
 }
+int orc_passes_given(OrcHandle* h, const double* R, int64_t n) {
+  if (n != (int64_t)orc_nc(h) * orc_nv(h)) return orc_fail(h, "length of the residual does not match");
+  DISPATCH(h, passes_given, R);
+  return KIN_OK;
+}
 int orc_set_moments(OrcHandle* h, const double* m, int64_t n) {
   if (n != 15LL * orc_nc(h)) return orc_fail(h, "length of the moments does not match");
   DISPATCH(h, set_moments, m);

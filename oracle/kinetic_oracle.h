@@ -38,6 +38,8 @@ int orc_internal_face_mass_flux(OrcHandle* h, const int32_t* cells, const int32_
 int orc_deq_counts(OrcHandle* h, KinDeqCounts* out);
 int orc_moment_sums(OrcHandle* h, double* out, int64_t n);
 int orc_set_moments(OrcHandle* h, const double* m, int64_t n);
+/* test support: the LU-SGS block passes on a given steady residual (storage order), f += the update */
+int orc_passes_given(OrcHandle* h, const double* R, int64_t n);
 int orc_discrete_maxwell(OrcHandle* h, const double* states, int64_t n, double tolerance, double* out,
                          int32_t* result);
 

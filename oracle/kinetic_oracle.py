@@ -36,6 +36,8 @@ def lib():
     L.orc_last_error.argtypes = [C.c_void_p]
     L.orc_last_error.restype = C.c_char_p
     abi.declare_backend_api(L, "orc_")
+    L.orc_passes_given.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int64]
+    L.orc_passes_given.restype = C.c_int
     _lib = L
     return L
 
@@ -53,6 +55,13 @@ class OracleBackend(KineticBackendABI):
         if L.orc_create(C.byref(desc), C.byref(h)) != 0:
             raise KineticError("orc_create failed")
         super().__init__(L, "orc_", h, s, lambda: L.orc_last_error(h).decode())
+
+    def passes_given(self, R) -> None:
+        """The LU-SGS block passes on the given steady residual (storage order): f += their update."""
+        import numpy as np
+
+        a = np.ascontiguousarray(R, dtype=np.float64).ravel()
+        self._call("passes_given", abi.as_ptr(a, C.c_double), a.size)
 
     def close(self):
         if self._h:

@@ -667,6 +667,18 @@ static void N(sweep)(N(State) * s, double* residual_cell) {
   }
 }
 
+/* the LU-SGS block passes on a given steady residual R (storage order, all velocities): f += the pass update, as
+   sweep does after its own residual (used by the adjoint tests as the transposed preconditioner on
+   velocity-reversed storage) */
+static void N(passes_given)(N(State) * s, const double* R) {
+  for (int k0 = 0; k0 < s->nv; k0 += s->chunk) {
+    const int kc = s->chunk < s->nv - k0 ? s->chunk : s->nv - k0;
+    for (int c = 0; c < s->nc; ++c)
+      for (int t = 0; t < kc; ++t) s->r[(int64_t)c * s->chunk + t] = (S)R[(int64_t)c * s->nv + k0 + t];
+    N(sweep_passes)(s, k0, kc);
+  }
+}
+
 /* CpuBackend::gsis_correction (src/kinetic/kinetic_backend_cpu.cpp:346-432) */
 static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const double* w_new, int32_t* flags) {
   int64_t replaced = 0;

@@ -220,3 +220,49 @@ def test_index_maps():
     assert np.array_equal(re[re[e]], e)
     with pytest.raises(adj.AdjointScopeError):
         adj.reversed_velocities(xi + 0.1)
+
+
+@pytest.mark.timeout(600)
+def test_reversed_velocity_sweeps_solve_the_adjoint():
+    """The iteration scheme of gsis_sim_b200.adjoint on the CPU: the exact operator O(y) of the reference adjoint,
+    the wall adjoint recomputed from the current lambda, and the forward LU-SGS block passes (the oracle's) run on
+    velocity-reversed storage as the transposed preconditioner. It converges, and to the GMRES adjoint's gradients."""
+    from oracle import adjoint_ref as ar
+    from oracle.kinetic_oracle import OracleBackend
+
+    sol, setup, host = _oracle_solution()
+    sm = ar.SteadyMap(setup, host)
+    f, rg = ar.state_of(sol)
+    mu0, Tw = sm.params_of()
+    ft, rt = f.clone().requires_grad_(True), rg.clone().requires_grad_(True)
+    mut = mu0.clone().requires_grad_(True)
+    R, Fw, J = sm.evaluate(ft, rt, mut, Tw)
+    gJ = torch.autograd.grad(J, (ft, rt), retain_graph=True)
+    Jf, Jw = gJ[0].numpy(), gJ[1].numpy()
+
+    def op(lam, nu):
+        gf, gr = torch.autograd.grad((R, Fw), (ft, rt), grad_outputs=(torch.as_tensor(lam), torch.as_tensor(nu)),
+                                     retain_graph=True)
+        return gf.numpy() - Jf, gr.numpy() - Jw
+
+    xi = np.stack([setup["xi_x"], setup["xi_y"], setup["xi_z"]], 1)
+    rev = adj.reversed_velocities(xi)
+    pre = OracleBackend(setup)  # its f holds lambda at the reversed positions; cell parameters of the forward state
+    pre.set_distribution(np.zeros((sol.nc, sol.nv)))
+    pre.set_moments(sol.moments_)
+    pre.update_cell_params()
+    lam, nu = np.zeros((sol.nc, sol.nv)), np.zeros(len(rg))
+    r0 = None
+    for _ in range(400):
+        nu = nu - op(lam, nu)[1]
+        Of, _ = op(lam, nu)
+        r = np.linalg.norm(Of)
+        r0 = r0 or r
+        if r < 1e-11 * r0:
+            break
+        pre.passes_given(Of[:, rev])
+        lam = pre.get_distribution()[:, rev]
+    assert r < 1e-11 * r0
+    (gmu,) = torch.autograd.grad((R, Fw), (mut,), grad_outputs=(torch.as_tensor(lam), torch.as_tensor(nu)))
+    dmu_ref, _, _ = ar.adjoint_gradient(sm, f, rg)
+    assert abs(-float(gmu) - dmu_ref) <= 1e-8 * abs(dmu_ref)

@@ -63,6 +63,37 @@ def test_gpu_adjoint_operator_matches_reference(kw):
         sol.backend.close()
 
 
+def test_gpu_adjoint_operator_on_tube_mesh():
+    """The operator on a small O-grid tube + reservoir (curved walls, reservoir back walls, near-vacuum outlet,
+    4 LU-SGS blocks): y^T dF/dx equals the reference's for random y."""
+    from gsis_sim_b200 import tube
+    from gsis_sim_b200.adjoint import KineticAdjoint
+    from gsis_sim_b200.backend import B200Backend
+    from oracle import adjoint_ref as ar
+
+    setup, host = tube.tube_case(delta=10.0, nv=12, precision="fp64", equilibrium="continuous",
+                                 pressure_boundary_reconstruction="cell", sweep_blocks=4,
+                                 mesh_kw=dict(n_x=6, n_c=2, n_r=2, n_o=2, n_xr=3))
+    be = B200Backend(setup)
+    try:
+        sol = converge(be, setup, host)
+        ka = KineticAdjoint(sol)
+        sm = ar.SteadyMap(setup, host)
+        f, rg = ar.state_of(sol)
+        rng = np.random.default_rng(5)
+        lam = rng.standard_normal((sol.nc, sol.nv))
+        nu = rng.standard_normal(len(ka.wall))
+        op_f, op_w = ka.operator(lam, nu, with_objective=False)
+        ref_f, ref_w = ar.transposed_jacobian_product(sm, f, rg, lam, nu)
+        assert np.max(np.abs(op_f - ref_f)) <= 1e-10 * np.max(np.abs(ref_f))
+        assert np.max(np.abs(op_w - ref_w)) <= 1e-10 * np.max(np.abs(ref_w))
+        res = ka.solve(tol=1e-8, max_iterations=2000)
+        assert res.residual < 1e-7
+        ka.close()
+    finally:
+        be.close()
+
+
 @pytest.mark.timeout(900)
 @pytest.mark.parametrize("kw", [dict(), dict(side="symmetry")])
 def test_gpu_adjoint_gradients_match_reference_and_finite_differences(kw):
