@@ -2,6 +2,7 @@
 // of include/gsis_b200.h. One KinHandle corresponds to one reference `CudaBackend<F>` object
 // (src/kinetic/kinetic_backend_cuda.cpp:89-502).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -127,6 +128,51 @@ struct PhaseTimer {
   }
 };
 
+// Factors a velocity set (m points, any order) as a tensor grid: per axis the distinct node values, every
+// (i, j, k) combination present exactly once, and weights w(q) = w_x[i] w_y[j] w_z[k] (w == nullptr: uniform, all
+// per-axis weights 1). Returns false when the set is not of that form; the caller then sums point by point.
+bool factor_tensor_grid(const double* x, const double* y, const double* z, const double* w, int64_t m,
+                        std::vector<double>& nodes, std::vector<double>& wax, int32_t (&n)[3]) {
+  const double* xs[3] = {x, y, z};
+  std::vector<double> ax[3];
+  for (int a = 0; a < 3; ++a) {
+    ax[a].assign(xs[a], xs[a] + m);
+    std::sort(ax[a].begin(), ax[a].end());
+    ax[a].erase(std::unique(ax[a].begin(), ax[a].end()), ax[a].end());
+    n[a] = static_cast<int32_t>(ax[a].size());
+  }
+  if (m <= 0 || static_cast<int64_t>(n[0]) * n[1] * n[2] != m) return false;
+  std::vector<int64_t> at(static_cast<size_t>(m), -1);  // grid index -> point
+  for (int64_t q = 0; q < m; ++q) {
+    int64_t g = 0;
+    for (int a = 2; a >= 0; --a) {
+      const auto it = std::lower_bound(ax[a].begin(), ax[a].end(), xs[a][q]);
+      g = g * n[a] + (it - ax[a].begin());
+    }
+    if (at[g] >= 0) return false;
+    at[g] = q;
+  }
+  nodes.clear();
+  wax.assign(static_cast<size_t>(n[0] + n[1] + n[2]), 1.0);
+  for (int a = 0; a < 3; ++a) nodes.insert(nodes.end(), ax[a].begin(), ax[a].end());
+  if (w != nullptr) {
+    auto wq = [&](int i, int j, int k) { return w[at[i + static_cast<int64_t>(n[0]) * (j + static_cast<int64_t>(n[1]) * k)]]; };
+    const double w000 = wq(0, 0, 0);
+    if (!(w000 > 0.0)) return false;
+    for (int i = 0; i < n[0]; ++i) wax[i] = wq(i, 0, 0);
+    for (int j = 0; j < n[1]; ++j) wax[n[0] + j] = wq(0, j, 0) / w000;
+    for (int k = 0; k < n[2]; ++k) wax[n[0] + n[1] + k] = wq(0, 0, k) / w000;
+    for (int k = 0; k < n[2]; ++k)
+      for (int j = 0; j < n[1]; ++j)
+        for (int i = 0; i < n[0]; ++i) {
+          const double prod = wax[i] * wax[n[0] + j] * wax[n[0] + n[1] + k];
+          const double ref = wq(i, j, k);
+          if (!(std::abs(prod - ref) <= 1e-13 * std::abs(ref))) return false;
+        }
+  }
+  return true;
+}
+
 }  // namespace
 
 struct KinHandle {
@@ -247,6 +293,10 @@ struct Backend final : KinHandle {
   DevBuf<M> dq_x, dq_y, dq_z;
   DevBuf<double> dq_xd, dq_yd, dq_zd, dq_w;
   int32_t dq_nv = 0;
+  // the equilibrium's velocity grid factored per axis (kin::DeqTensor; tn_n[0] == 0: not a tensor grid)
+  DevBuf<double> tn_nodes, tn_w;
+  DevBuf<int32_t> tn_pos;  // per stored velocity: packed node indices (kin::View::tn_pos), empty if not usable
+  int32_t tn_n[3] = {0, 0, 0};
   DevBuf<double> xid_x, xid_y, xid_z, wts;
   DevBuf<int32_t> csr_off;
   DevBuf<CsrE<M>> csr;
@@ -476,6 +526,48 @@ struct Backend final : KinHandle {
       dq_zd.upload(d.deq_xi_z, m, stream);
       if (d.deq_weights) dq_w.upload(d.deq_weights, m, stream);
       KCUDA(cudaStreamSynchronize(stream));
+    }
+    // KIN_VELOCITY_SUMS=pointwise keeps the per-velocity Maxwellians and Newton sums on a tensor grid too (both give
+    // the same results to rounding; the tests use this to cover both paths)
+    const char* sums_env = std::getenv("KIN_VELOCITY_SUMS");
+    const bool pointwise = sums_env != nullptr && std::strcmp(sums_env, "pointwise") == 0;
+    if (!pointwise) {
+      const bool shard = dq_nv > 0;
+      std::vector<double> nodes, wax;
+      int32_t n[3];
+      const bool tensor =
+          shard ? factor_tensor_grid(d.deq_xi_x, d.deq_xi_y, d.deq_xi_z, d.deq_weights, dq_nv, nodes, wax, n)
+                : factor_tensor_grid(dx.data(), dy.data(), dz.data(), d.weights ? hw.data() : nullptr, nv, nodes, wax,
+                                     n);
+      for (int a = 0; a < 3; ++a) tn_n[a] = tensor ? n[a] : 0;
+      if (tensor) {
+        tn_nodes.upload(nodes.data(), nodes.size(), stream);
+        tn_w.upload(wax.data(), wax.size(), stream);
+        // node indices of the stored velocities (a shard's velocities lie on the full grid's axes)
+        if (n[0] + n[1] + n[2] <= kin::kTensorNodesMax) {
+          std::vector<int32_t> pos(static_cast<size_t>(nv));
+          const double* xs[3] = {dx.data(), dy.data(), dz.data()};
+          bool all = true;
+          for (int q = 0; q < nv && all; ++q) {
+            int32_t packed = 0;
+            int base = 0;
+            for (int a = 0; a < 3; ++a) {
+              const auto b = nodes.begin() + base, e = b + n[a];
+              const auto it = std::lower_bound(b, e, xs[a][q]);
+              if (it == e || *it != xs[a][q]) {
+                all = false;
+                break;
+              }
+              packed |= static_cast<int32_t>(it - b) << (10 * a);
+              base += n[a];
+            }
+            pos[q] = packed;
+          }
+          if (all) tn_pos.upload(pos.data(), pos.size(), stream);
+          KCUDA(cudaStreamSynchronize(stream));
+        }
+        KCUDA(cudaStreamSynchronize(stream));
+      }
     }
     d_perm.upload(perm.data(), nv, stream);
     d_inv.upload(inv.data(), nv, stream);
@@ -833,6 +925,10 @@ struct Backend final : KinHandle {
     v.dq_zd = shard ? dq_zd.p : xid_z.p;
     v.dq_w = shard ? dq_w.p : wts.p;
     v.dq_nv = shard ? dq_nv : nv;
+    for (int a = 0; a < 3; ++a) v.dq_tensor.n[a] = tn_n[a];
+    v.dq_tensor.node = tn_nodes.p;
+    v.dq_tensor.w = tn_w.p;
+    v.tn_pos = tn_pos.p;
     if constexpr (kSplit) {
       kin::View<S, P>& w = pview;
       w.n_cells = nc;
@@ -865,6 +961,8 @@ struct Backend final : KinHandle {
       w.dq_zd = v.dq_zd;
       w.dq_w = v.dq_w;
       w.dq_nv = v.dq_nv;
+      w.dq_tensor = v.dq_tensor;
+      w.tn_pos = v.tn_pos;
     }
   }
 

@@ -43,6 +43,18 @@ struct Inflow {
   M scale;
 };
 
+// The velocity set of the discrete equilibrium as a tensor grid: node x_a[i] per axis and separable weights
+// w(q) = w_x[i] w_y[j] w_z[k] (all 1 for a uniform grid, whose scalar weight the Newton step applies). Every sum of
+// the Newton iteration is a sum over the grid of A exp(-B |xi - u'|^2) times a polynomial in c = xi - u, so it
+// factors into products of per-axis sums sum_i w_a[i] exp(-B (x_a[i] - u'_a)^2) (x_a[i] - u_a)^k, k = 0..5:
+// n_x + n_y + n_z exponentials per Newton iteration instead of n_x n_y n_z. n[0] == 0: not a tensor grid (the sums
+// run over the velocity points).
+struct DeqTensor {
+  int32_t n[3];
+  const double* node;  // n[0] + n[1] + n[2] nodes, axis by axis
+  const double* w;     // per-axis weights, same layout
+};
+
 template <class S, class M>
 struct View {
   int32_t n_cells, nv, n_bfaces;
@@ -83,6 +95,11 @@ struct View {
   const double* dq_zd;
   const double* dq_w;  // per-velocity weights, nullptr when uniform
   int32_t dq_nv;
+  DeqTensor dq_tensor;  // the same grid factored per axis (n[0] == 0 when it is not a tensor grid)
+  // per stored velocity its node indices in dq_tensor's axes, ix | iy << 10 | iz << 20; nullptr unless the stored
+  // velocities lie on that tensor grid with n_x + n_y + n_z <= kTensorNodesMax (the residual then forms the
+  // Maxwellian of its cells as A e_x[ix] e_y[iy] e_z[iz] from per-axis exponentials)
+  const int32_t* tn_pos;
 };
 
 template <class S>
@@ -245,10 +262,80 @@ __device__ inline T block_reduce_op(T val, T* sh, Op op) {
 // src/kinetic/kinetic_cuda_kernels.cu:71-145 and discrete_maxwell_seq, kinetic_kernels.hpp:499-540).
 // Terms in M, sums in double. Returns Newton iterations (0: resolved, -1: failed) in every thread.
 // ---------------------------------------------------------------------------------------------------------
+// per-axis sums X_a[k] = sum_i w_a[i] exp(-B (x_a[i] - u'_a)^2) c^k, c = x_a[i] - u_a, k = 0..5 (18 values, axis
+// by axis), reduced over the CTA; the result is valid in thread 0
+template <int B>
+__device__ inline void deq_axis_sums(const DeqTensor& tn, const double (&up)[3], const double (&uc)[3], double Bd,
+                                     double (&acc)[18], double* sh_red) {
+#pragma unroll
+  for (int k = 0; k < 18; ++k) acc[k] = 0.0;
+  int base = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    for (int i = threadIdx.x; i < tn.n[a]; i += B) {
+      const double x = tn.node[base + i];
+      const double r = x - up[a];
+      const double c = x - uc[a];
+      double p = tn.w[base + i] * exp(-Bd * (r * r));
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        acc[6 * a + k] += p;
+        p *= c;
+      }
+    }
+    base += tn.n[a];
+  }
+  block_sum<18, B>(acc, sh_red);
+}
+
+// the 20 Newton sums (deq_terms order) from the per-axis sums: sum e c^(i,j,k) = A X[i] Y[j] Z[k], with
+// h = |c|^2 / 2 and the Shakhov polynomial pm = coef (c . q) (|c|^2 / theta - 5) expanded into monomials
+__device__ inline void deq_sums_from_axes(const double (&ax)[18], double A, bool with_poly, double coef,
+                                          const double (&q)[3], double theta, double (&s)[kDeqSums]) {
+  const double* X = ax;
+  const double* Y = ax + 6;
+  const double* Z = ax + 12;
+  auto m3 = [&](int i, int j, int k) { return A * (X[i] * Y[j] * Z[k]); };
+  auto hh = [&](int i, int j, int k) { return 0.5 * (m3(i + 2, j, k) + m3(i, j + 2, k) + m3(i, j, k + 2)); };
+  auto pp = [&](int i, int j, int k) {
+    double r = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const int i1 = i + (a == 0), j1 = j + (a == 1), k1 = k + (a == 2);
+      const double q2 = m3(i1 + 2, j1, k1) + m3(i1, j1 + 2, k1) + m3(i1, j1, k1 + 2);
+      r += q[a] * (q2 / theta - 5.0 * m3(i1, j1, k1));
+    }
+    return coef * r;
+  };
+  s[0] = m3(0, 0, 0);
+  s[1] = m3(1, 0, 0);
+  s[2] = m3(0, 1, 0);
+  s[3] = m3(0, 0, 1);
+  s[4] = hh(0, 0, 0);
+  s[5] = m3(2, 0, 0);
+  s[6] = m3(1, 1, 0);
+  s[7] = m3(1, 0, 1);
+  s[8] = hh(1, 0, 0);
+  s[9] = m3(0, 2, 0);
+  s[10] = m3(0, 1, 1);
+  s[11] = hh(0, 1, 0);
+  s[12] = m3(0, 0, 2);
+  s[13] = hh(0, 0, 1);
+  s[14] = 0.5 * (hh(2, 0, 0) + hh(0, 2, 0) + hh(0, 0, 2));
+  if (with_poly) {
+    s[15] = pp(0, 0, 0);
+    s[16] = pp(1, 0, 0);
+    s[17] = pp(0, 1, 0);
+    s[18] = pp(0, 0, 1);
+    s[19] = 0.5 * (pp(2, 0, 0) + pp(0, 2, 0) + pp(0, 0, 2));
+  } else {
+    s[15] = s[16] = s[17] = s[18] = s[19] = 0.0;
+  }
+}
+
 template <class M, int B>
 __device__ int block_discrete_maxwell_on(const M* __restrict__ vx, const M* __restrict__ vy, const M* __restrict__ vz,
                                          const double* __restrict__ wts, int nv, double weight, const DeqGrid& deq,
-                                         double rho, double ux, double uy, double uz, double T,
+                                         const DeqTensor& tn, double rho, double ux, double uy, double uz, double T,
                                          const CellParams<M>* poly, Maxwell<M>& out, double (&gamma)[5],
                                          double* sh_red, double* sh_state) {
   for (double& x : gamma) x = 0.0;
@@ -271,20 +358,44 @@ __device__ int block_discrete_maxwell_on(const M* __restrict__ vx, const M* __re
     const double beta[5] = {sh_state[0], sh_state[1], sh_state[2], sh_state[3], sh_state[4]};
     const Maxwell<M> m = deq_params<M>(beta, ux, uy, uz);
     double acc[kDeqSums];
+    if (tn.n[0] > 0) {
+      // tensor grid: the same sums from per-axis sums (deq_params in FP64: B = -beta4 / 2, u' = u - beta_a / beta4,
+      // A = exp(beta0 + B |u' - u|^2))
+      const double Bd = -0.5 * beta[4];
+      const double dd[3] = {-beta[1] / beta[4], -beta[2] / beta[4], -beta[3] / beta[4]};
+      const double up[3] = {ux + dd[0], uy + dd[1], uz + dd[2]};
+      const double uc[3] = {static_cast<double>(fux), static_cast<double>(fuy), static_cast<double>(fuz)};
+      double ax[18];
+      deq_axis_sums<B>(tn, up, uc, Bd, ax, sh_red);
+      if (tid == 0) {
+        const double A = exp(beta[0] + Bd * (dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]));
+        double qv[3] = {0.0, 0.0, 0.0};
+        double coef = 0.0, theta = 1.0;
+        if (poly != nullptr) {
+          qv[0] = static_cast<double>(poly->qx);
+          qv[1] = static_cast<double>(poly->qy);
+          qv[2] = static_cast<double>(poly->qz);
+          coef = static_cast<double>(poly->coef);
+          theta = static_cast<double>(poly->theta);
+        }
+        deq_sums_from_axes(ax, A, poly != nullptr, coef, qv, theta, acc);
+      }
+    } else {
 #pragma unroll
-    for (int k = 0; k < kDeqSums; ++k) acc[k] = 0.0;
-    M t[kDeqSums];
-    for (int q = tid; q < nv; q += B) {
-      const M x = vx[q], y = vy[q], z = vz[q];
-      const M cx = x - fux, cy = y - fuy, cz = z - fuz;
-      M e = maxwellian(m, x, y, z);
-      const M pm = poly != nullptr ? shakhov_poly(*poly, cx, cy, cz, cx * cx + cy * cy + cz * cz) : M(0);
-      if (!uniform) e *= static_cast<M>(wts[q]);
-      deq_terms<M>(e, pm, cx, cy, cz, t);
+      for (int k = 0; k < kDeqSums; ++k) acc[k] = 0.0;
+      M t[kDeqSums];
+      for (int q = tid; q < nv; q += B) {
+        const M x = vx[q], y = vy[q], z = vz[q];
+        const M cx = x - fux, cy = y - fuy, cz = z - fuz;
+        M e = maxwellian(m, x, y, z);
+        const M pm = poly != nullptr ? shakhov_poly(*poly, cx, cy, cz, cx * cx + cy * cy + cz * cz) : M(0);
+        if (!uniform) e *= static_cast<M>(wts[q]);
+        deq_terms<M>(e, pm, cx, cy, cz, t);
 #pragma unroll
-      for (int k = 0; k < kDeqSums; ++k) acc[k] += static_cast<double>(t[k]);
+        for (int k = 0; k < kDeqSums; ++k) acc[k] += static_cast<double>(t[k]);
+      }
+      block_sum<kDeqSums, B>(acc, sh_red);
     }
-    block_sum<kDeqSums, B>(acc, sh_red);
     if (tid == 0) {
       double b[5] = {beta[0], beta[1], beta[2], beta[3], beta[4]};
       double rel = 0.0;
@@ -325,8 +436,8 @@ template <class S, class M, int B>
 __device__ inline int block_discrete_maxwell(const View<S, M>& v, double rho, double ux, double uy, double uz, double T,
                                              const CellParams<M>* poly, Maxwell<M>& out, double (&gamma)[5],
                                              double* sh_red, double* sh_state) {
-  return block_discrete_maxwell_on<M, B>(v.dq_x, v.dq_y, v.dq_z, v.dq_w, v.dq_nv, v.weight, v.deq, rho, ux, uy, uz, T,
-                                         poly, out, gamma, sh_red, sh_state);
+  return block_discrete_maxwell_on<M, B>(v.dq_x, v.dq_y, v.dq_z, v.dq_w, v.dq_nv, v.weight, v.deq, v.dq_tensor, rho, ux,
+                                         uy, uz, T, poly, out, gamma, sh_red, sh_state);
 }
 
 }  // namespace kin

@@ -71,6 +71,7 @@ struct CellParams {
   M qx, qy, qz;
   M theta, coef, g0, g4, gx, gy, gz;
   M coll, diag;
+  M inv_theta;  // 1 / theta: the Shakhov polynomial multiplies by it (no division per velocity)
 };
 
 // cell parameters in another precision (member by member)
@@ -97,20 +98,26 @@ __host__ __device__ inline CellParams<To> cast_cell_params(const CellParams<From
   o.gz = static_cast<To>(s.gz);
   o.coll = static_cast<To>(s.coll);
   o.diag = static_cast<To>(s.diag);
+  o.inv_theta = static_cast<To>(s.inv_theta);
   return o;
 }
 
 template <class M>
 __host__ __device__ inline M shakhov_poly(const CellParams<M>& s, M cx, M cy, M cz, M c2) {
-  return s.coef * (cx * s.qx + cy * s.qy + cz * s.qz) * (c2 / s.theta - M(5));
+  return s.coef * (cx * s.qx + cy * s.qy + cz * s.qz) * (c2 * s.inv_theta - M(5));
+}
+
+// Shakhov target with the Maxwellian value m = eq(x, y, z) given
+template <class M>
+__host__ __device__ inline M shakhov_target_of(const CellParams<M>& s, M m, M x, M y, M z) {
+  const M cx = x - s.ucx, cy = y - s.ucy, cz = z - s.ucz;
+  const M c2 = cx * cx + cy * cy + cz * cz;
+  return m * (M(1) + shakhov_poly(s, cx, cy, cz, c2) + (s.g0 + (s.gx * cx + s.gy * cy + s.gz * cz) + M(0.5) * s.g4 * c2));
 }
 
 template <class M>
 __host__ __device__ inline M shakhov_target(const CellParams<M>& s, M x, M y, M z) {
-  const M cx = x - s.ucx, cy = y - s.ucy, cz = z - s.ucz;
-  const M c2 = cx * cx + cy * cy + cz * cz;
-  const M m = maxwellian(s.eq, x, y, z);
-  return m * (M(1) + shakhov_poly(s, cx, cy, cz, c2) + (s.g0 + (s.gx * cx + s.gy * cy + s.gz * cz) + M(0.5) * s.g4 * c2));
+  return shakhov_target_of(s, maxwellian(s.eq, x, y, z), x, y, z);
 }
 
 // make_cell_params (src/kinetic/kinetic_kernels.hpp:451-471): Shakhov target from the 15 moments, mu = mu0 T^omega
@@ -132,6 +139,7 @@ __host__ __device__ inline CellParams<M> make_cell_params(const double* m, doubl
   cp.qy = static_cast<M>(m[13]);
   cp.qz = static_cast<M>(m[14]);
   cp.theta = static_cast<M>(T);
+  cp.inv_theta = static_cast<M>(1.0 / T);
   const double p = rho * T;
   const double coef = (1.0 - Pr) / (5.0 * p * T);
   cp.coef = T < cold_bgk_T ? M(0) : static_cast<M>(coef);

@@ -85,3 +85,22 @@ def test_gpu_sweep_kernels_agree(B200Backend, name, monkeypatch):
     for kernel in ["legacy", "staged8"]:
         for k in ["f1", "f3", "res1"]:
             assert common.max_rel(runs["auto"][k], runs[kernel][k]) < tol, (kernel, k)
+
+
+@pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64", "tet_positivity_fp32", "maxwell_wall_fp64"])
+def test_gpu_tensor_grid_sums_agree(B200Backend, name, monkeypatch):
+    """On a tensor velocity grid the discrete-equilibrium Newton sums and the residual's Maxwellian are formed from
+    per-axis factors; the per-velocity forms (KIN_VELOCITY_SUMS=pointwise) give the same operation sequence to
+    rounding."""
+    z, setup = common.load(name)
+    runs = {}
+    for mode in ["auto", "pointwise"]:
+        monkeypatch.setenv("KIN_VELOCITY_SUMS", mode)
+        with B200Backend(setup) as be:
+            runs[mode] = common.run_op_sequence(be, z)
+    # both stop the Newton iteration at its tolerance (1e-11 FP64, 1e-6 FP32), possibly one step apart
+    tol = common.TOL[common.precision_of(setup)]
+    for k in ["moments0", "bsums0", "f1", "f3", "moments2"]:
+        assert common.max_rel(runs["auto"][k], runs["pointwise"][k]) < tol, k
+    assert common.max_rel(runs["auto"]["res1"], runs["pointwise"]["res1"]) < 100 * tol
+    assert np.array_equal(runs["auto"]["flags"], runs["pointwise"]["flags"])
