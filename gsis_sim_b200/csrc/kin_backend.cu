@@ -295,7 +295,6 @@ struct Backend final : KinHandle {
   int32_t dq_nv = 0;
   // the equilibrium's velocity grid factored per axis (kin::DeqTensor; tn_n[0] == 0: not a tensor grid)
   DevBuf<double> tn_nodes, tn_w;
-  DevBuf<int32_t> tn_pos;  // per stored velocity: packed node indices (kin::View::tn_pos), empty if not usable
   int32_t tn_n[3] = {0, 0, 0};
   DevBuf<double> xid_x, xid_y, xid_z, wts;
   DevBuf<int32_t> csr_off;
@@ -527,8 +526,8 @@ struct Backend final : KinHandle {
       if (d.deq_weights) dq_w.upload(d.deq_weights, m, stream);
       KCUDA(cudaStreamSynchronize(stream));
     }
-    // KIN_VELOCITY_SUMS=pointwise keeps the per-velocity Maxwellians and Newton sums on a tensor grid too (both give
-    // the same results to rounding; the tests use this to cover both paths)
+    // KIN_VELOCITY_SUMS=pointwise keeps the per-velocity Newton sums of the discrete equilibrium on a tensor grid too
+    // (both give the same results to rounding; the tests use this to cover both paths)
     const char* sums_env = std::getenv("KIN_VELOCITY_SUMS");
     const bool pointwise = sums_env != nullptr && std::strcmp(sums_env, "pointwise") == 0;
     if (!pointwise) {
@@ -543,29 +542,6 @@ struct Backend final : KinHandle {
       if (tensor) {
         tn_nodes.upload(nodes.data(), nodes.size(), stream);
         tn_w.upload(wax.data(), wax.size(), stream);
-        // node indices of the stored velocities (a shard's velocities lie on the full grid's axes)
-        if (n[0] + n[1] + n[2] <= kin::kTensorNodesMax) {
-          std::vector<int32_t> pos(static_cast<size_t>(nv));
-          const double* xs[3] = {dx.data(), dy.data(), dz.data()};
-          bool all = true;
-          for (int q = 0; q < nv && all; ++q) {
-            int32_t packed = 0;
-            int base = 0;
-            for (int a = 0; a < 3; ++a) {
-              const auto b = nodes.begin() + base, e = b + n[a];
-              const auto it = std::lower_bound(b, e, xs[a][q]);
-              if (it == e || *it != xs[a][q]) {
-                all = false;
-                break;
-              }
-              packed |= static_cast<int32_t>(it - b) << (10 * a);
-              base += n[a];
-            }
-            pos[q] = packed;
-          }
-          if (all) tn_pos.upload(pos.data(), pos.size(), stream);
-          KCUDA(cudaStreamSynchronize(stream));
-        }
         KCUDA(cudaStreamSynchronize(stream));
       }
     }
@@ -928,7 +904,6 @@ struct Backend final : KinHandle {
     for (int a = 0; a < 3; ++a) v.dq_tensor.n[a] = tn_n[a];
     v.dq_tensor.node = tn_nodes.p;
     v.dq_tensor.w = tn_w.p;
-    v.tn_pos = tn_pos.p;
     if constexpr (kSplit) {
       kin::View<S, P>& w = pview;
       w.n_cells = nc;
@@ -962,7 +937,6 @@ struct Backend final : KinHandle {
       w.dq_w = v.dq_w;
       w.dq_nv = v.dq_nv;
       w.dq_tensor = v.dq_tensor;
-      w.tn_pos = v.tn_pos;
     }
   }
 

@@ -571,14 +571,10 @@ __device__ inline M residual_value(const View<S, M>& v, const Chunk<S>& ch, int 
 // residual of U velocities of one cell from staged entries (residual_value, kinetic_kernels.hpp:238-278). At an
 // internal face the upwind value is chosen with a select between the two reconstructions (the neighbour's loads are
 // predicated on a < 0), so the U velocities never branch apart; boundary faces follow the reference branches.
-// tab: the cell's per-axis Maxwellian factors e_a[i] = exp(-B (x_a[i] - u_a)^2) (axis by axis, n0 and n1 nodes on
-// the first two axes) and pos the chunk's packed node indices (View::tn_pos + k0, read where the Maxwellian is
-// formed so that they hold no registers through the entry loop), or tab == nullptr (the Maxwellian per velocity).
 template <class S, class M, int U, int NE>
 __device__ __forceinline__ void residual_tile(const View<S, M>& v, const Chunk<S>& ch, int c, const StagedEntry<M>* E,
                                               int ne, const int (&t)[U], const bool (&ok)[U], const M (&x)[U],
-                                              const M (&y)[U], const M (&z)[U], const M* tab, int n0, int n1,
-                                              const int32_t* __restrict__ pos, M (&R)[U], M (&fi)[U]) {
+                                              const M (&y)[U], const M (&z)[U], M (&R)[U], M (&fi)[U]) {
   // mixed precision (FP32 storage, FP64 arithmetic): the face reconstructions f + g . d are formed in the storage
   // precision of their inputs; the flux balance and the collision term are summed in FP64
   constexpr bool kLowRecon = sizeof(S) < sizeof(M);
@@ -663,17 +659,8 @@ __device__ __forceinline__ void residual_tile(const View<S, M>& v, const Chunk<S
     }
   });
   const CellParams<M> cp = v.cp[c];
-  if (tab != nullptr) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int pk = ok[u] ? __ldg(pos + t[u]) : 0;
-      const M m = cp.eq.A * (tab[pk & 1023] * tab[n0 + ((pk >> 10) & 1023)] * tab[n0 + n1 + (pk >> 20)]);
-      R[u] = R[u] - cp.coll * (shakhov_target_of(cp, m, x[u], y[u], z[u]) - fi[u]);
-    }
-  } else {
-#pragma unroll
-    for (int u = 0; u < U; ++u) R[u] = R[u] - cp.coll * (shakhov_target(cp, x[u], y[u], z[u]) - fi[u]);
-  }
+  for (int u = 0; u < U; ++u) R[u] = R[u] - cp.coll * (shakhov_target(cp, x[u], y[u], z[u]) - fi[u]);
 }
 
 // residual of one chunk; partial[c * partial_stride + tile * warps + warp] = sum of R^2 over the warp's velocities
@@ -684,7 +671,6 @@ __global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
   constexpr int kWarps = kTileThreads / 32;
   __shared__ StagedEntry<M> E[kStageMulti];
   __shared__ int off[kCellsPerCta + 1];
-  __shared__ M tab[kCellsPerCta * kTensorNodesMax];
   const int c0 = blockIdx.x * kCellsPerCta, c1 = min(v.n_cells, c0 + kCellsPerCta);
   const int tb = blockIdx.y * (kTileThreads * kTileIters);
   const int te = min(ch.kc, tb + kTileThreads * kTileIters);
@@ -694,7 +680,6 @@ __global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
   int t[U];
   bool ok[U];
   M x[U], y[U], z[U];
-  const bool tensor = v.tn_pos != nullptr;
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     t[u] = tb + threadIdx.x + u * kTileThreads;  // affine in u; used only where ok[u]
@@ -703,19 +688,6 @@ __global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
     x[u] = ok[u] ? v.xi_x[q] : M(0);
     y[u] = ok[u] ? v.xi_y[q] : M(0);
     z[u] = ok[u] ? v.xi_z[q] : M(0);
-  }
-  // per-axis Maxwellian factors of the CTA's cells: n_x + n_y + n_z exponentials per cell instead of one per
-  // velocity (exp(-B |c|^2) = exp(-B c_x^2) exp(-B c_y^2) exp(-B c_z^2) on a tensor grid)
-  const int n0 = v.dq_tensor.n[0], n1 = v.dq_tensor.n[1], nt = n0 + n1 + v.dq_tensor.n[2];
-  if (tensor) {
-    for (int k = threadIdx.x; k < (c1 - c0) * nt; k += kTileThreads) {
-      const int cl = k / nt, i = k - cl * nt;
-      const Maxwell<M> eq = v.cp[c0 + cl].eq;
-      const M u = i < n0 ? eq.ux : (i < n0 + n1 ? eq.uy : eq.uz);
-      const M d = static_cast<M>(v.dq_tensor.node[i]) - u;
-      tab[cl * kTensorNodesMax + i] = kexp(-eq.B * (d * d));
-    }
-    __syncthreads();
   }
   for (int c = c0; c < c1; ++c) {
     const int64_t row = static_cast<int64_t>(c) * ch.stride;
@@ -730,9 +702,7 @@ __global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
       }
     } else {
       M R[U], fi[U];
-      residual_tile<S, M, U, NE>(v, ch, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], t, ok, x, y, z,
-                                 tensor ? tab + (c - c0) * kTensorNodesMax : nullptr, n0, n1, v.tn_pos + ch.k0, R,
-                                 fi);
+      residual_tile<S, M, U, NE>(v, ch, c, E + off[c - c0], off[c - c0 + 1] - off[c - c0], t, ok, x, y, z, R, fi);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;

@@ -96,10 +96,6 @@ struct View {
   const double* dq_w;  // per-velocity weights, nullptr when uniform
   int32_t dq_nv;
   DeqTensor dq_tensor;  // the same grid factored per axis (n[0] == 0 when it is not a tensor grid)
-  // per stored velocity its node indices in dq_tensor's axes, ix | iy << 10 | iz << 20; nullptr unless the stored
-  // velocities lie on that tensor grid with n_x + n_y + n_z <= kTensorNodesMax (the residual then forms the
-  // Maxwellian of its cells as A e_x[ix] e_y[iy] e_z[iz] from per-axis exponentials)
-  const int32_t* tn_pos;
 };
 
 template <class S>

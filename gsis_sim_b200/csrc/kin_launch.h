@@ -9,7 +9,6 @@
 namespace kin {
 
 constexpr int kTileIters = 4;      // velocities per thread in the gradient / residual tiles
-constexpr int kTensorNodesMax = 192;  // n_x + n_y + n_z of the residual's per-axis Maxwellian tables
 constexpr int kSweepThreads = 256;  // one CTA per (direction, block, velocity tile): 8 warps share every level
 constexpr int kSweepTile = 32;      // velocities of one sweep CTA (one per lane)
 

@@ -107,17 +107,12 @@ __host__ __device__ inline M shakhov_poly(const CellParams<M>& s, M cx, M cy, M 
   return s.coef * (cx * s.qx + cy * s.qy + cz * s.qz) * (c2 * s.inv_theta - M(5));
 }
 
-// Shakhov target with the Maxwellian value m = eq(x, y, z) given
-template <class M>
-__host__ __device__ inline M shakhov_target_of(const CellParams<M>& s, M m, M x, M y, M z) {
-  const M cx = x - s.ucx, cy = y - s.ucy, cz = z - s.ucz;
-  const M c2 = cx * cx + cy * cy + cz * cz;
-  return m * (M(1) + shakhov_poly(s, cx, cy, cz, c2) + (s.g0 + (s.gx * cx + s.gy * cy + s.gz * cz) + M(0.5) * s.g4 * c2));
-}
-
 template <class M>
 __host__ __device__ inline M shakhov_target(const CellParams<M>& s, M x, M y, M z) {
-  return shakhov_target_of(s, maxwellian(s.eq, x, y, z), x, y, z);
+  const M cx = x - s.ucx, cy = y - s.ucy, cz = z - s.ucz;
+  const M c2 = cx * cx + cy * cy + cz * cz;
+  const M m = maxwellian(s.eq, x, y, z);
+  return m * (M(1) + shakhov_poly(s, cx, cy, cz, c2) + (s.g0 + (s.gx * cx + s.gy * cy + s.gz * cz) + M(0.5) * s.g4 * c2));
 }
 
 // make_cell_params (src/kinetic/kinetic_kernels.hpp:451-471): Shakhov target from the 15 moments, mu = mu0 T^omega

@@ -89,9 +89,8 @@ def test_gpu_sweep_kernels_agree(B200Backend, name, monkeypatch):
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64", "tet_positivity_fp32", "maxwell_wall_fp64"])
 def test_gpu_tensor_grid_sums_agree(B200Backend, name, monkeypatch):
-    """On a tensor velocity grid the discrete-equilibrium Newton sums and the residual's Maxwellian are formed from
-    per-axis factors; the per-velocity forms (KIN_VELOCITY_SUMS=pointwise) give the same operation sequence to
-    rounding."""
+    """On a tensor velocity grid the discrete-equilibrium Newton sums are formed from per-axis sums; the per-velocity
+    sums (KIN_VELOCITY_SUMS=pointwise) give the same operation sequence to rounding."""
     z, setup = common.load(name)
     runs = {}
     for mode in ["auto", "pointwise"]:
