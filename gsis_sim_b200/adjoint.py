@@ -358,3 +358,144 @@ class KineticAdjoint:
 
     def close(self):
         self.sol.backend.adjoint_end()
+
+
+# ---- torch.autograd: M_dot as a differentiable function of (delta, T_w per wall face, alpha per wall face) -----
+
+class MassFlowProblem:
+    """M_dot of one kinetic case as a function of the rarefaction parameter delta, the temperature of every diffuse
+    wall face and the accommodation of every diffuse wall face. The forward is a CIS solve on a B200Backend converged
+    to `tol`; the derivative is the discrete adjoint of that fixed point (KineticAdjoint). `mass_flow` makes it a
+    torch.autograd.Function.
+
+    setup, host: a set-up in the adjoint's scope (see KineticAdjoint.check_scope). Its mu_hat0 is 1 / (sqrt(2) delta)
+    (derive_quantities), so delta defaults to 1 / (sqrt(2) mu_hat0) and mu_hat0 scales as 1 / delta for other
+    values. `wall_faces` (internal boundary-face indices of the diffuse walls) is the order of the T_wall and alpha
+    vectors."""
+
+    def __init__(self, setup: abi.SetupArrays, host, delta: float | None = None, tol: float = 1e-12,
+                 max_iterations: int = 20000,
+                 adjoint_tol: float = 1e-12, adjoint_max_iterations: int = 20000,
+                 initial=(1.0, (0.0, 0.0, 0.0), 1.0), device: int = 0):
+        self.setup, self.host = setup, host
+        self.mu0_0 = float(setup["mu0"])
+        self.delta0 = 1.0 / (math.sqrt(2.0) * self.mu0_0) if delta is None else float(delta)
+        bpatch = np.asarray(setup["bface_patch"]) if setup.n_bfaces else np.zeros(0, np.int32)
+        bkind = host.patch_int[:, 0][bpatch] if setup.n_bfaces else np.zeros(0, np.int32)
+        self.wall_faces = np.flatnonzero(bkind == abi.BC_DIFFUSE_WALL)
+        self.T_patch = np.asarray(host.patch_dbl[bpatch[self.wall_faces], 0], float)
+        self.tol, self.max_iterations = float(tol), int(max_iterations)
+        self.adjoint_tol, self.adjoint_max_iterations = float(adjoint_tol), int(adjoint_max_iterations)
+        self.initial = initial
+        self.device = device
+
+    def solve(self, delta: float, T_wall=None, alpha=None):
+        """Converged forward solve at (delta, T_wall, alpha) -> (solver, M_dot). T_wall: one temperature per wall
+        face (None: the patch temperatures). alpha: one accommodation per wall face, which must be 1: the adjoint
+        gives the derivative at alpha = 1 from below (alpha <= 1), and walls with alpha < 1 are Maxwell walls, outside
+        its scope."""
+        from .backend import B200Backend
+        from .solver import KineticSolver
+
+        if not delta > 0:
+            raise ValueError(f"delta must be positive, got {delta}")
+        if alpha is not None and np.any(np.asarray(alpha, float).reshape(-1) != 1.0):
+            raise AdjointScopeError("the accommodation derivative is taken at alpha = 1 (from below); alpha < 1 makes "
+                                    "the walls Maxwell walls, outside the adjoint's scope")
+        s = abi.SetupArrays(dict(self.setup.arrays), dict(self.setup.scalars))  # arrays shared, scalars own
+        s["mu0"] = self.mu0_0 if float(delta) == self.delta0 else self.mu0_0 * (self.delta0 / float(delta))
+        be = B200Backend(s, device=self.device)
+        try:
+            sol = KineticSolver(s, self.host, be)
+            if T_wall is not None:
+                Tw = np.asarray(T_wall, float).reshape(-1)
+                if Tw.shape != self.wall_faces.shape:
+                    raise ValueError(f"T_wall: {Tw.shape[0]} values for {len(self.wall_faces)} wall faces")
+                T = np.ones(s.n_bfaces)
+                T[self.wall_faces] = Tw
+                sol.set_wall_temperature(T)
+            rho, u, T0 = self.initial
+            sol.initialize_uniform(rho, u, T0)
+            r = math.inf
+            for _ in range(self.max_iterations):
+                r = sol.sweep().residual
+                if r < self.tol:
+                    break
+            if not r < self.tol:
+                raise FloatingPointError(f"forward CIS stopped at residual {r:.3e} after {self.max_iterations} "
+                                         f"iterations (tolerance {self.tol:g})")
+        except BaseException:
+            be.close()
+            raise
+        return sol, sol.mass_flow()[2]
+
+    def gradients(self, sol, delta: float):
+        """(dM_dot/d delta, dM_dot/dT_w per wall face, dM_dot/d alpha per wall face at alpha = 1) at a converged
+        solve; the alpha derivative is NaN on wall faces not aligned with a coordinate axis."""
+        ka = KineticAdjoint(sol)
+        try:
+            res = ka.solve(tol=self.adjoint_tol, max_iterations=self.adjoint_max_iterations)
+        finally:
+            ka.close()
+        if not res.residual < self.adjoint_tol:
+            raise FloatingPointError(f"adjoint stopped at residual {res.residual:.3e} after {res.iterations} "
+                                     f"iterations (tolerance {self.adjoint_tol:g})")
+        w = self.wall_faces
+        return res.dJ_ddelta(float(sol.s["mu0"]), float(delta)), res.dJ_dTw[w].copy(), res.dJ_dalpha[w].copy()
+
+    def release(self, sol):
+        sol.backend.close()
+
+
+_FUNCTION = None
+
+
+def _mass_flow_function():
+    """The torch.autograd.Function of mass_flow (built on first use, so that importing this module needs no torch)."""
+    global _FUNCTION
+    if _FUNCTION is not None:
+        return _FUNCTION
+    import torch
+
+    class MassFlowFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, delta, T_wall, alpha, problem):
+            Tw = None if T_wall is None else T_wall.detach().to("cpu", torch.float64).numpy()
+            al = None if alpha is None else alpha.detach().to("cpu", torch.float64).numpy()
+            state, J = problem.solve(float(delta), Tw, al)
+            ctx.problem, ctx.state, ctx.delta = problem, state, float(delta)
+            ctx.given = (T_wall is not None, alpha is not None)
+            return torch.tensor(J, dtype=torch.float64, device=delta.device)
+
+        @staticmethod
+        def backward(ctx, grad):
+            # one adjoint solve per forward; its gradients serve every later backward through the same graph
+            if getattr(ctx, "grads", None) is None:
+                try:
+                    ctx.grads = ctx.problem.gradients(ctx.state, ctx.delta)
+                finally:
+                    ctx.problem.release(ctx.state)
+                    ctx.state = None
+            g_delta, g_T, g_alpha = ctx.grads
+            g = grad.to(torch.float64)
+            dev = g.device
+            out_delta = g * torch.tensor(g_delta, dtype=torch.float64, device=dev)
+            out_T = g * torch.as_tensor(g_T, dtype=torch.float64, device=dev) if ctx.given[0] else None
+            out_alpha = g * torch.as_tensor(g_alpha, dtype=torch.float64, device=dev) if ctx.given[1] else None
+            return out_delta, out_T, out_alpha, None
+
+    _FUNCTION = MassFlowFunction
+    return _FUNCTION
+
+
+def mass_flow(problem, delta, T_wall=None, alpha=None):
+    """M_dot as a differentiable torch scalar (float64): the forward solves the kinetic case to convergence, the
+    backward runs the discrete adjoint once and returns dM_dot/d delta, dM_dot/dT_w and dM_dot/d alpha (per wall
+    face, in problem.wall_faces order; alpha at 1 from below). `problem` is a MassFlowProblem, or any object with the
+    same solve / gradients / release methods. T_wall and alpha may be None (patch temperatures, alpha = 1; no
+    gradient). The converged solver is kept for the backward, which releases it after the adjoint solve."""
+    import torch
+
+    if not isinstance(delta, torch.Tensor):
+        delta = torch.tensor(float(delta), dtype=torch.float64)
+    return _mass_flow_function().apply(delta, T_wall, alpha, problem)

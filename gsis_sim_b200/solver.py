@@ -87,6 +87,7 @@ class KineticSolver:
         self.discrete_eq = bool(setup["discrete_eq"])
         self.deq_grid = (np.asarray(setup["deq_lo"], float), np.asarray(setup["deq_hi"], float),
                          np.asarray(setup["deq_d"], float), float(setup["deq_criterion"]))
+        self.wall_T = None  # per-face wall temperatures (set_wall_temperature), else the patch values
         self._build_pressure_stencils()
         self.init_static_inflow()
 
@@ -133,7 +134,7 @@ class KineticSolver:
         self.inflow[wall, 0] = 1.0
         self.inflow[wall, 1] = 1.0
         self.inflow[wall, 2:5] = h.patch_dbl[self.bpatch[wall], 2:5]
-        self.inflow[wall, 5] = T[wall]
+        self.inflow[wall, 5] = T[wall] if self.wall_T is None else self.wall_T[wall]
         self.correct_inflow(np.flatnonzero(wall))
         pres = self.bkind == abi.BC_PRESSURE
         self.inflow[pres, 0] = 1.0
@@ -143,6 +144,34 @@ class KineticSolver:
         self.wall_unit = np.zeros((self.nb, 10))
         if len(mw):
             self.wall_unit[mw] = self._wall_unit_sums(mw)
+
+    def set_wall_temperature(self, T_faces):
+        """Temperature of every wall face (internal boundary-face numbering, one value per boundary face; the values of
+        other faces are ignored) in place of the wall patch's temperature; None restores the patch temperatures.
+
+        The reference sets wall temperatures per patch. A per-face field is the parameter whose derivative the adjoint
+        gives (dM_dot / dT_w per face); the wall inflow state (rho = 1, patch velocity, T) is rebuilt at once, the
+        wall density rho_Gamma is kept, and the field stays in force through re-initialisation."""
+        if T_faces is None:
+            self.wall_T = None
+        else:
+            T = np.asarray(T_faces, float).reshape(-1)
+            if T.shape != (self.nb,):
+                raise KineticSolverError(f"wall temperatures: {T.shape[0]} values for {self.nb} boundary faces")
+            wall = (self.bkind == abi.BC_DIFFUSE_WALL) | (self.bkind == abi.BC_MAXWELL_WALL)
+            if not np.all(T[wall] > 0):
+                raise KineticSolverError("wall temperatures must be positive")
+            self.wall_T = T.copy()
+        wall = np.flatnonzero((self.bkind == abi.BC_DIFFUSE_WALL) | (self.bkind == abi.BC_MAXWELL_WALL))
+        h = self.h
+        self.inflow[wall, 1] = 1.0
+        self.inflow[wall, 2:5] = h.patch_dbl[self.bpatch[wall], 2:5]
+        self.inflow[wall, 5] = h.patch_dbl[self.bpatch[wall], 0] if self.wall_T is None else self.wall_T[wall]
+        self.correct_inflow(wall)
+        mw = np.flatnonzero(self.bkind == abi.BC_MAXWELL_WALL)
+        if len(mw):
+            self.wall_unit[mw] = self._wall_unit_sums(mw)
+        self.version += 1
 
     def _wall_unit_sums(self, faces):
         """compute_wall_unit_sums (src/kinetic/kinetic_solver.cpp:263-277): discrete half-space moments of the unit

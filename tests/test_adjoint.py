@@ -266,3 +266,97 @@ def test_reversed_velocity_sweeps_solve_the_adjoint():
     (gmu,) = torch.autograd.grad((R, Fw), (mut,), grad_outputs=(torch.as_tensor(lam), torch.as_tensor(nu)))
     dmu_ref, _, _ = ar.adjoint_gradient(sm, f, rg)
     assert abs(-float(gmu) - dmu_ref) <= 1e-8 * abs(dmu_ref)
+
+
+def _wall_field_solution(T_faces):
+    """The channel on the CPU oracle with a per-face wall temperature field (internal boundary-face numbering)."""
+    from oracle.kinetic_oracle import OracleBackend
+
+    setup, host = channel_case()
+    sol = KineticSolver(setup, host, OracleBackend(setup))
+    sol.set_wall_temperature(T_faces)
+    sol.initialize_uniform(0.75, (0.0, 0.0, 0.0), 1.0)
+    r = 1.0
+    for _ in range(3000):
+        r = sol.sweep().residual
+        if r < 1e-13:
+            break
+    assert r < 1e-12
+    return sol
+
+
+@pytest.mark.timeout(600)
+def test_wall_temperature_field_matches_reference_adjoint():
+    """KineticSolver.set_wall_temperature on the CPU oracle: the patch values leave the inflow table unchanged, and
+    the central difference of M_dot along a random per-face wall-temperature direction equals the reference
+    adjoint's per-face dM_dot/dT_w projected on that direction."""
+    from oracle import adjoint_ref as ar
+
+    sol, setup, host = _oracle_solution()
+    before = sol.inflow.copy()
+    T_patch = host.patch_dbl[np.asarray(setup["bface_patch"]), 0]
+    sol.set_wall_temperature(T_patch)
+    assert np.array_equal(sol.inflow, before)
+    sm = ar.SteadyMap(setup, host)
+    f, rg = ar.state_of(sol)
+    _, dTw, _ = ar.adjoint_gradient(sm, f, rg)
+    walls = np.flatnonzero(sol.bkind == ar.BC_DIFFUSE_WALL)
+    rng = np.random.default_rng(2026)
+    v = np.zeros(sol.nb)
+    v[walls] = rng.standard_normal(len(walls))
+    v /= np.linalg.norm(v)
+    h = 1e-5
+    Jp = _wall_field_solution(T_patch + h * v).mass_flow()[2]
+    Jm = _wall_field_solution(T_patch - h * v).mass_flow()[2]
+    fd = (Jp - Jm) / (2 * h)
+    assert abs(float(dTw @ v) - fd) <= 1e-6 * abs(fd)
+
+
+class _ClosedFormProblem:
+    """Stand-in for MassFlowProblem with a closed-form M_dot(delta, T, alpha) and its exact gradients."""
+
+    def __init__(self, n):
+        self.n = n
+        self.solves = self.adjoints = self.released = 0
+
+    @staticmethod
+    def J(d, T, a):
+        return d * d * np.sum(T ** 1.5) + np.sum(np.sin(T) * a) + math.log(d)
+
+    def solve(self, d, T, a):
+        T = np.linspace(0.9, 1.1, self.n) if T is None else T
+        a = np.ones(self.n) if a is None else a
+        self.solves += 1
+        return (d, T.copy(), a.copy()), self.J(d, T, a)
+
+    def gradients(self, state, d):
+        self.adjoints += 1
+        _, T, a = state
+        return 2 * d * np.sum(T ** 1.5) + 1 / d, 1.5 * d * d * np.sqrt(T) + np.cos(T) * a, np.sin(T)
+
+    def release(self, state):
+        self.released += 1
+
+
+def test_mass_flow_function_chain_rule():
+    """mass_flow, the torch.autograd.Function over a forward solve and one adjoint solve, on a closed-form stand-in:
+    gradcheck of all three inputs, the upstream gradient scales the result, one adjoint solve per forward even
+    through repeated backward passes, and inputs given as None get no gradient."""
+    prob = _ClosedFormProblem(4)
+    d = torch.tensor(0.7, dtype=torch.float64, requires_grad=True)
+    T = torch.tensor([1.0, 1.2, 0.8, 1.1], dtype=torch.float64, requires_grad=True)
+    a = torch.tensor([0.5, 0.9, 1.3, 1.0], dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(lambda d, T, a: adj.mass_flow(prob, d, T, a), (d, T, a))
+    prob.solves = prob.adjoints = prob.released = 0
+    J = adj.mass_flow(prob, d, T, a)
+    assert abs(float(J.detach()) - prob.J(0.7, T.detach().numpy(), a.detach().numpy())) < 1e-15
+    gd, gT, ga = torch.autograd.grad(3.0 * J, (d, T, a), retain_graph=True)
+    rd, rT, ra = _ClosedFormProblem(4).gradients((0.7, T.detach().numpy(), a.detach().numpy()), 0.7)
+    assert abs(float(gd) - 3 * rd) < 1e-12 and np.allclose(gT.numpy(), 3 * rT, rtol=1e-14, atol=0)
+    assert np.allclose(ga.numpy(), 3 * ra, rtol=1e-14, atol=0)
+    torch.autograd.grad(J, (d,))
+    assert (prob.solves, prob.adjoints, prob.released) == (1, 1, 1)
+    J2 = adj.mass_flow(prob, d)
+    (g2,) = torch.autograd.grad(J2, (d,))
+    T0 = np.linspace(0.9, 1.1, 4)
+    assert abs(float(g2) - (2 * 0.7 * np.sum(T0 ** 1.5) + 1 / 0.7)) < 1e-12
