@@ -31,10 +31,12 @@ sys.path.insert(0, ROOT)
 HBM_FALLBACK_GBS = 6650.0
 
 
-# DRAM bytes (read + write) per (cell, velocity) per launch from one ncu capture of the tube case at 62,848 cells x
-# 12^3 velocities in FP64 (profiles/gradient_residual_sweep_tiles_tube63k_12cube_fp64.md); the LU-SGS figure is
-# that of the first block pass. Scaled by the units of a full launch for roofline.traffic.
-DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 34.9, ("fp64", "k_residual"): 57.5, ("fp64", "k_sweep_tiles"): 36.5}
+# DRAM bytes (read + write) per (cell, velocity) per launch from ncu captures of the tube case at 62,848 cells x
+# 12^3 velocities (profiles/gradient_residual_sweep_tiles_tube63k_12cube_fp64.md, FP64;
+# profiles/residual_tube63k_12cube_mixed.md, mixed); the LU-SGS figure is that of the first block pass. Scaled by
+# the units of a full launch for roofline.traffic.
+DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 34.9, ("fp64", "k_residual"): 57.5, ("fp64", "k_sweep_tiles"): 36.5,
+                       ("mixed", "k_residual"): 23.7}
 
 
 def peaks():
