@@ -175,6 +175,49 @@ def run_case(name, mesh_kw, bcs, Kn, nv, kinetic, init, iterations) -> dict:
     return out
 
 
+# Converged runs (tests/golden/converged/<name>.npz): the reference KineticSolver iterated from a uniform state
+# until its residual falls below `tol`. Only the setup, the per-iteration history and the converged macroscopic
+# fields are stored (f alone would be 22 MB for the slab).
+# The planar Couette slab: x in [0, 1] in 200 cells, one cell thick with periodic y sides (the wall motion
+# direction) and symmetry z sides; diffuse walls at T = 1 moving along y at -+0.1 most-probable speeds
+# (u = -+0.1 sqrt(2) in units of sqrt(R T0)); delta_rp = 1, omega = 0.81, the reference's uniform midpoint 24^3
+# grid on [-5, 5]^3, FP64, default CIS settings, residual 1e-8.
+_U_WALL = float(0.1 * np.sqrt(2.0))
+CONVERGED = {
+    "couette_slab_200": (dict(n=(200, 1, 1), lo=(0, 0, 0), hi=(1, 1 / 200, 1 / 200),
+                              patches=["wall_left", "wall_right", "sym_y", "sym_y", "sym_z", "sym_z"]),
+                         [("wall_left", "diffuse_wall", dict(T=1.0, u=(0.0, -_U_WALL, 0.0))),
+                          ("wall_right", "diffuse_wall", dict(T=1.0, u=(0.0, _U_WALL, 0.0))),
+                          ("sym_y", "periodic_slab", {}), ("sym_z", "symmetry", {})],
+                         dict(delta_rp=1.0, omega=0.81, nv=(24, 24, 24)), dict(precision="fp64"),
+                         (1.0, (0.0, 0.0, 0.0), 1.0), 1e-8, 3000),
+}
+
+
+def run_converged(name, mesh_kw, bcs, conditions, kinetic, init, tol, max_iterations) -> dict:
+    mesh = ref.RefMesh.box(**mesh_kw)
+    spec = ref.case_spec(bcs, kinetic=kinetic, **conditions)
+    case = ref.RefCase(mesh, spec)
+    out = {}
+    out.update(case.setup.to_npz_dict())
+    out.update(host_arrays(case))
+    case.init_uniform(init[0], init[1], init[2])
+    infos = []
+    while len(infos) < max_iterations:
+        infos.append(case.sweep())
+        if len(infos) > 1 and infos[-1][6] < tol:
+            break
+    out["solver.init"] = np.array([init[0], *init[1], init[2]])
+    out["solver.tol"] = np.array(tol)
+    out["solver.infos"] = np.array(infos)
+    out["solver.patch_mass_flow"] = case.patch_mass_flow()
+    out["solver.moments"] = case.moments()
+    fp, fm, fs = case.boundary_fluxes()
+    out["solver.F_plus"], out["solver.F_minus"], out["solver.face_state"] = fp, fm, fs
+    out["meta.name"] = np.array(name)
+    return out
+
+
 def main(names=None):
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     for name, args in CASES.items():
@@ -184,6 +227,14 @@ def main(names=None):
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **data)
         print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB")
+    for name, args in CONVERGED.items():
+        if names and name not in names:
+            continue
+        data = run_converged(name, *args)
+        os.makedirs(os.path.join(HERE, "converged"), exist_ok=True)
+        path = os.path.join(HERE, "converged", f"{name}.npz")
+        np.savez_compressed(path, **data)
+        print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, {len(data['solver.infos'])} iterations")
 
 
 if __name__ == "__main__":

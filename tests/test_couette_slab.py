@@ -1,0 +1,72 @@
+"""The planar Couette slab at full size: 200 cells across x in [0, 1], diffuse walls at T = 1 moving along y at
+-+0.1 most-probable speeds, delta_rp = 1, omega = 0.81, the uniform 24^3 grid on [-5, 5]^3 (13,824 velocities),
+FP64, the reference's default CIS settings, iterated from rest to residual 1e-8.
+
+Golden values: the reference KineticSolver (src/kinetic/kinetic_solver.cpp) run to convergence
+(tests/golden/converged/couette_slab_200.npz, made by tests/golden/make_golden.py). The CPU tests pin the fixture
+by the physics of a steady planar Couette flow and check the first CIS iteration of the host loop on the CPU oracle
+against the reference's; tests/test_gpu_couette_slab.py runs the whole solve on the B200 backend."""
+import os
+
+import numpy as np
+import pytest
+
+from gsis_sim_b200 import abi
+from gsis_sim_b200.kinetic_setup import HostSetup
+from gsis_sim_b200.solver import KineticSolver
+from tests import common
+
+FIXTURE = os.path.join(common.GOLDEN, "converged", "couette_slab_200.npz")
+# moments order of the backend (src/kinetic/kinetic_types.hpp:107-109)
+RHO, UX, UY, UZ, T, P, SXX, SYY, SZZ, SXY, SYZ, SXZ, QX, QY, QZ = range(15)
+
+
+def load():
+    z = np.load(FIXTURE, allow_pickle=False)
+    return z, abi.SetupArrays.from_npz(z), HostSetup.from_npz(z)
+
+
+def x_order(z):
+    """Internal cell numbers sorted by the cell centre's x."""
+    return np.argsort(z["host.cell_center"][:, 0], kind="stable")
+
+
+def test_fixture_is_a_converged_couette_flow():
+    z, setup, _ = load()
+    infos = z["solver.infos"]
+    assert setup.n_cells == 200 and setup.nv == 24 ** 3
+    assert infos[-1][6] < float(z["solver.tol"]) <= infos[-2][6]
+    m = z["solver.moments"][x_order(z)]
+    # steady planar flow: no mass flux across the slab, uniform shear stress, the walls drag the gas along y
+    assert np.max(np.abs(m[:, RHO] * m[:, UX])) < 1e-6
+    # (the cell-centred P_xy of the wall cells differs from the interior by a few 1e-4: the one-sided
+    # reconstruction at the wall; away from the walls it is uniform to the discretisation's rounding)
+    sxy = m[:, SXY]
+    assert np.all(sxy < 0) and np.ptp(sxy) < 1e-3 * abs(sxy.mean())
+    assert np.ptp(sxy[5:-5]) < 1e-5 * abs(sxy.mean())
+    assert np.all(np.diff(m[:, UY]) > 0) and abs(m[:, UY]).max() < 0.1 * np.sqrt(2.0)
+    # mirror symmetry about the mid-plane x = 1/2: rho, T even; u_y odd
+    for k, sign in ((RHO, 1), (T, 1), (P, 1), (UY, -1), (SXY, 1)):
+        assert common.max_rel(m[:, k], sign * m[::-1, k]) < 1e-6, k
+    # closed domain: the walls carry no net mass
+    assert np.max(np.abs(z["solver.patch_mass_flow"])) < 1e-8
+
+
+def test_first_iterations_of_the_host_loop_on_the_oracle():
+    from oracle.kinetic_oracle import OracleBackend
+
+    z, setup, host = load()
+    sol = KineticSolver(setup, host, OracleBackend(setup))
+    init = z["solver.init"]
+    sol.initialize_uniform(init[0], init[1:4], init[4])
+    for ref in z["solver.infos"][:4]:
+        info = sol.sweep()
+        assert info.iteration == ref[0]
+        assert abs(info.residual - ref[6]) <= 1e-9 * ref[6]
+        assert abs(info.total_mass - ref[8]) <= 1e-12 * ref[8]
+
+
+@pytest.mark.parametrize("key", ["solver.moments", "solver.F_plus", "solver.F_minus"])
+def test_fixture_fields_are_finite(key):
+    z, _, _ = load()
+    assert np.all(np.isfinite(z[key]))
