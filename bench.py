@@ -521,7 +521,10 @@ def main():
     e2e = updates * jobs / t_wall
     hbm, peak_kind = peaks()
     s = 8 if args.precision == "fp64" else 4
-    # dominant kernel: gradient, residual or LU-SGS pass (per-launch algorithmic bytes in DESIGN.md)
+    # dominant kernel: gradient, residual or LU-SGS pass. Algorithmic bytes per (cell, velocity), s = stored value
+    # size: the gradient reads f and writes three components (4 s); the residual reads f and the gradient and
+    # writes R (5 s); an LU-SGS pass reads R and writes its update (2 s), the last pass also reads and writes f
+    # (4 s), so 3 s per pass on average over the two passes of an inner sweep
     n_sweeps = inner * args.steps
     kernels = {
         "k_gradient": (timings["gradient"] / n_sweeps, nc * nv * 4 * s),

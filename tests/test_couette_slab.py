@@ -5,7 +5,12 @@ FP64, the reference's default CIS settings, iterated from rest to residual 1e-8.
 Golden values: the reference KineticSolver (src/kinetic/kinetic_solver.cpp) run to convergence
 (tests/golden/converged/couette_slab_200.npz, made by tests/golden/make_golden.py). The CPU tests pin the fixture
 by the physics of a steady planar Couette flow and check the first CIS iteration of the host loop on the CPU oracle
-against the reference's; tests/test_gpu_couette_slab.py runs the whole solve on the B200 backend."""
+against the reference's; tests/test_gpu_couette_slab.py runs the whole solve on the B200 backend.
+
+Independent check: the reference's 1-D solver ref1d on the same problem (tests/golden/converged/
+couette_slab_ref1d.npz, made by tests/golden/make_ref1d.py), with the same 24-point x velocity grid (the solvers then
+differ only in their discretisation in x) and with its velocity-converged Gauss-Legendre grid (the physical answer;
+the 24^3 grid's velocity error is 0.2% on the shear stress and 2% on the flow velocity)."""
 import os
 
 import numpy as np
@@ -17,6 +22,7 @@ from gsis_sim_b200.solver import KineticSolver
 from tests import common
 
 FIXTURE = os.path.join(common.GOLDEN, "converged", "couette_slab_200.npz")
+REF1D = os.path.join(common.GOLDEN, "converged", "couette_slab_ref1d.npz")
 # moments order of the backend (src/kinetic/kinetic_types.hpp:107-109)
 RHO, UX, UY, UZ, T, P, SXX, SYY, SZZ, SXY, SYZ, SXZ, QX, QY, QZ = range(15)
 
@@ -64,6 +70,33 @@ def test_first_iterations_of_the_host_loop_on_the_oracle():
         assert info.iteration == ref[0]
         assert abs(info.residual - ref[6]) <= 1e-9 * ref[6]
         assert abs(info.total_mass - ref[8]) <= 1e-12 * ref[8]
+
+
+# field -> (moment column, tolerance against ref1d on the 24-point grid, against ref1d velocity-converged), both
+# relative to the field's largest magnitude over the slab
+REF1D_FIELDS = {"rho": (RHO, 1e-5, 1e-4), "uy": (UY, 5e-4, 3e-2), "T": (T, 2e-5, 1e-4), "qx": (QX, 3e-3, 5e-2),
+                "qy": (QY, 3e-3, 1e-1), "Pxy": (SXY, 1e-3, 5e-3)}
+
+
+def check_against_ref1d(z, moments):
+    """Fields of a converged slab (moments in internal cell order) against ref1d, interpolated to the cell centres."""
+    r = np.load(REF1D, allow_pickle=False)
+    order = x_order(z)
+    xc = z["host.cell_center"][order, 0]
+    m = moments[order]
+    for name, (k, tol_mid, tol_gl) in REF1D_FIELDS.items():
+        for grid, tol in (("mid24", tol_mid), ("gl", tol_gl)):
+            ref = np.interp(xc, r[f"{grid}.x"], r[f"{grid}.{name}"])
+            err = np.max(np.abs(m[:, k] - ref)) / np.max(np.abs(ref))
+            assert err < tol, (name, grid, err)
+    # away from the wall cells the shear stress agrees with ref1d's on the same velocity grid to 1e-4
+    sxy = m[5:-5, SXY]
+    assert np.max(np.abs(sxy - r["mid24.Pxy"].mean())) < 1e-4 * abs(r["mid24.Pxy"].mean())
+
+
+def test_fixture_agrees_with_the_independent_1d_solver():
+    z, _, _ = load()
+    check_against_ref1d(z, z["solver.moments"])
 
 
 @pytest.mark.parametrize("key", ["solver.moments", "solver.F_plus", "solver.F_minus"])

@@ -1,8 +1,8 @@
 """The planar Couette slab at full size solved on the B200 backend from rest to residual 1e-8, against the reference
 KineticSolver's converged run (tests/golden/converged/couette_slab_200.npz; case in tests/test_couette_slab.py).
 
-The north-star tolerance for FP64 moment fields is 1e-6 relative; the residual history, the iteration count and the
-wall fluxes are compared too."""
+FP64 moment fields must agree to 1e-6 relative; the residual history, the iteration count and the
+wall fluxes are compared too, and the converged fields against the reference's independent 1-D solver ref1d."""
 import time
 
 import numpy as np
@@ -10,7 +10,7 @@ import pytest
 
 from gsis_sim_b200.solver import KineticSolver
 from tests import common
-from tests.test_couette_slab import SXY, load, x_order
+from tests.test_couette_slab import SXY, check_against_ref1d, load, x_order
 
 pytestmark = pytest.mark.gpu
 
@@ -58,3 +58,5 @@ def test_gpu_couette_slab_converges_to_the_reference_state():
     assert common.max_rel(fp, z["solver.F_plus"]) < MOMENT_TOL
     assert common.max_rel(fm, z["solver.F_minus"]) < MOMENT_TOL
     assert np.max(np.abs(flows)) < 1e-8
+    # and the independent 1-D solver of the same problem
+    check_against_ref1d(z, moments)
