@@ -302,16 +302,17 @@ def run_time_to_mdot(args, local):
     print(json.dumps(line), flush=True)
 
 
-def channel_case(delta=5.0, Tw=1.0, nv=24, n=(64, 32, 1)):
+def channel_case(delta=5.0, Tw=1.0, nv=24, n=(64, 32, 1), alpha=1.0):
     """Pressure-driven channel: box n[0] x n[1] x 1 on x in [0, 4], y in [0, 1], one cell thick with periodic sides;
-    inlet p 1, outlet p 0.5, T 1; diffuse walls T_w; nv^3 uniform velocities on [-5, 5]^3; FP64 with the continuous
-    equilibrium and the "cell" pressure-boundary reconstruction (the adjoint's scope)."""
+    inlet p 1, outlet p 0.5, T 1; walls at T_w with accommodation alpha (diffuse at 1); nv^3 uniform velocities on
+    [-5, 5]^3; FP64 with the continuous equilibrium and the "cell" pressure-boundary reconstruction (the adjoint's
+    scope)."""
     from gsis_sim_b200 import kinetic_setup as ks
     from gsis_sim_b200.mesh import box_mesh
 
     m = box_mesh(n, (0.0, 0.0, 0.0), (4.0, 1.0, 1.0 / n[1]), ("inlet", "outlet", "wall", "wall", "side", "side"))
     bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "pressure_outlet", p=0.5),
-           ks.BC("wall", "diffuse_wall", T=Tw), ks.BC("side", "periodic_slab")]
+           ks.BC("wall", "diffuse_wall", T=Tw, alpha=alpha), ks.BC("side", "periodic_slab")]
     kp = ks.KineticParams(precision="fp64", equilibrium="continuous", pressure_boundary_reconstruction="cell")
     return ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, delta_rp=delta), bcs,
                                   ks.VelocityGrid(n=(nv, nv, nv)), kp)
@@ -342,7 +343,9 @@ def run_adjoint(args, local):
     """Adjoint / forward wall-time ratio on the channel (or, --adjoint-case tube, on the tube mesh): the forward CIS
     solve from rest to residual --fwd-tol, then
     the adjoint solve of dM_dot/d(delta, T_w) to --adj-tol (both through the public host loops, wall clock). With
-    --adjoint-fd also the central finite difference of M_dot in delta (two more forward solves)."""
+    --adjoint-fd also finite differences of the forward solver: central in delta (step --fd-step relative) and, on the
+    channel, central in a uniform wall temperature (step --fd-step) and second-order one-sided from below in a
+    uniform accommodation (alpha = 1 - h, 1 - 2h, h = 1e-4; Maxwell-wall solves)."""
     import numpy as np
     import torch
 
@@ -363,8 +366,8 @@ def run_adjoint(args, local):
     else:
         delta = 5.0
 
-        def make(d):
-            return channel_case(delta=d, nv=args.adj_nv)
+        def make(d, Tw=1.0, alpha=1.0):
+            return channel_case(delta=d, nv=args.adj_nv, Tw=Tw, alpha=alpha)
 
         workload = (f"kinetic CIS, channel 64x32x1 cells x in [0,4], inlet p 1 / outlet p 0.5, diffuse walls, "
                     f"{args.adj_nv}^3 velocities on [-5,5]^3, delta 5, continuous equilibrium")
@@ -396,16 +399,27 @@ def run_adjoint(args, local):
             "config": {"workload": workload, "cells": setup.n_cells, "velocities": setup.nv,
                        "forward_tol": args.fwd_tol, "adjoint_tol": args.adj_tol}}
     if args.adjoint_fd:
-        h = 1e-5
-        Js = []
-        for sgn in (1, -1):
-            sp, hp = make(delta * (1 + sgn * h))
+        h = args.fd_step
+
+        def mdot(*a, **kw):
+            sp, hp = make(*a, **kw)
             sp_sol = converge_channel(sp, hp, local, args.fwd_tol, args.max_iters)[0]
-            Js.append(sp_sol.mass_flow()[2])
+            J = sp_sol.mass_flow()[2]
             sp_sol.backend.close()
-        fd = (Js[0] - Js[1]) / (2 * h * delta)
+            return J
+
+        fd = (mdot(delta * (1 + h)) - mdot(delta * (1 - h))) / (2 * h * delta)
+        line["fd_step"] = h
         line["dM_dot_d_delta_fd"] = fd
         line["fd_rel_error"] = abs(dJ_ddelta - fd) / abs(fd)
+        if args.adjoint_case == "channel":
+            fd_T = (mdot(delta, Tw=1 + h) - mdot(delta, Tw=1 - h)) / (2 * h)
+            line["dM_dot_dT_w_sum_fd"] = fd_T
+            line["fd_T_w_rel_error"] = abs(line["dM_dot_dT_w_sum"] - fd_T) / abs(fd_T)
+            ha = 1e-4
+            fd_a = (3 * res.J - 4 * mdot(delta, alpha=1 - ha) + mdot(delta, alpha=1 - 2 * ha)) / (2 * ha)
+            line["dM_dot_d_alpha_fd"] = fd_a
+            line["fd_alpha_rel_error"] = abs(line["dM_dot_d_alpha"] - fd_a) / abs(fd_a)
     print(json.dumps(line), flush=True)
 
 
@@ -434,7 +448,9 @@ def main():
     ap.add_argument("--history", default=None, help="write per-iteration (wall s, M_dot, residual) to <prefix>_<prec>.txt")
     # third headline metric: adjoint / forward wall-time ratio on the channel
     ap.add_argument("--adjoint", action="store_true")
-    ap.add_argument("--adjoint-fd", action="store_true", help="with --adjoint: also the finite difference in delta")
+    ap.add_argument("--adjoint-fd", action="store_true",
+                    help="with --adjoint: also finite differences in delta and, on the channel, wall T and alpha")
+    ap.add_argument("--fd-step", type=float, default=1e-6, help="relative step of the central differences")
     ap.add_argument("--adj-nv", type=int, default=24)
     ap.add_argument("--adjoint-case", default="channel", choices=["channel", "tube"])
     ap.add_argument("--adj-inner", type=int, default=None, help="adjoint sweeps per coupling update (default: the "
