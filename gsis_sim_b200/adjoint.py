@@ -228,9 +228,9 @@ class KineticAdjoint:
         mu[j] = -C_J * self.sgn[j]
         return mu
 
-    def _reduce(self):
-        cell, face = self.sol.backend.adjoint_reduce(self._mu())
-        return cell.reshape(self.nc, 9), face.reshape(max(self.nb, 0), 10)
+    def _reduce(self, cells: bool = True, faces: bool = True):
+        cell, face = self.sol.backend.adjoint_reduce(self._mu(), cells=cells, faces=faces)
+        return (cell.reshape(self.nc, 9) if cells else None), (face.reshape(max(self.nb, 0), 10) if faces else None)
 
     def _coefficients(self, cell, face):
         sol = self.sol
@@ -299,7 +299,7 @@ class KineticAdjoint:
             # each sweep; a one-sweep lag on these strongly coupled unknowns can make the iteration unstable)
             nu_old = self.nu
             if walls:
-                _, face = self._reduce()
+                _, face = self._reduce(cells=False)
                 self.nu = -face[self.wall, 0]
             cell, face = self._reduce()
             coef, _ = self._coefficients(cell, face)
@@ -319,9 +319,10 @@ class KineticAdjoint:
                 break
             for _ in range(1, inner):
                 if walls:
-                    _, face = self._reduce()
+                    _, face = self._reduce(cells=False)
                     self.nu = -face[self.wall, 0]
-                self._reduce()
+                # the transport's seeds with the new nu (the coupling sums stay frozen over the inner sweeps)
+                self._reduce(cells=False, faces=False)
                 be.adjoint_update(coef, run_passes=True)
         return self.gradients(it, res)
 

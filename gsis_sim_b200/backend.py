@@ -96,13 +96,16 @@ class KineticBackendABI:
         self._call("adjoint_get", abi.as_ptr(out, C.c_double), out.size)
         return out.reshape(self.n_cells, self.nv)
 
-    def adjoint_reduce(self, mu):
+    def adjoint_reduce(self, mu, cells: bool = True, faces: bool = True):
+        """Transposed transport with the per-face weights mu, then the per-cell (9) and per-face sums; cells=False /
+        faces=False skip those sums (returned as None) when only the transport's seeds are wanted."""
         m = np.ascontiguousarray(mu, dtype=np.float64)
-        cell = np.empty(self.n_cells * 9, dtype=np.float64)
-        face = np.empty(max(self.n_bfaces, 1) * ADJ_FACE_SUMS, dtype=np.float64)
-        self._call("adjoint_reduce", abi.as_ptr(m, C.c_double), m.size, abi.as_ptr(cell, C.c_double), cell.size,
-                   abi.as_ptr(face, C.c_double), self.n_bfaces * ADJ_FACE_SUMS)
-        return cell, face[:self.n_bfaces * ADJ_FACE_SUMS]
+        cell = np.empty(self.n_cells * 9, dtype=np.float64) if cells else None
+        face = np.empty(max(self.n_bfaces, 1) * ADJ_FACE_SUMS, dtype=np.float64) if faces else None
+        self._call("adjoint_reduce", abi.as_ptr(m, C.c_double), m.size,
+                   abi.as_ptr(cell, C.c_double) if cells else None, cell.size if cells else 0,
+                   abi.as_ptr(face, C.c_double) if faces else None, self.n_bfaces * ADJ_FACE_SUMS if faces else 0)
+        return cell, (face[:self.n_bfaces * ADJ_FACE_SUMS] if faces else None)
 
     def adjoint_update(self, coef, run_passes: bool = True, want_operator: bool = False):
         c = np.ascontiguousarray(coef, dtype=np.float64).ravel()

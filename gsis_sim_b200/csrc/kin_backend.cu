@@ -1404,18 +1404,22 @@ struct Backend final : KinHandle {
                       int64_t n_face) override {
     if constexpr (std::is_same<S, double>::value && std::is_same<M, double>::value) {
       KCHECK(adj_on, "adjoint_begin first");
-      KCHECK(n_mu == nb && n_cell == static_cast<int64_t>(nc) * kin::kAdjCellSums &&
-                 n_face == static_cast<int64_t>(nb) * kin::kAdjFaceSums,
+      // a NULL output with length 0 skips that sum (the transport always runs)
+      const bool want_cells = cell_sums != nullptr;
+      const bool want_faces = face_sums != nullptr && nb > 0;
+      KCHECK(n_mu == nb && n_cell == (cell_sums != nullptr ? static_cast<int64_t>(nc) * kin::kAdjCellSums : 0) &&
+                 n_face == (face_sums != nullptr ? static_cast<int64_t>(nb) * kin::kAdjFaceSums : 0),
              "adjoint_reduce: array lengths do not match");
       if (nb > 0) KCUDA(cudaMemcpyAsync(adj_mu.p, mu, sizeof(double) * nb, cudaMemcpyHostToDevice, stream));
       const kin::AdjView a = adj_view();
-      kin::adj_cell_sums(view, a, adj_cell.p, stream);
+      if (want_cells) kin::adj_cell_sums(view, a, adj_cell.p, stream);
       kin::adj_transport(view, a, stream);
-      kin::adj_face_sums(view, a, adj_face.p, stream);
-      launched(nb > 0 ? 3 : 2);
+      if (want_faces) kin::adj_face_sums(view, a, adj_face.p, stream);
+      launched(1 + (want_cells ? 1 : 0) + (want_faces ? 1 : 0));
       KCUDA(cudaGetLastError());
-      KCUDA(cudaMemcpyAsync(cell_sums, adj_cell.p, sizeof(double) * n_cell, cudaMemcpyDeviceToHost, stream));
-      if (nb > 0)
+      if (want_cells)
+        KCUDA(cudaMemcpyAsync(cell_sums, adj_cell.p, sizeof(double) * n_cell, cudaMemcpyDeviceToHost, stream));
+      if (want_faces)
         KCUDA(cudaMemcpyAsync(face_sums, adj_face.p, sizeof(double) * n_face, cudaMemcpyDeviceToHost, stream));
       KCUDA(cudaStreamSynchronize(stream));
     } else {

@@ -303,7 +303,9 @@ int kin_adjoint_get(KinHandle* h, double* lambda, int64_t n);
    incoming inflow values against the inflow Maxwellian (M, M c, M c^2) and S5, S6 = sum_in w an M {c^2, 1}; per
    boundary face also (10 in all) A1 = sum_in a lambda f_spec, A2 = sum_in s_grad f_owner(reflected velocity),
    S_spec = sum_in w an f_spec (axis-aligned diffuse walls, f_spec = the owner's reconstructed face value at the
-   reflected velocity; zero elsewhere). */
+   reflected velocity; zero elsewhere). cell_sums = NULL with n_cell = 0 skips the per-cell sums, face_sums = NULL
+   with n_face = 0 the per-face sums; the transposed transport (the seeds that kin_adjoint_update gathers) always
+   runs. */
 int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,
                        double* face_sums, int64_t n_face);
 /* Finish O_f(y) with the per-cell moment-expansion coefficients coef (8 per cell: a0, a (3), a2, b (3); the term
