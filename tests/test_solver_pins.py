@@ -102,3 +102,69 @@ def test_slab_sides_build(side):
     setup, host = ks.build_kinetic_setup(mesh, ks.Gas(omega=0.66), ks.Conditions(Kn=0.2), bcs,
                                          ks.VelocityGrid(n=(10, 10, 10)), ks.KineticParams(precision="fp64"))
     assert setup.n_cells == 8 and setup.nv == 1000
+
+
+def _solver(mesh, bcs, grid, Kn=0.5, **kinetic):
+    from oracle.kinetic_oracle import OracleBackend
+
+    params = ks.KineticParams(precision="fp64", **kinetic)
+    setup, host = ks.build_kinetic_setup(mesh, ks.Gas(omega=0.66), ks.Conditions(L_ref=1.0, T0=273.15, Kn=Kn), bcs,
+                                         grid, params)
+    return KineticSolver(setup, host, OracleBackend(setup))
+
+
+@pytest.mark.parametrize("fallback", ["collisionless", "continuous"])
+def test_cells_the_grid_cannot_hold_become_collisionless_and_skip_the_correction(fallback):
+    """tests/kinetic/test_kinetic_phase5.cpp:264-321: on a grid with unit spacing (points +-0.5, +-1.5, ...) cell 0
+    holds a distribution on a few points, with negative values, whose temperature 0.05 is below the lowest one a
+    non-negative distribution on the grid can have at its velocity, so the discrete equilibrium does not exist."""
+    mesh = box_mesh((2, 1, 1), (0.0, 0.0, 0.0), (1.0, 0.5, 0.5), ("inlet", "outlet", "wall", "wall", "wall", "wall"))
+    bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "vacuum"), ks.BC("wall", "diffuse_wall")]
+    grid = ks.VelocityGrid(n=(12, 12, 12), lo=(-6.0,) * 3, hi=(6.0,) * 3)
+    s = _solver(mesh, bcs, grid, deq_fallback=fallback)
+    xs = [grid.axis(a) for a in range(3)]
+    # grid order: x fastest
+    X, Y, Z = (np.meshgrid(*xs, indexing="ij")[a].transpose(2, 1, 0).ravel() for a in range(3))
+    nv = X.size
+    f = np.zeros((2, nv))
+    f[1] = (2 * np.pi) ** -1.5 * np.exp(-0.5 * (X * X + Y * Y + Z * Z))
+    ax = np.where(np.abs(X - 1.5) < 1e-9, 1.1, np.where((np.abs(X - 0.5) < 1e-9) | (np.abs(X - 2.5) < 1e-9), -0.05, 0.0))
+    by = np.where((np.abs(Y - 0.5) < 1e-9) | (np.abs(Y - 1.5) < 1e-9), 0.5, 0.0)
+    cz = np.where(np.abs(Z - 0.5) < 1e-9, 1.0, 0.0)
+    f[0] = ax * by * cz  # the uniform weight is 1
+    s.set_distribution(f)
+    info = s.prepare()
+    assert info.deq_failed == 1
+    m = s.moments()
+    wh = m[:, :5].copy()
+    wn = wh.copy()
+    wn[:, 0] *= 1.02
+    replaced = s.apply_gsis_correction(wh, wn)
+    m2 = s.moments()
+    assert abs(m2[1, 0] / wn[1, 0] - 1.0) < 1e-6  # the equilibrium cell is corrected either way
+    d0 = np.max(np.abs(s.distribution()[0] - f[0]))
+    if fallback == "collisionless":
+        assert replaced == 1 and s.replaced[0] == 1
+        assert d0 == 0.0  # f of the collisionless cell is left as it is
+        s.sweep()
+        assert np.all(np.isfinite(s.distribution()))
+    else:
+        assert d0 > 0.0  # corrected with the continuous Maxwellian
+
+
+def test_cell_pressure_reconstruction_changes_the_inflow():
+    """tests/kinetic/test_kinetic_phase5.cpp:323-371: with a density gradient along x, the inlet's incoming mass flux
+    F- differs between the limited reconstruction of W_b and the cell state."""
+    mesh = box_mesh((4, 1, 1), (0.0, 0.0, 0.0), (1.0, 0.25, 0.25), ("inlet", "outlet", "side", "side", "side", "side"))
+    bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "vacuum"), ks.BC("side", "periodic_slab")]
+    grid = ks.VelocityGrid(n=(16, 16, 16), lo=(-8.0,) * 3, hi=(8.0,) * 3)
+    x = mesh_x(mesh)
+    w = np.column_stack([1.0 - 0.6 * x, 0.2 + 0.3 * x, np.zeros_like(x), np.zeros_like(x), np.ones_like(x)])
+    fm = []
+    for mode in ("limited", "cell"):
+        s = _solver(mesh, bcs, grid, equilibrium="continuous", pressure_boundary_reconstruction=mode)
+        s.initialize_equilibrium(w)
+        s.prepare()
+        _, F_minus, _ = s.boundary_fluxes()
+        fm.append(F_minus[0, 0])  # boundary face 0: the inlet, the first patch
+    assert abs(fm[0] - fm[1]) > 1e-4 * abs(fm[1])
