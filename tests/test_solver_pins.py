@@ -168,3 +168,55 @@ def test_cell_pressure_reconstruction_changes_the_inflow():
         _, F_minus, _ = s.boundary_fluxes()
         fm.append(F_minus[0, 0])  # boundary face 0: the inlet, the first patch
     assert abs(fm[0] - fm[1]) > 1e-4 * abs(fm[1])
+
+
+def test_closed_domain_keeps_total_mass_and_walls_have_zero_net_mass_flux():
+    """tests/kinetic/test_kinetic_cpu.cpp:99-139: a box closed by a hot, a cold and moving diffuse walls."""
+    mesh = box_mesh((5, 3, 2), (0.0, 0.0, 0.0), (1.0, 0.6, 0.4), ("hot", "cold", "wall", "wall", "wall", "wall"))
+    bcs = [ks.BC("hot", "diffuse_wall", T=1.3), ks.BC("cold", "diffuse_wall", T=0.8),
+           ks.BC("wall", "diffuse_wall", T=1.0, u=(0.2, 0.0, 0.0))]
+    s = _solver(mesh, bcs, ks.VelocityGrid(n=(10, 10, 10)), Kn=0.3, sweep_blocks=3)
+    assert s.h.closed_domain
+    s.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
+    total0 = float(np.sum(s.volume))
+    max_scale_dev = 0.0
+    for _ in range(15):
+        max_scale_dev = max(max_scale_dev, abs(s.prepare().mass_scale - 1.0))
+        s.sweep()
+    s.prepare()
+    total = float(np.sum(s.moments_[:, 0] * s.volume))
+    assert abs(total / s.mass_target - 1.0) < 1e-12
+    assert abs(s.mass_target / total0 - 1.0) < 1e-4
+    assert max_scale_dev < 1e-2
+    F_plus, F_minus, _ = s.boundary_fluxes()
+    assert np.max(np.abs(F_plus[:, 0] + F_minus[:, 0])) < 1e-6 * np.max(np.abs(F_plus[:, 0]))
+
+
+def test_discrete_equilibrium_keeps_cold_states_conservative():
+    """tests/kinetic/test_kinetic_phase5.cpp:135-198: on a grid with unit spacing the moments of a T = 0.3 Maxwellian
+    are 0.3% off; the discrete equilibrium initialises and corrects to the given states to 2e-6."""
+    mesh = box_mesh((3, 2, 1), (0.0, 0.0, 0.0), (1.0, 1.0, 0.5), ("inlet", "outlet", "wall", "wall", "wall", "wall"))
+    bcs = [ks.BC("inlet", "pressure_inlet", T=0.3, p=0.3), ks.BC("outlet", "vacuum"),
+           ks.BC("wall", "diffuse_wall", T=0.3)]
+    grid = ks.VelocityGrid(n=(12, 12, 12), lo=(-6.0,) * 3, hi=(6.0,) * 3)
+    c = np.arange(6, dtype=float)
+    w = np.column_stack([0.8 + 0.1 * c, 0.4 - 0.1 * c, np.full(6, 0.15), np.full(6, -0.05), 0.25 + 0.02 * c])
+    wn = np.column_stack([w[:, 0] * 1.03, w[:, 1] + 0.05, np.full(6, 0.1), np.zeros(6), w[:, 4] * 0.97])
+
+    def error(m, ref):
+        return max(np.max(np.abs(m[:, 0] / ref[:, 0] - 1.0)), np.max(np.abs(m[:, 4] / ref[:, 4] - 1.0)),
+                   np.max(np.abs(m[:, 1] - ref[:, 1]) / np.sqrt(ref[:, 4])))
+
+    cont = _solver(mesh, bcs, grid, equilibrium="continuous")
+    cont.initialize_equilibrium(w)
+    assert error(cont.moments(), w) > 1e-3
+    disc = _solver(mesh, bcs, grid, equilibrium="discrete")
+    assert disc.discrete_eq
+    disc.initialize_equilibrium(w)
+    assert error(disc.moments(), w) < 2e-6
+    disc.sweep()
+    half = disc.moments()
+    disc.apply_gsis_correction(half[:, :5], wn)
+    assert error(disc.moments(), wn) < 2e-6
+    info = disc.prepare()
+    assert info.deq_corrected == 6 and info.deq_failed == 0
