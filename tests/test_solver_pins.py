@@ -220,3 +220,42 @@ def test_discrete_equilibrium_keeps_cold_states_conservative():
     assert error(disc.moments(), wn) < 2e-6
     info = disc.prepare()
     assert info.deq_corrected == 6 and info.deq_failed == 0
+
+
+def test_boundary_iterations_solve_the_lag_without_changing_the_distribution():
+    """tests/kinetic/test_kinetic_cpu.cpp:511-560: boundary_iterations = 8 in one prepare equals eight prepares
+    (each invalidated by a zero GSIS correction, which leaves f as it is) of boundary_iterations = 1, and the repeated
+    boundary update changes the inflow. (The reference runs it on distorted tetrahedra; this box is hexahedral.)"""
+    mesh = box_mesh((3, 2, 2), (0.0, 0.0, 0.0), (3.0, 2.0, 2.0), ("inlet", "outlet", "wall", "wall", "wall", "wall"))
+    bcs = [ks.BC("inlet", "pressure_inlet"), ks.BC("outlet", "vacuum"), ks.BC("wall", "diffuse_wall")]
+    grid = ks.VelocityGrid(n=(10, 10, 10))
+    a = _solver(mesh, bcs, grid, sweep_blocks=1, positivity_limiter=True, boundary_iterations=1)
+    b = _solver(mesh, bcs, grid, sweep_blocks=1, positivity_limiter=True, boundary_iterations=8)
+    from gsis_sim_b200.mesh import compute_geometry
+
+    xc = compute_geometry(mesh).cell_center
+    w = np.column_stack([0.8 + 0.15 * xc[:, 0], 0.05 + 0.03 * xc[:, 1], 0.02 * xc[:, 2], np.zeros(len(xc)),
+                         0.9 + 0.04 * xc[:, 2]])
+    a.initialize_equilibrium(w)
+    b.initialize_equilibrium(w)
+    f = a.distribution()
+    first = a.boundary_fluxes()
+    m = a.moments()
+    repeated = first
+    for _ in range(1, 8):
+        a.apply_gsis_correction(m[:, :5], m[:, :5])
+        repeated = a.boundary_fluxes()
+    batched = b.boundary_fluxes()
+    assert np.array_equal(a.distribution(), f) and np.array_equal(b.distribution(), f)
+    np.testing.assert_allclose(batched[0], repeated[0], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(batched[1], repeated[1], rtol=0, atol=1e-12)
+    assert np.max(np.abs(first[1] - repeated[1])) > 1e-6
+    # the fixed-f boundary update converges: 64 updates as the reference, 8 are much closer to it than 1
+    reference = repeated
+    for _ in range(8, 64):
+        a.apply_gsis_correction(m[:, :5], m[:, :5])
+        reference = a.boundary_fluxes()
+    error1 = np.max(np.abs(first[1] - reference[1]))
+    error8 = np.max(np.abs(batched[1] - reference[1]))
+    assert error8 < 0.1 * error1
+    assert np.array_equal(a.distribution(), f)
