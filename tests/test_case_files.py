@@ -102,6 +102,42 @@ def test_toml_rules():
         case.kinetic_params(c)
 
 
+def _kp(kinetic: str):
+    return case.kinetic_params(case.parse_case_toml(BASE.format(cond="Kn = 0.1", extra="") + "\n[kinetic]\n" + kinetic))
+
+
+def test_kinetic_params_defaults_and_values():
+    """tests/kinetic/test_kinetic_params.cpp:44-71 and the [kinetic] part of test_kinetic_phase5.cpp:373-400."""
+    d = case.kinetic_params(case.parse_case_toml(BASE.format(cond="Kn = 0.1", extra="")))
+    assert d.pseudo_cfl == 0.0 and d.sweep_blocks == 0 and d.precision == "fp32" and d.boundary_iterations == 1
+    assert d.cold_bgk_temperature == 0.0 and d.deq_fallback == "collisionless"
+    assert d.pressure_boundary_reconstruction == "limited"
+    p = _kp('pseudo_cfl = 50\nsweep_blocks = 8\nprecision = "fp64"\nbackend = "cpu"\nboundary_iterations = 8\n')
+    assert p.pseudo_cfl == 50.0 and p.sweep_blocks == 8 and p.precision == "fp64" and p.boundary_iterations == 8
+    q = _kp('limiter = "none"\nlimiter_eps = "relative"\ninitial_pressure = 0.5\ninitial_temperature = 1.2\n'
+            'convergence_u_floor = 0.01\nlaunch_cells = 100\nsweep_cells_per_launch = 10\n')
+    assert q.limiter == "none" and q.limiter_eps == "relative" and q.initial_pressure == 0.5
+    assert q.initial_temperature == 1.2 and q.convergence_u_floor == 0.01
+    c = _kp('cold_bgk_temperature = 0.1\ndeq_fallback = "continuous"\npressure_boundary_reconstruction = "cell"\n')
+    assert c.cold_bgk_temperature == 0.1 and c.deq_fallback == "continuous"
+    assert c.pressure_boundary_reconstruction == "cell"
+
+
+@pytest.mark.parametrize("kinetic,word", [("boundary_iterations = 0", "boundary_iterations"),
+                                          ("boundary_iterations = 1001", "boundary_iterations"),
+                                          ("sweep_block = 8", "sweep_block"),
+                                          ('precision = "fp16"', "kinetic.precision"),
+                                          ('limiter = "minmod"', "kinetic.limiter"),
+                                          ("initial_pressure = 0", "initial"),
+                                          ('deq_fallback = "none"', "deq_fallback"),
+                                          ("cold_bgk_temperature = -1", "cold_bgk_temperature")])
+def test_kinetic_params_errors(kinetic, word):
+    """tests/kinetic/test_kinetic_params.cpp:73-86 and test_kinetic_phase5.cpp:398-401: each bad value is an error
+    that names the key."""
+    with pytest.raises(case.CaseError, match=word):
+        _kp(kinetic + "\n")
+
+
 def test_channel_fixture_builds():
     cfg = case.load_case(CHANNEL)
     setup, host = case.case_setup(cfg)
