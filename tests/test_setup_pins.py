@@ -4,7 +4,9 @@
 * octant sweep directions group the velocity points (tests/kinetic/test_kinetic_phase5.cpp:241-262);
 * a uniform equilibrium between pressure boundaries and walls at the same state is a fixed point of the CIS
   iteration (tests/kinetic/test_kinetic_cpu.cpp:71-97), with the C oracle as the backend (the B200 version on the
-  full-size tube is tests/test_gpu_fullsize.py)."""
+  full-size tube is tests/test_gpu_fullsize.py);
+* the equilibrium initialisation reproduces the given macroscopic states (tests/kinetic/test_kinetic_cpu.cpp:
+  275-306)."""
 import numpy as np
 import pytest
 
@@ -65,3 +67,24 @@ def test_equilibrium_is_preserved():
     m = s.moments()
     assert np.max(np.abs(m[:, 0] - 1.0)) < 1e-5 and np.max(np.abs(m[:, 4] - 1.0)) < 1e-5
     assert np.max(np.abs(m[:, 1])) < 1e-5
+
+
+def test_equilibrium_initialization_reproduces_the_macroscopic_state():
+    """tests/kinetic/test_kinetic_cpu.cpp:275-306, with the C oracle as the backend."""
+    from oracle.kinetic_oracle import OracleBackend
+
+    mesh = box_mesh((3, 2, 2), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ("inlet", "outlet", "wall", "wall", "wall", "wall"))
+    bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "vacuum"), ks.BC("wall", "diffuse_wall")]
+    grid = ks.VelocityGrid(n=(16, 16, 16), lo=(-8.0,) * 3, hi=(8.0,) * 3)
+    setup, host = ks.build_kinetic_setup(mesh, ks.Gas(omega=0.66), ks.Conditions(L_ref=1.0, T0=273.15, Kn=0.5), bcs,
+                                         grid, ks.KineticParams(precision="fp64"))
+    s = KineticSolver(setup, host, OracleBackend(setup))
+    c = np.arange(12, dtype=float)
+    w = np.column_stack([0.5 + 0.1 * c, 0.3 - 0.05 * c, np.full(12, 0.1), np.full(12, -0.2), 0.8 + 0.03 * c])
+    s.initialize_equilibrium(w)
+    m = s.moments()
+    np.testing.assert_allclose(m[:, 0], w[:, 0], rtol=1e-6, atol=0)
+    np.testing.assert_allclose(m[:, 1], w[:, 1], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(m[:, 3], w[:, 3], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(m[:, 4], w[:, 4], rtol=1e-5, atol=0)
+    assert np.max(np.abs(m[:, 12])) < 1e-5 and np.max(np.abs(m[:, 9])) < 1e-5  # q_x, P_xy
