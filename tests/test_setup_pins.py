@@ -6,7 +6,8 @@
   iteration (tests/kinetic/test_kinetic_cpu.cpp:71-97), with the C oracle as the backend (the B200 version on the
   full-size tube is tests/test_gpu_fullsize.py);
 * the equilibrium initialisation reproduces the given macroscopic states (tests/kinetic/test_kinetic_cpu.cpp:
-  275-306)."""
+  275-306);
+* the discrete equilibrium matches the conserved moments on the grid (tests/kinetic/test_kinetic_phase5.cpp:77-133)."""
 import numpy as np
 import pytest
 
@@ -88,3 +89,40 @@ def test_equilibrium_initialization_reproduces_the_macroscopic_state():
     np.testing.assert_allclose(m[:, 3], w[:, 3], rtol=0, atol=1e-6)
     np.testing.assert_allclose(m[:, 4], w[:, 4], rtol=1e-5, atol=0)
     assert np.max(np.abs(m[:, 12])) < 1e-5 and np.max(np.abs(m[:, 9])) < 1e-5  # q_x, P_xy
+
+
+def test_discrete_equilibrium_matches_the_conserved_moments_on_the_grid():
+    """tests/kinetic/test_kinetic_phase5.cpp:77-133 (Maxwellian part), on the C oracle: on the tube case's
+    30 x 24 x 24 grid a cold supersonic jet and flows near the grid's edge have continuous Maxwellians whose
+    discrete moments miss the state by more than 1e-4; the discrete equilibrium's parameters reproduce it to 1e-10,
+    and a well-resolved state is left as it is (Newton result 0)."""
+    from oracle.kinetic_oracle import OracleBackend
+
+    mesh = box_mesh((1, 1, 1), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ("wall",) * 6)
+    grid = ks.VelocityGrid(n=(30, 24, 24), lo=(-10.0, -8.0, -8.0), hi=(10.0, 8.0, 8.0))
+    setup, _ = ks.build_kinetic_setup(mesh, ks.Gas(omega=0.66), ks.Conditions(Kn=0.5), [ks.BC("wall", "diffuse_wall")],
+                                      grid, ks.KineticParams(precision="fp64"))
+    be = OracleBackend(setup)
+    X, Y, Z = (np.meshgrid(*[grid.axis(a) for a in range(3)], indexing="ij")[a].ravel() for a in range(3))
+    w = grid.delta(0) * grid.delta(1) * grid.delta(2)
+
+    def moments(rho, u, T):
+        f = rho * (2 * np.pi * T) ** -1.5 * np.exp(-((X - u[0]) ** 2 + (Y - u[1]) ** 2 + (Z - u[2]) ** 2) / (2 * T))
+        c2 = X * X + Y * Y + Z * Z
+        return w * np.array([f.sum(), (f * X).sum(), (f * Y).sum(), (f * Z).sum(), (f * c2).sum()])
+
+    def error(m, rho, u, T):
+        target = np.array([rho, rho * u[0], rho * u[1], rho * u[2], rho * (np.dot(u, u) + 3 * T)])
+        scale = np.array([rho, rho * np.sqrt(T), rho * np.sqrt(T), rho * np.sqrt(T), rho * T])
+        return float(np.max(np.abs(m - target) / scale))
+
+    states = np.array([[0.02, 2.0, 0.3, -0.4, 0.1], [0.5, 1.7, -0.2, 0.25, 0.05], [1.3, 0.33, 0.0, 0.0, 0.2],
+                       [1.0, 6.5, 0.0, 0.0, 1.0]])
+    params, result = be.discrete_maxwell(states, 1e-11)
+    for st, p, r in zip(states, params, result):
+        rho, u, T = st[0], st[1:4], st[4]
+        assert error(moments(rho, u, T), rho, u, T) > 1e-4
+        assert r > 0
+        assert error(moments(p[0], p[1:4], p[4]), rho, u, T) < 1e-10
+    _, r = be.discrete_maxwell(np.array([[1.0, 0.3, 0.1, 0.0, 1.0]]), 1e-11)
+    assert r[0] == 0
