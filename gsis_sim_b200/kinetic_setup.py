@@ -251,6 +251,9 @@ class HostSetup:
     boundary_iterations: int
     pressure_boundary_reconstruction: str = "limited"
     patch_names: list = field(default_factory=list)
+    # reference scales for SI output (ReferenceScales, src/config/case_config.hpp): p_ref and sqrt(R T0); 0 = unknown
+    ref_pressure: float = 0.0
+    ref_velocity: float = 0.0
 
     @classmethod
     def from_npz(cls, z) -> "HostSetup":
@@ -463,5 +466,5 @@ def build_kinetic_setup(mesh: PolyMesh, gas: Gas, cond: Conditions, bcs: list, g
                      closed_domain=closed, inner_sweeps=params.inner_sweeps,
                      inner_wall_update=params.inner_wall_update, boundary_iterations=params.boundary_iterations,
                      pressure_boundary_reconstruction=params.pressure_boundary_reconstruction,
-                     patch_names=list(m.patch_names))
+                     patch_names=list(m.patch_names), ref_pressure=d["ref_pressure"], ref_velocity=d["ref_velocity"])
     return s, host

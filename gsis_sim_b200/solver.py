@@ -29,6 +29,54 @@ class KineticSolverError(RuntimeError):
     pass
 
 
+def summarize_patches(names, types, patch_faces, area, normal, F_plus, F_minus, face_state, patch_dbl=None,
+                      patch_target=None, length=1.0, ref_pressure=0.0, ref_velocity=0.0) -> list:
+    """Per-patch boundary flows (summarize_kinetic_patches, src/kinetic/kinetic_output.cpp:198-268).
+
+    names, types: patch names and BoundaryType names; patch_faces: per patch the boundary-face indices of the arrays
+    below; area (nondimensional, per face), normal (outward unit normals), F_plus / F_minus (mass, momentum (3),
+    energy fluxes through the face, outward positive) and face_state (rho, u (3), T) per face. Returns one dict per
+    patch: the net nondimensional fluxes (outward positive), the area-averaged face state and, when the reference
+    scales are given (length L_ref, p_ref, sqrt(R T0)), SI flows with flow INTO the domain positive: mass (kg/s),
+    heat (W; the third central moment in the face's local rest frame), total energy (W), and the force (N)."""
+    si = ref_pressure > 0.0 and ref_velocity > 0.0
+    L2 = length * length
+    mass_flux, heat_flux = ref_pressure / ref_velocity if si else 0.0, ref_pressure * ref_velocity
+    out = []
+    for pi, faces in enumerate(patch_faces):
+        faces = np.asarray(faces, np.int64)
+        A = area[faces]
+        Fs = F_plus[faces] + F_minus[faces]
+        F = Fs.sum(axis=0) if len(faces) else np.zeros(5)
+        w = face_state[faces]
+        u = w[:, 1:4]
+        un = np.sum(u * normal[faces], axis=1)
+        heat = float(np.sum(Fs[:, 4] - np.sum(u * Fs[:, 1:4], axis=1) + 0.5 * np.sum(u * u, axis=1) * Fs[:, 0]
+                            - 1.5 * w[:, 0] * w[:, 4] * un * A))
+        a = float(A.sum())
+        p = {"name": names[pi], "type": types[pi], "faces": int(len(faces)), "area_nd": a, "mdot_nd": float(F[0]),
+             "momentum_flux_nd": [float(x) for x in F[1:4]], "energy_flux_nd": float(F[4])}
+        if types[pi] == "maxwell_wall" and patch_dbl is not None:
+            p["accommodation"] = float(patch_dbl[pi, 5])
+        if si:
+            p["mdot_kg_s"] = float(F[0]) * mass_flux * L2
+            if types[pi] == "mass_flow_inlet" and patch_dbl is not None and patch_target is not None:
+                p["pressure_Pa"] = float(patch_dbl[pi, 1]) * ref_pressure
+                p["target_mass_flow_kg_s"] = float(patch_target[pi]) * mass_flux * L2
+                p["mass_flow_relative_error"] = abs(float(F[0]) + patch_target[pi]) / patch_target[pi]
+            p["area_m2"] = a * L2
+            p["mass_flow_kg_s"] = -float(F[0]) * mass_flux * L2
+            p["heat_flow_W"] = -heat * heat_flux * L2
+            p["energy_flow_W"] = -float(F[4]) * heat_flux * L2
+            p["force_N"] = [float(x) * ref_pressure * L2 for x in F[1:4]]
+        if a > 0.0:
+            p["face_rho_nd"] = float(np.sum(A * w[:, 0]) / a)
+            p["face_u_nd"] = [float(np.sum(A * w[:, k]) / a) for k in (1, 2, 3)]
+            p["face_T_nd"] = float(np.sum(A * w[:, 4]) / a)
+        out.append(p)
+    return out
+
+
 @dataclass
 class IterationInfo:
     """KineticIterationInfo (src/kinetic/kinetic_solver.hpp:37-59)."""
@@ -549,6 +597,18 @@ class KineticSolver:
         mdot_in = -sum(pm[p] for p in range(len(pm)) if self.ptype[p] in (T_PRESSURE_INLET, T_MASS_FLOW_INLET))
         mdot_out = sum(pm[p] for p in range(len(pm)) if self.ptype[p] in (T_PRESSURE_OUTLET, T_VACUUM))
         return mdot_in * f, mdot_out * f, 0.5 * (mdot_in + mdot_out) * f
+
+    def patch_summary(self) -> list:
+        """Per-patch flows of the last prepare (summarize_patches; SI values when the set-up carries its reference
+        scales, as the builder's do)."""
+        self.prepare()
+        h = self.h
+        names = h.patch_names or [f"patch{i}" for i in range(len(h.patch_int))]
+        types = [BOUNDARY_TYPES[t] for t in h.patch_int[:, 3]]
+        faces = [np.flatnonzero(self.bpatch == pi) for pi in range(len(h.patch_int))]
+        return summarize_patches(names, types, faces, self.barea, h.face_normal[self.bf_global], self.F_plus,
+                                 self.F_minus, self.face_state, h.patch_dbl, h.patch_target, h.length_scale,
+                                 h.ref_pressure, h.ref_velocity)
 
     # ---- section cuts ------------------------------------------------------------------------------------------
     def section_cuts(self, spec):
