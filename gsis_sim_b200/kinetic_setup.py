@@ -262,7 +262,9 @@ class HostSetup:
         return cls(n_internal_faces=int(isc[0]), owner=z["host.owner"], cell_center=z["host.cell_center"],
                    face_center=z["host.face_center"], face_normal=z["host.face_normal"],
                    face_area=z["host.face_area"], lsq=z["host.lsq"], csr_faces=z["host.csr_faces"],
-                   patch_int=z["host.patch_int"], patch_dbl=z["host.patch_dbl"], patch_target=np.zeros(n_patches),
+                   patch_int=z["host.patch_int"], patch_dbl=z["host.patch_dbl"],
+                   patch_target=(np.asarray(z["host.patch_target"], float) if "host.patch_target" in z.files
+                                 else np.zeros(n_patches)),
                    cell_new_to_old=z["host.cell_new_to_old"], bface_new_to_old=z["host.bface_new_to_old"],
                    storage_to_grid=z["host.storage_to_grid"], length_scale=float(sc[0]), gamma=float(sc[1]),
                    limiter_k=float(sc[2]), wall_relaxation=float(sc[3]), convergence_u_floor=float(sc[4]),

@@ -160,6 +160,8 @@ def case_spec(bcs, Kn=None, delta_rp=None, nv=(10, 10, 10), vmax=5.0, vlo=None, 
             parts.append(f"u={u[0]!r},{u[1]!r},{u[2]!r}")
         if "alpha" in o:
             parts.append(f"alpha={o['alpha']!r}")
+        if "mdot" in o:  # mass_flow_inlet: nondimensional target mass flow, inflow positive
+            parts.append(f"mdot={o['mdot']!r}")
         lines.append("boundary = " + " ".join(parts))
     for k, v in (kinetic or {}).items():
         if isinstance(v, bool):

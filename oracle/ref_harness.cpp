@@ -83,7 +83,7 @@ BoundaryType boundary_type(const std::string& s) {
 
 struct NondimBc {
   std::string patch, type;
-  double T = 1.0, p = 1.0, alpha = 1.0;
+  double T = 1.0, p = 1.0, alpha = 1.0, mdot = 0.0;
   Vec3 u{};
 };
 
@@ -117,6 +117,7 @@ CaseConfig make_config(const char* spec) {
         if (key == "T") b.T = std::stod(val);
         else if (key == "p") b.p = std::stod(val);
         else if (key == "alpha") b.alpha = std::stod(val);
+        else if (key == "mdot") b.mdot = std::stod(val);
         else if (key == "u") {
           std::string t = val;
           for (char& ch : t) if (ch == ',') ch = ' ';
@@ -143,6 +144,11 @@ CaseConfig make_config(const char* spec) {
     } else if (b.type == "pressure_inlet") {
       s.temperature = b.T * d.ref.temperature;
       s.pressure = b.p * d.ref.pressure;
+    } else if (b.type == "mass_flow_inlet") {
+      // nondimensional target (inflow positive) -> kg/s, the inverse of kinetic_setup.cpp:372
+      s.temperature = b.T * d.ref.temperature;
+      s.pressure = b.p * d.ref.pressure;
+      s.mass_flow = b.mdot * d.ref.mass_flux * d.ref.length * d.ref.length;
     } else if (b.type == "pressure_outlet") {
       s.pressure = b.p * d.ref.pressure;
     }

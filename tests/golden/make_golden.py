@@ -64,6 +64,11 @@ CASES = {
                           [("inlet", "pressure_inlet", dict(T=1.0, p=1.1)), ("outlet", "pressure_outlet", dict(p=0.5)),
                            ("wall", "diffuse_wall", dict(T=1.0, alpha=0.8))],
                           0.2, (8, 8, 8), dict(sweep_blocks=2, precision="fp64"), (0.8, (0.05, 0, 0), 1.0), 3),
+    "mass_flow_inlet_fp64": (dict(n=(6, 2, 2), lo=(0, 0, 0), hi=(1.5, 0.5, 0.5),
+                                  patches=["inlet", "outlet", "wall", "wall", "wall", "wall"], distortion=0.1),
+                             [("inlet", "mass_flow_inlet", dict(T=1.0, p=1.0, mdot=0.05)),
+                              ("outlet", "pressure_outlet", dict(p=0.4)), ("wall", "diffuse_wall", dict(T=1.0))],
+                             0.3, (8, 8, 8), dict(sweep_blocks=2, precision="fp64"), (0.8, (0.1, 0, 0), 1.0), 4),
     "vacuum_tube_fp64": (dict(n=(6, 2, 2), lo=(0, 0, 0), hi=(1.5, 0.5, 0.5),
                               patches=["inlet", "outlet", "wall", "wall", "wall", "wall"], distortion=0.1),
                          [("inlet", "pressure_inlet", dict(T=1.0, p=1.0)), ("outlet", "vacuum", {}),
@@ -114,6 +119,11 @@ def run_case(name, mesh_kw, bcs, Kn, nv, kinetic, init, iterations) -> dict:
     out = {}
     out.update(s.to_npz_dict())
     out.update(host_arrays(case))
+    # target mass flow per patch (nondimensional, inflow positive; PatchCondition::target_mass_flow,
+    # src/kinetic/kinetic_setup.cpp:372): the mass_flow_inlet's given value, patches in order of first appearance
+    names = list(dict.fromkeys(mesh_kw["patches"]))
+    targets = {patch: o.get("mdot", 0.0) for patch, typ, o in bcs if typ == "mass_flow_inlet"}
+    out["host.patch_target"] = np.array([targets.get(n, 0.0) for n in names])
     nc, nb = s.n_cells, s.n_bfaces
     # --- operation sequence on the reference CpuBackend -------------------------------------------------------
     rng = np.random.default_rng(2026)
