@@ -351,6 +351,10 @@ struct Backend final : KinHandle {
   explicit Backend(const KinSetupDesc& d) {
     device = d.device;
     KCUDA(cudaSetDevice(device));
+    // the static scratch of kin_discrete_maxwell_noalloc becomes resident when its address is first taken (lazy
+    // module loading): take it now, before f and the velocity chunk are sized to the free memory, so that later
+    // calls of the allocation-free entry point reserve nothing
+    noalloc_scratch(device);
     nc = d.n_cells;
     nv = d.nv;
     nb = d.n_bfaces;

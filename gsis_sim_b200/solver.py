@@ -58,12 +58,14 @@ def summarize_patches(names, types, patch_faces, area, normal, F_plus, F_minus, 
              "momentum_flux_nd": [float(x) for x in F[1:4]], "energy_flux_nd": float(F[4])}
         if types[pi] == "maxwell_wall" and patch_dbl is not None:
             p["accommodation"] = float(patch_dbl[pi, 5])
+        if types[pi] == "mass_flow_inlet" and patch_target is not None:
+            # nondimensional: written with or without the SI scales (kinetic_output.cpp:233-237)
+            p["mass_flow_relative_error"] = abs(float(F[0]) + patch_target[pi]) / patch_target[pi]
         if si:
             p["mdot_kg_s"] = float(F[0]) * mass_flux * L2
             if types[pi] == "mass_flow_inlet" and patch_dbl is not None and patch_target is not None:
                 p["pressure_Pa"] = float(patch_dbl[pi, 1]) * ref_pressure
                 p["target_mass_flow_kg_s"] = float(patch_target[pi]) * mass_flux * L2
-                p["mass_flow_relative_error"] = abs(float(F[0]) + patch_target[pi]) / patch_target[pi]
             p["area_m2"] = a * L2
             p["mass_flow_kg_s"] = -float(F[0]) * mass_flux * L2
             p["heat_flow_W"] = -heat * heat_flux * L2

@@ -260,8 +260,9 @@ int kin_discrete_maxwell(KinHandle* h, const double* states, int64_t n, double t
    device: the input states, the corrected states and the Newton results of KIN_NOALLOC_MAX_STATES states), so it
    only copies, launches one kernel and waits for the handle's stream.
    - n > KIN_NOALLOC_MAX_STATES is refused with KIN_E_ARG and a message (split the batch); n == 0 does nothing.
-   - The first call on a device looks up the scratch address (cudaGetSymbolAddress) and keeps it; make that first
-     call before capturing any stream.
+   - Creating a handle looks up the scratch address on its device (cudaGetSymbolAddress, which also makes the
+     static array resident) before f and the velocity chunk are sized to the free memory, and keeps it; a call
+     therefore only copies, launches and waits, and changes no device memory use.
    - There is ONE scratch per device, shared by every handle on it: calls whose copies or kernels overlap on the
      GPU (from different host threads, or handles on different streams) race and overwrite each other's states.
      Calls made one after another from one thread do not overlap: each returns after its stream is done. */

@@ -303,3 +303,38 @@ class RefBackend(KineticBackendABI):
     def __init__(self, case: RefCase):
         super().__init__(case.L, "ref_kin_", C.c_void_p(case.h), case.setup, lambda: case.L.ref_error().decode())
         self._case = case
+
+
+def tube_spec(nv: int, precision: str = "fp64", delta: float = 10.0, p_out: float = 0.01, vmax: float = 5.0,
+              **kinetic) -> str:
+    """Config text of the tube case (gsis_sim_b200.tube.tube_case) for the reference solver: inlet p 1, T 1,
+    outlet p_out, diffuse walls T 1, omega 0.81, uniform nv^3 velocities on [-vmax, vmax]^3."""
+    kin = {"precision": precision}
+    kin.update(kinetic)
+    return case_spec([("inlet", "pressure_inlet", dict(T=1.0, p=1.0)), ("wall", "diffuse_wall", dict(T=1.0)),
+                      ("back", "diffuse_wall", dict(T=1.0)), ("outlet", "pressure_outlet", dict(p=p_out))],
+                     delta_rp=delta, nv=(nv,) * 3, vmax=vmax, omega=0.81, kinetic=kin)
+
+
+class HostArrays(dict):
+    """Host-side data of a RefCase in the key layout of the golden fixtures (HostSetup.from_npz reads it)."""
+
+    @property
+    def files(self):
+        return list(self.keys())
+
+
+def host_arrays(case: RefCase) -> HostArrays:
+    """Host-side data of the kinetic host loop (kinetic_solver.cpp) of a RefCase, internal numbering."""
+    g = case.geom
+    return HostArrays({
+        "host.cell_new_to_old": case.cell_new_to_old, "host.bface_new_to_old": case.bface_new_to_old,
+        "host.storage_to_grid": case.storage_to_grid, "host.patch_int": case.patch_int,
+        "host.patch_dbl": case.patch_dbl, "host.cell_center": g["cell_center"], "host.face_center": g["face_center"],
+        "host.face_normal": g["face_normal"], "host.face_area": g["face_area"], "host.owner": g["owner"],
+        "host.lsq": g["lsq"], "host.csr_faces": g["csr_faces"],
+        "host.scalars": np.array([case.length_scale, case.gamma, case.limiter_k, case.wall_relaxation,
+                                  case.convergence_u_floor, case.mass_flow_scale, case.mu_hat0, case.xi_max]),
+        "host.iscalars": np.array([case.n_internal_faces, int(case.closed_domain), case.inner_sweeps,
+                                   int(case.inner_wall_update), case.boundary_iterations, case.orbit_size]),
+    })

@@ -80,18 +80,7 @@ CASES = {
 
 def host_arrays(case: ref.RefCase) -> dict:
     """Host-side data of the kinetic host loop (kinetic_solver.cpp) in internal numbering."""
-    g = case.geom
-    return {
-        "host.cell_new_to_old": case.cell_new_to_old, "host.bface_new_to_old": case.bface_new_to_old,
-        "host.storage_to_grid": case.storage_to_grid, "host.patch_int": case.patch_int,
-        "host.patch_dbl": case.patch_dbl, "host.cell_center": g["cell_center"], "host.face_center": g["face_center"],
-        "host.face_normal": g["face_normal"], "host.face_area": g["face_area"], "host.owner": g["owner"],
-        "host.lsq": g["lsq"], "host.csr_faces": g["csr_faces"],
-        "host.scalars": np.array([case.length_scale, case.gamma, case.limiter_k, case.wall_relaxation,
-                                  case.convergence_u_floor, case.mass_flow_scale, case.mu_hat0, case.xi_max]),
-        "host.iscalars": np.array([case.n_internal_faces, int(case.closed_domain), case.inner_sweeps,
-                                   int(case.inner_wall_update), case.boundary_iterations, case.orbit_size]),
-    }
+    return dict(ref.host_arrays(case))
 
 
 def inflow_for(case: ref.RefCase) -> np.ndarray:

@@ -21,7 +21,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF1D = "/root/reference/verification/ref1d/src"
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.refpath import reference_path  # noqa: E402
+
+REF1D = reference_path("verification", "ref1d", "src")
 FIELDS = ["rho", "uy", "T", "qx", "qy", "Pxy"]
 
 

@@ -19,6 +19,19 @@ def test_header_and_loader_agree():
     assert sorted(_lib.EXPORTED_SYMBOLS) == declared_symbols()
 
 
+def test_header_constants_match_the_binding():
+    """Every #define KIN_* value the Python binding copies equals the header's."""
+    from gsis_sim_b200 import abi
+
+    text = open(os.path.join(ROOT, "include", "gsis_b200.h")).read()
+    defines = {k: int(v) for k, v in re.findall(r"#define\s+(KIN_[A-Z_0-9]+)\s+\(?(-?\d+)\)?", text)}
+    assert "KIN_NOALLOC_MAX_STATES" in defines
+    checked = [k for k in defines if hasattr(abi, k)]
+    assert len(checked) >= 8, checked
+    for k in checked:
+        assert getattr(abi, k) == defines[k], (k, getattr(abi, k), defines[k])
+
+
 def test_library_exports_every_declared_symbol():
     if not os.path.exists(_lib.LIB_PATH):
         pytest.fail(f"{_lib.LIB_PATH} missing: run __graft_entry__.build()")

@@ -15,10 +15,11 @@ import pytest
 from gsis_sim_b200 import case
 from gsis_sim_b200.mesh import box_mesh
 from gsis_sim_b200.pmesh import PmeshError, load_pmesh, read_pmesh, write_pmesh
+from oracle.refpath import reference_path
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CHANNEL = os.path.join(HERE, "golden", "case_channel", "channel.toml")
-REF_CASES = "/root/reference/cases"
+REF_CASES = reference_path("cases")
 
 
 def _box():

@@ -50,8 +50,12 @@ def test_noalloc_matches_discrete_maxwell():
         for n, seed in [(abi.KIN_NOALLOC_MAX_STATES, 1), (1000, 2)]:
             st = _states(n, seed)
             ref_out, ref_res = be.discrete_maxwell(st, tol)
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             rc, out, res = _noalloc(be, fn, st, tol)
             assert rc == abi.KIN_OK, be._error_fn()
+            # the point of the entry point: the call reserves no device memory
+            assert torch.cuda.mem_get_info()[0] == free_before
             np.testing.assert_array_equal(res, ref_res)
             assert (res > 0).any(), "no state was corrected: the case does not exercise the Newton solve"
             assert common.max_rel(out, ref_out) < common.TOL["fp64"]
