@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libgsis_b200.so")
-SOURCES = ["kin_kernels.cu", "kin_adjoint.cu", "kin_backend.cu"]
+SOURCES = ["kin_kernels.cu", "kin_sweep.cu", "kin_adjoint.cu", "kin_backend.cu"]
 HEADERS = ["kin_math.cuh", "kin_kernels.cuh", "kin_launch.h", "kin_adjoint.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]

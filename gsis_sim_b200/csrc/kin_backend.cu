@@ -270,6 +270,7 @@ struct Backend final : KinHandle {
   kin::View<S, M> view{};
   kin::View<S, P> pview{};  // mixed mode: the FP32 view of the gradient and the LU-SGS passes
   int32_t chunk = 0, partial_stride = 1, max_levels = 0, n_chains = 0, max_entries = 0;
+  int32_t wstride = 0;  // row length of the chunk work arrays: the chunk rounded up to whole 64-byte windows
 
   // host copies
   std::vector<int32_t> perm, inv;
@@ -284,6 +285,8 @@ struct Backend final : KinHandle {
     int32_t k0, kc;
     DevBuf<int4> items;
     int32_t n_items;
+    DevBuf<int4> ritems;  // resident block pass: (chain, window start, first valid, end valid)
+    int32_t n_ritems;
   };
   std::vector<std::unique_ptr<ChunkPlan>> chunks;
 
@@ -323,6 +326,16 @@ struct Backend final : KinHandle {
   DevBuf<Inflow<P>> pinflow;
   DevBuf<CellParams<P>> pcells;
   DevBuf<int32_t> sub_cells, sub_entries, sub_start, sub_count;
+  // resident block pass (k_sweep_resident): cell of every staged slot with its surface bit, the cells that have
+  // out-of-block neighbours with those entries (k_lout), the kernel's shared memory and the device status word
+  enum SweepMode { kSweepResident, kSweepTiles, kSweepLegacy };
+  SweepMode sweep_mode = kSweepResident;
+  int32_t resident_smem = 0, max_block_cells = 0, n_surf = 0;
+  std::vector<uint8_t> h_surface;
+  DevBuf<uint32_t> scells;
+  DevBuf<int4> surf;
+  DevBuf<kin::StageE<P>> sent;
+  DevBuf<int32_t> err_word;
   DevBuf<int32_t> d_perm, d_inv;
   DevBuf<double> moments, shift, residual_cell, bsums, partial, w_half, w_new, staging;
   DevBuf<int32_t> flags, face_cells, face_entries;
@@ -435,7 +448,11 @@ struct Backend final : KinHandle {
     f.alloc(ncs * static_cast<size_t>(nv));
     KCUDA(cudaMemsetAsync(f.p, 0, f.bytes(), stream));
 
-    const size_t work = ncs * static_cast<size_t>(chunk);
+    constexpr int32_t kWindow = kin::SweepLaunch<S, P>::kWidth;
+    wstride = (chunk + kWindow - 1) / kWindow * kWindow;
+    const size_t work = ncs * static_cast<size_t>(wstride);
+    err_word.alloc(1);
+    KCUDA(cudaMemsetAsync(err_word.p, 0, err_word.bytes(), stream));
     gx.alloc(work);
     gy.alloc(work);
     gz.alloc(work);
@@ -752,6 +769,39 @@ struct Backend final : KinHandle {
       hse[e].other = o >= 0 ? o : (d.bface_kind[d.csr_bface[e]] == kin::kPeriodic ? -2 : -1);
       for (int a = 0; a < 3; ++a) hse[e].s[a] = static_cast<P>(d.csr_geom[12 * e + a]);
     }
+    // cells with a neighbour in another block ("surface" cells) and those entries in CSR order: the later block
+    // passes couple them to the previous pass (k_lout)
+    h_surface.assign(ncs, 0);
+    {
+      std::vector<int4> hsurf;
+      std::vector<kin::StageE<P>> hsent;
+      for (int b = 0; b < n_blocks; ++b) {
+        const int cb = h_block_offsets[b], ce = h_block_offsets[b + 1];
+        max_block_cells = std::max(max_block_cells, ce - cb);
+        for (int c = cb; c < ce; ++c) {
+          const int first = static_cast<int>(hsent.size());
+          for (int e = d.csr_offsets[c]; e < d.csr_offsets[c + 1]; ++e) {
+            const int o = d.csr_other[e];
+            if (o < 0 || (o >= cb && o < ce)) continue;
+            kin::StageE<P> st{};
+            st.code = static_cast<uint32_t>(o);
+            for (int a3 = 0; a3 < 3; ++a3) st.s[a3] = hse[e].s[a3];
+            hsent.push_back(st);
+          }
+          const int cnt = static_cast<int>(hsent.size()) - first;
+          if (cnt > 0) {
+            h_surface[c] = 1;
+            hsurf.push_back(make_int4(c, first, cnt, 0));
+          }
+        }
+      }
+      n_surf = static_cast<int32_t>(hsurf.size());
+      if (n_surf > 0) {
+        surf.upload(hsurf.data(), hsurf.size(), stream);
+        sent.upload(hsent.data(), hsent.size(), stream);
+        KCUDA(cudaStreamSynchronize(stream));
+      }
+    }
     build_staged_schedule(hprog, hse, hstart, hlev_start, hlev_count, hbounds);
     prog.upload(hprog.data(), hprog.size(), stream);
     sweep_entries.upload(hse.data(), hse.size(), stream);
@@ -772,6 +822,7 @@ struct Backend final : KinHandle {
     constexpr uint32_t kKindPeriodic = 0, kKindBoundary = 1, kKindLower = 2, kKindUpper = 3, kKindOther = 4;
     constexpr uint32_t kKindShift = 28;
     staged_ne = 0;
+    sweep_mode = kSweepLegacy;
     if (nc >= (1 << kKindShift)) return;
     int max_ne = 0;
     for (const int4& p : hprog) max_ne = std::max(max_ne, p.z);
@@ -826,16 +877,34 @@ struct Backend final : KinHandle {
     KCHECK(se.size() < static_cast<size_t>(INT32_MAX), "staged LU-SGS schedule too large");
     sprog.upload(sp.data(), sp.size(), stream);
     sse.upload(se.data(), se.size(), stream);
+    {
+      std::vector<uint32_t> sc_cells(sp.size());
+      for (size_t k = 0; k < sp.size(); ++k)
+        sc_cells[k] = static_cast<uint32_t>(sp[k].x) | (h_surface[static_cast<size_t>(sp[k].x)] ? 0x80000000u : 0u);
+      scells.upload(sc_cells.data(), sc_cells.size(), stream);
+      KCUDA(cudaStreamSynchronize(stream));
+    }
     sub_cells.upload(sc.data(), sc.size(), stream);
     sub_entries.upload(sen.data(), sen.size(), stream);
     sub_start.upload(sst.data(), sst.size(), stream);
     sub_count.upload(scnt.data(), scnt.size(), stream);
     staged_ne = ne_bound;
-    // KIN_SWEEP_KERNEL=legacy selects k_sweep_pass, =staged8 the 8-entry instantiation of k_sweep_staged (both
-    // give the same results; the tests use this to cover every sweep kernel on the available meshes)
+    resident_smem = n_surf < (1 << 30) ? kin::SweepLaunch<S, P>::smem_bytes(max_block_cells) : 0;
+    sweep_mode = resident_smem > 0 ? kSweepResident : kSweepTiles;
+    // KIN_SWEEP_KERNEL selects another LU-SGS kernel: legacy (k_sweep_pass), tiles / staged8 (k_sweep_tiles with 6-
+    // or 8-entry bounds), resident8 (k_sweep_resident with the 8-entry bound). All give the same results; the tests
+    // use this to cover every sweep kernel on the available meshes.
     if (const char* e = std::getenv("KIN_SWEEP_KERNEL")) {
-      if (std::strcmp(e, "legacy") == 0) staged_ne = 0;
-      if (std::strcmp(e, "staged8") == 0) staged_ne = 8;
+      if (std::strcmp(e, "legacy") == 0) {
+        staged_ne = 0;
+        sweep_mode = kSweepLegacy;
+      }
+      if (std::strcmp(e, "tiles") == 0) sweep_mode = kSweepTiles;
+      if (std::strcmp(e, "staged8") == 0) {
+        staged_ne = 8;
+        sweep_mode = kSweepTiles;
+      }
+      if (std::strcmp(e, "resident8") == 0 && resident_smem > 0) staged_ne = 8;
     }
   }
 
@@ -858,6 +927,21 @@ struct Backend final : KinHandle {
       }
       cp->n_items = static_cast<int32_t>(items.size());
       cp->items.upload(items.data(), items.size(), stream);
+      // resident block pass: 64-byte windows aligned in the chunk's work-array rows, clipped to each direction
+      // group; a window that straddles two groups becomes two items with disjoint valid ranges
+      std::vector<int4> ritems;
+      constexpr int kW = kin::SweepLaunch<S, P>::kWidth;
+      for (const GroupRange& gr : group_ranges) {
+        const int s = std::max(gr.begin, k0) - k0, e = std::min(gr.end, k0 + cp->kc) - k0;
+        if (s >= e) continue;
+        for (int b = 0; b < n_blocks; ++b) {
+          if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
+          for (int w = s / kW * kW; w < e; w += kW)
+            ritems.push_back(make_int4(gr.g * n_blocks + b, w, std::max(s, w), std::min(e, w + kW)));
+        }
+      }
+      cp->n_ritems = static_cast<int32_t>(ritems.size());
+      if (!ritems.empty()) cp->ritems.upload(ritems.data(), ritems.size(), stream);
       chunks.push_back(std::move(cp));
     }
     KCUDA(cudaStreamSynchronize(stream));
@@ -1154,13 +1238,90 @@ struct Backend final : KinHandle {
     KCUDA(cudaStreamSynchronize(stream));
   }
 
+  // arguments of one LU-SGS block pass of a chunk (the schedule tables; R / dprev / out / update_f set by the caller)
+  kin::SweepArgs<S, P> sweep_args(const ChunkPlan& cp, int32_t stride) const {
+    kin::SweepArgs<S, P> a{};
+    a.items = cp.items.p;
+    a.n_items = cp.n_items;
+    a.n_blocks = n_blocks;
+    a.block_offsets = block_offsets.p;
+    a.prog = prog.p;
+    a.chain_start = chain_start.p;
+    a.lev_bounds = lev_bounds.p;
+    a.lev_start = lev_start.p;
+    a.lev_count = lev_count.p;
+    a.se = sweep_entries.p;
+    a.staged_ne = sweep_mode == kSweepLegacy ? 0 : staged_ne;
+    a.sprog = sprog.p;
+    a.sse = sse.p;
+    a.sub_cells = sub_cells.p;
+    a.sub_entries = sub_entries.p;
+    a.sub_start = sub_start.p;
+    a.sub_count = sub_count.p;
+    a.ritems = cp.ritems.p;
+    a.n_ritems = cp.n_ritems;
+    a.scells = scells.p;
+    a.err = err_word.p;
+    a.resident_smem = resident_smem;
+    a.max_block_cells = max_block_cells;
+    a.k0 = cp.k0;
+    a.stride = stride;
+    return a;
+  }
+
+  // block_passes x (forward + backward) on the residual in r for one chunk, correcting sv.f in the last pass.
+  // Resident kernel: pass k > 1 first folds the out-of-block coupling to pass k - 1 into R (k_lout -> gx); the
+  // kernels then read R, and Delta f goes to gz / gy alternately. Other kernels: pass k writes Delta f into gz / gy
+  // and reads pass k - 1 from the other one.
+  void run_block_passes(const kin::View<S, P>& sv, const ChunkPlan& cp, int32_t stride, bool timed) {
+    const bool resident = sweep_mode == kSweepResident && stride % kin::SweepLaunch<S, P>::kWidth == 0;
+    S* prev = nullptr;
+    for (int pass = 0; pass < block_passes; ++pass) {
+      const bool first = pass == 0, last = pass + 1 == block_passes;
+      S* out = (pass % 2 == 0) ? gz.p : gy.p;
+      kin::SweepArgs<S, P> a = sweep_args(cp, stride);
+      a.R = r.p;
+      a.dprev = prev;
+      a.out = out;
+      a.update_f = last ? 1 : 0;
+      if (resident) {
+        a.Rs = gx.p;
+        if (!first && n_surf > 0) {
+          const kin::LoutArgs<S, P> la{surf.p, n_surf, sent.p, r.p, prev, gx.p, cp.k0, cp.kc, stride};
+          if (timed) timer.begin(PhaseTimer::kBackward, stream);
+          kin::SweepLaunch<S, P>::lout(sv, la, stream);
+          launched();
+          if (timed) timer.end(stream);
+        }
+        if (timed) timer.begin(PhaseTimer::kForward, stream);
+        kin::SweepLaunch<S, P>::resident(sv, a, first, last, stream);
+      } else {
+        if (timed) timer.begin(PhaseTimer::kForward, stream);
+        LP::sweep_pass(sv, a, stream);
+      }
+      launched();
+      if (timed) timer.end(stream);
+      prev = out;
+    }
+  }
+
+  // the device status word: nonzero when a bounded wait of a kernel gave up (read after the stream is synchronised)
+  void check_status(const int32_t& h_err) {
+    if (h_err != 0) {
+      KCUDA(cudaMemsetAsync(err_word.p, 0, err_word.bytes(), stream));
+      KCUDA(cudaStreamSynchronize(stream));
+      throw KinError(KIN_E_TIMEOUT, "an LU-SGS block pass gave up waiting for its staged data (status " +
+                                        std::to_string(h_err) + "); the results of this sweep are not valid");
+    }
+  }
+
   // gradient, residual and block_passes x (forward + backward) per velocity chunk
   // (CudaBackend::sweep, kinetic_backend_cuda.cpp:317-372)
   void sweep(double* residual_out, int64_t n) override {
     KCHECK(n == nc, "length of the residual output does not match the number of cells");
     KCUDA(cudaMemsetAsync(residual_cell.p, 0, residual_cell.bytes(), stream));
     for (const auto& cp : chunks) {
-      kin::Chunk<S> ch{cp->k0, cp->kc, chunk, gx.p, gy.p, gz.p, r.p};
+      kin::Chunk<S> ch{cp->k0, cp->kc, wstride, gx.p, gy.p, gz.p, r.p};
       timer.begin(PhaseTimer::kGradient, stream);
       LP::gradient(sweep_view(), ch, stream);
       launched();
@@ -1169,45 +1330,15 @@ struct Backend final : KinHandle {
       L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);
       launched(2);
       timer.end(stream);
-      // gradients are dead after the residual: pass k writes Delta f into gz (odd k) / gy (even k) and reads
-      // the previous pass from the other one, R stays in r
-      S* prev = nullptr;
-      for (int pass = 0; pass < block_passes; ++pass) {
-        S* out = (pass % 2 == 0) ? gz.p : gy.p;
-        kin::SweepArgs<S, P> a{};
-        a.items = cp->items.p;
-        a.n_items = cp->n_items;
-        a.n_blocks = n_blocks;
-        a.block_offsets = block_offsets.p;
-        a.prog = prog.p;
-        a.chain_start = chain_start.p;
-        a.lev_bounds = lev_bounds.p;
-        a.lev_start = lev_start.p;
-        a.lev_count = lev_count.p;
-        a.se = sweep_entries.p;
-        a.staged_ne = staged_ne;
-        a.sprog = sprog.p;
-        a.sse = sse.p;
-        a.sub_cells = sub_cells.p;
-        a.sub_entries = sub_entries.p;
-        a.sub_start = sub_start.p;
-        a.sub_count = sub_count.p;
-        a.R = r.p;
-        a.dprev = prev;
-        a.out = out;
-        a.update_f = pass + 1 == block_passes ? 1 : 0;
-        a.k0 = cp->k0;
-        a.stride = chunk;
-        timer.begin(PhaseTimer::kForward, stream);
-        LP::sweep_pass(sweep_view(), a, stream);
-        launched();
-        timer.end(stream);
-        prev = out;
-      }
+      // gradients are dead after the residual
+      run_block_passes(sweep_view(), *cp, wstride, true);
     }
+    int32_t h_err = 0;
     KCUDA(cudaMemcpyAsync(residual_out, residual_cell.p, residual_cell.bytes(), cudaMemcpyDeviceToHost, stream));
+    KCUDA(cudaMemcpyAsync(&h_err, err_word.p, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     timer.flush(timings);
     KCUDA(cudaStreamSynchronize(stream));
+    check_status(h_err);
   }
 
   void gsis_correction(const double* wh, const double* wn, int64_t n, int32_t* out_flags,
@@ -1455,42 +1586,14 @@ struct Backend final : KinHandle {
         // the forward block passes on lambda (reversed storage) with R = O_f(y): lambda += -P^-T O_f(y)
         kin::View<S, P> av = sweep_view();
         av.f = adj_lam.p;
-        const auto& cp = chunks.front();
-        S* prev = nullptr;
-        for (int pass = 0; pass < block_passes; ++pass) {
-          S* out = (pass % 2 == 0) ? gz.p : gy.p;
-          kin::SweepArgs<S, P> sa{};
-          sa.items = cp->items.p;
-          sa.n_items = cp->n_items;
-          sa.n_blocks = n_blocks;
-          sa.block_offsets = block_offsets.p;
-          sa.prog = prog.p;
-          sa.chain_start = chain_start.p;
-          sa.lev_bounds = lev_bounds.p;
-          sa.lev_start = lev_start.p;
-          sa.lev_count = lev_count.p;
-          sa.se = sweep_entries.p;
-          sa.staged_ne = staged_ne;
-          sa.sprog = sprog.p;
-          sa.sse = sse.p;
-          sa.sub_cells = sub_cells.p;
-          sa.sub_entries = sub_entries.p;
-          sa.sub_start = sub_start.p;
-          sa.sub_count = sub_count.p;
-          sa.R = r.p;
-          sa.dprev = prev;
-          sa.out = out;
-          sa.update_f = pass + 1 == block_passes ? 1 : 0;
-          sa.k0 = cp->k0;
-          sa.stride = chunk;
-          LP::sweep_pass(av, sa, stream);
-          launched();
-          prev = out;
-        }
+        run_block_passes(av, *chunks.front(), chunk, false);
         KCUDA(cudaGetLastError());
       }
+      int32_t h_err = 0;
       KCUDA(cudaMemcpyAsync(res_cell, adj_res.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, stream));
+      KCUDA(cudaMemcpyAsync(&h_err, err_word.p, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
       KCUDA(cudaStreamSynchronize(stream));
+      check_status(h_err);
     } else {
       throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
     }

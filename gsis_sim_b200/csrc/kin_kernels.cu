@@ -375,6 +375,25 @@ __device__ __forceinline__ M venkat_face_sel(M d2, M dmax, M dmin, M eps2) {
   return r;
 }
 
+// Venkatakrishnan factor of one face kept as a fraction (FP64): phi = min over faces of clamp(num / den, 0, 1) is
+// tracked as pn / pd, a candidate num / den in (0, 1) replacing it when num * pd < pn * den. The one division per
+// velocity at the end divides the same num and den the reference divides for the minimising face, so phi is the
+// reference's value (candidates closer than a rounding error may select the other face: phi then differs in the
+// last bit). The cases that give exactly 0 or 1 follow venkat_face (src/physics/limiter.hpp via
+// kinetic_kernels.hpp:161-201).
+template <class M>
+__device__ __forceinline__ void venkat_frac_update(M d2, M dmax, M dmin, M eps2, M& pn, M& pd) {
+  const bool pos = d2 > M(0), neg = d2 < M(0);
+  const M d1 = pos ? dmax : dmin;
+  const M num = (d1 * d1 + eps2) + M(2) * d1 * d2;
+  const M den = d1 * d1 + M(2) * d2 * d2 + d1 * d2 + eps2;
+  const bool sided = pos || neg;
+  const bool zero = sided && (!(den > M(0)) || (num < den && !(num > M(0))));
+  const bool cand = sided && den > M(0) && num > M(0) && num < den && num * pd < pn * den;
+  pn = zero ? M(0) : (cand ? num : pn);
+  pd = zero ? M(1) : (cand ? den : pd);
+}
+
 // limited_gradient for U velocities of one cell at once (same arithmetic per velocity, entries in CSR order)
 template <class S, class M, int U, int NE>
 __device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int cell, const StagedEntry<M>* E, int ne,
@@ -419,7 +438,9 @@ __device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int c
     return;
   }
   const M eps2c = v.eps2[cell];
-  M eps2[U], phi[U], pmin[U], dmx[U], dmn[U];
+  // FP64: the limiter as a fraction (one division per velocity); FP32 keeps the per-face division
+  constexpr bool kFrac = sizeof(M) == 8;
+  M eps2[U], phi[U], pden[U], pmin[U], dmx[U], dmn[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     eps2[u] = eps2c;
@@ -428,11 +449,13 @@ __device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int c
       eps2[u] *= sc * sc;
     }
     phi[u] = M(1);
+    pden[u] = M(1);
     pmin[u] = M(0);
     dmx[u] = fmax[u] - fi[u];
     dmn[u] = fmin[u] - fi[u];
   }
   const bool limit = v.limiter_mode != kLimNone;
+  const bool posit = v.positivity != 0;
   for_entries<NE>(ne, [&](int j) {
     if (E[j].kind == kPeriodic) return;
     const CsrE<M>& c = E[j].e;
@@ -440,13 +463,19 @@ __device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int c
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const M proj = sx[u] * ds0 + sy[u] * ds1 + sz[u] * ds2;
-      if (limit) phi[u] = kmin(phi[u], venkat_face_sel(proj, dmx[u], dmn[u], eps2[u]));
-      pmin[u] = kmin(pmin[u], proj);
+      if (limit) {
+        if constexpr (kFrac) venkat_frac_update(proj, dmx[u], dmn[u], eps2[u], phi[u], pden[u]);
+        else phi[u] = kmin(phi[u], venkat_face_sel(proj, dmx[u], dmn[u], eps2[u]));
+      }
+      if (posit) pmin[u] = kmin(pmin[u], proj);
     }
   });
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     M ph = phi[u];
+    if constexpr (kFrac) {
+      if (limit) ph = phi[u] / pden[u];
+    }
     if (v.positivity != 0) {
       if (!(fi[u] > M(0))) ph = M(0);
       else if (pmin[u] < M(0)) ph = kmin(ph, fi[u] / (-pmin[u]));
@@ -467,7 +496,7 @@ struct TileOcc {
 };
 template <>
 struct TileOcc<double> {
-  static constexpr int kGradient = 4;
+  static constexpr int kGradient = 3;
   static constexpr int kResidual = 2;
   static constexpr int kGradientU = 2;
 };
@@ -863,8 +892,6 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep_pass(View<S, M> v, S
 //    between the two branches of the reference with selects: ap += (a > 0 ? a : 0) adds an exact zero where the
 //    reference adds nothing, and the coupling terms use (a > 0 ? 0 : a), so every sum equals the reference's.
 // ---------------------------------------------------------------------------------------------------------
-enum : uint32_t { kKindPeriodic = 0, kKindBoundary = 1, kKindLower = 2, kKindUpper = 3, kKindOther = 4 };
-constexpr uint32_t kKindShift = 28, kIndexMask = (1u << kKindShift) - 1;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));

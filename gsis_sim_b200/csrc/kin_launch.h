@@ -19,13 +19,15 @@ struct SweepE {
   M s[3];
 };
 
-// staged stencil entry of one chain: code = kind << 28 | neighbour cell (kinds in kin_kernels.cu: periodic,
-// boundary, in-block lower, in-block upper, other block)
+// staged stencil entry of one chain: code = kind << 28 | neighbour cell (kinds: periodic, boundary, in-block lower,
+// in-block upper, other block)
 template <class M>
 struct StageE {
   uint32_t code;
   M s[3];
 };
+enum : uint32_t { kKindPeriodic = 0, kKindBoundary = 1, kKindLower = 2, kKindUpper = 3, kKindOther = 4 };
+constexpr uint32_t kKindShift = 28, kIndexMask = (1u << kKindShift) - 1;
 
 constexpr int kTileThreadsSweep = 128;  // threads of one k_sweep_tiles CTA
 
@@ -70,6 +72,39 @@ struct SweepArgs {
   const int32_t* sub_entries;   // absolute sub-level boundaries in sse (n_sub + 1 per chain)
   const int32_t* sub_start;     // chain -> first index in sub_cells / sub_entries
   const int32_t* sub_count;     // chain -> number of sub-levels
+  // resident block pass (k_sweep_resident): one CTA per (chain, 64-byte velocity window) keeps the window of the
+  // whole block in shared memory through the forward and backward sweeps
+  const int4* ritems;           // per CTA: (chain, window start, first valid, end valid), chunk-local positions
+  int32_t n_ritems;
+  const uint32_t* scells;       // cell of every sprog slot | 1 << 31 when the cell has an out-of-block neighbour
+  const S* Rs;                  // passes after the first: R + out-of-block coupling of the surface cells (k_lout)
+  int32_t* err;                 // device status word (kSweepErrStaging: a staging wait gave up)
+  int32_t resident_smem;        // dynamic shared memory of k_sweep_resident in bytes (0: not usable)
+  int32_t max_block_cells;      // largest RCB block (rows of the resident window)
+};
+
+constexpr int32_t kSweepErrStaging = 1;
+
+// out-of-block upwind coupling of a later block pass, folded into the residual of the cells that have an
+// out-of-block neighbour (k_lout): Rs[c][t] = R[c][t] + sum over those entries of min(xi_t . S, 0) dprev[j][t]
+template <class S, class P>
+struct LoutArgs {
+  const int4* surf;            // (cell, first entry in sent, number of entries, -)
+  int32_t n_surf;
+  const StageE<P>* sent;       // code = neighbour cell, s = S_out, CSR order
+  const S* R;
+  const S* dprev;
+  S* Rs;
+  int32_t k0, kc, stride;
+};
+
+// the resident block pass and its coupling kernel (kin_sweep.cu)
+template <class S, class P>
+struct SweepLaunch {
+  static constexpr int kWidth = 64 / static_cast<int>(sizeof(S));  // velocities of a window: 64 bytes per cell row
+  static int smem_bytes(int max_block_cells);                       // dynamic shared memory, 0 if too large
+  static void resident(const View<S, P>& v, const SweepArgs<S, P>& a, bool first, bool last, cudaStream_t st);
+  static void lout(const View<S, P>& v, const LoutArgs<S, P>& a, cudaStream_t st);
 };
 
 constexpr int kStageCells = 64;     // cells of one staged sub-level

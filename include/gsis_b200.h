@@ -40,7 +40,8 @@ extern "C" {
 #define KIN_E_CUDA (-2)     /* CUDA runtime error (reference: GSIS_CUDA_CHECK) */
 #define KIN_E_MEMORY (-3)   /* f or the work arrays do not fit in device memory */
 #define KIN_E_STATE (-4)    /* call out of order (e.g. boundary sums before set_inflow) */
-#define KIN_E_TIMEOUT (-5)  /* a bounded device-side wait gave up (status read back from the device) */
+#define KIN_E_TIMEOUT (-5)  /* a bounded device-side wait gave up (the LU-SGS block pass's staging waits, read back
+                               from the device after kin_sweep / kin_adjoint_update) */
 
 /* storage / arithmetic precision of the distribution function */
 #define KIN_PREC_FP32 0  /* reference precision = "fp32": f and all per-point arithmetic in FP32 */
@@ -172,7 +173,9 @@ typedef struct KinInflowState {
   double T;
 } KinInflowState;
 
-/* StepTimings (src/kinetic/kinetic_backend.hpp:19-41), seconds */
+/* StepTimings (src/kinetic/kinetic_backend.hpp:19-41), seconds. The B200 block-pass kernels run the forward and the
+   backward sweep of a pass in one launch: sweep_forward holds those launches, sweep_backward the kernel that couples
+   a later pass to the previous one across block boundaries. */
 typedef struct KinStepTimings {
   double moments;
   double boundary;

@@ -74,15 +74,17 @@ def test_gpu_mixed_precision_matches_oracle(B200Backend, name):
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64", "tet_positivity_fp32", "dir13_fp32", "vacuum_tube_fp64"])
 def test_gpu_sweep_kernels_agree(B200Backend, name, monkeypatch):
-    """The staged LU-SGS kernel (6- and 8-entry instantiations) and the plain level kernel give the same sweep."""
+    """The resident LU-SGS block pass (default; 6- and 8-entry instantiations), the staged tile kernel (6 and 8) and
+    the plain level kernel give the same sweep."""
     z, setup = common.load(name)
     runs = {}
-    for kernel in ["auto", "legacy", "staged8"]:
+    kernels = ["auto", "resident8", "tiles", "legacy", "staged8"]
+    for kernel in kernels:
         monkeypatch.setenv("KIN_SWEEP_KERNEL", kernel)
         with B200Backend(setup) as be:
             runs[kernel] = common.run_op_sequence(be, z)
     tol = 1e-14 if common.precision_of(setup) == "fp64" else 1e-6
-    for kernel in ["legacy", "staged8"]:
+    for kernel in kernels[1:]:
         for k in ["f1", "f3", "res1"]:
             assert common.max_rel(runs["auto"][k], runs[kernel][k]) < tol, (kernel, k)
 
