@@ -350,6 +350,11 @@ struct Backend final : KinHandle {
 
   bool inflow_set = false;
   bool deq_valid = false;
+  // mixed precision: the defect of the FP32 residual against the FP64 one, [cell][nv] in FP32, taken at the first
+  // sweep after the cell parameters or f changed (defect_valid false); the inner sweeps after it run the FP32
+  // residual plus this defect, so the iteration's fixed point is the FP64 residual's zero
+  DevBuf<S> defect;
+  bool defect_valid = false;
   PhaseTimer timer;
   KinStepTimings timings{};
 
@@ -393,7 +398,7 @@ struct Backend final : KinHandle {
     // free device memory check for f (kinetic_backend_cuda.cpp:102-106)
     size_t free_b = 0, total_b = 0;
     KCUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t f_bytes = sizeof(S) * static_cast<size_t>(nc) * static_cast<size_t>(nv);
+    const size_t f_bytes = (kSplit ? 2 : 1) * sizeof(S) * static_cast<size_t>(nc) * static_cast<size_t>(nv);
     if (f_bytes + kMargin >= free_b)
       throw KinError(KIN_E_MEMORY, "distribution function of " + std::to_string(f_bytes / 1e9) +
                                        " GB does not fit in the free device memory of " +
@@ -447,6 +452,7 @@ struct Backend final : KinHandle {
     }
     f.alloc(ncs * static_cast<size_t>(nv));
     KCUDA(cudaMemsetAsync(f.p, 0, f.bytes(), stream));
+    if constexpr (kSplit) defect.alloc(ncs * static_cast<size_t>(nv));
 
     constexpr int32_t kWindow = kin::SweepLaunch<S, P>::kWidth;
     wstride = (chunk + kWindow - 1) / kWindow * kWindow;
@@ -1079,6 +1085,7 @@ struct Backend final : KinHandle {
     timer.begin(PhaseTimer::kOther, stream);
     L::set_equilibrium(view, d_states.p, shift.p, discrete_eq, stream);
     launched();
+    defect_valid = false;
     timer.end(stream);
     timer.flush(timings);
   }
@@ -1091,6 +1098,7 @@ struct Backend final : KinHandle {
       L::import_f(staging.p, f.p, d_perm.p, c0, cnt, nv, stream);
       launched();
     }
+    defect_valid = false;
     KCUDA(cudaStreamSynchronize(stream));
   }
 
@@ -1132,6 +1140,7 @@ struct Backend final : KinHandle {
     KCUDA(cudaMemcpyAsync(moments.p, m, moments.bytes(), cudaMemcpyHostToDevice, stream));
     L::shift_from_moments(moments.p, shift.p, nc, stream);
     launched();
+    defect_valid = false;
     KCUDA(cudaStreamSynchronize(stream));
   }
 
@@ -1145,6 +1154,7 @@ struct Backend final : KinHandle {
     timer.begin(PhaseTimer::kOther, stream);
     L::scale(f.p, static_cast<int64_t>(f.n), s, moments.p, nc, stream);
     launched(2);
+    defect_valid = false;
     timer.end(stream);
     timer.flush(timings);
   }
@@ -1159,6 +1169,7 @@ struct Backend final : KinHandle {
       launched();
     }
     deq_valid = discrete_eq != 0;
+    defect_valid = false;
     timer.end(stream);
     timer.flush(timings);
   }
@@ -1327,12 +1338,31 @@ struct Backend final : KinHandle {
       launched();
       timer.end(stream);
       timer.begin(PhaseTimer::kResidual, stream);
-      L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);
-      launched(2);
+      if constexpr (kSplit) {
+        // mixed precision: FP64 residual and the FP32 one's defect at the iteration's first sweep, FP32 residual +
+        // defect at the inner sweeps after it
+        kin::Chunk<S> cd = ch;
+        cd.defect = defect.p;
+        if (!defect_valid) {
+          L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);
+          launched(2);
+          cd.defect_mode = kin::kDefectStore;
+          LP::residual(sweep_view(), cd, partial.p, partial_stride, residual_cell.p, stream);
+          launched();
+        } else {
+          cd.defect_mode = kin::kDefectApply;
+          LP::residual(sweep_view(), cd, partial.p, partial_stride, residual_cell.p, stream);
+          launched(2);
+        }
+      } else {
+        L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);
+        launched(2);
+      }
       timer.end(stream);
       // gradients are dead after the residual
       run_block_passes(sweep_view(), *cp, wstride, true);
     }
+    if constexpr (kSplit) defect_valid = true;
     int32_t h_err = 0;
     KCUDA(cudaMemcpyAsync(residual_out, residual_cell.p, residual_cell.bytes(), cudaMemcpyDeviceToHost, stream));
     KCUDA(cudaMemcpyAsync(&h_err, err_word.p, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
@@ -1359,6 +1389,7 @@ struct Backend final : KinHandle {
     if (out_flags) std::copy(h.begin(), h.end(), out_flags);
     *replaced = cnt;
     deq_valid = false;
+    defect_valid = false;
   }
 
   void discrete_maxwell(const double* states, int64_t n, double tol, double* out, int32_t* result) override {

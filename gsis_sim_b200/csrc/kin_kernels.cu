@@ -718,6 +718,22 @@ __global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
     y[u] = ok[u] ? v.xi_y[q] : M(0);
     z[u] = ok[u] ? v.xi_z[q] : M(0);
   }
+  // store R (or, in the defect modes of the mixed precision's FP32 residual, store the defect / R + defect)
+  auto emit = [&](int c, int64_t row, int tt, M R, double& r2) {
+    if (ch.defect_mode == kDefectNone) {
+      ch.r[row + tt] = static_cast<S>(R);
+      r2 += static_cast<double>(R) * static_cast<double>(R);
+      return;
+    }
+    S* d = ch.defect + static_cast<int64_t>(c) * v.nv + ch.k0 + tt;
+    if (ch.defect_mode == kDefectStore) {
+      *d = static_cast<S>(ch.r[row + tt] - static_cast<S>(R));
+    } else {
+      const S Ru = static_cast<S>(static_cast<S>(R) + *d);
+      ch.r[row + tt] = Ru;
+      r2 += static_cast<double>(Ru) * static_cast<double>(Ru);
+    }
+  };
   for (int c = c0; c < c1; ++c) {
     const int64_t row = static_cast<int64_t>(c) * ch.stride;
     double r2 = 0.0;
@@ -725,9 +741,7 @@ __global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;
-        const M R = residual_value(v, ch, c, t[u]);
-        ch.r[row + t[u]] = static_cast<S>(R);
-        r2 += static_cast<double>(R) * static_cast<double>(R);
+        emit(c, row, t[u], residual_value(v, ch, c, t[u]), r2);
       }
     } else {
       M R[U], fi[U];
@@ -735,10 +749,10 @@ __global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;
-        ch.r[row + t[u]] = static_cast<S>(R[u]);
-        r2 += static_cast<double>(R[u]) * static_cast<double>(R[u]);
+        emit(c, row, t[u], R[u], r2);
       }
     }
+    if (ch.defect_mode == kDefectStore) continue;  // the FP64 residual of the same f wrote the sums
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
     if (lane == 0) partial[static_cast<int64_t>(c) * partial_stride + blockIdx.y * kWarps + warp] = r2;
@@ -1334,6 +1348,7 @@ void Launch<S, M>::residual(const View<S, M>& v, const Chunk<S>& ch, double* par
     k_residual<S, M, 6><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
   else
     k_residual<S, M, 0><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
+  if (ch.defect_mode == kDefectStore) return;  // no sums of its own: the FP64 residual's stand
   k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride, residual_tiles(ch.kc),
                                                              residual_cell, v.n_cells);
 }

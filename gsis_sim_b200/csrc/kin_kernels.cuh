@@ -105,7 +105,12 @@ struct Chunk {
   S* gy;
   S* gz;
   S* r;
+  // mixed precision, FP32 residual of the inner sweeps (kDefect*): defect [cell][nv] of the FP32 residual against
+  // the FP64 one at the iteration's first sweep
+  S* defect = nullptr;
+  int32_t defect_mode = 0;
 };
+enum : int32_t { kDefectNone = 0, kDefectStore = 1, kDefectApply = 2 };
 
 // ---------------------------------------------------------------------------------------------------------
 // boundary inflow and first-order boundary values

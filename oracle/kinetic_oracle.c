@@ -248,6 +248,10 @@ struct OrcHandle {
   /* mixed precision: an FP32-arithmetic state that shares f and the chunk work arrays with the FP64-arithmetic
      state; it runs the gradient and the LU-SGS passes, the FP64 state everything else (residual included) */
   State_f32* fast;
+  /* mixed precision: defect of the FP32 residual against the FP64 one, taken at the first sweep after the cell
+     parameters (or f) changed; the inner sweeps after it run the FP32 residual plus this defect */
+  float* defect;
+  int defect_valid;
   char err[512];
 };
 
@@ -326,6 +330,7 @@ int orc_create(const KinSetupDesc* d, OrcHandle** out) {
   else {
     h->state = create_mix(d);
     h->fast = mixed_fast_state(d, (State_mix*)h->state);
+    h->defect = (float*)calloc((size_t)d->n_cells * (size_t)d->nv, sizeof(float));
   }
   *out = h;
   return KIN_OK;
@@ -338,6 +343,7 @@ void orc_destroy(OrcHandle* h) {
   else {
     mixed_fast_destroy(h->fast);
     destroy_mix((State_mix*)h->state);
+    free(h->defect);
   }
   free(h);
 }
@@ -353,6 +359,7 @@ int orc_chunk_width(OrcHandle* h, int32_t* out) {
 
 int orc_set_equilibrium(OrcHandle* h, const double* st, int64_t n) {
   if (n != 5LL * orc_nc(h)) return orc_fail(h, "length of the initial states does not match the number of cells");
+  h->defect_valid = 0;
   DISPATCH(h, set_equilibrium, st);
   return KIN_OK;
 }
@@ -370,6 +377,7 @@ SETGET(_mix)
 
 int orc_set_distribution(OrcHandle* h, const double* f, int64_t n) {
   if (n != (int64_t)orc_nc(h) * orc_nv(h)) return orc_fail(h, "length of the distribution function does not match");
+  h->defect_valid = 0;
   DISPATCH(h, set_dist, f);
   return KIN_OK;
 }
@@ -384,10 +392,12 @@ int orc_compute_moments(OrcHandle* h, double* out, int64_t n) {
   return KIN_OK;
 }
 int orc_scale_distribution(OrcHandle* h, double s) {
+  h->defect_valid = 0;
   DISPATCH(h, scale, s);
   return KIN_OK;
 }
 int orc_update_cell_params(OrcHandle* h) {
+  h->defect_valid = 0;
   DISPATCH(h, update_cell_params);
   if (h->fast) mixed_cast_cell_params(h->fast, (State_mix*)h->state);
   return KIN_OK;
@@ -412,9 +422,16 @@ int orc_sweep(OrcHandle* h, double* res, int64_t n) {
     for (int k0 = 0; k0 < m->nv; k0 += m->chunk) {
       const int kc = m->chunk < m->nv - k0 ? m->chunk : m->nv - k0;
       sweep_gradient_f32(h->fast, k0, kc);
-      sweep_residual_mix(m, k0, kc, res);
+      if (!h->defect_valid) {
+        /* first sweep of the iteration: the FP64 residual, and the defect of the FP32 one at the same f */
+        sweep_residual_mix(m, k0, kc, res);
+        sweep_residual_defect_f32(h->fast, k0, kc, res, h->defect, 1);
+      } else {
+        sweep_residual_defect_f32(h->fast, k0, kc, res, h->defect, 2);
+      }
       sweep_passes_f32(h->fast, k0, kc);
     }
+    h->defect_valid = 1;
     return KIN_OK;
   }
   DISPATCH(h, sweep, res);
@@ -423,6 +440,7 @@ int orc_sweep(OrcHandle* h, double* res, int64_t n) {
 int orc_gsis_correction(OrcHandle* h, const double* wh, const double* wn, int64_t n, int32_t* flags,
                         int64_t* replaced) {
   if (n != 5LL * orc_nc(h)) return orc_fail(h, "length of the GSIS macroscopic states does not match");
+  h->defect_valid = 0;
   if (h->precision == KIN_PREC_FP32) *replaced = gsis_correction_f32((State_f32*)h->state, wh, wn, flags);
   else if (h->precision == KIN_PREC_FP64) *replaced = gsis_correction_f64((State_f64*)h->state, wh, wn, flags);
   else *replaced = gsis_correction_mix((State_mix*)h->state, wh, wn, flags);
@@ -477,6 +495,7 @@ int orc_passes_given(OrcHandle* h, const double* R, int64_t n) {
 }
 int orc_set_moments(OrcHandle* h, const double* m, int64_t n) {
   if (n != 15LL * orc_nc(h)) return orc_fail(h, "length of the moments does not match");
+  h->defect_valid = 0;
   DISPATCH(h, set_moments, m);
   return KIN_OK;
 }

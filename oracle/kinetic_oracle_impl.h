@@ -621,6 +621,31 @@ static void N(sweep_residual)(N(State) * s, int k0, int kc, double* residual_cel
   }
 }
 
+/* mixed precision, inner sweeps (no reference counterpart): the residual in the arithmetic of this state plus the
+   stored defect. mode 1 stores defect = r - R (r holds the higher-precision residual of the same f) and leaves r;
+   mode 2 sets r = R + defect and adds its squares to residual_cell. defect: [cell][nv], storage order. */
+__attribute__((unused)) static void N(sweep_residual_defect)(N(State) * s, int k0, int kc, double* residual_cell,
+                                                              S* defect, int mode) {
+  const int stride = s->chunk;
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < s->nc; ++c) {
+    double r2 = 0.0;
+    for (int t = 0; t < kc; ++t) {
+      const M R = N(residual)(s, k0, stride, c, t);
+      S* d = defect + (int64_t)c * s->nv + k0 + t;
+      S* rr = s->r + (int64_t)c * stride + t;
+      if (mode == 1) {
+        *d = (S)(*rr - (S)R);
+      } else {
+        const S Ru = (S)((S)R + *d);
+        *rr = Ru;
+        r2 += (double)Ru * (double)Ru;
+      }
+    }
+    if (mode != 1) residual_cell[c] += r2;
+  }
+}
+
 static void N(sweep_passes)(N(State) * s, int k0, int kc) {
   const int stride = s->chunk;
   const size_t work = (size_t)s->nc * (size_t)stride;

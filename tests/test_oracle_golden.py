@@ -28,3 +28,17 @@ def test_oracle_chunk_independence(name):
     b = common.run_op_sequence(OracleBackend(setup, velocity_chunk=96), z)
     for k in ["f1", "f3", "res1", "res2", "bsums0"]:
         assert common.max_rel(a[k], b[k]) < 1e-13, k
+
+
+@pytest.mark.parametrize("name", ["mixed_strong_fp64", "vacuum_tube_fp64"])
+def test_oracle_mixed_precision_within_fp32_of_fp64(name):
+    """Mixed precision (f in FP32; FP64 residual at the first sweep after the cell parameters change, FP32 residual
+    plus the stored defect at the sweeps after it) stays within the FP32 tolerance of the FP64 reference through the
+    golden operation sequence, whose second sweep runs on the defect."""
+    z, setup = common.load(name)
+    out = common.run_op_sequence(OracleBackend(setup, precision="mixed"), z)
+    tol = common.TOL["fp32"]
+    for k in ["f1", "f3", "moments2", "face_flux"]:
+        assert common.max_rel(out[k], z["op." + k]) < tol, k
+    for k in ["res1", "res2"]:
+        assert common.max_rel(out[k], z["op." + k]) < 100 * tol, k
