@@ -35,8 +35,8 @@ HBM_FALLBACK_GBS = 6650.0
 # 12^3 velocities (profiles/gradient_residual_sweep_tiles_tube63k_12cube_fp64.md, FP64;
 # profiles/residual_tube63k_12cube_mixed.md, mixed); the LU-SGS figure is that of the first block pass. Scaled by
 # the units of a full launch for roofline.traffic.
-DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 34.9, ("fp64", "k_residual"): 57.5, ("fp64", "k_sweep_tiles"): 36.5,
-                       ("mixed", "k_residual"): 23.7}
+DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 34.9, ("fp64", "k_residual"): 57.5, ("mixed", "k_residual"): 23.7}
+DRAM_SOURCE = "ncu DRAM bytes per cell-velocity of the 62,848-cell 12^3 capture, scaled to this launch"
 
 
 def peaks():
@@ -61,6 +61,8 @@ class ClockSampler:
         self.file = None
 
     def __enter__(self):
+        if self.dev < 0:
+            return self
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
@@ -353,6 +355,10 @@ def converge_channel(setup, host, local, tol, max_iters):
 
 
 def run_adjoint(args, local):
+    print(json.dumps(adjoint_ratio(args, local)), flush=True)
+
+
+def adjoint_ratio(args, local):
     """Adjoint / forward wall-time ratio on the channel (or, --adjoint-case tube, on the tube mesh): the forward CIS
     solve from rest to residual --fwd-tol, then
     the adjoint solve of dM_dot/d(delta, T_w) to --adj-tol (both through the public host loops, wall clock). With
@@ -433,7 +439,7 @@ def run_adjoint(args, local):
             fd_a = (3 * res.J - 4 * mdot(delta, alpha=1 - ha) + mdot(delta, alpha=1 - 2 * ha)) / (2 * ha)
             line["dM_dot_d_alpha_fd"] = fd_a
             line["fd_alpha_rel_error"] = abs(line["dM_dot_d_alpha"] - fd_a) / abs(fd_a)
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -449,6 +455,8 @@ def main():
     ap.add_argument("--cpu-nv", type=int, default=8)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision, adjoint and reference-GPU legs of the default line")
     # smaller variants of the tube case for profiler captures (the benchmark itself uses the defaults)
     ap.add_argument("--nx", type=int, default=100, help="axial cells of the tube (100: 134,528 cells)")
     ap.add_argument("--velocity-chunk", type=int, default=None, help="velocities per chunk (default: all that fit)")
@@ -485,34 +493,95 @@ def main():
             run_adjoint(args, local)
         return
 
-    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    run = time_iterations(args, args.precision, ws, rank, local)
+    nc, nv, inner = run["n_cells"], run["nv"], run["inner"]
+    jobs = 1 if args.shard else ws  # sharded: one case over all ranks; replicas: one case per rank
+    updates = float(nc) * nv * inner * args.steps
+    value = updates * jobs / run["device_s"]
+    e2e = updates * jobs / run["wall_s"]
+    hbm, peak_kind = peaks()
+    kern = kernel_rooflines(run, args.precision, args.steps, hbm)
+    dom = max(kern, key=lambda k: kern[k]["seconds_per_step"])
+    d = kern[dom]
+    line = {
+        "metric": "cell_velocity_updates_per_s", "value": value, "unit": "cell*velocity updates/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * run["wall_s"] / args.steps,
+        "higher_is_better": True, "scaling": "strong" if args.shard else "weak", "vs_baseline": None,
+        "dtype": DTYPES[args.precision], "data": "synthetic",
+        "config": dict(workload_config(args, n_cells=nc),
+                       parallelism=(f"velocity shards x{ws}" if args.shard else f"replicas x{ws}")),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": d["achieved_gbs"] / hbm, "peak_source": peak_kind, "traffic": d["traffic"],
+                     "traffic_source": d["traffic_source"],
+                     "algorithmic_bytes_per_launch": d["bytes_per_launch"], "avg_launch_ms": d["avg_launch_ms"],
+                     "kernels": kern,
+                     "step": step_fraction(run, args.precision, args.steps, hbm)},
+        "e2e": {"value": e2e, "unit": "cell*velocity updates/s", "h2d_bytes_per_step": run["h2d"],
+                "d2h_bytes_per_step": run["d2h"]},
+        "gpu_launches": run["launches"], "clocks": run["clocks"],
+        "phase_seconds_per_step": {k: v / args.steps for k, v in run["timings"].items()},
+        "mass_flow": run["mass_flow"], "setup_seconds": run["setup_s"],
+    }
+    if ws == 1 and rank == 0 and not args.no_extras:
+        # the other parts of the headline metric on the same box: mixed precision on the same tube, the adjoint /
+        # forward ratio, and the reference's own CUDA backend rebuilt for sm_100a
+        line["mixed"] = mixed_leg(args, local, hbm)
+        line["adjoint"] = adjoint_leg(args, local)
+        line["gpu_baseline"] = gpu_baseline(args, run)
+    if rank == 0 and not args.no_cpu_baseline:
+        # same velocity grid on the coarse tube (the headline CPU rate), and the benchmark mesh on an 8^3 grid
+        line["cpu_baseline"] = cpu_baseline(args)
+        line["cpu_baseline"].pop("seconds_per_iteration", None)
+        full = cpu_baseline(args, nv=args.cpu_nv, coarse=False)
+        full.pop("seconds_per_iteration", None)
+        line["cpu_baseline"]["benchmark_mesh_sample"] = full
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+DTYPES = {"fp64": "f64", "fp32": "f32", "mixed": "f32 (f, gradient, LU-SGS, inner-sweep residual) / f64 (first residual, "
+          "sums)"}
+
+
+def time_iterations(args, precision, ws=1, rank=0, local=0, steps=None, warmup=None, clocks=True):
+    """K CIS iterations of the tube case through the public host loop (host buffers, H2D/D2H inside the timed region),
+    after W untimed ones; device time from the backend's CUDA events, wall time max over ranks."""
     import torch
 
     from gsis_sim_b200.backend import B200Backend
     from gsis_sim_b200.solver import KineticSolver
 
-    torch.cuda.set_device(local)
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    prev = args.precision
+    args.precision = precision
     setup, host, t_setup = build_case(args)
+    args.precision = prev
     nc, nv = setup.n_cells, setup.nv
     inner = host.inner_sweeps
-    if args.shard:
+    if args.shard and ws > 1:
         # one velocity shard of the case per rank; moments, boundary sums and residuals all-reduced (NCCL)
         from gsis_sim_b200 import shard
 
         ranges = shard.shard_ranges(setup, ws)
         local_be = B200Backend(shard.shard_setup(setup, *ranges[rank]), device=local,
                                velocity_chunk=args.velocity_chunk)
-        be = shard.ShardedBackend(setup, [local_be], [ranges[rank]],
-                                  shard.torch_allreduce(device="cuda") if ws > 1 else None)
+        be = shard.ShardedBackend(setup, [local_be], [ranges[rank]], shard.torch_allreduce(device="cuda"))
     else:
         be = B200Backend(setup, device=local, velocity_chunk=args.velocity_chunk)
     sol = KineticSolver(setup, host, be)
     sol.initialize_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         sol.sweep()
     be.take_timings()
     launches0 = be.launch_count()
-    bytes_h2d = bytes_d2h = 0
 
     def barrier():
         if ws > 1:
@@ -520,12 +589,11 @@ def main():
 
             dist.barrier()
 
-    # timed region: K CIS iterations through the public host loop (host buffers, H2D/D2H inside)
     barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    with ClockSampler(local if clocks else -1) as clk:
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(steps):
             sol.sweep()
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t0
@@ -541,64 +609,143 @@ def main():
     per_prepare_h2d = 2 * nb * 6 * 8 + n_pres * 5 * 8
     bytes_d2h = per_prepare_d2h + inner * nc * 8 + (inner - 1) * 20 * nb * 8
     bytes_h2d = per_prepare_h2d + (inner - 1) * nb * 6 * 8
-
     t_wall, device_busy = max_over_ranks([t_wall, device_busy], ws)
-
-    updates = float(nc) * nv * inner * args.steps
-    jobs = 1 if args.shard else ws  # sharded: one case over all ranks; replicas: one case per rank
-    value = updates * jobs / device_busy
-    e2e = updates * jobs / t_wall
-    hbm, peak_kind = peaks()
-    s = 8 if args.precision == "fp64" else 4
-    # dominant kernel: gradient, residual or LU-SGS pass. Algorithmic bytes per (cell, velocity), s = stored value
-    # size: the gradient reads f and writes three components (4 s); the residual reads f and the gradient and
-    # writes R (5 s); an LU-SGS pass reads R and writes its update (2 s), the last pass also reads and writes f
-    # (4 s), so 3 s per pass on average over the two passes of an inner sweep
-    n_sweeps = inner * args.steps
-    kernels = {
-        "k_gradient": (timings["gradient"] / n_sweeps, nc * nv * 4 * s),
-        "k_residual": (timings["residual"] / n_sweeps, nc * nv * 5 * s),
-        "k_sweep_tiles": (timings["sweep_forward"] / (2 * n_sweeps), nc * nv * 3 * s),
-    }
-    dom = max(kernels, key=lambda k: kernels[k][0])
-    t_launch, bytes_launch = kernels[dom]
-    achieved = bytes_launch / t_launch / 1e9
-    per_unit = DRAM_BYTES_PER_UNIT.get((args.precision, dom))
-    traffic = per_unit * nc * nv if per_unit is not None else None
-    clocks = clk.summary()
-    line = {
-        "metric": "cell_velocity_updates_per_s", "value": value, "unit": "cell*velocity updates/s", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_wall / args.steps,
-        "higher_is_better": True, "scaling": "strong" if args.shard else "weak", "vs_baseline": None,
-        "dtype": {"fp64": "f64", "fp32": "f32", "mixed": "f32 (f, gradient, LU-SGS) / f64 (residual, sums)"}[args.precision],
-        "data": "synthetic",
-        "config": dict(workload_config(args, n_cells=nc),
-                       parallelism=(f"velocity shards x{ws}" if args.shard else f"replicas x{ws}")),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
-                     "traffic_source": ("ncu DRAM bytes per cell-velocity of the 62,848-cell 12^3 capture, scaled "
-                                        "to this launch" if traffic is not None else None),
-                     "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": 1e3 * t_launch},
-        "e2e": {"value": e2e, "unit": "cell*velocity updates/s", "h2d_bytes_per_step": bytes_h2d,
-                "d2h_bytes_per_step": bytes_d2h},
-        "gpu_launches": launches, "clocks": clocks,
-        "phase_seconds_per_step": {k: v / args.steps for k, v in timings.items()},
-        "mass_flow": sol.mass_flow()[2], "setup_seconds": t_setup,
-    }
-    if rank == 0 and not args.no_cpu_baseline:
-        # same velocity grid on the coarse tube (the headline CPU rate), and the benchmark mesh on an 8^3 grid
-        line["cpu_baseline"] = cpu_baseline(args)
-        line["cpu_baseline"].pop("seconds_per_iteration", None)
-        full = cpu_baseline(args, nv=args.cpu_nv, coarse=False)
-        full.pop("seconds_per_iteration", None)
-        line["cpu_baseline"]["benchmark_mesh_sample"] = full
+    out = {"n_cells": nc, "nv": nv, "inner": inner, "passes": int(setup["block_passes"]), "device_s": device_busy,
+           "wall_s": t_wall, "timings": timings, "launches": launches, "clocks": clk.summary() if clocks else None,
+           "h2d": bytes_h2d, "d2h": bytes_d2h, "mass_flow": sol.mass_flow()[2], "setup_s": t_setup,
+           "lout_bytes_per_unit": lout_bytes_per_unit(setup, 8 if precision == "fp64" else 4)}
     be.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
+    return out
 
-        dist.destroy_process_group()
+
+def lout_bytes_per_unit(setup, s):
+    """Algorithmic bytes of the out-of-block coupling kernel per (cell, velocity) of the mesh: for every cell with a
+    neighbour in another RCB block, read R and write R + Lout (2 s), and read Delta f of each such neighbour (s)."""
+    import numpy as np
+
+    off = np.asarray(setup["csr_offsets"], np.int64)
+    other = np.asarray(setup["csr_other"], np.int64)
+    bo = np.asarray(setup["block_offsets"], np.int64)
+    nc = len(off) - 1
+    block = np.searchsorted(bo, np.arange(nc), side="right") - 1
+    owner = np.repeat(np.arange(nc), np.diff(off))
+    out = (other >= 0) & (block[np.maximum(other, 0)] != block[owner])
+    n_entries = int(out.sum())
+    n_cells = int(len(np.unique(owner[out])))
+    return (2 * n_cells + n_entries) * s / nc
+
+
+def kernel_rooflines(run, precision, steps, hbm):
+    """Per kernel: device seconds per step, launches, algorithmic bytes per launch (per (cell, velocity) figure x the
+    cells x velocities a launch processes) over its average launch time, against the measured HBM peak."""
+    s = 8 if precision == "fp64" else 4
+    units = float(run["n_cells"]) * run["nv"]
+    inner, passes = run["inner"], run["passes"]
+    t = run["timings"]
+    n_sweeps = inner * steps
+    kern = {}
+    # gradient: read f, write the three components (4 s)
+    kern["k_gradient"] = (t["gradient"], n_sweeps, 4 * s, "read f, write g_x, g_y, g_z")
+    # residual: read f, g_x, g_y, g_z, write R (5 s); mixed: first sweep FP64 residual (5 s) + FP32 defect store
+    # (read f, g, R; write the defect: 6 s), inner sweeps FP32 residual + defect (read f, g, defect; write R: 6 s)
+    if precision == "mixed":
+        kern["k_residual"] = (t["residual"], n_sweeps, (11 * s + 6 * s * (inner - 1)) / inner,
+                              "mixed: per inner sweep on average")
+    else:
+        kern["k_residual"] = (t["residual"], n_sweeps, 5 * s, "read f, g_x, g_y, g_z, write R")
+    # resident block pass: read R and write Delta f (2 s); the last pass reads R and reads and writes f (3 s)
+    kern["k_sweep_resident"] = (t["sweep_forward"], n_sweeps * passes, (2 * s * (passes - 1) + 3 * s) / passes,
+                                "read R, write Delta f; last pass read R, read + write f")
+    if t.get("sweep_backward", 0.0) > 0.0:
+        # coupling of a later pass: read R and write R + Lout for the surface cells, read Delta f of their
+        # out-of-block neighbours (per (cell, velocity) of the whole mesh: the surface share)
+        share = run.get("lout_bytes_per_unit")
+        kern["k_lout"] = (t["sweep_backward"], n_sweeps * (passes - 1), share if share else 3 * s,
+                          "read R + out-of-block Delta f, write R + Lout (surface cells)")
+    out = {}
+    for k, (sec, launches, b_unit, what) in kern.items():
+        if launches <= 0 or sec <= 0:
+            continue
+        t_launch = sec / launches
+        b_launch = b_unit * units
+        per_unit = DRAM_BYTES_PER_UNIT.get((precision, k))
+        out[k] = {"seconds_per_step": sec / steps, "launches_per_step": launches / steps,
+                  "avg_launch_ms": 1e3 * t_launch, "bytes_per_unit": b_unit, "bytes_per_launch": b_launch,
+                  "achieved_gbs": b_launch / t_launch / 1e9, "frac": b_launch / t_launch / 1e9 / hbm,
+                  "algorithmic_bytes": what,
+                  "traffic": per_unit * units if per_unit is not None else None,
+                  "traffic_source": (DRAM_SOURCE if per_unit is not None else None)}
+    return out
+
+
+def step_fraction(run, precision, steps, hbm):
+    """The whole CIS iteration against the path's algorithmic bytes: per inner sweep and (cell, velocity)
+    3 s_F + 2 s_W, plus 3 s_W per further block pass, plus s_F for the moments per iteration."""
+    s = 8 if precision == "fp64" else 4
+    units = float(run["n_cells"]) * run["nv"]
+    per_unit = run["inner"] * (3 * s + 2 * s + 3 * s * (run["passes"] - 1)) + s
+    t_step = run["device_s"] / steps
+    achieved = per_unit * units / t_step / 1e9
+    return {"bytes_per_unit_per_iteration": per_unit, "seconds_per_iteration": t_step, "achieved": achieved,
+            "frac": achieved / hbm}
+
+
+def mixed_leg(args, local, hbm):
+    """Mixed precision on the same tube and grid: updates/s (device and wall) and seconds per CIS iteration."""
+    steps = max(3, min(args.steps, 5))
+    run = time_iterations(args, "mixed", local=local, steps=steps, warmup=max(3, min(args.warmup, 3)),
+                          clocks=False)
+    updates = float(run["n_cells"]) * run["nv"] * run["inner"] * steps
+    return {"value": updates / run["device_s"], "e2e": updates / run["wall_s"], "unit": "cell*velocity updates/s",
+            "seconds_per_iteration": run["device_s"] / steps, "wall_seconds_per_iteration": run["wall_s"] / steps,
+            "steps": steps, "phase_seconds_per_step": {k: v / steps for k, v in run["timings"].items()},
+            "kernels": kernel_rooflines(run, "mixed", steps, hbm), "step": step_fraction(run, "mixed", steps, hbm),
+            "mass_flow": run["mass_flow"]}
+
+
+def adjoint_leg(args, local, repeats=3):
+    """Adjoint / forward wall-time ratio on the channel of the adjoint check (median of repeats)."""
+    ratios, fwd, adj = [], [], []
+    for _ in range(repeats):
+        r = adjoint_ratio(args, local)
+        ratios.append(r["value"])
+        fwd.append(r["forward_seconds"])
+        adj.append(r["adjoint_seconds"])
+    return {"value": statistics.median(ratios), "unit": "x", "repeats": ratios, "forward_seconds": fwd,
+            "adjoint_seconds": adj, "workload": r["config"]["workload"], "bound": "<= 2 (north star)",
+            "gradients": {k: r[k] for k in ("dM_dot_d_delta", "dM_dot_dT_w_sum", "dM_dot_d_alpha")}}
+
+
+def gpu_baseline(args, run):
+    """The reference's own CudaBackend (src/kinetic/kinetic_backend_cuda.cpp, kinetic_cuda_kernels.cu) rebuilt
+    unchanged for sm_100a (oracle/Makefile target refcuda) under the reference KineticSolver, on the same tube, grid
+    and precision, on the same GPU after this repository's backend is released: one warm-up and one timed CIS
+    iteration, with the reference's per-phase device times."""
+    try:
+        from oracle import ref
+        from gsis_sim_b200 import tube
+
+        if not (ref.available() and ref.available(refcuda=True)):
+            return {"unavailable": "oracle/_ref/libgsisrefcuda.so not built"}
+        prec = args.precision if args.precision != "mixed" else "fp32"
+        rm = ref.RefMesh.from_arrays(tube.tube_mesh().as_dict())
+        case = ref.RefCase(rm, ref.tube_spec(args.nv, prec), refcuda=True)
+        case.init_uniform(1.0, (0.0, 0.0, 0.0), 1.0)
+        case.sweep()
+        t0 = time.perf_counter()
+        case.sweep()
+        dt = time.perf_counter() - t0
+        ph = case.last_timings()
+        nc, inner = case.setup.n_cells, case.inner_sweeps
+        del case
+        ours = {k: v / args.steps for k, v in run["timings"].items()}
+        out = {"kind": "reference CudaBackend rebuilt for sm_100a", "value": nc * args.nv ** 3 * inner / dt,
+               "unit": "cell*velocity updates/s", "seconds_per_iteration": dt, "phase_seconds": ph,
+               "speedup_per_phase": {k: (ph[k] / ours[k]) if ours.get(k) else None for k in ph},
+               "speedup_iteration": dt / (run["wall_s"] / args.steps)}
+        return out
+    except Exception as e:  # the baseline is reported, not required
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 if __name__ == "__main__":

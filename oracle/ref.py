@@ -19,6 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libgsisref.so")
 # the reference KineticSolver linked with the B200 KineticBackend shim (gsis_sim_b200/integration/b200_backend.cpp)
 DROPIN_PATH = os.path.join(HERE, "_ref", "libgsisdropin.so")
+# the reference KineticSolver on the reference's own CudaBackend, rebuilt for sm_100a (bench.py's GPU baseline)
+REFCUDA_PATH = os.path.join(HERE, "_ref", "libgsisrefcuda.so")
 _libs = {}
 
 _dp = C.POINTER(C.c_double)
@@ -26,12 +28,16 @@ _ip = C.POINTER(C.c_int32)
 _lp = C.POINTER(C.c_int64)
 
 
-def available(dropin: bool = False) -> bool:
-    return os.path.exists(DROPIN_PATH if dropin else LIB_PATH)
+def _path(dropin: bool, refcuda: bool) -> str:
+    return REFCUDA_PATH if refcuda else (DROPIN_PATH if dropin else LIB_PATH)
 
 
-def lib(dropin: bool = False):
-    path = DROPIN_PATH if dropin else LIB_PATH
+def available(dropin: bool = False, refcuda: bool = False) -> bool:
+    return os.path.exists(_path(dropin, refcuda))
+
+
+def lib(dropin: bool = False, refcuda: bool = False):
+    path = _path(dropin, refcuda)
     if path in _libs:
         return _libs[path]
     L = C.CDLL(path)
@@ -57,6 +63,7 @@ def lib(dropin: bool = False):
     L.ref_solver_prepare.argtypes = [C.c_void_p, _dp]
     L.ref_solver_sweep.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ref_solver_patch_mass_flow.argtypes = [C.c_void_p, _dp]
+    L.ref_solver_last_timings.argtypes = [C.c_void_p, _dp]
     L.ref_solver_moments.argtypes = [C.c_void_p, _dp]
     L.ref_solver_boundary_fluxes.argtypes = [C.c_void_p, _dp, _dp, _dp]
     L.ref_solver_distribution.argtypes = [C.c_void_p, _dp]
@@ -177,11 +184,11 @@ def case_spec(bcs, Kn=None, delta_rp=None, nv=(10, 10, 10), vmax=5.0, vlo=None, 
 class RefCase:
     """The reference KineticSolver (backend = "cpu") on one mesh + config, and a separate CpuBackend."""
 
-    def __init__(self, mesh: RefMesh, spec: str, dropin: bool = False):
+    def __init__(self, mesh: RefMesh, spec: str, dropin: bool = False, refcuda: bool = False):
         self.mesh = mesh
-        self.L = lib(dropin)
-        if dropin:
-            # the drop-in library has its own copy of the mesh types: rebuild the mesh there from arrays
+        self.L = lib(dropin, refcuda)
+        if dropin or refcuda:
+            # the drop-in / reference-CUDA library has its own copy of the mesh types: rebuild the mesh there
             self._mesh_arrays = mesh.export()
             m = self._mesh_arrays
             pts = np.ascontiguousarray(m["points"], dtype=np.float64)
@@ -256,6 +263,13 @@ class RefCase:
         info = np.zeros(12)
         self._chk(self.L.ref_solver_sweep(self.h, int(update_pressure), _p(info)))
         return info
+
+    def last_timings(self) -> dict:
+        """Backend times of the last CIS iteration (StepTimings, src/kinetic/kinetic_backend.hpp:18-40), seconds."""
+        out = np.zeros(7)
+        self._chk(self.L.ref_solver_last_timings(self.h, _p(out)))
+        return dict(zip(["moments", "boundary", "gradient", "residual", "sweep_forward", "sweep_backward", "other"],
+                        (float(x) for x in out)))
 
     def patch_mass_flow(self):
         out = np.zeros(self.n_patches)

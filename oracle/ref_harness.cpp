@@ -158,6 +158,7 @@ CaseConfig make_config(const char* spec) {
 }
 
 struct RefCase {
+  kinetic::StepTimings last_timings;  // backend times of the last CIS iteration
   CaseConfig cfg;
   KineticParams params;
   std::unique_ptr<KineticSolver> solver;
@@ -306,8 +307,9 @@ void* ref_case_create(void* mp, const char* spec) {
     const LoadedMesh& lm = *static_cast<LoadedMesh*>(mp);
     auto rc = std::make_unique<RefCase>();
     rc->cfg = make_config(spec);
-#ifdef REF_HARNESS_DROPIN
-    // drop-in build: the reference KineticSolver on the B200 backend (gsis_sim_b200/integration/b200_backend.cpp)
+#if defined(REF_HARNESS_DROPIN) || defined(REF_HARNESS_REFCUDA)
+    // drop-in build: the reference KineticSolver on the B200 backend (gsis_sim_b200/integration/b200_backend.cpp);
+    // reference-CUDA build: the reference KineticSolver on the reference's own CudaBackend
     rc->cfg.module_sections["kinetic"].values["backend"] = std::string("cuda");
 #else
     rc->cfg.module_sections["kinetic"].values["backend"] = std::string("cpu");
@@ -315,11 +317,6 @@ void* ref_case_create(void* mp, const char* spec) {
     rc->params = parse_kinetic_params(rc->cfg);
     rc->solver = std::make_unique<KineticSolver>(rc->cfg, lm.mesh, lm.geometry, rc->params);
     const kinetic::KineticSetup& s = rc->solver->setup();
-#ifdef REF_HARNESS_DROPIN
-    rc->backend = kinetic::make_cuda_backend(s);
-#else
-    rc->backend = kinetic::make_cpu_backend(s);
-#endif
     // flatten the setup
     rc->xi_x = s.velocity.xi_x;
     rc->xi_y = s.velocity.xi_y;
@@ -551,7 +548,25 @@ int ref_solver_prepare(void* cp, double* info) {
 
 int ref_solver_sweep(void* cp, int update_pressure, double* info) {
   GUARD_BEGIN
-  fill_info(static_cast<RefCase*>(cp)->solver->sweep(update_pressure != 0), info);
+  RefCase* rc = static_cast<RefCase*>(cp);
+  const KineticIterationInfo& i = rc->solver->sweep(update_pressure != 0);
+  rc->last_timings = i.timings;
+  fill_info(i, info);
+  GUARD_END
+}
+
+// per-phase backend times of the last CIS iteration (StepTimings, src/kinetic/kinetic_backend.hpp:18-40): moments,
+// boundary, gradient, residual, sweep_forward, sweep_backward, other [s]
+int ref_solver_last_timings(void* cp, double* out) {
+  GUARD_BEGIN
+  const auto& t = static_cast<RefCase*>(cp)->last_timings;
+  out[0] = t.moments;
+  out[1] = t.boundary;
+  out[2] = t.gradient;
+  out[3] = t.residual;
+  out[4] = t.sweep_forward;
+  out[5] = t.sweep_backward;
+  out[6] = t.other;
   GUARD_END
 }
 
@@ -640,7 +655,19 @@ int ref_solver_section_mass_flow(void* cp, int32_t axis, const double* positions
 
 // --- reference CpuBackend, operation by operation (same signatures as the kin_* entry points) --------------
 
-#define BK(cp) (*static_cast<RefCase*>(cp)->backend)
+// the separate backend of the operation-level checks, created on first use (a solver-only run allocates no second f)
+static kinetic::KineticBackend& backend_of(void* cp) {
+  RefCase* rc = static_cast<RefCase*>(cp);
+  if (!rc->backend) {
+#if defined(REF_HARNESS_DROPIN) || defined(REF_HARNESS_REFCUDA)
+    rc->backend = kinetic::make_cuda_backend(rc->solver->setup());
+#else
+    rc->backend = kinetic::make_cpu_backend(rc->solver->setup());
+#endif
+  }
+  return *rc->backend;
+}
+#define BK(cp) backend_of(cp)
 
 int ref_kin_set_equilibrium(void* cp, const double* states, int64_t n) {
   GUARD_BEGIN BK(cp).set_equilibrium(std::span<const double>(states, static_cast<std::size_t>(n))); GUARD_END
