@@ -228,6 +228,8 @@ def declare_backend_api(lib, prefix: str, handle_type=C.c_void_p):
         "boundary_sums": [h, _dp, C.c_int64],
         "sweep": [h, _dp, C.c_int64],
         "gsis_correction": [h, _dp, _dp, C.c_int64, _ip, _lp],
+        "gsis_correction_extrema": [h, _dp, _dp, C.c_int64, _dp, C.c_int64],
+        "gsis_correction_apply": [h, _dp, _dp, C.c_int64, _dp, C.c_int64, _ip, _lp],
         "internal_face_mass_flux": [h, _ip, _ip, C.c_int64, _dp],
         "deq_counts": [h, C.POINTER(KinDeqCounts)],
         "chunk_width": [h, _ip],

@@ -151,6 +151,26 @@ class KineticBackendABI:
                    abi.as_ptr(flags, C.c_int32), C.byref(replaced))
         return replaced.value, flags
 
+    def gsis_correction_extrema(self, w_half, w_new) -> np.ndarray:
+        """This handle's part of the per-cell negativity reduction of a velocity-sharded GSIS correction (reduce
+        the shards' arrays with an element-wise minimum)."""
+        wh = np.ascontiguousarray(w_half, dtype=np.float64).ravel()
+        wn = np.ascontiguousarray(w_new, dtype=np.float64).ravel()
+        ext = np.empty(self.n_cells, dtype=np.float64)
+        self._call("gsis_correction_extrema", abi.as_ptr(wh, C.c_double), abi.as_ptr(wn, C.c_double), wh.size,
+                   abi.as_ptr(ext, C.c_double), ext.size)
+        return ext
+
+    def gsis_correction_apply(self, w_half, w_new, ext):
+        wh = np.ascontiguousarray(w_half, dtype=np.float64).ravel()
+        wn = np.ascontiguousarray(w_new, dtype=np.float64).ravel()
+        e = np.ascontiguousarray(ext, dtype=np.float64)
+        flags = np.zeros(self.n_cells, dtype=np.int32)
+        replaced = C.c_int64()
+        self._call("gsis_correction_apply", abi.as_ptr(wh, C.c_double), abi.as_ptr(wn, C.c_double), wh.size,
+                   abi.as_ptr(e, C.c_double), e.size, abi.as_ptr(flags, C.c_int32), C.byref(replaced))
+        return replaced.value, flags
+
     def internal_face_mass_flux(self, cells, entries) -> np.ndarray:
         c = np.ascontiguousarray(cells, dtype=np.int32)
         e = np.ascontiguousarray(entries, dtype=np.int32)

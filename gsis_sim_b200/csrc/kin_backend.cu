@@ -195,6 +195,9 @@ struct KinHandle {
   virtual void boundary_sums(double* out, int64_t n) = 0;
   virtual void sweep(double* residual_cell, int64_t n) = 0;
   virtual void gsis_correction(const double* wh, const double* wn, int64_t n, int32_t* flags, int64_t* replaced) = 0;
+  virtual void gsis_correction_extrema(const double* wh, const double* wn, int64_t n, double* ext, int64_t n_ext) = 0;
+  virtual void gsis_correction_apply(const double* wh, const double* wn, int64_t n, const double* ext, int64_t n_ext,
+                                     int32_t* flags, int64_t* replaced) = 0;
   virtual void internal_face_mass_flux(const int32_t* cells, const int32_t* entries, int64_t n, double* out) = 0;
   virtual void take_timings(KinStepTimings* out) = 0;
   virtual void deq_counts(KinDeqCounts* out) = 0;
@@ -340,6 +343,7 @@ struct Backend final : KinHandle {
   DevBuf<double> moments, shift, residual_cell, bsums, partial, w_half, w_new, staging;
   DevBuf<int32_t> flags, face_cells, face_entries;
   DevBuf<double> face_out;
+  DevBuf<double> corr_ext;  // per-cell extrema of a velocity-sharded GSIS correction
   DevBuf<S> f, gx, gy, gz, r;
 
   // discrete adjoint: lambda in velocity-reversed storage, seeds of the transposed gradient
@@ -1371,15 +1375,28 @@ struct Backend final : KinHandle {
     check_status(h_err);
   }
 
-  void gsis_correction(const double* wh, const double* wn, int64_t n, int32_t* out_flags,
-                       int64_t* replaced) override {
+  // the GSIS correction in one pass (phase 0), or one of the two phases of a velocity-sharded correction
+  void gsis_correction_phase(const double* wh, const double* wn, int64_t n, int phase, const double* ext_in,
+                             double* ext_out, int32_t* out_flags, int64_t* replaced) {
     KCHECK(n == 5LL * nc, "length of the GSIS macroscopic states does not match the number of cells");
     KCUDA(cudaMemcpyAsync(w_half.p, wh, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
     KCUDA(cudaMemcpyAsync(w_new.p, wn, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+    if (phase != 0) {
+      if (corr_ext.n != static_cast<size_t>(nc)) corr_ext.alloc(static_cast<size_t>(nc));
+      if (phase == 2)
+        KCUDA(cudaMemcpyAsync(corr_ext.p, ext_in, sizeof(double) * nc, cudaMemcpyHostToDevice, stream));
+    }
     timer.begin(PhaseTimer::kOther, stream);
-    L::gsis_correction(view, w_half.p, w_new.p, flags.p, shift.p, negative_mode, discrete_eq, collisionless, stream);
+    L::gsis_correction(view, w_half.p, w_new.p, flags.p, shift.p, negative_mode, discrete_eq, collisionless, phase,
+                       phase != 0 ? corr_ext.p : nullptr, stream);
     launched();
     timer.end(stream);
+    if (phase == 1) {
+      KCUDA(cudaMemcpyAsync(ext_out, corr_ext.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, stream));
+      timer.flush(timings);
+      KCUDA(cudaStreamSynchronize(stream));
+      return;
+    }
     std::vector<int32_t> h(nc);
     KCUDA(cudaMemcpyAsync(h.data(), flags.p, flags.bytes(), cudaMemcpyDeviceToHost, stream));
     timer.flush(timings);
@@ -1390,6 +1407,22 @@ struct Backend final : KinHandle {
     *replaced = cnt;
     deq_valid = false;
     defect_valid = false;
+  }
+
+  void gsis_correction(const double* wh, const double* wn, int64_t n, int32_t* out_flags,
+                       int64_t* replaced) override {
+    gsis_correction_phase(wh, wn, n, 0, nullptr, nullptr, out_flags, replaced);
+  }
+
+  void gsis_correction_extrema(const double* wh, const double* wn, int64_t n, double* ext, int64_t n_ext) override {
+    KCHECK(n_ext == nc, "length of the per-cell extrema does not match the number of cells");
+    gsis_correction_phase(wh, wn, n, 1, nullptr, ext, nullptr, nullptr);
+  }
+
+  void gsis_correction_apply(const double* wh, const double* wn, int64_t n, const double* ext, int64_t n_ext,
+                             int32_t* out_flags, int64_t* replaced) override {
+    KCHECK(n_ext == nc, "length of the per-cell extrema does not match the number of cells");
+    gsis_correction_phase(wh, wn, n, 2, ext, nullptr, out_flags, replaced);
   }
 
   void discrete_maxwell(const double* states, int64_t n, double tol, double* out, int32_t* result) override {
@@ -1732,6 +1765,14 @@ int kin_sweep(KinHandle* h, double* res, int64_t n) { return guard(h, [&] { h->s
 int kin_gsis_correction(KinHandle* h, const double* wh, const double* wn, int64_t n, int32_t* flags,
                         int64_t* replaced) {
   return guard(h, [&] { h->gsis_correction(wh, wn, n, flags, replaced); });
+}
+int kin_gsis_correction_extrema(KinHandle* h, const double* wh, const double* wn, int64_t n, double* ext,
+                                int64_t n_ext) {
+  return guard(h, [&] { h->gsis_correction_extrema(wh, wn, n, ext, n_ext); });
+}
+int kin_gsis_correction_apply(KinHandle* h, const double* wh, const double* wn, int64_t n, const double* ext,
+                              int64_t n_ext, int32_t* flags, int64_t* replaced) {
+  return guard(h, [&] { h->gsis_correction_apply(wh, wn, n, ext, n_ext, flags, replaced); });
 }
 int kin_internal_face_mass_flux(KinHandle* h, const int32_t* cells, const int32_t* entries, int64_t n, double* out) {
   return guard(h, [&] { h->internal_face_mass_flux(cells, entries, n, out); });

@@ -1106,7 +1106,11 @@ template <class S, class M>
 __global__ void __launch_bounds__(kCellThreads)
     k_gsis_correction(View<S, M> v, const double* __restrict__ w_half, const double* __restrict__ w_new,
                       int* __restrict__ flags, double* __restrict__ shift, int mode, int discrete,
-                      int collisionless) {
+                      int collisionless, int phase, double* __restrict__ ext) {
+  // phase 0: the whole correction. Velocity shards split it: phase 1 writes this shard's part of the negativity
+  // rule's reduction over the velocities into ext[c] (the minimum of the limit factor, the negated maximum of the
+  // blend factor, or the minimum of the check value: the minimum over all shards is the whole grid's) and changes
+  // nothing; phase 2 applies the correction with the reduced ext[c].
   __shared__ double sh_red[kDeqSums * (kCellThreads / 32)];
   __shared__ double sh_state[12];
   __shared__ M sh_m[kCellThreads / 32 + 1];
@@ -1122,6 +1126,10 @@ __global__ void __launch_bounds__(kCellThreads)
     const int rn = block_discrete_maxwell<S, M, kCellThreads>(v, wn[0], wn[1], wn[2], wn[3], wn[4], nullptr, mn,
                                                               gamma, sh_red, sh_state);
     if (collisionless && (rh < 0 || rn < 0)) {
+      if (phase == 1) {
+        if (threadIdx.x == 0) ext[c] = 1e300;
+        return;
+      }
       if (threadIdx.x == 0) {
         flags[c] = kCorrectionSkipped;
         shift[3 * static_cast<int64_t>(c) + 0] = wh[1];
@@ -1137,11 +1145,18 @@ __global__ void __launch_bounds__(kCellThreads)
   bool replace;
   if (mode == kNegLimit) {
     M alpha = M(1);
-    for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
-      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
-      alpha = kmin(alpha, correction_alpha_limit(static_cast<M>(fc[q]), maxwellian(mn, x, y, z) - maxwellian(mh, x, y, z), thr));
+    if (phase != 2) {
+      for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+        const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+        alpha = kmin(alpha, correction_alpha_limit(static_cast<M>(fc[q]), maxwellian(mn, x, y, z) - maxwellian(mh, x, y, z), thr));
+      }
+      alpha = block_reduce_op<kCellThreads>(alpha, sh_m, [](M p, M r) { return kmin(p, r); });
     }
-    alpha = block_reduce_op<kCellThreads>(alpha, sh_m, [](M p, M r) { return kmin(p, r); });
+    if (phase == 1) {
+      if (threadIdx.x == 0) ext[c] = static_cast<double>(alpha);
+      return;
+    }
+    if (phase == 2) alpha = static_cast<M>(ext[c]);
     for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
       const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
       fc[q] = static_cast<S>(static_cast<M>(fc[q]) + alpha * (maxwellian(mn, x, y, z) - maxwellian(mh, x, y, z)));
@@ -1149,12 +1164,19 @@ __global__ void __launch_bounds__(kCellThreads)
     replace = alpha < M(1);
   } else if (mode == kNegBlend) {
     M theta = M(0);
-    for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
-      const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
-      const M e = maxwellian(mn, x, y, z);
-      theta = kmax(theta, blend_theta(static_cast<M>(fc[q]), e - maxwellian(mh, x, y, z), e, thr));
+    if (phase != 2) {
+      for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
+        const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
+        const M e = maxwellian(mn, x, y, z);
+        theta = kmax(theta, blend_theta(static_cast<M>(fc[q]), e - maxwellian(mh, x, y, z), e, thr));
+      }
+      theta = block_reduce_op<kCellThreads>(theta, sh_m, [](M p, M r) { return kmax(p, r); });
     }
-    theta = block_reduce_op<kCellThreads>(theta, sh_m, [](M p, M r) { return kmax(p, r); });
+    if (phase == 1) {
+      if (threadIdx.x == 0) ext[c] = -static_cast<double>(theta);
+      return;
+    }
+    if (phase == 2) theta = static_cast<M>(-ext[c]);
     for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
       const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
       const M e = maxwellian(mn, x, y, z);
@@ -1170,13 +1192,18 @@ __global__ void __launch_bounds__(kCellThreads)
       const M x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
       const M old = static_cast<M>(fc[q]);
       const M xnew = old + (maxwellian(mn, x, y, z) - maxwellian(mh, x, y, z));
-      fc[q] = static_cast<S>(xnew);
+      if (phase != 1) fc[q] = static_cast<S>(xnew);
       const M chk = negative_check_value(old, xnew, mode == kNegCreated);
       fmin = first ? chk : kmin(fmin, chk);
       first = false;
     }
     if (first) fmin = M(1e30);  // threads without points do not take part in the minimum
     fmin = block_reduce_op<kCellThreads>(fmin, sh_m, [](M p, M r) { return kmin(p, r); });
+    if (phase == 1) {
+      if (threadIdx.x == 0) ext[c] = static_cast<double>(fmin);
+      return;
+    }
+    if (phase == 2) fmin = static_cast<M>(ext[c]);
     replace = static_cast<double>(fmin) < threshold;
     if (replace) {
       for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
@@ -1372,10 +1399,11 @@ void Launch<S, M>::sweep_pass(const View<S, M>& v, const SweepArgs<S, M>& a, cud
 
 template <class S, class M>
 void Launch<S, M>::gsis_correction(const View<S, M>& v, const double* wh, const double* wn, int* flags, double* shift,
-                                   int mode, int discrete, int collisionless, cudaStream_t st) {
+                                   int mode, int discrete, int collisionless, int phase, double* ext,
+                                   cudaStream_t st) {
   if (v.n_cells > 0)
     k_gsis_correction<S, M><<<v.n_cells, kCellThreads, 0, st>>>(v, wh, wn, flags, shift, mode, discrete,
-                                                                 collisionless);
+                                                                 collisionless, phase, ext);
 }
 
 template <class S, class M>

@@ -132,7 +132,7 @@ struct Launch {
                        double* residual_cell, cudaStream_t st);
   static void sweep_pass(const View<S, M>& v, const SweepArgs<S, M>& a, cudaStream_t st);
   static void gsis_correction(const View<S, M>& v, const double* wh, const double* wn, int* flags, double* shift,
-                              int mode, int discrete, int collisionless, cudaStream_t st);
+                              int mode, int discrete, int collisionless, int phase, double* ext, cudaStream_t st);
   static void discrete_maxwell_states(const View<S, M>& v, const DeqGrid& deq, const double* states, double* out,
                                       int* result, int n, cudaStream_t st);
   static void import_f(const double* src, S* f, const int32_t* perm, int64_t c0, int n, int nv, cudaStream_t st);

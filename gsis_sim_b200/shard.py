@@ -10,8 +10,10 @@ face finds its mirrored velocity in its own shard. What couples the shards is re
 
 `ShardedBackend` presents the shards as one backend with the methods `KineticSolver` calls, so the host loop runs
 unchanged. Its shards are either all in this process (a list of backends) or one per rank of a process group
-(`allreduce` adds a NumPy array over the ranks, e.g. `torch_allreduce()`). Maxwell walls with a non-mirror
-reflection and the GSIS correction (its negativity rules take minima over all velocities of a cell) are not sharded.
+(`allreduce(a, op)` reduces a NumPy array over the ranks with op "sum" or "min", e.g. `torch_allreduce()`).
+The GSIS correction's negativity rules reduce over all velocities of a cell: it runs in two phases, the per-cell
+extrema of every shard reduced with a minimum in between (kin_gsis_correction_extrema / _apply). Maxwell walls with
+a non-mirror reflection are not sharded (their reflection may leave the shard).
 """
 from __future__ import annotations
 
@@ -85,14 +87,16 @@ def shard_setup(setup: abi.SetupArrays, lo: int, hi: int) -> abi.SetupArrays:
 
 
 def torch_allreduce(group=None, device="cpu"):
-    """An all-reduce (sum) of NumPy arrays over a torch.distributed process group (gloo on CPU, or NCCL with
-    device="cuda"); every rank must call it in the same order."""
+    """An all-reduce (op "sum" or "min") of NumPy arrays over a torch.distributed process group (gloo on CPU, or NCCL
+    with device="cuda"); every rank must call it in the same order."""
     import torch
     import torch.distributed as dist
 
-    def reduce(a: np.ndarray) -> np.ndarray:
+    ops = {"sum": dist.ReduceOp.SUM, "min": dist.ReduceOp.MIN}
+
+    def reduce(a: np.ndarray, op: str = "sum") -> np.ndarray:
         t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(device)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        dist.all_reduce(t, op=ops[op], group=group)
         return t.cpu().numpy().reshape(a.shape)
 
     return reduce
@@ -115,6 +119,12 @@ class ShardedBackend:
         for a in arrays[1:]:
             total += a
         return self.allreduce(total) if self.allreduce is not None else total
+
+    def _min(self, arrays):
+        low = arrays[0].copy()
+        for a in arrays[1:]:
+            np.minimum(low, a, out=low)
+        return self.allreduce(low, "min") if self.allreduce is not None else low
 
     # --- KineticBackend methods ------------------------------------------------------------------------------
     def set_equilibrium(self, states):
@@ -172,7 +182,16 @@ class ShardedBackend:
             be.set_distribution(np.ascontiguousarray(f[:, lo:hi]))
 
     def gsis_correction(self, w_half, w_new):
-        raise NotImplementedError("the GSIS correction's negativity rules are not sharded")
+        """GSIS correction of every shard: the per-cell extrema of the negativity rule reduced over all shards
+        (minimum), then applied by each shard; every shard reaches the same per-cell decision."""
+        ext = self._min([be.gsis_correction_extrema(w_half, w_new) for be in self.backends])
+        out = [be.gsis_correction_apply(w_half, w_new, ext) for be in self.backends]
+        self.shift = np.asarray(w_new, float).reshape(self.n_cells, 5)[:, 1:4].copy()
+        flags = out[0][1]
+        skipped = flags == 2
+        if skipped.any():
+            self.shift[skipped] = np.asarray(w_half, float).reshape(self.n_cells, 5)[skipped, 1:4]
+        return out[0][0], flags
 
     def launch_count(self):
         return sum(be.launch_count() for be in self.backends)

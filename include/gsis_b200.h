@@ -282,6 +282,17 @@ int kin_moment_sums(KinHandle* h, double* out, int64_t n);
 /* Velocity sharding: install the finalised moments (15 per cell, reduced over all shards) as the handle's moments
    (they feed kin_update_cell_params) and move the shift to their velocity, as kin_compute_moments does. */
 int kin_set_moments(KinHandle* h, const double* moments, int64_t n);
+/* Velocity sharding of the GSIS correction (no reference counterpart; kin_gsis_correction is the unsharded form,
+   KineticBackend::gsis_correction :86-87). The negativity rule of a cell reduces over all its velocities, so a
+   sharded correction runs in two phases. kin_gsis_correction_extrema writes, per cell (n_ext = n_cells), this
+   handle's part of that reduction: the minimum of the limit factor ("limit"), the negated maximum of the blend
+   factor ("blend"), or the minimum of the check value (the replacing rules); it changes nothing. The caller reduces
+   the shards' arrays with an element-wise MINIMUM and passes the result to kin_gsis_correction_apply, which applies
+   the correction exactly as kin_gsis_correction would on the whole grid (flags and replaced as there). */
+int kin_gsis_correction_extrema(KinHandle* h, const double* w_half, const double* w_new, int64_t n, double* ext,
+                                int64_t n_ext);
+int kin_gsis_correction_apply(KinHandle* h, const double* w_half, const double* w_new, int64_t n, const double* ext,
+                              int64_t n_ext, int32_t* replaced_flags, int64_t* replaced);
 
 /* ---- discrete adjoint of the converged fixed point (no reference counterpart; FP64 handles, one velocity chunk,
    continuous equilibrium, no Maxwell walls) ----------------------------------------------------------------------

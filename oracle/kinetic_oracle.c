@@ -446,6 +446,24 @@ int orc_gsis_correction(OrcHandle* h, const double* wh, const double* wn, int64_
   else *replaced = gsis_correction_mix((State_mix*)h->state, wh, wn, flags);
   return KIN_OK;
 }
+int orc_gsis_correction_extrema(OrcHandle* h, const double* wh, const double* wn, int64_t n, double* ext,
+                                int64_t n_ext) {
+  if (n != 5LL * orc_nc(h) || n_ext != orc_nc(h)) return orc_fail(h, "length of the GSIS correction arrays");
+  if (h->precision == KIN_PREC_FP32) gsis_correction_phase_f32((State_f32*)h->state, wh, wn, NULL, ext, 1);
+  else if (h->precision == KIN_PREC_FP64) gsis_correction_phase_f64((State_f64*)h->state, wh, wn, NULL, ext, 1);
+  else gsis_correction_phase_mix((State_mix*)h->state, wh, wn, NULL, ext, 1);
+  return KIN_OK;
+}
+int orc_gsis_correction_apply(OrcHandle* h, const double* wh, const double* wn, int64_t n, const double* ext,
+                              int64_t n_ext, int32_t* flags, int64_t* replaced) {
+  if (n != 5LL * orc_nc(h) || n_ext != orc_nc(h)) return orc_fail(h, "length of the GSIS correction arrays");
+  h->defect_valid = 0;
+  double* e = (double*)ext;
+  if (h->precision == KIN_PREC_FP32) *replaced = gsis_correction_phase_f32((State_f32*)h->state, wh, wn, flags, e, 2);
+  else if (h->precision == KIN_PREC_FP64) *replaced = gsis_correction_phase_f64((State_f64*)h->state, wh, wn, flags, e, 2);
+  else *replaced = gsis_correction_phase_mix((State_mix*)h->state, wh, wn, flags, e, 2);
+  return KIN_OK;
+}
 int orc_internal_face_mass_flux(OrcHandle* h, const int32_t* cells, const int32_t* entries, int64_t n, double* out) {
   DISPATCH(h, internal_flux, cells, entries, n, out);
   return KIN_OK;

@@ -38,6 +38,10 @@ int orc_internal_face_mass_flux(OrcHandle* h, const int32_t* cells, const int32_
 int orc_deq_counts(OrcHandle* h, KinDeqCounts* out);
 int orc_moment_sums(OrcHandle* h, double* out, int64_t n);
 int orc_set_moments(OrcHandle* h, const double* m, int64_t n);
+int orc_gsis_correction_extrema(OrcHandle* h, const double* wh, const double* wn, int64_t n, double* ext,
+                                int64_t n_ext);
+int orc_gsis_correction_apply(OrcHandle* h, const double* wh, const double* wn, int64_t n, const double* ext,
+                              int64_t n_ext, int32_t* flags, int64_t* replaced);
 /* test support: the LU-SGS block passes on a given steady residual (storage order), f += the update */
 int orc_passes_given(OrcHandle* h, const double* R, int64_t n);
 int orc_discrete_maxwell(OrcHandle* h, const double* states, int64_t n, double tolerance, double* out,

@@ -704,8 +704,13 @@ static void N(passes_given)(N(State) * s, const double* R) {
   }
 }
 
-/* CpuBackend::gsis_correction (src/kinetic/kinetic_backend_cpu.cpp:346-432) */
-static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const double* w_new, int32_t* flags) {
+/* CpuBackend::gsis_correction (src/kinetic/kinetic_backend_cpu.cpp:346-432).
+   phase 0: the whole correction. Velocity sharding (no reference counterpart) splits it in two: phase 1 writes, per
+   cell, this state's part of the negativity rule's reduction over the velocities into ext (the minimum of the limit
+   factor, the negated maximum of the blend factor, or the minimum of the check value; the minimum over all shards is
+   the whole grid's value) and changes nothing; phase 2 applies the correction with the reduced ext. */
+static int64_t N(gsis_correction_phase)(N(State) * s, const double* w_half, const double* w_new, int32_t* flags,
+                                       double* ext, int phase) {
   int64_t replaced = 0;
 #pragma omp parallel for schedule(static) reduction(+ : replaced)
   for (int c = 0; c < s->nc; ++c) {
@@ -715,6 +720,10 @@ static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const doub
     const N(Mx) mh = N(eq_params)(s, wh[0], wh[1], wh[2], wh[3], wh[4], &rh);
     const N(Mx) mn = N(eq_params)(s, wn[0], wn[1], wn[2], wn[3], wn[4], &rn);
     if (s->collisionless && (rh < 0 || rn < 0)) {
+      if (phase == 1) {
+        ext[c] = 1e300;
+        continue;
+      }
       ++replaced;
       if (flags) flags[c] = 2;
       s->shift[3 * c] = wh[1];
@@ -728,17 +737,24 @@ static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const doub
     int replace = 0;
     if (s->negmode == KIN_NEGATIVE_LIMIT) {
       M alpha = 1;
-      for (int p = 0; p < s->nv; ++p) {
-        const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
-        const M d = N(maxw)(&mn, x, y, z) - N(maxw)(&mh, x, y, z);
-        const M old = (M)fc[p];
-        M lim = 1;
-        if (d < (M)0) {
-          const M room = old - (N(mmin)(old, 0) + thr);
-          lim = N(mmin)(1, room / (-d));
+      if (phase != 2) {
+        for (int p = 0; p < s->nv; ++p) {
+          const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
+          const M d = N(maxw)(&mn, x, y, z) - N(maxw)(&mh, x, y, z);
+          const M old = (M)fc[p];
+          M lim = 1;
+          if (d < (M)0) {
+            const M room = old - (N(mmin)(old, 0) + thr);
+            lim = N(mmin)(1, room / (-d));
+          }
+          alpha = N(mmin)(alpha, lim);
         }
-        alpha = N(mmin)(alpha, lim);
       }
+      if (phase == 1) {
+        ext[c] = (double)alpha;
+        continue;
+      }
+      if (phase == 2) alpha = (M)ext[c];
       for (int p = 0; p < s->nv; ++p) {
         const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
         fc[p] = (S)((M)fc[p] + alpha * (N(maxw)(&mn, x, y, z) - N(maxw)(&mh, x, y, z)));
@@ -746,19 +762,26 @@ static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const doub
       replace = alpha < (M)1;
     } else if (s->negmode == KIN_NEGATIVE_BLEND) {
       M theta = 0;
-      for (int p = 0; p < s->nv; ++p) {
-        const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
-        const M e = N(maxw)(&mn, x, y, z);
-        const M old = (M)fc[p];
-        const M d = e - N(maxw)(&mh, x, y, z);
-        const M g = old + d, bound = N(mmin)(old, 0) + thr;
-        M th = 0;
-        if (g < bound) {
-          const M den = e - g;
-          th = den > (M)0 ? N(mmin)(1, (bound - g) / den) : (M)1;
+      if (phase != 2) {
+        for (int p = 0; p < s->nv; ++p) {
+          const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
+          const M e = N(maxw)(&mn, x, y, z);
+          const M old = (M)fc[p];
+          const M d = e - N(maxw)(&mh, x, y, z);
+          const M g = old + d, bound = N(mmin)(old, 0) + thr;
+          M th = 0;
+          if (g < bound) {
+            const M den = e - g;
+            th = den > (M)0 ? N(mmin)(1, (bound - g) / den) : (M)1;
+          }
+          theta = N(mmax)(theta, th);
         }
-        theta = N(mmax)(theta, th);
       }
+      if (phase == 1) {
+        ext[c] = -(double)theta;
+        continue;
+      }
+      if (phase == 2) theta = (M)(-ext[c]);
       for (int p = 0; p < s->nv; ++p) {
         const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
         const M e = N(maxw)(&mn, x, y, z);
@@ -772,10 +795,15 @@ static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const doub
         const M x = s->xi_x[p], y = s->xi_y[p], z = s->xi_z[p];
         const M old = (M)fc[p];
         const M xn = old + (N(maxw)(&mn, x, y, z) - N(maxw)(&mh, x, y, z));
-        fc[p] = (S)xn;
+        if (phase != 1) fc[p] = (S)xn;
         const M chk = s->negmode == KIN_NEGATIVE_CREATED ? xn - N(mmin)(old, 0) : xn;
         fmin = p == 0 ? chk : N(mmin)(fmin, chk);
       }
+      if (phase == 1) {
+        ext[c] = (double)fmin;
+        continue;
+      }
+      if (phase == 2) fmin = (M)ext[c];
       replace = (double)fmin < threshold;
       if (replace)
         for (int p = 0; p < s->nv; ++p) fc[p] = (S)N(maxw)(&mn, s->xi_x[p], s->xi_y[p], s->xi_z[p]);
@@ -786,8 +814,12 @@ static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const doub
     s->shift[3 * c + 1] = wn[2];
     s->shift[3 * c + 2] = wn[3];
   }
-  s->deq_valid = 0;
+  if (phase != 1) s->deq_valid = 0;
   return replaced;
+}
+
+static int64_t N(gsis_correction)(N(State) * s, const double* w_half, const double* w_new, int32_t* flags) {
+  return N(gsis_correction_phase)(s, w_half, w_new, flags, NULL, 0);
 }
 
 static N(State) * N(create)(const KinSetupDesc* d) {

@@ -43,3 +43,38 @@ def test_two_shards_on_one_gpu_match_unsharded(name, precision, tol):
     assert common.max_rel(got[0], ref[0]) < tol
     assert common.max_rel(got[1], ref[1]) < tol
     assert abs(got[2] - ref[2]) <= tol * abs(ref[2])
+
+
+@pytest.mark.parametrize("mode", ["all", "limit", "blend"])
+def test_two_shards_gsis_correction_on_one_gpu(mode):
+    """The two-phase GSIS correction (kin_gsis_correction_extrema / _apply) over two B200 shards makes the same
+    decisions and the same f as kin_gsis_correction on the whole grid."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("no CUDA device")
+    from gsis_sim_b200 import abi, shard
+    from gsis_sim_b200.backend import B200Backend
+
+    z, setup = common.load("mixed_strong_fp64")
+    setup = setup.copy()
+    setup.scalars["negative_check_mode"] = abi.NEGATIVE_MODES[mode]
+
+    def run(be):
+        be.set_equilibrium(z["op.states"])
+        be.compute_moments()
+        be.update_cell_params()
+        r, fl = be.gsis_correction(z["op.w_half"], z["op.w_new"])
+        return r, fl, be.compute_moments()
+
+    with B200Backend(setup) as be:
+        ref = run(be)
+    ranges = shard.shard_ranges(setup, 2)
+    bes = [B200Backend(shard.shard_setup(setup, lo, hi)) for lo, hi in ranges]
+    try:
+        got = run(shard.ShardedBackend(setup, bes, ranges))
+    finally:
+        for be in bes:
+            be.close()
+    assert got[0] == ref[0] and np.array_equal(got[1], ref[1])
+    assert common.max_rel(got[2], ref[2]) < 1e-12

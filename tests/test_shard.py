@@ -106,3 +106,85 @@ def test_sharded_over_two_gloo_ranks():
         assert p.exitcode == 0
     for _, m, res, mdot in got:
         _check((m, res, mdot), ref)
+
+
+def _correction(backend, setup, z):
+    """An equilibrium state, then the golden GSIS correction (w_half, w_new) with its negativity rule."""
+    backend.set_equilibrium(z["op.states"])
+    backend.compute_moments()
+    backend.update_cell_params()
+    replaced, flags = backend.gsis_correction(z["op.w_half"], z["op.w_new"])
+    backend.compute_moments()
+    f = backend.get_distribution()
+    return replaced, flags, f
+
+
+@pytest.mark.parametrize("mode", ["all", "created", "limit", "blend"])
+@pytest.mark.parametrize("n", [2, 3])
+def test_sharded_gsis_correction_matches_unsharded(mode, n):
+    """The two-phase GSIS correction over velocity shards (per-cell extrema reduced with a minimum) makes the same
+    per-cell decisions and the same f as the correction on the whole grid, for every negativity rule."""
+    from gsis_sim_b200 import abi
+    from oracle.kinetic_oracle import OracleBackend
+
+    z, setup = common.load("mixed_strong_fp64")
+    setup = setup.copy()
+    setup.scalars["negative_check_mode"] = abi.NEGATIVE_MODES[mode]
+    r0, fl0, f0 = _correction(OracleBackend(setup), setup, z)
+    r1, fl1, f1 = _correction(_sharded(setup, n), setup, z)
+    assert r0 == r1 and np.array_equal(fl0, fl1)
+    assert (fl0 != 0).any() and (fl0 == 0).any(), "the case must exercise both outcomes of the rule"
+    assert common.max_rel(f1, f0) < 1e-14
+
+
+def _rank_correction(rank, port, mode, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=2, timeout=datetime.timedelta(seconds=120))
+    from gsis_sim_b200 import abi, shard
+
+    z, setup = common.load("mixed_strong_fp64")
+    setup = setup.copy()
+    setup.scalars["negative_check_mode"] = abi.NEGATIVE_MODES[mode]
+    be = _sharded(setup, 2, shard.torch_allreduce(), ranks=[rank])
+    be.set_equilibrium(z["op.states"])
+    be.compute_moments()
+    be.update_cell_params()
+    replaced, flags = be.gsis_correction(z["op.w_half"], z["op.w_new"])
+    m = be.compute_moments()
+    dist.barrier()
+    out.put((rank, replaced, flags, m))
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode", ["limit", "blend"])
+def test_sharded_gsis_correction_over_two_gloo_ranks(mode):
+    """The same over two gloo ranks: the per-cell extrema are all-reduced with a minimum between the phases."""
+    import torch.multiprocessing as mp
+
+    from gsis_sim_b200 import abi
+    from oracle.kinetic_oracle import OracleBackend
+
+    z, setup = common.load("mixed_strong_fp64")
+    setup = setup.copy()
+    setup.scalars["negative_check_mode"] = abi.NEGATIVE_MODES[mode]
+    be = OracleBackend(setup)
+    r0, fl0, _ = _correction(be, setup, z)
+    m0 = be.compute_moments()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_correction, args=(r, port, mode, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for _, r, fl, m in got:
+        assert r == r0 and np.array_equal(fl, fl0)
+        assert common.max_rel(m, m0) < 1e-12
