@@ -573,7 +573,8 @@ def time_iterations(args, precision, ws=1, rank=0, local=0, steps=None, warmup=N
         ranges = shard.shard_ranges(setup, ws)
         local_be = B200Backend(shard.shard_setup(setup, *ranges[rank]), device=local,
                                velocity_chunk=args.velocity_chunk)
-        be = shard.ShardedBackend(setup, [local_be], [ranges[rank]], shard.torch_allreduce(device="cuda"))
+        be = shard.ShardedBackend(setup, [local_be], [ranges[rank]], shard.torch_allreduce(device="cuda"),
+                                  device=True, device_allreduce=shard.torch_device_allreduce())
     else:
         be = B200Backend(setup, device=local, velocity_chunk=args.velocity_chunk)
     sol = KineticSolver(setup, host, be)

@@ -15,6 +15,7 @@ KIN_ABI_VERSION = 2
 KIN_OK = 0
 KIN_E_ARG, KIN_E_CUDA, KIN_E_MEMORY, KIN_E_STATE, KIN_E_TIMEOUT = -1, -2, -3, -4, -5
 KIN_NOALLOC_MAX_STATES = 4096
+KIN_SUMS_MOMENTS, KIN_SUMS_BOUNDARY, KIN_SUMS_RESIDUAL = 0, 1, 2
 KIN_PREC_FP32, KIN_PREC_FP64, KIN_PREC_MIXED = 0, 1, 2
 PRECISIONS = {"fp32": KIN_PREC_FP32, "fp64": KIN_PREC_FP64, "mixed": KIN_PREC_MIXED}
 
@@ -229,6 +230,9 @@ def declare_backend_api(lib, prefix: str, handle_type=C.c_void_p):
         "sweep": [h, _dp, C.c_int64],
         "gsis_correction": [h, _dp, _dp, C.c_int64, _ip, _lp],
         "gsis_correction_extrema": [h, _dp, _dp, C.c_int64, _dp, C.c_int64],
+        "device_sums": [h, C.c_int32, C.POINTER(_dp), _lp],
+        "finalize_moments": [h, _dp, C.c_int64],
+        "read_sums": [h, C.c_int32, _dp, C.c_int64],
         "gsis_correction_apply": [h, _dp, _dp, C.c_int64, _dp, C.c_int64, _ip, _lp],
         "internal_face_mass_flux": [h, _ip, _ip, C.c_int64, _dp],
         "deq_counts": [h, C.POINTER(KinDeqCounts)],

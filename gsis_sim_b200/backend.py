@@ -195,6 +195,15 @@ class KineticBackendABI:
         return d.corrected, d.failed, d.max_iterations
 
 
+class _DeviceArray:
+    """__cuda_array_interface__ of n device doubles (torch.as_tensor wraps it without a copy)."""
+
+    def __init__(self, ptr: int, n: int, device: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+        self.device = device
+
+
 class B200Backend(KineticBackendABI):
     """The B200 CUDA backend (libgsis_b200.so). Creating it uploads the setup and allocates f on the device."""
 
@@ -214,6 +223,7 @@ class B200Backend(KineticBackendABI):
             raise KineticError(f"kin_create failed ({rc}): {lib.kin_last_error(None).decode()}")
         super().__init__(lib, "kin_", h, s, lambda: lib.kin_last_error(h).decode())
         self._owned = True
+        self.device = device
 
     def close(self):
         if getattr(self, "_owned", False) and self._h:
@@ -241,6 +251,39 @@ class B200Backend(KineticBackendABI):
         out = C.c_int64()
         self._call("launch_count", C.byref(out))
         return out.value
+
+    # --- velocity sharding with the reductions in device memory --------------------------------------------------
+    def device_sums(self, which: int):
+        """A torch CUDA tensor viewing the handle's device buffer of one kind of sum (abi.KIN_SUMS_*), for an
+        in-place reduction across shards (no copy)."""
+        import torch
+
+        ptr = C.POINTER(C.c_double)()
+        n = C.c_int64()
+        self._call("device_sums", C.c_int32(which), C.byref(ptr), C.byref(n))
+        return torch.as_tensor(_DeviceArray(C.cast(ptr, C.c_void_p).value or 0, n.value, self.device),
+                               device=f"cuda:{self.device}")
+
+    def moment_sums_to_device(self) -> None:
+        """The 13 moment sums per cell into the device buffer KIN_SUMS_MOMENTS (no copy to the host)."""
+        self._call("moment_sums", None, 0)
+
+    def boundary_sums_to_device(self) -> None:
+        self._call("boundary_sums", None, 0)
+
+    def sweep_to_device(self) -> None:
+        self._call("sweep", None, 0)
+
+    def finalize_moments(self) -> np.ndarray:
+        """Moments from the (reduced) device moment sums, installed on the device; returned to the host."""
+        out = np.empty(self.n_cells * 15, dtype=np.float64)
+        self._call("finalize_moments", abi.as_ptr(out, C.c_double), out.size)
+        return out.reshape(self.n_cells, 15)
+
+    def read_sums(self, which: int, n: int) -> np.ndarray:
+        out = np.empty(n, dtype=np.float64)
+        self._call("read_sums", C.c_int32(which), abi.as_ptr(out, C.c_double), out.size)
+        return out
 
     def device_f(self):
         p = C.c_void_p()

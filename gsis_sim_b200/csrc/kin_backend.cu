@@ -209,6 +209,9 @@ struct KinHandle {
                                         int32_t* result) = 0;
   virtual void moment_sums(double* out, int64_t n) = 0;
   virtual void set_moments(const double* m, int64_t n) = 0;
+  virtual void device_sums(int32_t which, double** ptr, int64_t* n) = 0;
+  virtual void finalize_moments(double* out, int64_t n) = 0;
+  virtual void read_sums(int32_t which, double* out, int64_t n) = 0;
   // discrete adjoint (FP64 handles with one velocity chunk)
   virtual void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries,
                              const int32_t* flip_velocity, const int32_t* face_axis) = 0;
@@ -1129,13 +1132,56 @@ struct Backend final : KinHandle {
   }
 
   void moment_sums(double* out, int64_t n) override {
-    KCHECK(n == 13LL * nc, "length of the moment-sum output does not match");
+    KCHECK(out == nullptr || n == 13LL * nc, "length of the moment-sum output does not match");
     timer.begin(PhaseTimer::kMoments, stream);
     L::moment_sums(view, shift.p, staging_sums(), stream);
     launched();
     timer.end(stream);
-    KCUDA(cudaMemcpyAsync(out, sums.p, sizeof(double) * 13 * nc, cudaMemcpyDeviceToHost, stream));
+    if (out != nullptr)  // NULL: the sums stay in the device buffer (KIN_SUMS_MOMENTS) for a device reduction
+      KCUDA(cudaMemcpyAsync(out, sums.p, sizeof(double) * 13 * nc, cudaMemcpyDeviceToHost, stream));
     timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  // device buffer of one kind of velocity sum, for an in-place reduction across velocity shards
+  void device_sums(int32_t which, double** ptr, int64_t* n) override {
+    switch (which) {
+      case KIN_SUMS_MOMENTS:
+        *ptr = staging_sums();
+        *n = 13LL * nc;
+        break;
+      case KIN_SUMS_BOUNDARY:
+        *ptr = bsums.p;
+        *n = 20LL * nb;
+        break;
+      case KIN_SUMS_RESIDUAL:
+        *ptr = residual_cell.p;
+        *n = nc;
+        break;
+      default:
+        throw KinError(KIN_E_ARG, "kin_device_sums: unknown buffer " + std::to_string(which));
+    }
+  }
+
+  // the moments from the (reduced) moment sums in device memory: finalised, installed, shift moved
+  void finalize_moments(double* out, int64_t n) override {
+    KCHECK(out == nullptr || n == 15LL * nc, "length of the moment output does not match");
+    timer.begin(PhaseTimer::kMoments, stream);
+    L::finalize_sums(staging_sums(), view.wts == nullptr ? view.weight : 1.0, shift.p, moments.p, nc, stream);
+    launched();
+    timer.end(stream);
+    defect_valid = false;
+    if (out != nullptr) KCUDA(cudaMemcpyAsync(out, moments.p, moments.bytes(), cudaMemcpyDeviceToHost, stream));
+    timer.flush(timings);
+    KCUDA(cudaStreamSynchronize(stream));
+  }
+
+  void read_sums(int32_t which, double* out, int64_t n) override {
+    double* p = nullptr;
+    int64_t m = 0;
+    device_sums(which, &p, &m);
+    KCHECK(n == m, "length of the sums output does not match");
+    if (m > 0) KCUDA(cudaMemcpyAsync(out, p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
     KCUDA(cudaStreamSynchronize(stream));
   }
 
@@ -1216,7 +1262,7 @@ struct Backend final : KinHandle {
   }
 
   void boundary_sums(double* out, int64_t n) override {
-    KCHECK(n == 20LL * nb, "length of the boundary-sum output does not match");
+    KCHECK(out == nullptr || n == 20LL * nb, "length of the boundary-sum output does not match");
     if (nb == 0) return;
     timer.begin(PhaseTimer::kBoundary, stream);
     if (n_maxwell > 0) {
@@ -1230,7 +1276,8 @@ struct Backend final : KinHandle {
     L::boundary_sums(view, bsums.p, stream);
     launched();
     timer.end(stream);
-    KCUDA(cudaMemcpyAsync(out, bsums.p, sizeof(double) * 20 * nb, cudaMemcpyDeviceToHost, stream));
+    if (out != nullptr)  // NULL: the sums stay in the device buffer (KIN_SUMS_BOUNDARY)
+      KCUDA(cudaMemcpyAsync(out, bsums.p, sizeof(double) * 20 * nb, cudaMemcpyDeviceToHost, stream));
     timer.flush(timings);
     KCUDA(cudaStreamSynchronize(stream));
   }
@@ -1333,7 +1380,7 @@ struct Backend final : KinHandle {
   // gradient, residual and block_passes x (forward + backward) per velocity chunk
   // (CudaBackend::sweep, kinetic_backend_cuda.cpp:317-372)
   void sweep(double* residual_out, int64_t n) override {
-    KCHECK(n == nc, "length of the residual output does not match the number of cells");
+    KCHECK(residual_out == nullptr || n == nc, "length of the residual output does not match the number of cells");
     KCUDA(cudaMemsetAsync(residual_cell.p, 0, residual_cell.bytes(), stream));
     for (const auto& cp : chunks) {
       kin::Chunk<S> ch{cp->k0, cp->kc, wstride, gx.p, gy.p, gz.p, r.p};
@@ -1368,7 +1415,8 @@ struct Backend final : KinHandle {
     }
     if constexpr (kSplit) defect_valid = true;
     int32_t h_err = 0;
-    KCUDA(cudaMemcpyAsync(residual_out, residual_cell.p, residual_cell.bytes(), cudaMemcpyDeviceToHost, stream));
+    if (residual_out != nullptr)  // NULL: the per-cell sums stay in the device buffer (KIN_SUMS_RESIDUAL)
+      KCUDA(cudaMemcpyAsync(residual_out, residual_cell.p, residual_cell.bytes(), cudaMemcpyDeviceToHost, stream));
     KCUDA(cudaMemcpyAsync(&h_err, err_word.p, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     timer.flush(timings);
     KCUDA(cudaStreamSynchronize(stream));
@@ -1818,6 +1866,13 @@ int kin_adjoint_update(KinHandle* h, const double* coef, int64_t n_coef, double*
 }
 int kin_adjoint_end(KinHandle* h) { return guard(h, [&] { h->adjoint_end(); }); }
 int kin_set_moments(KinHandle* h, const double* m, int64_t n) { return guard(h, [&] { h->set_moments(m, n); }); }
+int kin_device_sums(KinHandle* h, int32_t which, double** ptr, int64_t* n) {
+  return guard(h, [&] { h->device_sums(which, ptr, n); });
+}
+int kin_finalize_moments(KinHandle* h, double* out, int64_t n) { return guard(h, [&] { h->finalize_moments(out, n); }); }
+int kin_read_sums(KinHandle* h, int32_t which, double* out, int64_t n) {
+  return guard(h, [&] { h->read_sums(which, out, n); });
+}
 int kin_schedule_info(const KinHandle* h, int32_t* max_levels, int32_t* n_chains) {
   return guard(const_cast<KinHandle*>(h), [&] { h->schedule_info(max_levels, n_chains); });
 }

@@ -91,6 +91,22 @@ __global__ void __launch_bounds__(kCellThreads)
   }
 }
 
+// moments from moment sums already reduced over velocity shards in device memory (kin_finalize_moments): the
+// finalisation and shift update of k_moments, one thread per cell
+__global__ void k_finalize_sums(const double* __restrict__ sums, double weight, double* __restrict__ shift,
+                                double* __restrict__ out, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double* sh = shift + 3 * static_cast<int64_t>(c);
+  double* m = out + 15 * static_cast<int64_t>(c);
+  finalize_moments(sums + kMomentSums * static_cast<int64_t>(c), weight, sh[0], sh[1], sh[2], m);
+  if (m[0] > 0.0) {
+    sh[0] = m[1];
+    sh[1] = m[2];
+    sh[2] = m[3];
+  }
+}
+
 // the shift of the next moment sums after moments were installed from outside (kin_set_moments)
 __global__ void k_shift_from_moments(const double* __restrict__ m, double* __restrict__ shift, int n) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1302,6 +1318,12 @@ void Launch<S, M>::moments(const View<S, M>& v, double* shift, double* out, cuda
 template <class S, class M>
 void Launch<S, M>::moment_sums(const View<S, M>& v, double* shift, double* out, cudaStream_t st) {
   if (v.n_cells > 0) k_moments<S, M, false><<<v.n_cells, kCellThreads, 0, st>>>(v, shift, out);
+}
+
+template <class S, class M>
+void Launch<S, M>::finalize_sums(const double* sums, double weight, double* shift, double* moments, int n,
+                                 cudaStream_t st) {
+  if (n > 0) k_finalize_sums<<<ceil_div(n, 128), 128, 0, st>>>(sums, weight, shift, moments, n);
 }
 
 template <class S, class M>

@@ -117,6 +117,7 @@ struct Launch {
   static void moments(const View<S, M>& v, double* shift, double* out, cudaStream_t st);
   static void moment_sums(const View<S, M>& v, double* shift, double* out, cudaStream_t st);
   static void shift_from_moments(const double* moments, double* shift, int n, cudaStream_t st);
+  static void finalize_sums(const double* sums, double weight, double* shift, double* moments, int n, cudaStream_t st);
   static void scale(S* f, int64_t n, double s, double* moments, int n_cells, cudaStream_t st);
   static void cell_params(const View<S, M>& v, const double* moments, const double* volume, const double* vdt,
                           double mu0, double omega, double Pr, double cold_bgk_T, int discrete, int collisionless,

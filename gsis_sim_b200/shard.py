@@ -102,14 +102,33 @@ def torch_allreduce(group=None, device="cpu"):
     return reduce
 
 
-class ShardedBackend:
-    """Velocity shards presented as one kinetic backend (the methods KineticSolver uses)."""
+def torch_device_allreduce(group=None):
+    """An in-place sum all-reduce of a CUDA tensor over a torch.distributed process group (NCCL over NVLink): the
+    device data plane of ShardedBackend(device_allreduce=...)."""
+    import torch.distributed as dist
 
-    def __init__(self, setup: abi.SetupArrays, backends: list, ranges: list, allreduce=None):
+    def reduce(t):
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+
+    return reduce
+
+
+class ShardedBackend:
+    """Velocity shards presented as one kinetic backend (the methods KineticSolver uses).
+
+    device=True (B200 shards): the moment sums, boundary sums and per-cell residual sums are reduced in device
+    memory: the local shards' device buffers are added on the device, `device_allreduce` (e.g.
+    torch_device_allreduce(), NCCL) reduces them across ranks in place, and the moments are finalised on the device
+    (kin_moment_sums / kin_boundary_sums / kin_sweep with NULL outputs, kin_device_sums, kin_finalize_moments)."""
+
+    def __init__(self, setup: abi.SetupArrays, backends: list, ranges: list, allreduce=None, device=False,
+                 device_allreduce=None):
         self.setup = setup
         self.backends = list(backends)
         self.ranges = list(ranges)
         self.allreduce = allreduce
+        self.device = device
+        self.device_allreduce = device_allreduce
         self.n_cells, self.nv, self.n_bfaces = setup.n_cells, setup.nv, setup.n_bfaces
         self.weight = float(setup.scalars["weight"]) if setup.arrays.get("weights") is None else 1.0
         self.shift = np.zeros((self.n_cells, 3))
@@ -119,6 +138,22 @@ class ShardedBackend:
         for a in arrays[1:]:
             total += a
         return self.allreduce(total) if self.allreduce is not None else total
+
+    def _device_reduce(self, which):
+        """Sum the local shards' device buffers of one kind into every one of them, then across ranks (in place)."""
+        import torch
+
+        ts = [be.device_sums(which) for be in self.backends]
+        total = ts[0]
+        for t in ts[1:]:
+            total.add_(t.to(total.device))
+        if self.device_allreduce is not None:
+            self.device_allreduce(total)
+        for t in ts[1:]:
+            t.copy_(total.to(t.device))
+        for t in ts:
+            torch.cuda.synchronize(t.device)
+        return ts
 
     def _min(self, arrays):
         low = arrays[0].copy()
@@ -134,6 +169,16 @@ class ShardedBackend:
         self.shift = st[:, 1:4].copy()
 
     def compute_moments(self):
+        if self.device:
+            for be in self.backends:
+                be.moment_sums_to_device()
+            self._device_reduce(abi.KIN_SUMS_MOMENTS)
+            m = self.backends[0].finalize_moments()
+            for be in self.backends[1:]:
+                be.finalize_moments()
+            pos = m[:, 0] > 0.0
+            self.shift[pos] = m[pos, 1:4]
+            return m
         sums = self._sum([be.moment_sums() for be in self.backends])
         m = finalize_moments(sums, self.weight, self.shift)
         for be in self.backends:
@@ -158,9 +203,20 @@ class ShardedBackend:
             be.set_inflow(inflow)
 
     def boundary_sums(self):
+        if self.device:
+            for be in self.backends:
+                be.boundary_sums_to_device()
+            self._device_reduce(abi.KIN_SUMS_BOUNDARY)
+            out = self.backends[0].read_sums(abi.KIN_SUMS_BOUNDARY, 20 * self.n_bfaces)
+            return out.reshape(self.n_bfaces, abi.BOUNDARY_SUMS_PER_FACE)
         return self._sum([be.boundary_sums() for be in self.backends])
 
     def sweep(self):
+        if self.device:
+            for be in self.backends:
+                be.sweep_to_device()
+            self._device_reduce(abi.KIN_SUMS_RESIDUAL)
+            return self.backends[0].read_sums(abi.KIN_SUMS_RESIDUAL, self.n_cells)
         return self._sum([be.sweep() for be in self.backends])
 
     def internal_face_mass_flux(self, cells, entries):

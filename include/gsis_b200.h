@@ -282,6 +282,22 @@ int kin_moment_sums(KinHandle* h, double* out, int64_t n);
 /* Velocity sharding: install the finalised moments (15 per cell, reduced over all shards) as the handle's moments
    (they feed kin_update_cell_params) and move the shift to their velocity, as kin_compute_moments does. */
 int kin_set_moments(KinHandle* h, const double* moments, int64_t n);
+/* Velocity sharding with the reductions in device memory (no reference counterpart). kin_moment_sums,
+   kin_boundary_sums and kin_sweep accept out == NULL: the sums then stay in the handle's device buffer, which
+   kin_device_sums returns (pointer and length in doubles), for a multi-GPU caller to reduce IN PLACE across the
+   shards (a sum all-reduce of the same buffer on every rank, e.g. NCCL over NVLink) before the call that consumes it:
+     KIN_SUMS_MOMENTS   13 * n_cells, consumed by kin_finalize_moments (the moments finalised, installed and the
+                        shift moved on the device; out: NULL or 15 * n_cells host doubles)
+     KIN_SUMS_BOUNDARY  20 * n_bfaces, read back with kin_read_sums
+     KIN_SUMS_RESIDUAL  n_cells, read back with kin_read_sums
+   Every call returns with the handle's stream idle; the caller's reduction must be complete before the next call
+   on the handle. */
+#define KIN_SUMS_MOMENTS 0
+#define KIN_SUMS_BOUNDARY 1
+#define KIN_SUMS_RESIDUAL 2
+int kin_device_sums(KinHandle* h, int32_t which, double** ptr, int64_t* n);
+int kin_finalize_moments(KinHandle* h, double* out, int64_t n);
+int kin_read_sums(KinHandle* h, int32_t which, double* out, int64_t n);
 /* Velocity sharding of the GSIS correction (no reference counterpart; kin_gsis_correction is the unsharded form,
    KineticBackend::gsis_correction :86-87). The negativity rule of a cell reduces over all its velocities, so a
    sharded correction runs in two phases. kin_gsis_correction_extrema writes, per cell (n_ext = n_cells), this

@@ -22,7 +22,10 @@ def _run(backend, setup, name, iters=2):
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64"])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
-def test_two_shards_on_one_gpu_match_unsharded(name, precision, tol):
+@pytest.mark.parametrize("device", [False, True])
+def test_two_shards_on_one_gpu_match_unsharded(name, precision, tol, device):
+    """device=True: the sums are added in device memory (kin_device_sums) and the moments finalised on the device
+    (kin_finalize_moments), the path a multi-GPU run takes with NCCL between the ranks."""
     import torch
 
     if not torch.cuda.is_available():
@@ -36,7 +39,7 @@ def test_two_shards_on_one_gpu_match_unsharded(name, precision, tol):
     ranges = shard.shard_ranges(setup, 2)
     bes = [B200Backend(shard.shard_setup(setup, lo, hi), precision=precision) for lo, hi in ranges]
     try:
-        got = _run(shard.ShardedBackend(setup, bes, ranges), setup, name)
+        got = _run(shard.ShardedBackend(setup, bes, ranges, device=device), setup, name)
     finally:
         for be in bes:
             be.close()
