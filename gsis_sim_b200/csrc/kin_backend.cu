@@ -334,8 +334,9 @@ struct Backend final : KinHandle {
   DevBuf<int32_t> sub_cells, sub_entries, sub_start, sub_count;
   // resident block pass (k_sweep_resident): cell of every staged slot with its surface bit, the cells that have
   // out-of-block neighbours with those entries (k_lout), the kernel's shared memory and the device status word
-  enum SweepMode { kSweepResident, kSweepTiles, kSweepLegacy };
-  SweepMode sweep_mode = kSweepResident;
+  enum SweepMode { kSweepWindow, kSweepResident, kSweepTiles, kSweepLegacy };
+  SweepMode sweep_mode = kSweepWindow;
+  int32_t window_ctas = 6;  // CTAs per SM the window kernel is compiled for
   int32_t resident_smem = 0, max_block_cells = 0, n_surf = 0;
   std::vector<uint8_t> h_surface;
   DevBuf<uint32_t> scells;
@@ -903,7 +904,7 @@ struct Backend final : KinHandle {
     sub_count.upload(scnt.data(), scnt.size(), stream);
     staged_ne = ne_bound;
     resident_smem = n_surf < (1 << 30) ? kin::SweepLaunch<S, P>::smem_bytes(max_block_cells) : 0;
-    sweep_mode = resident_smem > 0 ? kSweepResident : kSweepTiles;
+    sweep_mode = kSweepWindow;
     // KIN_SWEEP_KERNEL selects another LU-SGS kernel: legacy (k_sweep_pass), tiles / staged8 (k_sweep_tiles with 6-
     // or 8-entry bounds), resident8 (k_sweep_resident with the 8-entry bound). All give the same results; the tests
     // use this to cover every sweep kernel on the available meshes.
@@ -917,7 +918,16 @@ struct Backend final : KinHandle {
         staged_ne = 8;
         sweep_mode = kSweepTiles;
       }
-      if (std::strcmp(e, "resident8") == 0 && resident_smem > 0) staged_ne = 8;
+      if (std::strcmp(e, "resident") == 0 && resident_smem > 0) sweep_mode = kSweepResident;
+      if (std::strcmp(e, "resident8") == 0 && resident_smem > 0) {
+        sweep_mode = kSweepResident;
+        staged_ne = 8;
+      }
+      if (std::strncmp(e, "window", 6) == 0) {
+        sweep_mode = kSweepWindow;
+        if (std::strcmp(e, "window8e") == 0) staged_ne = 8;
+        else if (e[6] >= '4' && e[6] <= '8') window_ctas = e[6] - '0';
+      }
     }
   }
 
@@ -1336,7 +1346,9 @@ struct Backend final : KinHandle {
   // kernels then read R, and Delta f goes to gz / gy alternately. Other kernels: pass k writes Delta f into gz / gy
   // and reads pass k - 1 from the other one.
   void run_block_passes(const kin::View<S, P>& sv, const ChunkPlan& cp, int32_t stride, bool timed) {
-    const bool resident = sweep_mode == kSweepResident && stride % kin::SweepLaunch<S, P>::kWidth == 0;
+    const bool windowed = stride % kin::SweepLaunch<S, P>::kWidth == 0;
+    const bool resident = sweep_mode == kSweepResident && windowed;
+    const bool window = sweep_mode == kSweepWindow && windowed;
     S* prev = nullptr;
     for (int pass = 0; pass < block_passes; ++pass) {
       const bool first = pass == 0, last = pass + 1 == block_passes;
@@ -1357,6 +1369,9 @@ struct Backend final : KinHandle {
         }
         if (timed) timer.begin(PhaseTimer::kForward, stream);
         kin::SweepLaunch<S, P>::resident(sv, a, first, last, stream);
+      } else if (window) {
+        if (timed) timer.begin(PhaseTimer::kForward, stream);
+        kin::SweepLaunch<S, P>::window(sv, a, first, window_ctas, stream);
       } else {
         if (timed) timer.begin(PhaseTimer::kForward, stream);
         LP::sweep_pass(sv, a, stream);

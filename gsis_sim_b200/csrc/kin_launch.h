@@ -105,6 +105,8 @@ struct SweepLaunch {
   static int smem_bytes(int max_block_cells);                       // dynamic shared memory, 0 if too large
   static void resident(const View<S, P>& v, const SweepArgs<S, P>& a, bool first, bool last, cudaStream_t st);
   static void lout(const View<S, P>& v, const LoutArgs<S, P>& a, cudaStream_t st);
+  // one block pass, one (cell, velocity) per thread per step, Delta f* through L2 (k_sweep_window)
+  static void window(const View<S, P>& v, const SweepArgs<S, P>& a, bool first, int ctas_per_sm, cudaStream_t st);
 };
 
 constexpr int kStageCells = 64;     // cells of one staged sub-level

@@ -74,11 +74,11 @@ def test_gpu_mixed_precision_matches_oracle(B200Backend, name):
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64", "tet_positivity_fp32", "dir13_fp32", "vacuum_tube_fp64"])
 def test_gpu_sweep_kernels_agree(B200Backend, name, monkeypatch):
-    """The resident LU-SGS block pass (default; 6- and 8-entry instantiations), the staged tile kernel (6 and 8) and
-    the plain level kernel give the same sweep."""
+    """Every LU-SGS block-pass kernel gives the same sweep: the window kernel (default; 4, 6 and 8 CTAs per SM, 6-
+    and 8-entry bounds), the resident kernel (6 and 8), the staged tile kernel (6 and 8) and the plain level kernel."""
     z, setup = common.load(name)
     runs = {}
-    kernels = ["auto", "resident8", "tiles", "legacy", "staged8"]
+    kernels = ["auto", "window4", "window8", "window8e", "resident", "resident8", "tiles", "legacy", "staged8"]
     for kernel in kernels:
         monkeypatch.setenv("KIN_SWEEP_KERNEL", kernel)
         with B200Backend(setup) as be:
