@@ -335,7 +335,7 @@ struct Backend final : KinHandle {
   // resident block pass (k_sweep_resident): cell of every staged slot with its surface bit, the cells that have
   // out-of-block neighbours with those entries (k_lout), the kernel's shared memory and the device status word
   enum SweepMode { kSweepWindow, kSweepResident, kSweepTiles, kSweepLegacy };
-  SweepMode sweep_mode = kSweepWindow;
+  SweepMode sweep_mode = kSweepTiles;
   int32_t window_ctas = 6;  // CTAs per SM the window kernel is compiled for
   int32_t resident_smem = 0, max_block_cells = 0, n_surf = 0;
   std::vector<uint8_t> h_surface;
@@ -363,6 +363,8 @@ struct Backend final : KinHandle {
   // residual plus this defect, so the iteration's fixed point is the FP64 residual's zero
   DevBuf<S> defect;
   bool defect_valid = false;
+  bool defect_scheme = std::getenv("KIN_MIXED_RESIDUAL") == nullptr ||
+                       std::strcmp(std::getenv("KIN_MIXED_RESIDUAL"), "fp64") != 0;
   PhaseTimer timer;
   KinStepTimings timings{};
 
@@ -422,7 +424,7 @@ struct Backend final : KinHandle {
     orbit_size = xor_all + 1;
     KCHECK((orbit_size & (orbit_size - 1)) == 0 && nv % orbit_size == 0, "mirror orbits do not tile the velocity grid");
     {
-      const double per_velocity = static_cast<double>(nc) * (4.0 * sizeof(S) + 8.0 / (256.0 * kin::kTileIters));
+      const double per_velocity = static_cast<double>(nc) * (4.0 * sizeof(S) + 8.0 / (256.0 * 2));
       int64_t k;
       if (d.velocity_chunk > 0) {
         k = (d.velocity_chunk + orbit_size - 1) / orbit_size * orbit_size;
@@ -904,7 +906,7 @@ struct Backend final : KinHandle {
     sub_count.upload(scnt.data(), scnt.size(), stream);
     staged_ne = ne_bound;
     resident_smem = n_surf < (1 << 30) ? kin::SweepLaunch<S, P>::smem_bytes(max_block_cells) : 0;
-    sweep_mode = kSweepWindow;
+    sweep_mode = kSweepTiles;
     // KIN_SWEEP_KERNEL selects another LU-SGS kernel: legacy (k_sweep_pass), tiles / staged8 (k_sweep_tiles with 6-
     // or 8-entry bounds), resident8 (k_sweep_resident with the 8-entry bound). All give the same results; the tests
     // use this to cover every sweep kernel on the available meshes.
@@ -943,7 +945,7 @@ struct Backend final : KinHandle {
         if (s >= e) continue;
         for (int b = 0; b < n_blocks; ++b) {
           if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
-          const int tile = staged_ne != 0 ? 32 * kin::SweepTile<P>::kU : kin::kSweepTile;
+          const int tile = staged_ne != 0 ? 32 * kin::kernel_shape<P>().tile_u : kin::kSweepTile;
           for (int t = s; t < e; t += tile)
             items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + tile, e) - k0, 0));
         }
@@ -1404,7 +1406,10 @@ struct Backend final : KinHandle {
       launched();
       timer.end(stream);
       timer.begin(PhaseTimer::kResidual, stream);
-      if constexpr (kSplit) {
+      if (kSplit && !defect_scheme) {
+        L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);
+        launched(2);
+      } else if constexpr (kSplit) {
         // mixed precision: FP64 residual and the FP32 one's defect at the iteration's first sweep, FP32 residual +
         // defect at the inner sweeps after it
         kin::Chunk<S> cd = ch;

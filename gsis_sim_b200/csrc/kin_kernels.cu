@@ -1,5 +1,11 @@
 // Kernels of the B200 kinetic backend. See kin_kernels.cuh for the data layout; every kernel names the
 // reference routine whose semantics it reproduces.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <type_traits>
+
 #include "kin_kernels.cuh"
 #include "kin_launch.h"
 
@@ -502,27 +508,11 @@ __device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int c
   }
 }
 
-// resident CTAs per SM the gradient / residual kernels are register-budgeted for (FP32 arithmetic needs fewer
-// registers per velocity, so three CTAs fit)
-template <class M>
-struct TileOcc {
-  static constexpr int kGradient = 4;
-  static constexpr int kResidual = 3;
-  static constexpr int kGradientU = 2;  // velocities per thread of the gradient
-};
-template <>
-struct TileOcc<double> {
-  static constexpr int kGradient = 3;
-  static constexpr int kResidual = 2;
-  static constexpr int kGradientU = 2;
-};
-
-template <class S, class M, int NE>
-__global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kGradient) k_gradient(View<S, M> v, Chunk<S> ch) {
+template <class S, class M, int NE, int U, int OCC>
+__global__ void __launch_bounds__(kTileThreads, OCC) k_gradient(View<S, M> v, Chunk<S> ch) {
   __shared__ StagedEntry<M> E[kStageMulti];
   __shared__ int off[kCellsPerCta + 1];
   const int c0 = blockIdx.x * kCellsPerCta, c1 = min(v.n_cells, c0 + kCellsPerCta);
-  constexpr int U = TileOcc<M>::kGradientU;
   const int tb = blockIdx.y * (kTileThreads * U);
   const int te = min(ch.kc, tb + kTileThreads * U);
   const bool staged = stage_cells(v, c0, c1, E, off) <= kStageMulti;
@@ -710,18 +700,17 @@ __device__ __forceinline__ void residual_tile(const View<S, M>& v, const Chunk<S
 
 // residual of one chunk; partial[c * partial_stride + tile * warps + warp] = sum of R^2 over the warp's velocities
 // (summed in a fixed order by k_residual_reduce: deterministic)
-template <class S, class M, int NE>
-__global__ void __launch_bounds__(kTileThreads, TileOcc<M>::kResidual)
+template <class S, class M, int NE, int U, int OCC>
+__global__ void __launch_bounds__(kTileThreads, OCC)
     k_residual(View<S, M> v, Chunk<S> ch, double* __restrict__ partial, int partial_stride) {
   constexpr int kWarps = kTileThreads / 32;
   __shared__ StagedEntry<M> E[kStageMulti];
   __shared__ int off[kCellsPerCta + 1];
   const int c0 = blockIdx.x * kCellsPerCta, c1 = min(v.n_cells, c0 + kCellsPerCta);
-  const int tb = blockIdx.y * (kTileThreads * kTileIters);
-  const int te = min(ch.kc, tb + kTileThreads * kTileIters);
+  const int tb = blockIdx.y * (kTileThreads * U);
+  const int te = min(ch.kc, tb + kTileThreads * U);
   const bool staged = stage_cells(v, c0, c1, E, off) <= kStageMulti;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int U = kTileIters;
   int t[U];
   bool ok[U];
   M x[U], y[U], z[U];
@@ -964,12 +953,12 @@ template <class M>
 __device__ __forceinline__ M neg_part(M af) { return af > M(0) ? M(0) : af; }
 
 // forward value of SweepTile<M>::kU velocities of one cell; First: first block pass (no previous Delta f)
-template <class S, class M, int NE, bool First>
+template <class S, class M, int NE, bool First, int KU>
 __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
-                                                  const StageE<M>* E, int4 p, const int (&t)[SweepTile<M>::kU],
-                                                  const bool (&ok)[SweepTile<M>::kU], const M (&x)[SweepTile<M>::kU],
-                                                  const M (&y)[SweepTile<M>::kU], const M (&z)[SweepTile<M>::kU]) {
-  M val[NE][SweepTile<M>::kU];
+                                                  const StageE<M>* E, int4 p, const int (&t)[KU],
+                                                  const bool (&ok)[KU], const M (&x)[KU],
+                                                  const M (&y)[KU], const M (&z)[KU]) {
+  M val[NE][KU];
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     const uint32_t code = j < p.z ? E[p.y + j].code : 0u;
@@ -978,16 +967,16 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
     const bool load = kind == kKindLower || (!First && kind == kKindOther);
     const S* src = kind == kKindLower ? a.out : a.dprev;
 #pragma unroll
-    for (int u = 0; u < SweepTile<M>::kU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(src[row + t[u]]) : M(0);
+    for (int u = 0; u < KU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(src[row + t[u]]) : M(0);
   }
   const int64_t crow = static_cast<int64_t>(p.x) * a.stride;
-  M own[SweepTile<M>::kU];
+  M own[KU];
 #pragma unroll
-  for (int u = 0; u < SweepTile<M>::kU; ++u) own[u] = ok[u] ? static_cast<M>(__ldcs(a.R + crow + t[u])) : M(0);
+  for (int u = 0; u < KU; ++u) own[u] = ok[u] ? static_cast<M>(__ldcs(a.R + crow + t[u])) : M(0);
   const M diag = v.cp[p.x].diag;
-  M ap[SweepTile<M>::kU], lo[SweepTile<M>::kU], ext[SweepTile<M>::kU];  // ext: am_out (first pass) or Lout (later passes)
+  M ap[KU], lo[KU], ext[KU];  // ext: am_out (first pass) or Lout (later passes)
 #pragma unroll
-  for (int u = 0; u < SweepTile<M>::kU; ++u) ap[u] = lo[u] = ext[u] = M(0);
+  for (int u = 0; u < KU; ++u) ap[u] = lo[u] = ext[u] = M(0);
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     if (j >= p.z) break;
@@ -996,7 +985,7 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
     if (kind == kKindPeriodic) continue;
     const M s0 = e.s[0], s1 = e.s[1], s2 = e.s[2];
 #pragma unroll
-    for (int u = 0; u < SweepTile<M>::kU; ++u) {
+    for (int u = 0; u < KU; ++u) {
       const M af = x[u] * s0 + y[u] * s1 + z[u] * s2;
       ap[u] += pos_part(af);
       if (kind == kKindLower) lo[u] += neg_part(af) * val[j][u];
@@ -1007,7 +996,7 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
     }
   }
 #pragma unroll
-  for (int u = 0; u < SweepTile<M>::kU; ++u) {
+  for (int u = 0; u < KU; ++u) {
     if (!ok[u]) continue;
     const M am_out = First ? ext[u] : M(0), Lout = First ? M(0) : ext[u];
     const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out;
@@ -1015,33 +1004,33 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
   }
 }
 
-// backward value of SweepTile<M>::kU velocities of one cell (and f += Delta f in the last pass)
-template <class S, class M, int NE, bool First>
+// backward value of KU velocities of one cell (and f += Delta f in the last pass)
+template <class S, class M, int NE, bool First, int KU>
 __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
-                                                   const StageE<M>* E, int4 p, const int (&t)[SweepTile<M>::kU],
-                                                   const bool (&ok)[SweepTile<M>::kU], const M (&x)[SweepTile<M>::kU],
-                                                   const M (&y)[SweepTile<M>::kU], const M (&z)[SweepTile<M>::kU]) {
-  M val[NE][SweepTile<M>::kU];
+                                                   const StageE<M>* E, int4 p, const int (&t)[KU],
+                                                   const bool (&ok)[KU], const M (&x)[KU],
+                                                   const M (&y)[KU], const M (&z)[KU]) {
+  M val[NE][KU];
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     const uint32_t code = j < p.z ? E[p.y + j].code : 0u;
     const bool load = (code >> kKindShift) == kKindUpper;
     const int64_t row = static_cast<int64_t>(code & kIndexMask) * a.stride;
 #pragma unroll
-    for (int u = 0; u < SweepTile<M>::kU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(a.out[row + t[u]]) : M(0);
+    for (int u = 0; u < KU; ++u) val[j][u] = (load && ok[u]) ? static_cast<M>(a.out[row + t[u]]) : M(0);
   }
   const int64_t crow = static_cast<int64_t>(p.x) * a.stride;
   const int64_t frow = static_cast<int64_t>(p.x) * v.nv + a.k0;
-  M own[SweepTile<M>::kU], fv[SweepTile<M>::kU];
+  M own[KU], fv[KU];
 #pragma unroll
-  for (int u = 0; u < SweepTile<M>::kU; ++u) {
+  for (int u = 0; u < KU; ++u) {
     own[u] = ok[u] ? static_cast<M>(a.out[crow + t[u]]) : M(0);
     fv[u] = (ok[u] && a.update_f) ? static_cast<M>(__ldcs(v.f + frow + t[u])) : M(0);
   }
   const M diag = v.cp[p.x].diag;
-  M ap[SweepTile<M>::kU], up[SweepTile<M>::kU], am_out[SweepTile<M>::kU];
+  M ap[KU], up[KU], am_out[KU];
 #pragma unroll
-  for (int u = 0; u < SweepTile<M>::kU; ++u) ap[u] = up[u] = am_out[u] = M(0);
+  for (int u = 0; u < KU; ++u) ap[u] = up[u] = am_out[u] = M(0);
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     if (j >= p.z) break;
@@ -1050,7 +1039,7 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
     if (kind == kKindPeriodic) continue;
     const M s0 = e.s[0], s1 = e.s[1], s2 = e.s[2];
 #pragma unroll
-    for (int u = 0; u < SweepTile<M>::kU; ++u) {
+    for (int u = 0; u < KU; ++u) {
       const M af = x[u] * s0 + y[u] * s1 + z[u] * s2;
       ap[u] += pos_part(af);
       if (kind == kKindUpper) up[u] += neg_part(af) * val[j][u];
@@ -1058,7 +1047,7 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
     }
   }
 #pragma unroll
-  for (int u = 0; u < SweepTile<M>::kU; ++u) {
+  for (int u = 0; u < KU; ++u) {
     if (!ok[u]) continue;
     const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out[u];
     const M df = own[u] - up[u] / D;
@@ -1067,8 +1056,8 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
   }
 }
 
-template <class S, class M, int NE, bool First>
-__global__ void __launch_bounds__(kTileThreadsSweep, SweepTile<M>::kBlocks) k_sweep_tiles(View<S, M> v, SweepArgs<S, M> a) {
+template <class S, class M, int NE, bool First, int KU, int KB>
+__global__ void __launch_bounds__(kTileThreadsSweep, KB) k_sweep_tiles(View<S, M> v, SweepArgs<S, M> a) {
   constexpr int W = kTileThreadsSweep / 32;
   __shared__ __align__(16) StageBuf<M> sh_buf[2];
   __shared__ int32_t sh_sc[kMaxSubLevels + 1], sh_se[kMaxSubLevels + 1];
@@ -1082,11 +1071,11 @@ __global__ void __launch_bounds__(kTileThreadsSweep, SweepTile<M>::kBlocks) k_sw
     sh_sc[k] = a.sub_cells[s0 + k];
     sh_se[k] = a.sub_entries[s0 + k];
   }
-  int t[SweepTile<M>::kU];
-  bool ok[SweepTile<M>::kU];
-  M x[SweepTile<M>::kU], y[SweepTile<M>::kU], z[SweepTile<M>::kU];
+  int t[KU];
+  bool ok[KU];
+  M x[KU], y[KU], z[KU];
 #pragma unroll
-  for (int u = 0; u < SweepTile<M>::kU; ++u) {
+  for (int u = 0; u < KU; ++u) {
     t[u] = it.y + lane + 32 * u;
     ok[u] = t[u] < it.z;
     const int q = a.k0 + (ok[u] ? t[u] : it.y);
@@ -1105,9 +1094,9 @@ __global__ void __launch_bounds__(kTileThreadsSweep, SweepTile<M>::kBlocks) k_sw
     const int l = s < nsub ? s : nsteps - 1 - s;
     const int ncl = sh_sc[l + 1] - sh_sc[l];
     if (s < nsub) {
-      for (int k = warp; k < ncl; k += W) tile_forward_cell<S, M, NE, First>(v, a, cur.se, cur.prog[k], t, ok, x, y, z);
+      for (int k = warp; k < ncl; k += W) tile_forward_cell<S, M, NE, First, KU>(v, a, cur.se, cur.prog[k], t, ok, x, y, z);
     } else {
-      for (int k = warp; k < ncl; k += W) tile_backward_cell<S, M, NE, First>(v, a, cur.se, cur.prog[k], t, ok, x, y, z);
+      for (int k = warp; k < ncl; k += W) tile_backward_cell<S, M, NE, First, KU>(v, a, cur.se, cur.prog[k], t, ok, x, y, z);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -1373,48 +1362,150 @@ void Launch<S, M>::internal_face_flux(const View<S, M>& v, const int32_t* cells,
   if (n > 0) k_internal_face_flux<S, M><<<n, kFaceThreads, 0, st>>>(v, cells, entries, out);
 }
 
+// ---- kernel shapes: velocities per thread x CTAs per SM of the gradient, residual and LU-SGS tile kernels -------
+template <>
+KernelShape default_shape<double>() {
+  return {4, 2, 2, 3, 2, 6};
+}
+template <>
+KernelShape default_shape<float>() {
+  return {4, 3, 2, 4, 4, 6};
+}
+
+template <class M>
+const KernelShape& kernel_shape() {
+  // KIN_SHAPE = "res=UxB,grad=UxB,tile=UxB" selects another compiled shape (all give the same results)
+  static const KernelShape shape = [] {
+    KernelShape k = default_shape<M>();
+    if (const char* e = std::getenv("KIN_SHAPE")) {
+      std::string str(e);
+      auto pick = [&](const char* key, int& uu, int& bb) {
+        const size_t pos = str.find(key);
+        if (pos == std::string::npos) return;
+        int a = 0, b2 = 0;
+        if (std::sscanf(str.c_str() + pos + std::strlen(key), "%dx%d", &a, &b2) == 2) {
+          uu = a;
+          bb = b2;
+        }
+      };
+      pick("res=", k.res_u, k.res_occ);
+      pick("grad=", k.grad_u, k.grad_occ);
+      pick("tile=", k.tile_u, k.tile_blocks);
+    }
+    return k;
+  }();
+  return shape;
+}
+template const KernelShape& kernel_shape<double>();
+template const KernelShape& kernel_shape<float>();
+
 template <class S, class M>
 int Launch<S, M>::residual_tiles(int kc) {
-  return ceil_div(kc, kTileThreads * kTileIters) * (kTileThreads / 32);
+  return ceil_div(kc, kTileThreads * kernel_shape<M>().res_u) * (kTileThreads / 32);
+}
+
+template <class S, class M, int NE>
+static void launch_gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st) {
+  const KernelShape& k = kernel_shape<M>();
+#define KIN_GRAD(U, B)                                                                                           \
+  if (k.grad_u == U && k.grad_occ == B) {                                                                        \
+    const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * U));                       \
+    k_gradient<S, M, NE, U, B><<<grid, kTileThreads, 0, st>>>(v, ch);                                            \
+    return;                                                                                                      \
+  }
+  if constexpr (std::is_same<S, M>::value && std::is_same<M, double>::value) {
+    KIN_GRAD(1, 4)
+    KIN_GRAD(1, 6)
+    KIN_GRAD(2, 4)
+  }
+  if constexpr (std::is_same<S, M>::value && std::is_same<M, float>::value) {
+    KIN_GRAD(4, 3)
+    KIN_GRAD(2, 6)
+  }
+#undef KIN_GRAD
+  constexpr int U = std::is_same<M, double>::value ? 2 : 2, B = std::is_same<M, double>::value ? 3 : 4;
+  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * U));
+  k_gradient<S, M, NE, U, B><<<grid, kTileThreads, 0, st>>>(v, ch);
 }
 
 template <class S, class M>
 void Launch<S, M>::gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st) {
   if (v.n_cells <= 0 || ch.kc <= 0) return;
-  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * TileOcc<M>::kGradientU));
   if (v.max_entries <= 6)
-    k_gradient<S, M, 6><<<grid, kTileThreads, 0, st>>>(v, ch);
+    launch_gradient<S, M, 6>(v, ch, st);
   else
-    k_gradient<S, M, 0><<<grid, kTileThreads, 0, st>>>(v, ch);
+    launch_gradient<S, M, 0>(v, ch, st);
+}
+
+template <class S, class M, int NE>
+static void launch_residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
+                            cudaStream_t st) {
+  const KernelShape& k = kernel_shape<M>();
+#define KIN_RES(U, B)                                                                                            \
+  if (k.res_u == U && k.res_occ == B) {                                                                          \
+    const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * U));                       \
+    k_residual<S, M, NE, U, B><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);                   \
+    return;                                                                                                      \
+  }
+  if constexpr (std::is_same<M, double>::value) {
+    KIN_RES(2, 3)
+    KIN_RES(2, 4)
+  } else {
+    KIN_RES(4, 4)
+    KIN_RES(2, 6)
+  }
+#undef KIN_RES
+  constexpr int U = 4, B = std::is_same<M, double>::value ? 2 : 3;
+  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * U));
+  k_residual<S, M, NE, U, B><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
 }
 
 template <class S, class M>
 void Launch<S, M>::residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
                             double* residual_cell, cudaStream_t st) {
   if (v.n_cells <= 0 || ch.kc <= 0) return;
-  const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * kTileIters));
   if (v.max_entries <= 6)
-    k_residual<S, M, 6><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
+    launch_residual<S, M, 6>(v, ch, partial, partial_stride, st);
   else
-    k_residual<S, M, 0><<<grid, kTileThreads, 0, st>>>(v, ch, partial, partial_stride);
+    launch_residual<S, M, 0>(v, ch, partial, partial_stride, st);
   if (ch.defect_mode == kDefectStore) return;  // no sums of its own: the FP64 residual's stand
   k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride, residual_tiles(ch.kc),
                                                              residual_cell, v.n_cells);
 }
 
+template <class S, class M, int NE, bool First>
+static void launch_tiles(const View<S, M>& v, const SweepArgs<S, M>& a, cudaStream_t st) {
+  const KernelShape& k = kernel_shape<M>();
+#define KIN_TILE(KU, KB)                                                                                         \
+  if (k.tile_u == KU && k.tile_blocks == KB) {                                                                   \
+    k_sweep_tiles<S, M, NE, First, KU, KB><<<a.n_items, kTileThreadsSweep, 0, st>>>(v, a);                       \
+    return;                                                                                                      \
+  }
+  if constexpr (std::is_same<S, M>::value && std::is_same<M, double>::value) {
+    KIN_TILE(2, 8)
+    KIN_TILE(4, 4)
+    KIN_TILE(1, 8)
+  }
+  if constexpr (std::is_same<S, M>::value && std::is_same<M, float>::value) {
+    KIN_TILE(4, 8)
+    KIN_TILE(2, 8)
+  }
+#undef KIN_TILE
+  constexpr int KU = std::is_same<M, double>::value ? 2 : 4;
+  k_sweep_tiles<S, M, NE, First, KU, 6><<<a.n_items, kTileThreadsSweep, 0, st>>>(v, a);
+}
+
 template <class S, class M>
 void Launch<S, M>::sweep_pass(const View<S, M>& v, const SweepArgs<S, M>& a, cudaStream_t st) {
   if (a.n_items <= 0) return;
-#define KIN_TILES(NE, FIRST) \
-  k_sweep_tiles<S, M, NE, FIRST><<<a.n_items, kTileThreadsSweep, 0, st>>>(v, a)
   if (a.staged_ne == 6 && a.dprev == nullptr)
-    KIN_TILES(6, true);
+    launch_tiles<S, M, 6, true>(v, a, st);
   else if (a.staged_ne == 6)
-    KIN_TILES(6, false);
+    launch_tiles<S, M, 6, false>(v, a, st);
   else if (a.staged_ne == 8 && a.dprev == nullptr)
-    KIN_TILES(8, true);
+    launch_tiles<S, M, 8, true>(v, a, st);
   else if (a.staged_ne == 8)
-    KIN_TILES(8, false);
+    launch_tiles<S, M, 8, false>(v, a, st);
   else
     k_sweep_pass<S, M><<<a.n_items, kSweepThreads, 0, st>>>(v, a);
 }

@@ -8,7 +8,6 @@
 
 namespace kin {
 
-constexpr int kTileIters = 4;      // velocities per thread in the gradient / residual tiles
 constexpr int kSweepThreads = 256;  // one CTA per (direction, block, velocity tile): 8 warps share every level
 constexpr int kSweepTile = 32;      // velocities of one sweep CTA (one per lane)
 
@@ -30,19 +29,6 @@ enum : uint32_t { kKindPeriodic = 0, kKindBoundary = 1, kKindLower = 2, kKindUpp
 constexpr uint32_t kKindShift = 28, kIndexMask = (1u << kKindShift) - 1;
 
 constexpr int kTileThreadsSweep = 128;  // threads of one k_sweep_tiles CTA
-
-// k_sweep_tiles shape per arithmetic type: velocities per thread (a CTA covers 32 * kU velocities) and the resident
-// CTAs per SM its register budget is sized for
-template <class M>
-struct SweepTile {
-  static constexpr int kU = 4;
-  static constexpr int kBlocks = 6;
-};
-template <>
-struct SweepTile<double> {
-  static constexpr int kU = 2;
-  static constexpr int kBlocks = 6;
-};
 
 // arguments of one LU-SGS block pass over a velocity chunk
 template <class S, class M>
@@ -108,6 +94,15 @@ struct SweepLaunch {
   // one block pass, one (cell, velocity) per thread per step, Delta f* through L2 (k_sweep_window)
   static void window(const View<S, P>& v, const SweepArgs<S, P>& a, bool first, int ctas_per_sm, cudaStream_t st);
 };
+
+// velocities per thread x resident CTAs per SM of the gradient, residual and LU-SGS tile kernels (per arithmetic type)
+struct KernelShape {
+  int res_u, res_occ, grad_u, grad_occ, tile_u, tile_blocks;
+};
+template <class M>
+KernelShape default_shape();
+template <class M>
+const KernelShape& kernel_shape();
 
 constexpr int kStageCells = 64;     // cells of one staged sub-level
 constexpr int kStageEntries = 384;  // stencil entries of one staged sub-level
