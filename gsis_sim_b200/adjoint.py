@@ -17,8 +17,14 @@ Shakhov target and the per-face sums against the inflow Maxwellians run on the d
 module finishes the per-cell / per-face algebra: the moments -> cell parameter chain, the pressure-face chain
 (App. A.2 acoustic correction), the wall-density equations and the parameter gradients.
 
-Scope (`check_scope`): FP64 backend with one velocity chunk; continuous equilibrium (kinetic.equilibrium =
-"continuous") or every state resolved by the velocity grid; diffuse walls, pressure inlets / outlets with
+Equilibrium: continuous, or discrete (the reference default). Where the grid does not resolve a cell's state the
+Shakhov target is built on the discrete Maxwellian of a Newton solve with the conservative correction gamma; the
+derivative goes through both solves by the implicit function theorem (gsis_sim_b200.deq_adjoint: the device gives
+the lambda sums at fixed (beta, gamma), the host the 5 x 5 chain). Inflow states of walls and pressure faces that
+the reference corrects to their discrete Maxwellian are differentiated through that correction the same way.
+
+Scope (`check_scope`): FP64 backend with one velocity chunk; a tensor velocity grid when the equilibrium is discrete
+(every grid of the reference is one) and no failed Newton solve; diffuse walls, pressure inlets / outlets with
 pressure_boundary_reconstruction = "cell", vacuum, symmetry, periodic faces; no Maxwell walls, mass-flow inlets,
 positivity limiter or closed-domain scaling.
 """
@@ -30,6 +36,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import abi
+from .deq_adjoint import CellDerivatives, InflowDerivatives, TensorGrid
 from .kinetic_setup import BOUNDARY_TYPES
 
 C_J = 0.5 * math.sqrt(2.0 / math.pi)
@@ -186,6 +193,69 @@ class KineticAdjoint:
         self.sgn[(bk != abi.BC_PRESSURE) & (bk != abi.BC_VACUUM)] = 0.0
         self.nu = np.zeros(len(self.wall))
         self.history = []
+        self._discrete_chains()
+
+    # ---- derivatives through the discrete equilibrium ---------------------------------------------------------
+    def _discrete_chains(self):
+        """The cells whose Shakhov target is built on the discrete Maxwellian and the inflow faces corrected to it,
+        with the per-state constants of their derivative chains (gsis_sim_b200.deq_adjoint)."""
+        sol = self.sol
+        s = sol.s
+        self.deq_cells = np.zeros(0, np.int64)
+        self.deq_pres = np.zeros(0, np.int64)
+        self.deq_wall = np.zeros(0, np.int64)
+        if not sol.discrete_eq:
+            return
+        grid = TensorGrid.from_setup(s)
+        m = sol.moments_
+        st = m[:, [0, 1, 2, 3, 4]]
+        self.deq_cells = np.flatnonzero(~sol._deq_resolved(st))
+        if len(self.deq_cells):
+            self.cell_deq = CellDerivatives(grid, m[self.deq_cells], float(s["Pr"]), float(s["cold_bgk_temperature"]),
+                                            float(s["deq_tolerance"]), int(s["deq_max_iterations"]))
+            if not self.cell_deq.ok.all():
+                raise AdjointScopeError("a cell's discrete-equilibrium Newton solve did not converge")
+        # pressure faces: W_b of the owner ("cell" reconstruction) before the correction
+        if len(self.pres):
+            wb = self._pressure_states()
+            need = (wb[:, 0] > 0) & (wb[:, 4] > 0) & ~sol._deq_resolved(wb)
+            self.deq_pres = self.pres[need]
+            if len(self.deq_pres):
+                self.pres_deq = InflowDerivatives(grid, wb[need])
+                keep = self.pres_deq.ok
+                self.deq_pres = self.deq_pres[keep]
+                self.pres_deq = InflowDerivatives(grid, wb[need][keep])
+        if len(self.wall):
+            h = sol.h
+            T = h.patch_dbl[sol.bpatch[self.wall], 0] if sol.wall_T is None else sol.wall_T[self.wall]
+            ws = np.column_stack([np.ones(len(self.wall)), h.patch_dbl[sol.bpatch[self.wall], 2:5], T])
+            need = ~sol._deq_resolved(ws)
+            if need.any():
+                idv = InflowDerivatives(grid, ws[need])
+                sel = np.flatnonzero(need)[idv.ok]
+                self.deq_wall = sel  # indices into self.wall
+                self.wall_deq = InflowDerivatives(grid, ws[sel])
+
+    def _pressure_states(self):
+        """(rho_b, u_b, T_b) of the pressure faces from their owner cells (update_pressure_inflow, "cell"
+        reconstruction, src/kinetic/kinetic_solver.cpp:172-260)."""
+        sol = self.sol
+        h = sol.h
+        b = self.pres
+        m = sol.moments_
+        o = sol.bowner[b]
+        p_o, u_o, T_o = m[o, 5], m[o, 1:4], m[o, 4]
+        patch = sol.bpatch[b]
+        p_b = h.patch_dbl[patch, 1]
+        inlet = np.isin(sol.ptype[patch], _INLETS)
+        T_b = np.where(inlet, h.patch_dbl[patch, 0], T_o)
+        cs = np.sqrt(h.gamma * T_o)
+        du = (p_o - p_b) / ((p_o / T_o) * cs)
+        n = h.face_normal[sol.bf_global[b]]
+        un = np.einsum("na,na->n", u_o, n)
+        zero_tan = h.patch_dbl[patch, 6] > 0.5
+        u_b = np.where(zero_tan[:, None], (un + du)[:, None] * n, u_o + du[:, None] * n)
+        return np.column_stack([p_b / T_b, u_b, T_b])
 
     # ---- scope ---------------------------------------------------------------------------------------------------
     def check_scope(self):
@@ -206,14 +276,11 @@ class KineticAdjoint:
         if float(s["cold_bgk_temperature"]) > 0.0:
             raise AdjointScopeError("cold-BGK switch")
         if sol.discrete_eq:
+            if TensorGrid.from_setup(s) is None:
+                raise AdjointScopeError("the discrete equilibrium's derivative needs a tensor velocity grid")
             sol.prepare()
-            m = sol.moments_
-            st = np.stack([m[:, 0], m[:, 1], m[:, 2], m[:, 3], m[:, 4]], 1)
-            used = (sol.bkind == abi.BC_DIFFUSE_WALL) | (sol.bkind == abi.BC_PRESSURE)
-            if not np.all(sol._deq_resolved(st)) or (np.any(used) and
-                                                     not np.all(sol._deq_resolved(sol.inflow[used][:, 1:6]))):
-                raise AdjointScopeError('a state is not resolved by the velocity grid: use kinetic.equilibrium = '
-                                        '"continuous" or a wider / finer velocity grid')
+            if sol.backend.deq_counts()[1] > 0:
+                raise AdjointScopeError("a cell's discrete-equilibrium Newton solve failed")
 
     # ---- one evaluation of O(y) ----------------------------------------------------------------------------------
     def _mu(self):
@@ -230,7 +297,16 @@ class KineticAdjoint:
 
     def _reduce(self, cells: bool = True, faces: bool = True):
         cell, face = self.sol.backend.adjoint_reduce(self._mu(), cells=cells, faces=faces)
-        return (cell.reshape(self.nc, 9) if cells else None), (face.reshape(max(self.nb, 0), 10) if faces else None)
+        from .backend import ADJ_CELL_SUMS, ADJ_FACE_SUMS
+
+        if cells:
+            cell = cell.reshape(self.nc, ADJ_CELL_SUMS)
+            out = cell[:, :9].copy()
+            d = self.deq_cells
+            if len(d):
+                out[d, 1:9] = self.cell_deq.lambda_sums(cell[d, 1:9], cell[d, 9:14], cell[d, 14:19])
+            cell = out
+        return (cell if cells else None), (face.reshape(max(self.nb, 0), ADJ_FACE_SUMS) if faces else None)
 
     def _coefficients(self, cell, face):
         sol = self.sol
@@ -246,6 +322,12 @@ class KineticAdjoint:
             rho_bar = S[:, 0] / rb
             u_bar = S[:, 1:4] / Tb[:, None]
             T_bar = S[:, 4] / (2.0 * Tb * Tb) - 1.5 * S[:, 0] / Tb
+            if len(self.deq_pres):
+                # through the correction of W_b to its discrete Maxwellian
+                k = np.searchsorted(b, self.deq_pres)
+                tb = self.pres_deq.pullback(np.column_stack([rho_bar[k], u_bar[k], T_bar[k]]))
+                rho_bar, u_bar, T_bar = rho_bar.copy(), u_bar.copy(), T_bar.copy()
+                rho_bar[k], u_bar[k], T_bar[k] = tb[:, 0], tb[:, 1:4], tb[:, 4]
             o = sol.bowner[b]
             h = sol.h
             n = h.face_normal[sol.bf_global[b]]
@@ -335,16 +417,23 @@ class KineticAdjoint:
         dTw = np.zeros(self.nb)
         w = self.wall
         if len(w):
-            T = sol.inflow[w, 5]
+            # adjoint of the wall inflow Maxwellian's parameters (rho', u', T'): through the wall term rho_Gamma M of
+            # the residual and through sm5 of the wall-density equation
+            rp, T = sol.inflow[w, 1], sol.inflow[w, 5]
             S = face[w]
             rg = sol.inflow[w, 0]
             sm0, sm5 = sol.bsums[w, 0], sol.bsums[w, 5]
-            dR = rg * (S[:, 4] / (2.0 * T * T) - 1.5 * S[:, 0] / T)
-            D5 = S[:, 5] / (2.0 * T * T) - 1.5 * S[:, 6] / T
+            dR = np.column_stack([rg * S[:, 0] / rp, rg[:, None] * S[:, 1:4] / T[:, None],
+                                  rg * (S[:, 4] / (2.0 * T * T) - 1.5 * S[:, 0] / T)])
+            D5 = np.column_stack([S[:, 6] / rp, S[:, 10:13] / T[:, None], S[:, 5] / (2.0 * T * T) - 1.5 * S[:, 6] / T])
             with np.errstate(divide="ignore", invalid="ignore"):
                 pos = (sm5 < 0) & (-sm0 / sm5 > 0)
-                dPhi = np.where(pos, sm0 / (sm5 * sm5) * D5, 0.0)
-            dTw[w] = -(dR - self.nu * dPhi)
+                dPhi = np.where(pos[:, None], (sm0 / (sm5 * sm5))[:, None] * D5, 0.0)
+            th = -(dR - self.nu[:, None] * dPhi)
+            if len(self.deq_wall):
+                # through the correction of (1, u_w, T_w) to its discrete Maxwellian
+                th[self.deq_wall] = self.wall_deq.pullback(th[self.deq_wall])
+            dTw[w] = th[:, 4]
         # accommodation at alpha = 1: the inflow rho M + (1 - alpha) f_spec of a Maxwell wall and its zero-net-flux
         # density rho = -(sm0 + (1 - alpha) S_spec) / sm5; dJ/dalpha = A1 + A2 + nu S_spec / sm5
         dA = np.zeros(self.nb)

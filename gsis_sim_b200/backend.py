@@ -15,7 +15,8 @@ from . import abi
 from ._lib import load_library
 
 
-ADJ_FACE_SUMS = 10  # per boundary face sums of kin_adjoint_reduce
+ADJ_FACE_SUMS = 13  # per boundary face sums of kin_adjoint_reduce
+ADJ_CELL_SUMS = 19  # per cell sums of kin_adjoint_reduce
 
 
 class KineticError(RuntimeError):
@@ -97,10 +98,10 @@ class KineticBackendABI:
         return out.reshape(self.n_cells, self.nv)
 
     def adjoint_reduce(self, mu, cells: bool = True, faces: bool = True):
-        """Transposed transport with the per-face weights mu, then the per-cell (9) and per-face sums; cells=False /
+        """Transposed transport with the per-face weights mu, then the per-cell (19) and per-face sums; cells=False /
         faces=False skip those sums (returned as None) when only the transport's seeds are wanted."""
         m = np.ascontiguousarray(mu, dtype=np.float64)
-        cell = np.empty(self.n_cells * 9, dtype=np.float64) if cells else None
+        cell = np.empty(self.n_cells * ADJ_CELL_SUMS, dtype=np.float64) if cells else None
         face = np.empty(max(self.n_bfaces, 1) * ADJ_FACE_SUMS, dtype=np.float64) if faces else None
         self._call("adjoint_reduce", abi.as_ptr(m, C.c_double), m.size,
                    abi.as_ptr(cell, C.c_double) if cells else None, cell.size if cells else 0,

@@ -24,8 +24,11 @@ __device__ __forceinline__ double entry_value(const View<double, double>& v, con
   return c.other >= 0 ? f_at(v, c.other, q) : boundary_value_first_order(v, c, cell, q, x, y, z, fi);
 }
 
-// k_adj_cell: per cell, sum_q lambda_q * {f^S_q - f_q, d f^S_q / d(rho, u, T, q)} of the (continuous) Shakhov target
-// f^S = M (1 + P), P = coef (c.q)(c^2 / T - 5) (shakhov_target, src/kinetic/kinetic_types.hpp:79-90)
+// k_adj_cell: per cell, sum_q lambda_q * {f^S_q - f_q, d f^S_q / d(rho, u, T, q)} of the Shakhov target
+// (shakhov_target, src/kinetic/kinetic_types.hpp:79-90). Continuous equilibrium: f^S = M (1 + P),
+// P = coef (c.q)(c^2 / T - 5). Discrete equilibrium (deq_flags > 0): f^S = E F, F = 1 + P + gamma . psi,
+// psi = (1, c, c^2 / 2), E = A exp(-B |xi - u'|^2) from the Newton solve: the derivative sums at fixed (beta, gamma)
+// and sum lambda E F psi, sum lambda E psi for the chain through the Newton and gamma solves (host).
 __global__ void __launch_bounds__(kAdjThreads) k_adj_cell(View<double, double> v, AdjView a, double* __restrict__ out) {
   __shared__ double sh[kAdjCellSums * (kAdjThreads / 32)];
   const int cell = blockIdx.x;
@@ -33,6 +36,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_cell(View<double, double> v
   const CellParams<double> cp = v.cp[cell];
   const double rho = a.moments[static_cast<int64_t>(cell) * 15];
   const double T = cp.theta, kap = cp.coef;
+  const bool discrete = a.deq_flags != nullptr && a.deq_flags[cell] > 0;
   double s[kAdjCellSums];
 #pragma unroll
   for (int k = 0; k < kAdjCellSums; ++k) s[k] = 0.0;
@@ -47,16 +51,41 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_cell(View<double, double> v
     const double lam = lam_at(a, nv, cell, q);
     const double fi = f_at(v, cell, q);
     const double lm = lam * M;
-    s[0] += lam * (M * (1.0 + P) - fi);
-    s[1] += lm / rho;
-    const double onep = 1.0 + P;
-    s[2] += lm * (cx / T * onep + kap * (-cp.qx * h - 2.0 * cq * cx / T));
-    s[3] += lm * (cy / T * onep + kap * (-cp.qy * h - 2.0 * cq * cy / T));
-    s[4] += lm * (cz / T * onep + kap * (-cp.qz * h - 2.0 * cq * cz / T));
-    s[5] += lm * ((c2 / (2.0 * T * T) - 1.5 / T) * onep + cq * (-2.0 * kap / T * h - kap * c2 / (T * T)));
-    s[6] += lm * kap * cx * h;
-    s[7] += lm * kap * cy * h;
-    s[8] += lm * kap * cz * h;
+    if (!discrete) {
+      s[0] += lam * (M * (1.0 + P) - fi);
+      s[1] += lm / rho;
+      const double onep = 1.0 + P;
+      s[2] += lm * (cx / T * onep + kap * (-cp.qx * h - 2.0 * cq * cx / T));
+      s[3] += lm * (cy / T * onep + kap * (-cp.qy * h - 2.0 * cq * cy / T));
+      s[4] += lm * (cz / T * onep + kap * (-cp.qz * h - 2.0 * cq * cz / T));
+      s[5] += lm * ((c2 / (2.0 * T * T) - 1.5 / T) * onep + cq * (-2.0 * kap / T * h - kap * c2 / (T * T)));
+      s[6] += lm * kap * cx * h;
+      s[7] += lm * kap * cy * h;
+      s[8] += lm * kap * cz * h;
+    } else {
+      const double F = 1.0 + P + (cp.g0 + (cp.gx * cx + cp.gy * cy + cp.gz * cz) + 0.5 * cp.g4 * c2);
+      const double lmf = lm * F;
+      const double twoB = 2.0 * cp.eq.B;
+      s[0] += lam * (M * F - fi);
+      s[1] += -lm * P / rho;
+      s[2] += lmf * twoB * (x - cp.eq.ux) + lm * (kap * (-cp.qx * h - 2.0 * cq * cx / T) - (cp.gx + cp.g4 * cx));
+      s[3] += lmf * twoB * (y - cp.eq.uy) + lm * (kap * (-cp.qy * h - 2.0 * cq * cy / T) - (cp.gy + cp.g4 * cy));
+      s[4] += lmf * twoB * (z - cp.eq.uz) + lm * (kap * (-cp.qz * h - 2.0 * cq * cz / T) - (cp.gz + cp.g4 * cz));
+      s[5] += lm * cq * (-2.0 * kap / T * h - kap * c2 / (T * T));
+      s[6] += lm * kap * cx * h;
+      s[7] += lm * kap * cy * h;
+      s[8] += lm * kap * cz * h;
+      s[9] += lmf;
+      s[10] += lmf * cx;
+      s[11] += lmf * cy;
+      s[12] += lmf * cz;
+      s[13] += lmf * 0.5 * c2;
+      s[14] += lm;
+      s[15] += lm * cx;
+      s[16] += lm * cy;
+      s[17] += lm * cz;
+      s[18] += lm * 0.5 * c2;
+    }
   }
   block_sum<kAdjCellSums, kAdjThreads>(s, sh);
   if (threadIdx.x == 0) {
@@ -264,6 +293,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<double, double> 
       const double wa = wq * ae / bf.area * M;
       s[5] += wa * c2;
       s[6] += wa;
+      s[10] += wa * cx;
+      s[11] += wa * cy;
+      s[12] += wa * cz;
       if (bf.kind == kDiffuseWall && a.face_axis != nullptr && a.face_axis[b] >= 0) {
         const int r = a.flip[a.face_axis[b] * nv + q];
         const double xr = v.xi_x[r], yr = v.xi_y[r], zr = v.xi_z[r];

@@ -22,8 +22,11 @@
 
 namespace kin {
 
-constexpr int kAdjCellSums = 9;   // Lambda0, Lambda_rho, Lambda_u (3), Lambda_T, Lambda_q (3)
-constexpr int kAdjFaceSums = 10;  // S0, S1 (3), S2, S5, S6, A1, A2, S_spec (k_adj_faces)
+// per cell: Lambda0 and the derivative sums with respect to (rho, u (3), T, q (3)); for a cell whose equilibrium is
+// the discrete one also sum lambda E F psi (5) and sum lambda E psi (5), the derivative sums then at fixed
+// (beta, gamma) (the host finishes the chain through the Newton solve)
+constexpr int kAdjCellSums = 19;
+constexpr int kAdjFaceSums = 13;  // S0, S1 (3), S2, S5, S6, A1, A2, S_spec, S6 c (3) (k_adj_faces)
 constexpr int kAdjCoefs = 8;      // a0, a (3), a2, b (3)
 
 struct AdjView {
@@ -43,6 +46,7 @@ struct AdjView {
   const int32_t* face_axis;  // per boundary face: the axis its normal is aligned with, -1 if none
   const double* coef;      // per cell: moment expansion coefficients (kAdjCoefs)
   const double* moments;   // per cell: the 15 moments of the forward state
+  const int32_t* deq_flags;  // per cell: the discrete-equilibrium result of the forward state (> 0: discrete)
   double* out;             // O_f(y) at the reversed position [cell][rev[q]]
 };
 

@@ -1639,6 +1639,7 @@ struct Backend final : KinHandle {
     a.face_axis = adj_face_axis.p;
     a.coef = adj_coef.p;
     a.moments = moments.p;
+    a.deq_flags = deq_valid ? flags.p : nullptr;
     a.out = reinterpret_cast<double*>(r.p);
     return a;
   }

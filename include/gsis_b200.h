@@ -329,12 +329,15 @@ int kin_adjoint_set(KinHandle* h, const double* lambda, int64_t n);
 int kin_adjoint_get(KinHandle* h, double* lambda, int64_t n);
 /* Transposed transport and the per-cell / per-face sums. mu[b] (n_bfaces): weight of the seed w_q a_q mu[b] on the
    outgoing face values of boundary face b (diffuse walls: nu_b / (area_b sm5_b); inlet / outlet faces: the objective's
-   -dJ/d(patch flow) factor), also applied to the incoming values of pressure faces. Outputs, per cell (9): the sums of
-   lambda against f^S - f and d f^S / d(rho, u, T, q); per boundary face: S0, S1 (3), S2 of the seeds on the
-   incoming inflow values against the inflow Maxwellian (M, M c, M c^2) and S5, S6 = sum_in w an M {c^2, 1}; per
-   boundary face also (10 in all) A1 = sum_in a lambda f_spec, A2 = sum_in s_grad f_owner(reflected velocity),
-   S_spec = sum_in w an f_spec (axis-aligned diffuse walls, f_spec = the owner's reconstructed face value at the
-   reflected velocity; zero elsewhere). cell_sums = NULL with n_cell = 0 skips the per-cell sums, face_sums = NULL
+   -dJ/d(patch flow) factor), also applied to the incoming values of pressure faces. Outputs, per cell (19): the sums
+   of lambda against f^S - f and d f^S / d(rho, u, T, q); where the cell's equilibrium is the discrete one (the
+   Newton solve of the cell parameters succeeded) those derivatives are taken at fixed (beta, gamma) and the cell adds
+   sum lambda E F psi (5) and sum lambda E psi (5), psi = (1, c, c^2 / 2), F = the Shakhov factor (zeros for the
+   other cells); per boundary face: S0, S1 (3), S2 of the seeds on the incoming inflow values against the inflow
+   Maxwellian (M, M c, M c^2) and S5, S6 = sum_in w an M {c^2, 1} / area; A1 = sum_in a lambda f_spec,
+   A2 = sum_in s_grad f_owner(reflected velocity), S_spec = sum_in w an f_spec (axis-aligned diffuse walls,
+   f_spec = the owner's reconstructed face value at the reflected velocity; zero elsewhere); and (13 in all)
+   sum_in w an M c / area (3). cell_sums = NULL with n_cell = 0 skips the per-cell sums, face_sums = NULL
    with n_face = 0 the per-face sums; the transposed transport (the seeds that kin_adjoint_update gathers) always
    runs. */
 int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,

@@ -22,8 +22,16 @@ dJ/dp = dJ/dp|_x - y^T dF/dp.
 Scope (the same as the B200 adjoint; `check_scope` raises outside it): diffuse walls, pressure inlets / outlets with
 the "cell" boundary reconstruction (W_b from the owner cell, App. A.2 acoustic correction), vacuum, symmetry and
 periodic faces; Venkatakrishnan limiter (absolute or relative epsilon) or none; no positivity limiter, no closed-domain
-scaling, no mass-flow inlets, no Maxwell walls; every cell and inflow state resolved by the velocity grid (the
-discrete-equilibrium Newton inactive, deq_resolved of src/kinetic/discrete_equilibrium.hpp:35-48).
+scaling, no mass-flow inlets, no Maxwell walls.
+
+Equilibrium: the continuous Maxwellian, or the discrete one (kinetic.equilibrium = "discrete", the reference default):
+for every cell and inflow state the velocity grid does not resolve (deq_resolved, src/kinetic/
+discrete_equilibrium.hpp:35-48) the Maxwellian is E = exp(beta . psi(c)), psi = (1, c, |c|^2 / 2), c = xi - u, with
+beta solving sum_q w E psi = (rho, 0, 0, 0, 3/2 rho T) (deq_* :56-188), and the cells' Shakhov target carries the
+correction gamma . psi that makes its polynomial part conservative (deq_shakhov_correction :183-188). The Newton
+iteration runs without gradients to convergence; one Newton step from the converged beta then carries the
+derivative (dbeta = -J^-1 dG, the implicit function theorem), and gamma = -J^-1 sum w E P psi is differentiated as it
+is.
 """
 from __future__ import annotations
 
@@ -89,6 +97,10 @@ class SteadyMap:
         self.bkind = torch.as_tensor(bkind)
         self.bpatch = np.asarray(s["bface_patch"])
         self.volume = _t(s["volume"])
+        self.discrete = bool(int(s["discrete_eq"]))
+        self.deq_lo, self.deq_hi = np.asarray(s["deq_lo"], float), np.asarray(s["deq_hi"], float)
+        self.deq_d, self.deq_crit = np.asarray(s["deq_d"], float), float(s["deq_criterion"])
+        self.deq_tol, self.deq_maxit = float(s["deq_tolerance"]), int(s["deq_max_iterations"])
         self.omega, self.Pr = float(s["omega"]), float(s["Pr"])
         self.mu0 = float(s["mu0"])
         self.cold = float(s["cold_bgk_temperature"])
@@ -136,14 +148,9 @@ class SteadyMap:
             raise ScopeError("mass-flow inlets")
         if torch.any(self.bkind == BC_PRESSURE) and h.pressure_boundary_reconstruction != "cell":
             raise ScopeError('pressure boundaries need pressure_boundary_reconstruction = "cell"')
-        if solver is not None and solver.discrete_eq:
-            m = solver.moments_
-            st = np.stack([m[:, 0], m[:, 1], m[:, 2], m[:, 3], m[:, 4]], 1)
-            if not np.all(solver._deq_resolved(st)):
-                raise ScopeError("a cell state is not resolved by the velocity grid (discrete equilibrium active)")
-            used = (solver.bkind == BC_DIFFUSE_WALL) | (solver.bkind == BC_PRESSURE)
-            if np.any(used) and not np.all(solver._deq_resolved(solver.inflow[used][:, 1:6])):
-                raise ScopeError("an inflow state is not resolved by the velocity grid")
+        if int(s["deq_fallback_collisionless"]) and solver is not None and solver.discrete_eq:
+            if solver.backend.deq_counts()[1] > 0:
+                raise ScopeError("a cell's discrete equilibrium failed (collisionless fallback)")
 
     # ---- pieces --------------------------------------------------------------------------------------------------
     def moments(self, f):
@@ -157,6 +164,92 @@ class SteadyMap:
         q = 0.5 * ((f * w * c2)[..., None] * c).sum(1)
         return rho, u, T, p, q
 
+    def resolved(self, rho, u, T):
+        """deq_resolved (src/kinetic/discrete_equilibrium.hpp:35-48) of n states (no gradient)."""
+        u = u.detach().numpy()
+        T = T.detach().numpy()
+        ok = T > 0
+        for a in range(3):
+            ok &= ~(2.0 * math.pi ** 2 * T / (self.deq_d[a] * self.deq_d[a]) < self.deq_crit)
+            m1, m2 = self.deq_hi[a] - u[:, a], u[:, a] - self.deq_lo[a]
+            ok &= (m1 > 0) & (m2 > 0)
+            ok &= ~((m1 * m1 < 2.0 * T * self.deq_crit) | (m2 * m2 < 2.0 * T * self.deq_crit))
+        return torch.as_tensor(ok)
+
+    def discrete_maxwell(self, rho, u, T, poly=None, tol=None, max_iterations=None):
+        """The discrete Maxwellian E (n, nv) of n states and, with the Shakhov polynomial P (n, nv), the correction
+        gamma . psi (n, nv) (deq_* and deq_shakhov_correction, src/kinetic/discrete_equilibrium.hpp:56-188). The
+        Newton iteration is the solver's (initial beta, damped step, stopping rule: deq_newton_step :159-180,
+        deq_accept, kinetic_kernels.hpp:489-493), so beta is the one the forward solve used."""
+        tol = self.deq_tol if tol is None else tol
+        max_iterations = self.deq_maxit if max_iterations is None else max_iterations
+        c = self.xi[None, :, :] - u[:, None, :]
+        psi = torch.cat([torch.ones_like(c[..., :1]), c, 0.5 * (c * c).sum(-1, keepdim=True)], -1)  # (n, nv, 5)
+        w = self.w[None, :, None]
+        W = torch.stack([rho, torch.zeros_like(rho), torch.zeros_like(rho), torch.zeros_like(rho), 1.5 * rho * T], 1)
+        with torch.no_grad():
+            p0 = psi.detach()
+            Td, rd = T.detach(), rho.detach()
+            beta = torch.stack([torch.log(rd / (2.0 * math.pi * Td) ** 1.5), torch.zeros_like(Td),
+                                torch.zeros_like(Td), torch.zeros_like(Td), -1.0 / Td], 1)
+            Wd = W.detach()
+            prev = torch.full_like(Td, 1e300)
+            done = torch.zeros(len(Td), dtype=torch.bool)
+            for it in range(max_iterations):
+                E = torch.exp((p0 * beta[:, None, :]).sum(-1))
+                G = (w * E[..., None] * p0).sum(1) - Wd
+                su = rd * torch.sqrt(Td)
+                rel = torch.maximum(G[:, 0].abs() / rd, torch.maximum(G[:, 1:4].abs().amax(1) / su,
+                                                                      G[:, 4].abs() / (rd * Td)))
+                last = it + 1 == max_iterations
+                accept = ~done & ((rel < tol) | ((rel < 1e-4) & ((rel > 0.5 * prev) | last)))
+                done = done | accept
+                if bool(done.all()):
+                    break
+                J = torch.einsum("nq,nqa,nqb->nab", self.w[None, :] * E, p0, p0)
+                d = torch.linalg.solve(J, -G)
+                scale = torch.ones_like(Td)
+                big = d[:, 4].abs() > 0.5 * beta[:, 4].abs()
+                scale = torch.where(big, 0.5 * beta[:, 4].abs() / d[:, 4].abs(), scale)
+                scale = torch.where(d[:, 0].abs() * scale > 1.0, 1.0 / d[:, 0].abs(), scale)
+                step = ~done
+                beta = torch.where(step[:, None], beta + scale[:, None] * d, beta)
+                prev = torch.where(step, rel, prev)
+            if not bool(done.all()):
+                raise ScopeError("the discrete-equilibrium Newton iteration did not converge for a state")
+            E = torch.exp((p0 * beta[:, None, :]).sum(-1))
+            J = torch.einsum("nq,nqa,nqb->nab", self.w[None, :] * E, p0, p0)
+        # beta as a function of the state: the value of the accepted iterate, the derivative of the implicit
+        # function, dbeta = -J^-1 dG (G - G.detach() is zero in value and carries dG)
+        E0 = torch.exp((psi * beta[:, None, :]).sum(-1))
+        G = (w * E0[..., None] * psi).sum(1) - W
+        beta_g = beta - torch.linalg.solve(J, G - G.detach())
+        E = torch.exp((psi * beta_g[:, None, :]).sum(-1))
+        if poly is None:
+            return E, None
+        Jg = torch.einsum("nq,nqa,nqb->nab", self.w[None, :] * E, psi, psi)
+        r = (w * (E * poly)[..., None] * psi).sum(1)
+        gamma = -torch.linalg.solve(Jg, r)
+        return E, (psi * gamma[:, None, :]).sum(-1)
+
+    def equilibrium(self, rho, u, T, poly=None, tol=None):
+        """The equilibrium of n states: continuous where the grid resolves the state (or the continuous equilibrium is
+        chosen), discrete elsewhere; with poly, the Shakhov factor (1 + P + gamma . psi)."""
+        M = self.maxwell(rho, u, T)
+        fac = None if poly is None else 1.0 + poly
+        if not self.discrete:
+            return M if poly is None else M * fac
+        res = self.resolved(rho, u, T)
+        if bool(res.all()):
+            return M if poly is None else M * fac
+        idx = torch.nonzero(~res).ravel()
+        E, gp = self.discrete_maxwell(rho[idx], u[idx], T[idx], None if poly is None else poly[idx], tol=tol)
+        M = M.index_put((idx,), E)
+        if poly is None:
+            return M
+        fac = fac.index_put((idx,), fac[idx] + gp)
+        return M * fac
+
     def maxwell(self, rho, u, T):
         """rho, T: (n,), u: (n, 3) -> (n, nv)."""
         c = self.xi[None, :, :] - u[:, None, :]
@@ -169,7 +262,7 @@ class SteadyMap:
         c2 = (c * c).sum(-1)
         coef = torch.where(T < self.cold, torch.zeros_like(T), (1.0 - self.Pr) / (5.0 * (rho * T) * T))
         poly = coef[:, None] * (c * q[:, None, :]).sum(-1) * (c2 / T[:, None] - 5.0)
-        fS = self.maxwell(rho, u, T) * (1.0 + poly)
+        fS = self.equilibrium(rho, u, T, poly)
         coll = self.volume * p / (mu0 * T ** self.omega)
         return coll, fS, (rho, u, T, p, q)
 
@@ -197,7 +290,8 @@ class SteadyMap:
         use = wall | pres
         safe_T = torch.where(use, T_s, torch.ones_like(T_s))
         safe_rho = torch.where(use, rho_s, torch.ones_like(rho_s))
-        M = self.maxwell(safe_rho, u_s, safe_T)
+        # the inflow states corrected to their discrete Maxwellian (correct_inflow, kinetic_solver.cpp:103-114)
+        M = self.equilibrium(safe_rho, u_s, safe_T, tol=1e-10)
         rg = torch.zeros(nb, dtype=torch.float64)
         if len(self.wall_idx):
             rg = rg.index_put((self.wall_idx,), rho_gamma)

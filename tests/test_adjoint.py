@@ -19,7 +19,7 @@ from gsis_sim_b200.solver import KineticSolver
 
 
 def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="periodic_slab", limiter="venkatakrishnan",
-                 eps="relative", half=False, quarter=False, alpha=1.0):
+                 eps="relative", half=False, quarter=False, alpha=1.0, equilibrium="continuous"):
     """Pressure-driven channel (inlet p 1, outlet p 0.5, diffuse walls) in the adjoint's scope; `half`: symmetry
     plane at y = 0 instead of the lower wall; `quarter`: a duct quarter, symmetry planes at y = 0 and z = 0, walls at
     y = 1 and z = 0.7 (a flow that varies in y and z)."""
@@ -36,7 +36,7 @@ def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="perio
     if quarter:
         bcs.append(ks.BC("symz", "symmetry"))
     kp = ks.KineticParams(precision="fp64", pressure_boundary_reconstruction="cell", limiter=limiter,
-                          limiter_eps=eps, sweep_blocks=1, equilibrium="continuous")
+                          limiter_eps=eps, sweep_blocks=1, equilibrium=equilibrium)
     setup, host = ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, Kn=0.3), bcs,
                                          ks.VelocityGrid(n=nv), kp)
     if mu_scale != 1.0:
@@ -64,10 +64,16 @@ def _oracle_solution(**kw):
 
 
 @pytest.mark.timeout(600)
-def test_reference_adjoint_matches_finite_differences():
+@pytest.mark.parametrize("equilibrium", ["continuous", "discrete"])
+def test_reference_adjoint_matches_finite_differences(equilibrium):
+    """discrete: the reference default; on this 10^3 grid the Newton solve of the discrete Maxwellian is active in
+    every cell and for every wall and pressure-face inflow state."""
     from oracle import adjoint_ref as ar
 
-    sol, setup, host = _oracle_solution()
+    eq = dict(equilibrium=equilibrium)
+    sol, setup, host = _oracle_solution(**eq)
+    if equilibrium == "discrete":
+        assert sol.backend.deq_counts()[0] == sol.nc
     sm = ar.SteadyMap(setup, host)
     sm.check_scope(sol)
     f, rg = ar.state_of(sol)
@@ -78,19 +84,19 @@ def test_reference_adjoint_matches_finite_differences():
     assert abs(float(J) - sol.mass_flow()[2]) < 1e-14
     dmu, dTw, info = ar.adjoint_gradient(sm, f, rg)
     h = 1e-5
-    Jp = _oracle_solution(mu_scale=1 + h)[0].mass_flow()[2]
-    Jm = _oracle_solution(mu_scale=1 - h)[0].mass_flow()[2]
+    Jp = _oracle_solution(mu_scale=1 + h, **eq)[0].mass_flow()[2]
+    Jm = _oracle_solution(mu_scale=1 - h, **eq)[0].mass_flow()[2]
     fd_mu = (Jp - Jm) / (2 * h * sm.mu0)
     assert abs(dmu - fd_mu) <= 1e-6 * abs(fd_mu)
-    Jp = _oracle_solution(Tw=1 + h)[0].mass_flow()[2]
-    Jm = _oracle_solution(Tw=1 - h)[0].mass_flow()[2]
+    Jp = _oracle_solution(Tw=1 + h, **eq)[0].mass_flow()[2]
+    Jm = _oracle_solution(Tw=1 - h, **eq)[0].mass_flow()[2]
     fd_T = (Jp - Jm) / (2 * h)
     assert abs(dTw.sum() - fd_T) <= 1e-6 * abs(fd_T)
     assert np.all(dTw[sm.bkind.numpy() != ar.BC_DIFFUSE_WALL] == 0.0)
     # accommodation at alpha = 1, from below (alpha <= 1): second-order one-sided difference of Maxwell-wall solves
     ha = 1e-4
-    J1 = _oracle_solution(alpha=1 - ha)[0].mass_flow()[2]
-    J2 = _oracle_solution(alpha=1 - 2 * ha)[0].mass_flow()[2]
+    J1 = _oracle_solution(alpha=1 - ha, **eq)[0].mass_flow()[2]
+    J2 = _oracle_solution(alpha=1 - 2 * ha, **eq)[0].mass_flow()[2]
     fd_a = (3 * sol.mass_flow()[2] - 4 * J1 + J2) / (2 * ha)
     dal = info[4]
     assert abs(dal.sum() - fd_a) <= 1e-6 * abs(fd_a)

@@ -1,7 +1,8 @@
 """Discrete adjoint on the B200 (csrc/kin_adjoint.cu + gsis_sim_b200/adjoint.py) against the reference adjoint of
 oracle/adjoint_ref.py (the steady map transposed by torch autograd, itself pinned against finite differences in
 tests/test_adjoint.py), at the fixed point the B200 forward solver converged to:
-* the operator y^T dF/dx (and the objective term dJ/dx) for random adjoint states, to 1e-10;
+* the operator y^T dF/dx (and the objective term dJ/dx) for random adjoint states, to 1e-10, with the continuous
+  and with the discrete equilibrium (the Newton solve active in every cell and inflow state);
 * the converged adjoint's dM_dot/d mu_hat0, dM_dot/dT_w and dM_dot/d alpha (at alpha = 1), to 1e-8 against the
   reference adjoint and to 1e-5 against finite differences of the B200 forward solver (alpha: one-sided, through
   Maxwell-wall solves)."""
@@ -28,7 +29,8 @@ def _gpu_solution(**kw):
 # extremum (the cell's own value) and autograd splits the seed; both agree on every mirror-symmetric direction, which
 # the gradient test covers (side="symmetry").
 @pytest.mark.parametrize("kw", [dict(), dict(half=True), dict(limiter="none"), dict(eps="absolute"),
-                                dict(n=(5, 3, 3), quarter=True), dict(n=(5, 3, 3), quarter=True, limiter="none")])
+                                dict(n=(5, 3, 3), quarter=True), dict(n=(5, 3, 3), quarter=True, limiter="none"),
+                                dict(equilibrium="discrete"), dict(n=(5, 3, 3), quarter=True, equilibrium="discrete")])
 def test_gpu_adjoint_operator_matches_reference(kw):
     from gsis_sim_b200.adjoint import KineticAdjoint
     from oracle import adjoint_ref as ar
@@ -100,7 +102,7 @@ def test_gpu_adjoint_operator_on_tube_mesh():
 
 
 @pytest.mark.timeout(900)
-@pytest.mark.parametrize("kw", [dict(), dict(side="symmetry")])
+@pytest.mark.parametrize("kw", [dict(), dict(side="symmetry"), dict(equilibrium="discrete")])
 def test_gpu_adjoint_gradients_match_reference_and_finite_differences(kw):
     from gsis_sim_b200.adjoint import KineticAdjoint
     from oracle import adjoint_ref as ar
