@@ -277,6 +277,8 @@ struct Backend final : KinHandle {
   kin::View<S, P> pview{};  // mixed mode: the FP32 view of the gradient and the LU-SGS passes
   int32_t chunk = 0, partial_stride = 1, max_levels = 0, n_chains = 0, max_entries = 0;
   int32_t wstride = 0;  // row length of the chunk work arrays: the chunk rounded up to whole 64-byte windows
+  // kernel shapes of the two arithmetic types (read when the handle is created)
+  kin::KernelShape shape_m = kin::read_shape<M>(), shape_p = kin::read_shape<P>();
 
   // host copies
   std::vector<int32_t> perm, inv;
@@ -334,9 +336,8 @@ struct Backend final : KinHandle {
   DevBuf<int32_t> sub_cells, sub_entries, sub_start, sub_count;
   // resident block pass (k_sweep_resident): cell of every staged slot with its surface bit, the cells that have
   // out-of-block neighbours with those entries (k_lout), the kernel's shared memory and the device status word
-  enum SweepMode { kSweepWindow, kSweepResident, kSweepTiles, kSweepLegacy };
+  enum SweepMode { kSweepResident, kSweepTiles, kSweepLegacy };
   SweepMode sweep_mode = kSweepTiles;
-  int32_t window_ctas = 6;  // CTAs per SM the window kernel is compiled for
   int32_t resident_smem = 0, max_block_cells = 0, n_surf = 0;
   std::vector<uint8_t> h_surface;
   DevBuf<uint32_t> scells;
@@ -363,8 +364,10 @@ struct Backend final : KinHandle {
   // residual plus this defect, so the iteration's fixed point is the FP64 residual's zero
   DevBuf<S> defect;
   bool defect_valid = false;
-  bool defect_scheme = std::getenv("KIN_MIXED_RESIDUAL") == nullptr ||
-                       std::strcmp(std::getenv("KIN_MIXED_RESIDUAL"), "fp64") != 0;
+  // KIN_MIXED_RESIDUAL=defect selects the defect scheme; by default every sweep evaluates the FP64 residual (faster
+  // on B200: the FP32 residual is latency-bound like the FP64 one and the defect adds a read per sweep)
+  bool defect_scheme = std::getenv("KIN_MIXED_RESIDUAL") != nullptr &&
+                       std::strcmp(std::getenv("KIN_MIXED_RESIDUAL"), "defect") == 0;
   PhaseTimer timer;
   KinStepTimings timings{};
 
@@ -408,7 +411,7 @@ struct Backend final : KinHandle {
     // free device memory check for f (kinetic_backend_cuda.cpp:102-106)
     size_t free_b = 0, total_b = 0;
     KCUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t f_bytes = (kSplit ? 2 : 1) * sizeof(S) * static_cast<size_t>(nc) * static_cast<size_t>(nv);
+    const size_t f_bytes = (kSplit && defect_scheme ? 2 : 1) * sizeof(S) * static_cast<size_t>(nc) * static_cast<size_t>(nv);
     if (f_bytes + kMargin >= free_b)
       throw KinError(KIN_E_MEMORY, "distribution function of " + std::to_string(f_bytes / 1e9) +
                                        " GB does not fit in the free device memory of " +
@@ -462,7 +465,7 @@ struct Backend final : KinHandle {
     }
     f.alloc(ncs * static_cast<size_t>(nv));
     KCUDA(cudaMemsetAsync(f.p, 0, f.bytes(), stream));
-    if constexpr (kSplit) defect.alloc(ncs * static_cast<size_t>(nv));
+    if (kSplit && defect_scheme) defect.alloc(ncs * static_cast<size_t>(nv));
 
     constexpr int32_t kWindow = kin::SweepLaunch<S, P>::kWidth;
     wstride = (chunk + kWindow - 1) / kWindow * kWindow;
@@ -473,7 +476,7 @@ struct Backend final : KinHandle {
     gy.alloc(work);
     gz.alloc(work);
     r.alloc(work);
-    partial_stride = L::residual_tiles(chunk);
+    partial_stride = std::max(L::residual_tiles(chunk, shape_m.res_u), LP::residual_tiles(chunk, shape_p.res_u));
     partial.alloc(ncs * static_cast<size_t>(partial_stride));
     build_chunks();
     staging_alloc();
@@ -925,11 +928,7 @@ struct Backend final : KinHandle {
         sweep_mode = kSweepResident;
         staged_ne = 8;
       }
-      if (std::strncmp(e, "window", 6) == 0) {
-        sweep_mode = kSweepWindow;
-        if (std::strcmp(e, "window8e") == 0) staged_ne = 8;
-        else if (e[6] >= '4' && e[6] <= '8') window_ctas = e[6] - '0';
-      }
+
     }
   }
 
@@ -945,7 +944,7 @@ struct Backend final : KinHandle {
         if (s >= e) continue;
         for (int b = 0; b < n_blocks; ++b) {
           if (h_block_offsets[b + 1] == h_block_offsets[b]) continue;
-          const int tile = staged_ne != 0 ? 32 * kin::kernel_shape<P>().tile_u : kin::kSweepTile;
+          const int tile = staged_ne != 0 ? 32 * shape_p.tile_u : kin::kSweepTile;
           for (int t = s; t < e; t += tile)
             items.push_back(make_int4(gr.g * n_blocks + b, t - k0, std::min(t + tile, e) - k0, 0));
         }
@@ -1336,6 +1335,8 @@ struct Backend final : KinHandle {
     a.n_ritems = cp.n_ritems;
     a.scells = scells.p;
     a.err = err_word.p;
+    a.tile_u = shape_p.tile_u;
+    a.tile_blocks = shape_p.tile_blocks;
     a.resident_smem = resident_smem;
     a.max_block_cells = max_block_cells;
     a.k0 = cp.k0;
@@ -1348,9 +1349,7 @@ struct Backend final : KinHandle {
   // kernels then read R, and Delta f goes to gz / gy alternately. Other kernels: pass k writes Delta f into gz / gy
   // and reads pass k - 1 from the other one.
   void run_block_passes(const kin::View<S, P>& sv, const ChunkPlan& cp, int32_t stride, bool timed) {
-    const bool windowed = stride % kin::SweepLaunch<S, P>::kWidth == 0;
-    const bool resident = sweep_mode == kSweepResident && windowed;
-    const bool window = sweep_mode == kSweepWindow && windowed;
+    const bool resident = sweep_mode == kSweepResident && stride % kin::SweepLaunch<S, P>::kWidth == 0;
     S* prev = nullptr;
     for (int pass = 0; pass < block_passes; ++pass) {
       const bool first = pass == 0, last = pass + 1 == block_passes;
@@ -1371,9 +1370,6 @@ struct Backend final : KinHandle {
         }
         if (timed) timer.begin(PhaseTimer::kForward, stream);
         kin::SweepLaunch<S, P>::resident(sv, a, first, last, stream);
-      } else if (window) {
-        if (timed) timer.begin(PhaseTimer::kForward, stream);
-        kin::SweepLaunch<S, P>::window(sv, a, first, window_ctas, stream);
       } else {
         if (timed) timer.begin(PhaseTimer::kForward, stream);
         LP::sweep_pass(sv, a, stream);
@@ -1401,10 +1397,12 @@ struct Backend final : KinHandle {
     KCUDA(cudaMemsetAsync(residual_cell.p, 0, residual_cell.bytes(), stream));
     for (const auto& cp : chunks) {
       kin::Chunk<S> ch{cp->k0, cp->kc, wstride, gx.p, gy.p, gz.p, r.p};
+      ch.shape = shape_p;
       timer.begin(PhaseTimer::kGradient, stream);
       LP::gradient(sweep_view(), ch, stream);
       launched();
       timer.end(stream);
+      ch.shape = shape_m;
       timer.begin(PhaseTimer::kResidual, stream);
       if (kSplit && !defect_scheme) {
         L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);
@@ -1413,6 +1411,7 @@ struct Backend final : KinHandle {
         // mixed precision: FP64 residual and the FP32 one's defect at the iteration's first sweep, FP32 residual +
         // defect at the inner sweeps after it
         kin::Chunk<S> cd = ch;
+        cd.shape = shape_p;
         cd.defect = defect.p;
         if (!defect_valid) {
           L::residual(view, ch, partial.p, partial_stride, residual_cell.p, stream);

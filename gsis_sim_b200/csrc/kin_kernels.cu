@@ -4,7 +4,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <initializer_list>
 #include <type_traits>
+#include <utility>
 
 #include "kin_kernels.cuh"
 #include "kin_launch.h"
@@ -1363,50 +1365,70 @@ void Launch<S, M>::internal_face_flux(const View<S, M>& v, const int32_t* cells,
 }
 
 // ---- kernel shapes: velocities per thread x CTAs per SM of the gradient, residual and LU-SGS tile kernels -------
+// measured on the 134,528-cell tube, 32^3 (FP64 and the mixed precision's FP32 gradient / sweeps)
 template <>
 KernelShape default_shape<double>() {
-  return {4, 2, 2, 3, 2, 6};
+  return {4, 2, 1, 6, 2, 6};
 }
 template <>
 KernelShape default_shape<float>() {
-  return {4, 3, 2, 4, 4, 6};
+  return {4, 3, 2, 6, 4, 6};
 }
 
 template <class M>
-const KernelShape& kernel_shape() {
-  // KIN_SHAPE = "res=UxB,grad=UxB,tile=UxB" selects another compiled shape (all give the same results)
-  static const KernelShape shape = [] {
-    KernelShape k = default_shape<M>();
-    if (const char* e = std::getenv("KIN_SHAPE")) {
-      std::string str(e);
-      auto pick = [&](const char* key, int& uu, int& bb) {
-        const size_t pos = str.find(key);
-        if (pos == std::string::npos) return;
-        int a = 0, b2 = 0;
-        if (std::sscanf(str.c_str() + pos + std::strlen(key), "%dx%d", &a, &b2) == 2) {
-          uu = a;
-          bb = b2;
-        }
-      };
-      pick("res=", k.res_u, k.res_occ);
-      pick("grad=", k.grad_u, k.grad_occ);
-      pick("tile=", k.tile_u, k.tile_blocks);
-    }
-    return k;
-  }();
-  return shape;
+KernelShape read_shape() {
+  KernelShape k = default_shape<M>();
+  if (const char* e = std::getenv("KIN_SHAPE")) {
+    const std::string str(e);
+    auto pick = [&](const char* key, int32_t& uu, int32_t& bb) {
+      const size_t pos = str.find(key);
+      if (pos == std::string::npos) return;
+      int a = 0, b2 = 0;
+      if (std::sscanf(str.c_str() + pos + std::strlen(key), "%dx%d", &a, &b2) == 2) {
+        uu = a;
+        bb = b2;
+      }
+    };
+    pick("res=", k.res_u, k.res_occ);
+    pick("grad=", k.grad_u, k.grad_occ);
+    pick("tile=", k.tile_u, k.tile_blocks);
+  }
+  // only the compiled shapes (the launchers' candidates); anything else falls back to the default
+  const KernelShape d = default_shape<M>();
+  const bool fp64 = std::is_same<M, double>::value;
+  auto one_of = [](int32_t u, int32_t b, std::initializer_list<std::pair<int, int>> ok) {
+    for (const auto& p : ok)
+      if (p.first == u && p.second == b) return true;
+    return false;
+  };
+  if (!one_of(k.res_u, k.res_occ, fp64 ? std::initializer_list<std::pair<int, int>>{{4, 2}, {2, 3}}
+                                       : std::initializer_list<std::pair<int, int>>{{4, 3}, {4, 4}})) {
+    k.res_u = d.res_u;
+    k.res_occ = d.res_occ;
+  }
+  if (!one_of(k.grad_u, k.grad_occ, fp64 ? std::initializer_list<std::pair<int, int>>{{1, 6}, {2, 3}}
+                                         : std::initializer_list<std::pair<int, int>>{{2, 6}, {2, 4}})) {
+    k.grad_u = d.grad_u;
+    k.grad_occ = d.grad_occ;
+  }
+  if (!one_of(k.tile_u, k.tile_blocks, fp64 ? std::initializer_list<std::pair<int, int>>{{2, 6}, {4, 4}}
+                                            : std::initializer_list<std::pair<int, int>>{{4, 6}, {2, 8}})) {
+    k.tile_u = d.tile_u;
+    k.tile_blocks = d.tile_blocks;
+  }
+  return k;
 }
-template const KernelShape& kernel_shape<double>();
-template const KernelShape& kernel_shape<float>();
+template KernelShape read_shape<double>();
+template KernelShape read_shape<float>();
 
 template <class S, class M>
-int Launch<S, M>::residual_tiles(int kc) {
-  return ceil_div(kc, kTileThreads * kernel_shape<M>().res_u) * (kTileThreads / 32);
+int Launch<S, M>::residual_tiles(int kc, int res_u) {
+  return ceil_div(kc, kTileThreads * res_u) * (kTileThreads / 32);
 }
 
 template <class S, class M, int NE>
 static void launch_gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st) {
-  const KernelShape& k = kernel_shape<M>();
+  const KernelShape& k = ch.shape;
 #define KIN_GRAD(U, B)                                                                                           \
   if (k.grad_u == U && k.grad_occ == B) {                                                                        \
     const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * U));                       \
@@ -1414,16 +1436,13 @@ static void launch_gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_
     return;                                                                                                      \
   }
   if constexpr (std::is_same<S, M>::value && std::is_same<M, double>::value) {
-    KIN_GRAD(1, 4)
-    KIN_GRAD(1, 6)
-    KIN_GRAD(2, 4)
+    KIN_GRAD(2, 3)
   }
   if constexpr (std::is_same<S, M>::value && std::is_same<M, float>::value) {
-    KIN_GRAD(4, 3)
-    KIN_GRAD(2, 6)
+    KIN_GRAD(2, 4)
   }
 #undef KIN_GRAD
-  constexpr int U = std::is_same<M, double>::value ? 2 : 2, B = std::is_same<M, double>::value ? 3 : 4;
+  constexpr int U = std::is_same<M, double>::value ? 1 : 2, B = 6;
   const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * U));
   k_gradient<S, M, NE, U, B><<<grid, kTileThreads, 0, st>>>(v, ch);
 }
@@ -1440,7 +1459,7 @@ void Launch<S, M>::gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_
 template <class S, class M, int NE>
 static void launch_residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
                             cudaStream_t st) {
-  const KernelShape& k = kernel_shape<M>();
+  const KernelShape& k = ch.shape;
 #define KIN_RES(U, B)                                                                                            \
   if (k.res_u == U && k.res_occ == B) {                                                                          \
     const dim3 grid(ceil_div(v.n_cells, kCellsPerCta), ceil_div(ch.kc, kTileThreads * U));                       \
@@ -1449,10 +1468,8 @@ static void launch_residual(const View<S, M>& v, const Chunk<S>& ch, double* par
   }
   if constexpr (std::is_same<M, double>::value) {
     KIN_RES(2, 3)
-    KIN_RES(2, 4)
   } else {
     KIN_RES(4, 4)
-    KIN_RES(2, 6)
   }
 #undef KIN_RES
   constexpr int U = 4, B = std::is_same<M, double>::value ? 2 : 3;
@@ -1469,25 +1486,22 @@ void Launch<S, M>::residual(const View<S, M>& v, const Chunk<S>& ch, double* par
   else
     launch_residual<S, M, 0>(v, ch, partial, partial_stride, st);
   if (ch.defect_mode == kDefectStore) return;  // no sums of its own: the FP64 residual's stand
-  k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride, residual_tiles(ch.kc),
+  k_residual_reduce<<<ceil_div(v.n_cells, 256), 256, 0, st>>>(partial, partial_stride,
+                                                             residual_tiles(ch.kc, ch.shape.res_u),
                                                              residual_cell, v.n_cells);
 }
 
 template <class S, class M, int NE, bool First>
 static void launch_tiles(const View<S, M>& v, const SweepArgs<S, M>& a, cudaStream_t st) {
-  const KernelShape& k = kernel_shape<M>();
 #define KIN_TILE(KU, KB)                                                                                         \
-  if (k.tile_u == KU && k.tile_blocks == KB) {                                                                   \
+  if (a.tile_u == KU && a.tile_blocks == KB) {                                                                   \
     k_sweep_tiles<S, M, NE, First, KU, KB><<<a.n_items, kTileThreadsSweep, 0, st>>>(v, a);                       \
     return;                                                                                                      \
   }
   if constexpr (std::is_same<S, M>::value && std::is_same<M, double>::value) {
-    KIN_TILE(2, 8)
     KIN_TILE(4, 4)
-    KIN_TILE(1, 8)
   }
   if constexpr (std::is_same<S, M>::value && std::is_same<M, float>::value) {
-    KIN_TILE(4, 8)
     KIN_TILE(2, 8)
   }
 #undef KIN_TILE

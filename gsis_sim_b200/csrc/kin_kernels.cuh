@@ -98,6 +98,11 @@ struct View {
   DeqTensor dq_tensor;  // the same grid factored per axis (n[0] == 0 when it is not a tensor grid)
 };
 
+// velocities per thread x resident CTAs per SM of the gradient, residual and LU-SGS tile kernels
+struct KernelShape {
+  int32_t res_u, res_occ, grad_u, grad_occ, tile_u, tile_blocks;
+};
+
 template <class S>
 struct Chunk {
   int32_t k0, kc, stride;
@@ -109,6 +114,7 @@ struct Chunk {
   // the FP64 one at the iteration's first sweep
   S* defect = nullptr;
   int32_t defect_mode = 0;
+  KernelShape shape{};  // of the kernel the chunk is given to (gradient or residual)
 };
 enum : int32_t { kDefectNone = 0, kDefectStore = 1, kDefectApply = 2 };
 

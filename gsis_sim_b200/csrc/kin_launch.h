@@ -65,6 +65,7 @@ struct SweepArgs {
   const uint32_t* scells;       // cell of every sprog slot | 1 << 31 when the cell has an out-of-block neighbour
   const S* Rs;                  // passes after the first: R + out-of-block coupling of the surface cells (k_lout)
   int32_t* err;                 // device status word (kSweepErrStaging: a staging wait gave up)
+  int32_t tile_u, tile_blocks;  // shape of k_sweep_tiles (velocities per thread, CTAs per SM)
   int32_t resident_smem;        // dynamic shared memory of k_sweep_resident in bytes (0: not usable)
   int32_t max_block_cells;      // largest RCB block (rows of the resident window)
 };
@@ -91,18 +92,14 @@ struct SweepLaunch {
   static int smem_bytes(int max_block_cells);                       // dynamic shared memory, 0 if too large
   static void resident(const View<S, P>& v, const SweepArgs<S, P>& a, bool first, bool last, cudaStream_t st);
   static void lout(const View<S, P>& v, const LoutArgs<S, P>& a, cudaStream_t st);
-  // one block pass, one (cell, velocity) per thread per step, Delta f* through L2 (k_sweep_window)
-  static void window(const View<S, P>& v, const SweepArgs<S, P>& a, bool first, int ctas_per_sm, cudaStream_t st);
 };
 
-// velocities per thread x resident CTAs per SM of the gradient, residual and LU-SGS tile kernels (per arithmetic type)
-struct KernelShape {
-  int res_u, res_occ, grad_u, grad_occ, tile_u, tile_blocks;
-};
+// the kernel shapes of an arithmetic type: the measured defaults, or another compiled shape named by the environment
+// variable KIN_SHAPE ("res=UxB,grad=UxB,tile=UxB"; read when a handle is created)
 template <class M>
 KernelShape default_shape();
 template <class M>
-const KernelShape& kernel_shape();
+KernelShape read_shape();
 
 constexpr int kStageCells = 64;     // cells of one staged sub-level
 constexpr int kStageEntries = 384;  // stencil entries of one staged sub-level
@@ -124,7 +121,7 @@ struct Launch {
   static void boundary_sums(const View<S, M>& v, double* out, cudaStream_t st);
   static void internal_face_flux(const View<S, M>& v, const int32_t* cells, const int32_t* entries, double* out, int n,
                                  cudaStream_t st);
-  static int residual_tiles(int kc);
+  static int residual_tiles(int kc, int res_u);
   static void gradient(const View<S, M>& v, const Chunk<S>& ch, cudaStream_t st);
   static void residual(const View<S, M>& v, const Chunk<S>& ch, double* partial, int partial_stride,
                        double* residual_cell, cudaStream_t st);

@@ -260,134 +260,6 @@ __global__ void __launch_bounds__(kResThreads, 1) k_sweep_resident(View<S, P> v,
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// k_sweep_window: one LU-SGS block pass of one chain for one 64-byte velocity window, one (cell, velocity) per
-// thread per step, several CTAs per SM.
-// The window is the resident kernel's (8 FP64 or 16 FP32 velocities), but Delta f* and Delta f go to the work array
-// in global memory: at 6-8 CTAs per SM the chains in flight hold about (CTAs per SM) x 148 x block cells x 64 bytes
-// of it, which stays in the 126 MB L2, so the backward reads Delta f* back from L2. Per step every thread issues
-// all loads of its (cell, velocity) first (the in-block neighbours' Delta f*, R or Delta f*, the previous pass at
-// out-of-block neighbours, f in the last pass), then accumulates entry by entry in CSR order with the reference's
-// arithmetic (sweep_forward_cell / sweep_backward_cell, src/kinetic/kinetic_kernels.hpp:289-358). The next
-// sub-level's program and stencil entries are copied into shared memory with cp.async while the current one
-// computes (double buffer, one barrier per step).
-// ---------------------------------------------------------------------------------------------------------
-constexpr int kWinThreads = 256;
-
-__device__ __forceinline__ void cp_async_16(void* smem, const void* gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all_groups() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// copy sub-level l (absolute bounds in sh_sc / sh_se) of the staged schedule into dst (every thread its share)
-template <class S, class P>
-__device__ __forceinline__ void window_stage(const SweepArgs<S, P>& a, const int32_t* sh_sc, const int32_t* sh_se,
-                                             int l, ResidentStage<P>* dst) {
-  constexpr int kWords = static_cast<int>(sizeof(StageE<P>) / 16);
-  const int p0 = sh_sc[l], np = sh_sc[l + 1] - p0;
-  const int e0 = sh_se[l], ne = sh_se[l + 1] - e0;
-  const int n16 = np + ne * kWords;
-  const char* src_e = reinterpret_cast<const char*>(a.sse + e0);
-  char* dst_e = reinterpret_cast<char*>(dst->se);
-  for (int k = threadIdx.x; k < n16; k += kWinThreads) {
-    if (k < np) {
-      cp_async_16(&dst->prog[k], a.sprog + p0 + k);
-    } else {
-      const int w = k - np;
-      cp_async_16(dst_e + 16 * w, src_e + 16 * static_cast<int64_t>(w));
-    }
-  }
-  cp_async_commit_group();
-}
-
-template <class S, class P, int NE, bool First, int KB>
-__global__ void __launch_bounds__(kWinThreads, KB) k_sweep_window(View<S, P> v, SweepArgs<S, P> a) {
-  constexpr int V = 64 / static_cast<int>(sizeof(S));
-  constexpr int kRows = kWinThreads / V;  // cell slots of one round of the threads
-  __shared__ __align__(16) ResidentStage<P> buf[2];
-  __shared__ int32_t sh_sc[kMaxSubLevels + 1], sh_se[kMaxSubLevels + 1];
-  const int4 it = a.ritems[blockIdx.x];  // (chain, window start, first valid, end valid)
-  const int chain = it.x, wb = it.y;
-  const int nsub = a.sub_count[chain];
-  if (nsub <= 0) return;
-  const int s0 = a.sub_start[chain];
-  const int tid = threadIdx.x;
-  const int u = tid % V, slot0 = tid / V;
-  const bool act = wb + u >= it.z && wb + u < it.w;
-  const int t = wb + u;  // chunk-local velocity of this thread
-  const int q = a.k0 + (act ? t : it.z);
-  const P x = v.xi_x[q], y = v.xi_y[q], z = v.xi_z[q];
-  for (int k = tid; k <= nsub; k += kWinThreads) {
-    sh_sc[k] = a.sub_cells[s0 + k];
-    sh_se[k] = a.sub_entries[s0 + k];
-  }
-  __syncthreads();
-  window_stage(a, sh_sc, sh_se, 0, &buf[0]);
-  cp_async_wait_all_groups();
-  __syncthreads();
-  const int nsteps = 2 * nsub;
-  for (int s = 0; s < nsteps; ++s) {
-    const ResidentStage<P>& cur = buf[s & 1];
-    if (s + 1 < nsteps) window_stage(a, sh_sc, sh_se, s + 1 < nsub ? s + 1 : nsteps - 2 - s, &buf[(s + 1) & 1]);
-    const int l = s < nsub ? s : nsteps - 1 - s;
-    const int ncl = sh_sc[l + 1] - sh_sc[l];
-    const bool fwd = s < nsub;
-    if (act) {
-      for (int k = slot0; k < ncl; k += kRows) {
-        const int4 p = cur.prog[k];
-        const int64_t crow = static_cast<int64_t>(p.x) * a.stride + t;
-        // every load of this (cell, velocity) first
-        P val[NE];
-#pragma unroll
-        for (int j = 0; j < NE; ++j) {
-          const uint32_t code = j < p.z ? cur.se[p.y + j].code : 0u;
-          const uint32_t kind = code >> kKindShift;
-          const int64_t row = static_cast<int64_t>(code & kIndexMask) * a.stride + t;
-          if (fwd) {
-            const bool load = kind == kKindLower || (!First && kind == kKindOther);
-            val[j] = load ? static_cast<P>((kind == kKindLower ? a.out : a.dprev)[row]) : P(0);
-          } else {
-            val[j] = kind == kKindUpper ? static_cast<P>(a.out[row]) : P(0);
-          }
-        }
-        const P own = static_cast<P>(fwd ? __ldcs(a.R + crow) : a.out[crow]);
-        const int64_t frow = static_cast<int64_t>(p.x) * v.nv + a.k0 + t;
-        const P fv = (!fwd && a.update_f) ? static_cast<P>(__ldcs(v.f + frow)) : P(0);
-        const P diag = v.cp[p.x].diag;
-        P ap = P(0), cpl = P(0), ext = P(0);  // sum a+, in-block coupling, am_out (first pass) or Lout
-#pragma unroll
-        for (int j = 0; j < NE; ++j) {
-          if (j >= p.z) break;
-          const StageE<P>& e = cur.se[p.y + j];
-          const uint32_t kind = e.code >> kKindShift;
-          if (kind == kKindPeriodic) continue;
-          const P af = x * e.s[0] + y * e.s[1] + z * e.s[2];
-          ap += pos_part_r(af);
-          if (kind == (fwd ? kKindLower : kKindUpper)) {
-            cpl += neg_part_r(af) * val[j];
-          } else if (kind == kKindOther) {
-            if (First) ext -= neg_part_r(af);
-            else if (fwd) ext += neg_part_r(af) * val[j];
-          }
-        }
-        if (fwd) {
-          const P am_out = First ? ext : P(0), Lout = First ? P(0) : ext;
-          const P D = diag + v.diag_scale * ap + v.interface_damping * am_out;
-          a.out[crow] = static_cast<S>((-own - Lout - cpl) / D);
-        } else {
-          const P D = diag + v.diag_scale * ap + v.interface_damping * (First ? ext : P(0));
-          const P df = own - cpl / D;
-          a.out[crow] = static_cast<S>(df);
-          if (a.update_f) __stcs(v.f + frow, static_cast<S>(fv + df));
-        }
-      }
-    }
-    cp_async_wait_all_groups();
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------------------------------------
 // k_lout: R + out-of-block upwind coupling of the previous pass for the cells that have out-of-block neighbours
 // (the Lout of sweep_forward_cell, src/kinetic/kinetic_kernels.hpp:289-324, in CSR order)
 // grid: (groups of kLoutCells surface cells, velocity tiles of kLoutThreads * kLoutU)
@@ -480,30 +352,6 @@ void SweepLaunch<S, P>::resident(const View<S, P>& v, const SweepArgs<S, P>& a, 
     KIN_RES(8)
   }
 #undef KIN_RES
-}
-
-template <class S, class P>
-void SweepLaunch<S, P>::window(const View<S, P>& v, const SweepArgs<S, P>& a, bool first, int ctas_per_sm,
-                               cudaStream_t st) {
-  if (a.n_ritems <= 0) return;
-#define KIN_WIN(NE, KB)                                                                           \
-  if (first) k_sweep_window<S, P, NE, true, KB><<<a.n_ritems, kWinThreads, 0, st>>>(v, a);      \
-  else k_sweep_window<S, P, NE, false, KB><<<a.n_ritems, kWinThreads, 0, st>>>(v, a);
-#define KIN_WIN_OCC(NE)       \
-  if (ctas_per_sm <= 4) {     \
-    KIN_WIN(NE, 4)            \
-  } else if (ctas_per_sm <= 6) { \
-    KIN_WIN(NE, 6)            \
-  } else {                    \
-    KIN_WIN(NE, 8)            \
-  }
-  if (a.staged_ne == 6) {
-    KIN_WIN_OCC(6)
-  } else {
-    KIN_WIN_OCC(8)
-  }
-#undef KIN_WIN_OCC
-#undef KIN_WIN
 }
 
 template <class S, class P>

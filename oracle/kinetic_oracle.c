@@ -252,6 +252,7 @@ struct OrcHandle {
      parameters (or f) changed; the inner sweeps after it run the FP32 residual plus this defect */
   float* defect;
   int defect_valid;
+  int defect_scheme; /* KIN_MIXED_RESIDUAL=defect at creation; else the FP64 residual at every sweep */
   char err[512];
 };
 
@@ -330,7 +331,9 @@ int orc_create(const KinSetupDesc* d, OrcHandle** out) {
   else {
     h->state = create_mix(d);
     h->fast = mixed_fast_state(d, (State_mix*)h->state);
-    h->defect = (float*)calloc((size_t)d->n_cells * (size_t)d->nv, sizeof(float));
+    const char* mode = getenv("KIN_MIXED_RESIDUAL");
+    h->defect_scheme = mode != NULL && strcmp(mode, "defect") == 0;
+    if (h->defect_scheme) h->defect = (float*)calloc((size_t)d->n_cells * (size_t)d->nv, sizeof(float));
   }
   *out = h;
   return KIN_OK;
@@ -422,7 +425,9 @@ int orc_sweep(OrcHandle* h, double* res, int64_t n) {
     for (int k0 = 0; k0 < m->nv; k0 += m->chunk) {
       const int kc = m->chunk < m->nv - k0 ? m->chunk : m->nv - k0;
       sweep_gradient_f32(h->fast, k0, kc);
-      if (!h->defect_valid) {
+      if (!h->defect_scheme) {
+        sweep_residual_mix(m, k0, kc, res);
+      } else if (!h->defect_valid) {
         /* first sweep of the iteration: the FP64 residual, and the defect of the FP32 one at the same f */
         sweep_residual_mix(m, k0, kc, res);
         sweep_residual_defect_f32(h->fast, k0, kc, res, h->defect, 1);

@@ -53,12 +53,14 @@ def test_gpu_deterministic_and_chunk_independent(B200Backend, name):
 
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "maxwell_wall_fp64", "couette_fp64"])
-def test_gpu_mixed_precision_matches_oracle(B200Backend, name):
+@pytest.mark.parametrize("scheme", ["fp64", "defect"])
+def test_gpu_mixed_precision_matches_oracle(B200Backend, name, scheme, monkeypatch):
     """Mixed precision (f, gradients and LU-SGS passes in FP32; residual, moments and sums in FP64) against the
     same scheme on the CPU oracle. Quantities computed in FP64 from the same FP32 f agree to 1e-6; the FP32
     arithmetic of the sweeps gets the reference's FP32 tolerance (FMA contraction differs between the two)."""
     from oracle.kinetic_oracle import OracleBackend
 
+    monkeypatch.setenv("KIN_MIXED_RESIDUAL", scheme)  # both the B200 backend and the oracle read it
     z, setup = common.load(name)
     with B200Backend(setup, precision="mixed") as be:
         g = common.run_op_sequence(be, z)
@@ -74,13 +76,16 @@ def test_gpu_mixed_precision_matches_oracle(B200Backend, name):
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "couette_fp64", "tet_positivity_fp32", "dir13_fp32", "vacuum_tube_fp64"])
 def test_gpu_sweep_kernels_agree(B200Backend, name, monkeypatch):
-    """Every LU-SGS block-pass kernel gives the same sweep: the window kernel (default; 4, 6 and 8 CTAs per SM, 6-
-    and 8-entry bounds), the resident kernel (6 and 8), the staged tile kernel (6 and 8) and the plain level kernel."""
+    """Every LU-SGS block-pass kernel gives the same sweep: the staged tile kernel (default; 6- and 8-entry bounds,
+    and another compiled tile shape), the resident kernel (6 and 8) and the plain level kernel."""
     z, setup = common.load(name)
     runs = {}
-    kernels = ["auto", "window4", "window8", "window8e", "resident", "resident8", "tiles", "legacy", "staged8"]
+    kernels = ["auto", "staged8", "shape", "resident", "resident8", "legacy"]
     for kernel in kernels:
         monkeypatch.setenv("KIN_SWEEP_KERNEL", kernel)
+        if kernel == "shape":  # the other compiled tile shape of the arithmetic type (velocities per thread x CTAs)
+            monkeypatch.setenv("KIN_SWEEP_KERNEL", "auto")
+            monkeypatch.setenv("KIN_SHAPE", "tile=4x4" if common.precision_of(setup) == "fp64" else "tile=2x8")
         with B200Backend(setup) as be:
             runs[kernel] = common.run_op_sequence(be, z)
     tol = 1e-14 if common.precision_of(setup) == "fp64" else 1e-6

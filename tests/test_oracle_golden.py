@@ -31,10 +31,13 @@ def test_oracle_chunk_independence(name):
 
 
 @pytest.mark.parametrize("name", ["mixed_strong_fp64", "vacuum_tube_fp64"])
-def test_oracle_mixed_precision_within_fp32_of_fp64(name):
-    """Mixed precision (f in FP32; FP64 residual at the first sweep after the cell parameters change, FP32 residual
-    plus the stored defect at the sweeps after it) stays within the FP32 tolerance of the FP64 reference through the
-    golden operation sequence, whose second sweep runs on the defect."""
+@pytest.mark.parametrize("scheme", ["fp64", "defect"])
+def test_oracle_mixed_precision_within_fp32_of_fp64(name, scheme, monkeypatch):
+    """Mixed precision (f in FP32, FP32 gradient and sweeps) stays within the FP32 tolerance of the FP64 reference
+    through the golden operation sequence, with the FP64 residual at every sweep (default) and with the defect scheme
+    (KIN_MIXED_RESIDUAL=defect: FP64 residual at the first sweep after the cell parameters change, FP32 residual plus
+    the stored defect at the sweeps after it; the sequence's second sweep runs on the defect)."""
+    monkeypatch.setenv("KIN_MIXED_RESIDUAL", scheme)
     z, setup = common.load(name)
     out = common.run_op_sequence(OracleBackend(setup, precision="mixed"), z)
     tol = common.TOL["fp32"]
