@@ -354,6 +354,113 @@ def converge_channel(setup, host, local, tol, max_iters):
     return sol, time.perf_counter() - t0, it
 
 
+def wall_temperature_field(prob, seed=2026, sigma=0.02):
+    """Seeded N(1, sigma^2) temperature per diffuse wall face (the order of prob.wall_faces)."""
+    import numpy as np
+
+    return 1.0 + sigma * np.random.default_rng(seed).standard_normal(len(prob.wall_faces))
+
+
+def tube_adjoint(args, local):
+    """dM_dot/dT_w per wall face on the tube (delta 10, --nv^3 velocities, the reference's discrete equilibrium,
+    "cell" pressure-boundary reconstruction) at a seeded N(1, 0.02^2) wall-temperature field, by the mixed-precision
+    adjoint: the mixed forward solve to --fwd-tol and the mixed adjoint solve to --adj-tol, timed through the public
+    host loops (wall clock). The gradient is checked against central differences of FP64 forward solves along
+    --fd-directions seeded random unit directions of the per-face field, on the coarse tube of the same geometry
+    (--fd-mesh coarse: 1,312 cells; a full-size FP64 solve takes minutes, 16 of them hours) or on the same mesh."""
+    import numpy as np
+    import torch
+
+    from gsis_sim_b200 import tube
+    from gsis_sim_b200.adjoint import KineticAdjoint, MassFlowProblem
+
+    torch.cuda.set_device(local)
+
+    def case(precision, mesh_kw):
+        return tube.tube_case(delta=10.0, nv=args.nv, precision=precision, pressure_boundary_reconstruction="cell",
+                              mesh_kw=mesh_kw)
+
+    def mixed_gradient(mesh_kw, timed):
+        setup, host = case("mixed", mesh_kw)
+        prob = MassFlowProblem(setup, host, tol=args.fwd_tol, max_iterations=args.max_iters, device=local)
+        Tw = wall_temperature_field(prob)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sol, J = prob.solve(prob.delta0, Tw)
+        torch.cuda.synchronize()
+        t_fwd = time.perf_counter() - t0
+        it_fwd = sol.iteration
+        t0 = time.perf_counter()
+        ka = KineticAdjoint(sol)
+        res = ka.solve(tol=args.adj_tol, max_iterations=args.adj_max_iters)
+        torch.cuda.synchronize()
+        t_adj = time.perf_counter() - t0
+        ka.close()
+        prob.release(sol)
+        out = {"cells": setup.n_cells, "velocities": setup.nv, "wall_faces": len(prob.wall_faces), "M_dot": J,
+               "forward_seconds": t_fwd, "forward_iterations": it_fwd, "adjoint_seconds": t_adj,
+               "adjoint_iterations": res.iterations, "adjoint_residual": res.residual,
+               "ratio": t_adj / t_fwd}
+        return out, res.dJ_dTw[prob.wall_faces].copy(), Tw, setup, host
+
+    if args.adj_mesh == "coarse":
+        mk_full = dict(COARSE_TUBE)
+    else:
+        mk_full = None if args.nx == 100 else {"n_x": args.nx}
+    main_run, g_main, _, _, _ = mixed_gradient(mk_full, True)
+    line = {"metric": "adjoint / forward wall-time ratio, mixed precision, dM_dot/dT_w per wall face",
+            "value": main_run["ratio"], "unit": "x", "higher_is_better": False, "dtype": DTYPES["mixed"],
+            "data": "synthetic", "run": main_run,
+            "dM_dot_dT_w": {"sum": float(g_main.sum()), "max_abs": float(np.abs(g_main).max())},
+            "config": {"workload": f"kinetic CIS, O-grid tube + reservoir {main_run['cells']} cells, inlet p 1 / "
+                                   f"outlet p 0.01, diffuse walls at T_w ~ N(1, 0.02^2) per face (seed 2026), "
+                                   f"delta 10, {args.nv}^3 velocities on [-5,5]^3, discrete equilibrium",
+                       "forward_tol": args.fwd_tol, "adjoint_tol": args.adj_tol}}
+    if args.fd_mesh != "none":
+        mk = dict(COARSE_TUBE) if args.fd_mesh == "coarse" else mk_full
+        if args.fd_mesh == "coarse" and args.adj_mesh != "coarse":
+            fd_run, g, Tw, _, _ = mixed_gradient(mk, False)
+        else:
+            fd_run, g, Tw = main_run, g_main, None
+        s64, h64 = case("fp64", mk)
+        prob = MassFlowProblem(s64, h64, tol=1e-12, max_iterations=max(args.max_iters, 4000), device=local)
+        if Tw is None:
+            Tw = wall_temperature_field(prob)
+        # the FP64 adjoint at the FP64 fixed point on the same mesh and field
+        t0 = time.perf_counter()
+        sol, _ = prob.solve(prob.delta0, Tw)
+        ka = KineticAdjoint(sol)
+        r64 = ka.solve(tol=1e-10, max_iterations=max(args.adj_max_iters, 4000))
+        ka.close()
+        prob.release(sol)
+        g64 = r64.dJ_dTw[prob.wall_faces]
+        line["fp64_adjoint"] = {"max_rel_difference": float(np.abs(g - g64).max() / np.abs(g64).max()),
+                                "sum_rel_difference": float(abs(g.sum() - g64.sum()) / abs(g64.sum())),
+                                "iterations": r64.iterations, "residual": r64.residual,
+                                "seconds": time.perf_counter() - t0}
+        rng = np.random.default_rng(7)
+        h = args.fd_tw_step
+        dirs = []
+        t0 = time.perf_counter()
+        for _ in range(args.fd_directions):
+            v = rng.standard_normal(len(prob.wall_faces))
+            v /= np.linalg.norm(v)
+            Js = []
+            for sgn in (1.0, -1.0):
+                sol, Jv = prob.solve(prob.delta0, Tw + sgn * h * v)
+                prob.release(sol)
+                Js.append(Jv)
+            fd = (Js[0] - Js[1]) / (2 * h)
+            ad = float(g @ v)
+            dirs.append({"adjoint": ad, "fd": fd, "rel_error": abs(ad - fd) / abs(fd)})
+        line["fd_check"] = {"mesh": "coarse tube (same geometry), 1,312 cells" if mk == COARSE_TUBE
+                            else "the tube above", "run": fd_run, "step": h, "directions": dirs,
+                            "max_rel_error": max(d["rel_error"] for d in dirs),
+                            "fd_seconds": time.perf_counter() - t0,
+                            "fd_solver": "FP64 forward, residual 1e-12, central differences"}
+    return line
+
+
 def run_adjoint(args, local):
     print(json.dumps(adjoint_ratio(args, local)), flush=True)
 
@@ -478,6 +585,16 @@ def main():
                     "set-up's inner_sweeps, as the forward)")
     ap.add_argument("--fwd-tol", type=float, default=1e-10)
     ap.add_argument("--adj-tol", type=float, default=1e-10)
+    # the tube adjoint in mixed precision (per-wall-face temperature gradient)
+    ap.add_argument("--tube-adjoint", action="store_true",
+                    help="mixed-precision adjoint of the tube with a seeded N(1, 0.02^2) wall-temperature field: "
+                    "adjoint / forward time on the tube (--nx, --nv), directional FP64 differences on the coarse tube")
+    ap.add_argument("--fd-directions", type=int, default=8)
+    ap.add_argument("--adj-mesh", default="full", choices=["full", "coarse"],
+                    help="mesh of the timed tube adjoint: the benchmark tube (--nx) or the 1,312-cell coarse tube")
+    ap.add_argument("--adj-max-iters", type=int, default=2000, help="outer iterations of the adjoint solve at most")
+    ap.add_argument("--fd-mesh", default="coarse", choices=["coarse", "same", "none"])
+    ap.add_argument("--fd-tw-step", type=float, default=1e-5, help="step of the directional wall-temperature differences")
     args = ap.parse_args()
 
     rank, ws, local = dist_init() if args.gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1 else (0, 1, 0)
@@ -491,6 +608,10 @@ def main():
     if args.adjoint:
         if rank == 0:
             run_adjoint(args, local)
+        return
+    if args.tube_adjoint:
+        if rank == 0:
+            print(json.dumps(tube_adjoint(args, local)), flush=True)
         return
 
     import torch
@@ -546,8 +667,7 @@ def main():
         dist.destroy_process_group()
 
 
-DTYPES = {"fp64": "f64", "fp32": "f32", "mixed": "f32 (f, gradient, LU-SGS, inner-sweep residual) / f64 (first residual, "
-          "sums)"}
+DTYPES = {"fp64": "f64", "fp32": "f32", "mixed": "f32 (f, gradient, LU-SGS) / f64 (residual, sums)"}
 
 
 def time_iterations(args, precision, ws=1, rank=0, local=0, steps=None, warmup=None, clocks=True):
@@ -636,6 +756,24 @@ def lout_bytes_per_unit(setup, s):
     return (2 * n_cells + n_entries) * s / nc
 
 
+def sweep_kernel_bytes(s, passes):
+    """The LU-SGS block-pass kernel the backend runs (KIN_SWEEP_KERNEL) and its algorithmic bytes per launch and
+    (cell, velocity), averaged over the passes of one inner sweep."""
+    sel = os.environ.get("KIN_SWEEP_KERNEL", "")
+    if sel.startswith("resident"):
+        # resident block pass: read R and write Delta f (2 s); the last pass reads R and reads and writes f (3 s);
+        # the out-of-block coupling of a later pass is the separate k_lout
+        return ("k_sweep_resident", (2 * s * (passes - 1) + 3 * s) / passes,
+                "read R, write Delta f; last pass read R, read + write f")
+    name = "k_sweep_pass" if sel == "legacy" else "k_sweep_tiles"
+    # first pass: read R, write Delta f (2 s); a middle pass also reads the previous pass (3 s); the last pass reads
+    # R and the previous pass and reads and writes f (4 s); a single pass reads R and reads and writes f (3 s)
+    if passes == 1:
+        return name, 3 * s, "read R, read + write f"
+    return (name, (2 * s + 3 * s * (passes - 2) + 4 * s) / passes,
+            "read R (+ previous pass), write Delta f; last pass read R + previous pass, read + write f")
+
+
 def kernel_rooflines(run, precision, steps, hbm):
     """Per kernel: device seconds per step, launches, algorithmic bytes per launch (per (cell, velocity) figure x the
     cells x velocities a launch processes) over its average launch time, against the measured HBM peak."""
@@ -647,16 +785,16 @@ def kernel_rooflines(run, precision, steps, hbm):
     kern = {}
     # gradient: read f, write the three components (4 s)
     kern["k_gradient"] = (t["gradient"], n_sweeps, 4 * s, "read f, write g_x, g_y, g_z")
-    # residual: read f, g_x, g_y, g_z, write R (5 s); mixed: first sweep FP64 residual (5 s) + FP32 defect store
-    # (read f, g, R; write the defect: 6 s), inner sweeps FP32 residual + defect (read f, g, defect; write R: 6 s)
-    if precision == "mixed":
+    # residual: read f, g_x, g_y, g_z, write R (5 s); the mixed defect scheme (KIN_MIXED_RESIDUAL=defect): first
+    # sweep FP64 residual (5 s) + defect store (read f, g, R; write the defect: 6 s), further sweeps FP32 residual +
+    # defect (read f, g, defect; write R: 6 s)
+    if precision == "mixed" and os.environ.get("KIN_MIXED_RESIDUAL", "") == "defect":
         kern["k_residual"] = (t["residual"], n_sweeps, (11 * s + 6 * s * (inner - 1)) / inner,
-                              "mixed: per inner sweep on average")
+                              "mixed defect scheme: per inner sweep on average")
     else:
         kern["k_residual"] = (t["residual"], n_sweeps, 5 * s, "read f, g_x, g_y, g_z, write R")
-    # resident block pass: read R and write Delta f (2 s); the last pass reads R and reads and writes f (3 s)
-    kern["k_sweep_resident"] = (t["sweep_forward"], n_sweeps * passes, (2 * s * (passes - 1) + 3 * s) / passes,
-                                "read R, write Delta f; last pass read R, read + write f")
+    name, b_pass, what = sweep_kernel_bytes(s, passes)
+    kern[name] = (t["sweep_forward"], n_sweeps * passes, b_pass, what)
     if t.get("sweep_backward", 0.0) > 0.0:
         # coupling of a later pass: read R and write R + Lout for the surface cells, read Delta f of their
         # out-of-block neighbours (per (cell, velocity) of the whole mesh: the surface share)
@@ -740,9 +878,17 @@ def gpu_baseline(args, run):
         nc, inner = case.setup.n_cells, case.inner_sweeps
         del case
         ours = {k: v / args.steps for k, v in run["timings"].items()}
+        # the reference times its forward and backward sweep kernels apart; here one kernel runs both (the
+        # coupling kernel of the resident variant is the backward slot), so the sweep is compared as a whole
+        def merged(d):
+            m = {k: v for k, v in d.items() if k not in ("sweep_forward", "sweep_backward")}
+            m["sweep"] = d.get("sweep_forward", 0.0) + d.get("sweep_backward", 0.0)
+            return m
+
+        ph_m, ours_m = merged(ph), merged(ours)
         out = {"kind": "reference CudaBackend rebuilt for sm_100a", "value": nc * args.nv ** 3 * inner / dt,
                "unit": "cell*velocity updates/s", "seconds_per_iteration": dt, "phase_seconds": ph,
-               "speedup_per_phase": {k: (ph[k] / ours[k]) if ours.get(k) else None for k in ph},
+               "speedup_per_phase": {k: (ph_m[k] / ours_m[k]) if ours_m.get(k) else None for k in ph_m},
                "speedup_iteration": dt / (run["wall_s"] / args.steps)}
         return out
     except Exception as e:  # the baseline is reported, not required

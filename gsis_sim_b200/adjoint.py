@@ -23,7 +23,13 @@ derivative goes through both solves by the implicit function theorem (gsis_sim_b
 the lambda sums at fixed (beta, gamma), the host the 5 x 5 chain). Inflow states of walls and pressure faces that
 the reference corrects to their discrete Maxwellian are differentiated through that correction the same way.
 
-Scope (`check_scope`): FP64 backend with one velocity chunk; a tensor velocity grid when the equilibrium is discrete
+Precision: FP64, or mixed (f of the converged mixed-precision solve stored in FP32). In mixed precision lambda and
+the transport seeds are stored in FP32 and the transposed block passes run in FP32, while O(y) is evaluated in FP64
+arithmetic from the stored values and every sum the host reads is FP64: the adjoint counterpart of the forward's
+FP64 residual with FP32 sweeps. Its fixed point holds to the FP32 storage of lambda (relative residual floor about
+1e-6 instead of 1e-12).
+
+Scope (`check_scope`): FP64 or mixed-precision backend with one velocity chunk; a tensor velocity grid when the equilibrium is discrete
 (every grid of the reference is one) and no failed Newton solve; diffuse walls, pressure inlets / outlets with
 pressure_boundary_reconstruction = "cell", vacuum, symmetry, periodic faces; no Maxwell walls, mass-flow inlets,
 positivity limiter or closed-domain scaling.
@@ -170,7 +176,7 @@ class AdjointResult:
 
 
 class KineticAdjoint:
-    """Adjoint of M_dot at the converged state of a KineticSolver whose backend is a B200Backend (FP64)."""
+    """Adjoint of M_dot at the converged state of a KineticSolver whose backend is a B200Backend (FP64 or mixed)."""
 
     def __init__(self, solver):
         self.sol = solver
@@ -261,8 +267,8 @@ class KineticAdjoint:
     def check_scope(self):
         sol = self.sol
         s, h = sol.s, sol.h
-        if int(s["precision"]) != abi.KIN_PREC_FP64:
-            raise AdjointScopeError("the adjoint needs precision = fp64")
+        if int(s["precision"]) not in (abi.KIN_PREC_FP64, abi.KIN_PREC_MIXED):
+            raise AdjointScopeError("the adjoint needs precision = fp64 or mixed")
         if int(s["positivity"]) != 0:
             raise AdjointScopeError("positivity limiter")
         if h.closed_domain:

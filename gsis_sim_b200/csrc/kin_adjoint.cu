@@ -1,4 +1,4 @@
-// Discrete adjoint of the converged CIS fixed point (FP64, sm_100a): the transposed-Jacobian kernels of
+// Discrete adjoint of the converged CIS fixed point (FP64 arithmetic, FP64 or FP32 storage; sm_100a): the transposed-Jacobian kernels of
 // kin_adjoint.h. The forward map they transpose is residual_value / limited_gradient / boundary_value_first_order
 // (src/kinetic/kinetic_kernels.hpp:145-278), make_cell_params (:451-471) and the boundary sums of the wall density
 // (src/kinetic/kinetic_cuda_kernels.cu:275-323, src/kinetic/kinetic_solver.cpp:280-335); every derivative below is
@@ -15,11 +15,18 @@ namespace {
 
 constexpr int kAdjThreads = 256;
 
-__device__ __forceinline__ double lam_at(const AdjView& a, int nv, int cell, int q) {
-  return a.lam[static_cast<int64_t>(cell) * nv + a.rev[q]];
+template <class S>
+__device__ __forceinline__ double lam_at(const AdjView<S>& a, int nv, int cell, int q) {
+  return static_cast<double>(a.lam[static_cast<int64_t>(cell) * nv + a.rev[q]]);
 }
 
-__device__ __forceinline__ double entry_value(const View<double, double>& v, const CsrE<double>& c, int cell, int q,
+template <class S>
+__device__ __forceinline__ double ld(const S* p, int64_t i) {
+  return static_cast<double>(p[i]);
+}
+
+template <class S>
+__device__ __forceinline__ double entry_value(const View<S, double>& v, const CsrE<double>& c, int cell, int q,
                                               double x, double y, double z, double fi) {
   return c.other >= 0 ? f_at(v, c.other, q) : boundary_value_first_order(v, c, cell, q, x, y, z, fi);
 }
@@ -29,7 +36,8 @@ __device__ __forceinline__ double entry_value(const View<double, double>& v, con
 // P = coef (c.q)(c^2 / T - 5). Discrete equilibrium (deq_flags > 0): f^S = E F, F = 1 + P + gamma . psi,
 // psi = (1, c, c^2 / 2), E = A exp(-B |xi - u'|^2) from the Newton solve: the derivative sums at fixed (beta, gamma)
 // and sum lambda E F psi, sum lambda E psi for the chain through the Newton and gamma solves (host).
-__global__ void __launch_bounds__(kAdjThreads) k_adj_cell(View<double, double> v, AdjView a, double* __restrict__ out) {
+template <class S>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_cell(View<S, double> v, AdjView<S> a, double* __restrict__ out) {
   __shared__ double sh[kAdjCellSums * (kAdjThreads / 32)];
   const int cell = blockIdx.x;
   const int nv = v.nv;
@@ -96,8 +104,10 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_cell(View<double, double> v
 
 // k_adj_transport: the transposed upwind flux and limited gradient at (cell, q). Writes the seeds that stay in the
 // cell (lfb), the gradient seed G_bar and the limiter-extremum seeds for the gathers of k_adj_gather / k_adj_faces.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_transport(View<double, double> v, AdjView a) {
-  const int cell = blockIdx.x;
+template <class S>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_transport(View<S, double> v, AdjView<S> a,
+                                                              const int32_t* __restrict__ cells) {
+  const int cell = cells != nullptr ? cells[blockIdx.x] : static_cast<int>(blockIdx.x);
   const int nv = v.nv;
   const int e0 = v.csr_off[cell], e1 = v.csr_off[cell + 1];
   const double coll = v.cp[cell].coll;
@@ -236,12 +246,12 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_transport(View<double, doub
     }
     lf -= sumc;
     const int64_t i = static_cast<int64_t>(cell) * nv + q;
-    a.lfb[i] = lf;
-    a.gbx[i] = gbx;
-    a.gby[i] = gby;
-    a.gbz[i] = gbz;
-    a.hmax[i] = hmx;
-    a.hmin[i] = hmn;
+    a.lfb[i] = static_cast<S>(lf);
+    a.gbx[i] = static_cast<S>(gbx);
+    a.gby[i] = static_cast<S>(gby);
+    a.gbz[i] = static_cast<S>(gbz);
+    a.hmax[i] = static_cast<S>(hmx);
+    a.hmin[i] = static_cast<S>(hmn);
     a.imax[i] = static_cast<int8_t>(amax);
     a.imin[i] = static_cast<int8_t>(amin);
   }
@@ -255,7 +265,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_transport(View<double, doub
 // alpha = 1 from A1 = sum_in a lambda f_spec (f_spec: the owner's reconstructed face value at the reflected
 // velocity), A2 = sum_in s_grad f_o(reflected) (the first-order specular value of the gradient) and
 // S_spec = sum_in w an f_spec.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<double, double> v, AdjView a, double* __restrict__ out) {
+template <class S>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<S, double> v, AdjView<S> a, double* __restrict__ out) {
   __shared__ double sh[kAdjFaceSums * (kAdjThreads / 32)];
   const int b = blockIdx.x;
   const int nv = v.nv;
@@ -279,8 +290,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<double, double> 
       if (ae >= 0.0) continue;
       const double wq = v.wts != nullptr ? v.wts[q] : v.weight;
       const int64_t i = static_cast<int64_t>(o) * nv + q;
-      const double seed = ae * (lam_at(a, nv, o, q) + wq * mu) + c.c[0] * a.gbx[i] + c.c[1] * a.gby[i] +
-                          c.c[2] * a.gbz[i] + (a.imax[i] == k ? a.hmax[i] : 0.0) + (a.imin[i] == k ? a.hmin[i] : 0.0);
+      const double seed = ae * (lam_at(a, nv, o, q) + wq * mu) + c.c[0] * ld(a.gbx, i) + c.c[1] * ld(a.gby, i) +
+                          c.c[2] * ld(a.gbz, i) + (a.imax[i] == k ? ld(a.hmax, i) : 0.0) +
+                          (a.imin[i] == k ? ld(a.hmin, i) : 0.0);
       const double M = maxwellian(m, x, y, z);
       const double cx = x - m.ux, cy = y - m.uy, cz = z - m.uz;
       const double c2 = cx * cx + cy * cy + cz * cz;
@@ -320,7 +332,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<double, double> 
 // k_adj_gather: O_f(y) at (cell, q) = the cell's own seeds + the neighbours' gradient and extremum seeds that point at
 // it + the mirrored half of the symmetry values + the moment expansion; stored at the reversed position. Per-cell
 // sum of squares into res_cell.
-__global__ void __launch_bounds__(kAdjThreads) k_adj_gather(View<double, double> v, AdjView a,
+template <class S>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_gather(View<S, double> v, AdjView<S> a,
                                                            double* __restrict__ res_cell) {
   __shared__ double sh[kAdjThreads / 32];
   const int cell = blockIdx.x;
@@ -333,7 +346,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_gather(View<double, double>
   double acc[1] = {0.0};
   for (int q = threadIdx.x; q < nv; q += kAdjThreads) {
     const int64_t i = static_cast<int64_t>(cell) * nv + q;
-    double r = a.lfb[i];
+    double r = ld(a.lfb, i);
     for (int e = e0; e < e1; ++e) {
       const CsrE<double>& c = v.csr[e];
       if (c.other >= 0) {
@@ -343,17 +356,17 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_gather(View<double, double>
         const CsrE<double>& cn = v.csr[eb];
         const int k = eb - v.csr_off[n];
         const int64_t j = static_cast<int64_t>(n) * nv + q;
-        r += cn.c[0] * a.gbx[j] + cn.c[1] * a.gby[j] + cn.c[2] * a.gbz[j];
-        if (a.imax[j] == k) r += a.hmax[j];
-        if (a.imin[j] == k) r += a.hmin[j];
+        r += cn.c[0] * ld(a.gbx, j) + cn.c[1] * ld(a.gby, j) + cn.c[2] * ld(a.gbz, j);
+        if (a.imax[j] == k) r += ld(a.hmax, j);
+        if (a.imin[j] == k) r += ld(a.hmin, j);
       } else {
         const BFace<double>& b = v.bf[c.bface];
         if (b.kind != kSymmetry) continue;
         const int qm = v.mirror_map[b.mirror * nv + q];
         const int64_t j = static_cast<int64_t>(cell) * nv + qm;
         const int k = e - e0;
-        const double s = c.c[0] * a.gbx[j] + c.c[1] * a.gby[j] + c.c[2] * a.gbz[j] +
-                         (a.imax[j] == k ? a.hmax[j] : 0.0) + (a.imin[j] == k ? a.hmin[j] : 0.0);
+        const double s = c.c[0] * ld(a.gbx, j) + c.c[1] * ld(a.gby, j) + c.c[2] * ld(a.gbz, j) +
+                         (a.imax[j] == k ? ld(a.hmax, j) : 0.0) + (a.imin[j] == k ? ld(a.hmin, j) : 0.0);
         r += 0.5 * s;
       }
     }
@@ -362,7 +375,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_gather(View<double, double>
     const double c2 = cx * cx + cy * cy + cz * cz;
     const double wq = v.wts != nullptr ? v.wts[q] : v.weight;
     r += wq * (a0 + ax * cx + ay * cy + az * cz + a2 * c2 + (bx * cx + by * cy + bz * cz) * c2);
-    a.out[static_cast<int64_t>(cell) * nv + a.rev[q]] = r;
+    a.out[static_cast<int64_t>(cell) * nv + a.rev[q]] = static_cast<S>(r);
     acc[0] += r * r;
   }
   block_sum<1, kAdjThreads>(acc, sh);
@@ -371,20 +384,34 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_gather(View<double, double>
 
 }  // namespace
 
-void adj_cell_sums(const View<double, double>& v, const AdjView& a, double* out, cudaStream_t st) {
-  k_adj_cell<<<v.n_cells, kAdjThreads, 0, st>>>(v, a, out);
+template <class S>
+void adj_cell_sums(const View<S, double>& v, const AdjView<S>& a, double* out, cudaStream_t st) {
+  k_adj_cell<S><<<v.n_cells, kAdjThreads, 0, st>>>(v, a, out);
 }
 
-void adj_transport(const View<double, double>& v, const AdjView& a, cudaStream_t st) {
-  k_adj_transport<<<v.n_cells, kAdjThreads, 0, st>>>(v, a);
+template <class S>
+void adj_transport(const View<S, double>& v, const AdjView<S>& a, const int32_t* cells, int n, cudaStream_t st) {
+  const int grid = cells != nullptr ? n : v.n_cells;
+  if (grid > 0) k_adj_transport<S><<<grid, kAdjThreads, 0, st>>>(v, a, cells);
 }
 
-void adj_face_sums(const View<double, double>& v, const AdjView& a, double* out, cudaStream_t st) {
-  if (v.n_bfaces > 0) k_adj_faces<<<v.n_bfaces, kAdjThreads, 0, st>>>(v, a, out);
+template <class S>
+void adj_face_sums(const View<S, double>& v, const AdjView<S>& a, double* out, cudaStream_t st) {
+  if (v.n_bfaces > 0) k_adj_faces<S><<<v.n_bfaces, kAdjThreads, 0, st>>>(v, a, out);
 }
 
-void adj_gather(const View<double, double>& v, const AdjView& a, double* res_cell, cudaStream_t st) {
-  k_adj_gather<<<v.n_cells, kAdjThreads, 0, st>>>(v, a, res_cell);
+template <class S>
+void adj_gather(const View<S, double>& v, const AdjView<S>& a, double* res_cell, cudaStream_t st) {
+  k_adj_gather<S><<<v.n_cells, kAdjThreads, 0, st>>>(v, a, res_cell);
 }
+
+#define KIN_ADJ_INSTANTIATE(S)                                                                   \
+  template void adj_cell_sums<S>(const View<S, double>&, const AdjView<S>&, double*, cudaStream_t); \
+  template void adj_transport<S>(const View<S, double>&, const AdjView<S>&, const int32_t*, int, cudaStream_t); \
+  template void adj_face_sums<S>(const View<S, double>&, const AdjView<S>&, double*, cudaStream_t); \
+  template void adj_gather<S>(const View<S, double>&, const AdjView<S>&, double*, cudaStream_t);
+KIN_ADJ_INSTANTIATE(double)
+KIN_ADJ_INSTANTIATE(float)
+#undef KIN_ADJ_INSTANTIATE
 
 }  // namespace kin

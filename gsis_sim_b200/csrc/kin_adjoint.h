@@ -1,4 +1,7 @@
-// Discrete adjoint of the converged CIS fixed point (FP64): launch interface of kin_adjoint.cu.
+// Discrete adjoint of the converged CIS fixed point: launch interface of kin_adjoint.cu. Arithmetic is FP64; the
+// stored arrays (f, lambda, the seeds and the operator output) are of the handle's storage type S: double for FP64
+// handles, float for mixed-precision ones (lambda stored and swept in FP32, the operator O(y) evaluated in FP64
+// arithmetic on the stored values: the adjoint counterpart of the forward's FP64 residual with FP32 sweeps).
 //
 // The steady discrete problem of the kinetic solver (residual_value with the limited LSQ gradient, the Shakhov target
 // of the cell moments and the boundary inflow, src/kinetic/kinetic_kernels.hpp) together with the zero-net-flux
@@ -29,30 +32,36 @@ constexpr int kAdjCellSums = 19;
 constexpr int kAdjFaceSums = 13;  // S0, S1 (3), S2, S5, S6, A1, A2, S_spec, S6 c (3) (k_adj_faces)
 constexpr int kAdjCoefs = 8;      // a0, a (3), a2, b (3)
 
+template <class S>
 struct AdjView {
-  const double* lam;       // [cell][p]: the adjoint of velocity rev[p] (velocity-reversed storage)
+  const S* lam;            // [cell][p]: the adjoint of velocity rev[p] (velocity-reversed storage)
   const int32_t* rev;      // position of -xi for every position
   const int32_t* rev_entry;  // for an internal CSR entry (cell j -> i): the entry of cell i that points back to j
-  double* gbx;             // gradient seeds G_bar [cell][q]
-  double* gby;
-  double* gbz;
-  double* hmax;            // seed on the stencil maximum / minimum of the limiter when it is a stencil entry
-  double* hmin;
+  S* gbx;                  // gradient seeds G_bar [cell][q]
+  S* gby;
+  S* gbz;
+  S* hmax;                 // seed on the stencil maximum / minimum of the limiter when it is a stencil entry
+  S* hmin;
   int8_t* imax;            // that entry (offset within the cell's CSR row), -1 none
   int8_t* imin;
-  double* lfb;             // seeds that land on f[cell][q] itself
+  S* lfb;                  // seeds that land on f[cell][q] itself
   const double* mu;        // per boundary face: seed weight of the outgoing face values (nu and objective terms)
   const int32_t* flip;     // [axis][q]: position of xi with component `axis` negated (3 x nv)
   const int32_t* face_axis;  // per boundary face: the axis its normal is aligned with, -1 if none
   const double* coef;      // per cell: moment expansion coefficients (kAdjCoefs)
   const double* moments;   // per cell: the 15 moments of the forward state
   const int32_t* deq_flags;  // per cell: the discrete-equilibrium result of the forward state (> 0: discrete)
-  double* out;             // O_f(y) at the reversed position [cell][rev[q]]
+  S* out;                  // O_f(y) at the reversed position [cell][rev[q]]
 };
 
-void adj_cell_sums(const View<double, double>& v, const AdjView& a, double* out, cudaStream_t st);
-void adj_transport(const View<double, double>& v, const AdjView& a, cudaStream_t st);
-void adj_face_sums(const View<double, double>& v, const AdjView& a, double* out, cudaStream_t st);
-void adj_gather(const View<double, double>& v, const AdjView& a, double* res_cell, cudaStream_t st);
+template <class S>
+void adj_cell_sums(const View<S, double>& v, const AdjView<S>& a, double* out, cudaStream_t st);
+// cells != nullptr: only the n listed cells (the owners of wall and pressure faces, for the per-face sums)
+template <class S>
+void adj_transport(const View<S, double>& v, const AdjView<S>& a, const int32_t* cells, int n, cudaStream_t st);
+template <class S>
+void adj_face_sums(const View<S, double>& v, const AdjView<S>& a, double* out, cudaStream_t st);
+template <class S>
+void adj_gather(const View<S, double>& v, const AdjView<S>& a, double* res_cell, cudaStream_t st);
 
 }  // namespace kin

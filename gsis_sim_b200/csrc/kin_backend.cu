@@ -353,9 +353,12 @@ struct Backend final : KinHandle {
 
   // discrete adjoint: lambda in velocity-reversed storage, seeds of the transposed gradient
   bool adj_on = false;
-  DevBuf<double> adj_lam, adj_lfb, adj_hmax, adj_hmin, adj_mu, adj_coef, adj_cell, adj_face, adj_res;
+  DevBuf<S> adj_lam, adj_lfb, adj_hmax, adj_hmin;  // of the storage type (FP32 in mixed precision)
+  DevBuf<double> adj_mu, adj_coef, adj_cell, adj_face, adj_res;
   DevBuf<int8_t> adj_imax, adj_imin;
   DevBuf<int32_t> adj_rev, adj_rev_entry, adj_perm2, adj_inv2, adj_flip, adj_face_axis;
+  DevBuf<int32_t> adj_face_cells;  // owners of wall and pressure faces (the transport the per-face sums need)
+  int n_adj_face_cells = 0;
 
   bool inflow_set = false;
   bool deq_valid = false;
@@ -1562,8 +1565,8 @@ struct Backend final : KinHandle {
   // the in-block lower / upper couplings of velocity -xi are the transposes of the upper / lower ones of xi.
   void adjoint_begin(const int32_t* rev_velocity, const int32_t* rev_entry, int64_t n_entries,
                      const int32_t* flip_velocity, const int32_t* face_axis) override {
-    if constexpr (!std::is_same<S, double>::value || !std::is_same<M, double>::value) {
-      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
+    if constexpr (!std::is_same<M, double>::value) {
+      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 or mixed-precision handle");
     } else {
       KCHECK(chunk == nv, "the adjoint needs one velocity chunk (velocity_chunk = 0 with enough device memory)");
       KCHECK(n_maxwell == 0, "the adjoint does not cover Maxwell walls");
@@ -1601,6 +1604,20 @@ struct Backend final : KinHandle {
         adj_flip.upload(flip.data(), flip.size(), stream);
         adj_face_axis.upload(face_axis, static_cast<size_t>(nb), stream);
       }
+      {
+        std::vector<kin::BFace<M>> hb(static_cast<size_t>(nb));
+        if (nb > 0)
+          KCUDA(cudaMemcpy(hb.data(), bfaces.p, sizeof(kin::BFace<M>) * static_cast<size_t>(nb),
+                           cudaMemcpyDeviceToHost));
+        std::vector<int32_t> owners;
+        for (const auto& b : hb)
+          if (b.kind == kin::kDiffuseWall || b.kind == kin::kPressure) owners.push_back(b.owner);
+        std::sort(owners.begin(), owners.end());
+        owners.erase(std::unique(owners.begin(), owners.end()), owners.end());
+        n_adj_face_cells = static_cast<int>(owners.size());
+        adj_face_cells.release();
+        if (!owners.empty()) adj_face_cells.upload(owners.data(), owners.size(), stream);
+      }
       adj_lam.alloc(nf);
       KCUDA(cudaMemsetAsync(adj_lam.p, 0, adj_lam.bytes(), stream));
       adj_lfb.alloc(nf);
@@ -1620,14 +1637,14 @@ struct Backend final : KinHandle {
     }
   }
 
-  kin::AdjView adj_view() {
-    kin::AdjView a{};
+  kin::AdjView<S> adj_view() {
+    kin::AdjView<S> a{};
     a.lam = adj_lam.p;
     a.rev = adj_rev.p;
     a.rev_entry = adj_rev_entry.p;
-    a.gbx = reinterpret_cast<double*>(gx.p);
-    a.gby = reinterpret_cast<double*>(gy.p);
-    a.gbz = reinterpret_cast<double*>(gz.p);
+    a.gbx = gx.p;
+    a.gby = gy.p;
+    a.gbz = gz.p;
     a.hmax = adj_hmax.p;
     a.hmin = adj_hmin.p;
     a.imax = adj_imax.p;
@@ -1639,7 +1656,7 @@ struct Backend final : KinHandle {
     a.coef = adj_coef.p;
     a.moments = moments.p;
     a.deq_flags = deq_valid ? flags.p : nullptr;
-    a.out = reinterpret_cast<double*>(r.p);
+    a.out = r.p;
     return a;
   }
 
@@ -1649,7 +1666,7 @@ struct Backend final : KinHandle {
     for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
       const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
       KCUDA(cudaMemcpyAsync(staging.p, h + c0 * nv, sizeof(double) * cnt * nv, cudaMemcpyHostToDevice, stream));
-      kin::Launch<double, double>::import_f(staging.p, adj_lam.p, adj_perm2.p, c0, cnt, nv, stream);
+      kin::Launch<S, M>::import_f(staging.p, adj_lam.p, adj_perm2.p, c0, cnt, nv, stream);
       launched();
     }
     KCUDA(cudaStreamSynchronize(stream));
@@ -1660,7 +1677,7 @@ struct Backend final : KinHandle {
     KCHECK(n == static_cast<int64_t>(nc) * nv, "length of lambda does not match");
     for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
       const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
-      kin::Launch<double, double>::export_f(adj_lam.p, staging.p, adj_inv2.p, c0, cnt, nv, stream);
+      kin::Launch<S, M>::export_f(adj_lam.p, staging.p, adj_inv2.p, c0, cnt, nv, stream);
       launched();
       KCUDA(cudaMemcpyAsync(h + c0 * nv, staging.p, sizeof(double) * cnt * nv, cudaMemcpyDeviceToHost, stream));
     }
@@ -1669,7 +1686,7 @@ struct Backend final : KinHandle {
 
   void adjoint_reduce(const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell, double* face_sums,
                       int64_t n_face) override {
-    if constexpr (std::is_same<S, double>::value && std::is_same<M, double>::value) {
+    if constexpr (std::is_same<M, double>::value) {
       KCHECK(adj_on, "adjoint_begin first");
       // a NULL output with length 0 skips that sum (the transport always runs)
       const bool want_cells = cell_sums != nullptr;
@@ -1678,9 +1695,14 @@ struct Backend final : KinHandle {
                  n_face == (face_sums != nullptr ? static_cast<int64_t>(nb) * kin::kAdjFaceSums : 0),
              "adjoint_reduce: array lengths do not match");
       if (nb > 0) KCUDA(cudaMemcpyAsync(adj_mu.p, mu, sizeof(double) * nb, cudaMemcpyHostToDevice, stream));
-      const kin::AdjView a = adj_view();
+      const kin::AdjView<S> a = adj_view();
       if (want_cells) kin::adj_cell_sums(view, a, adj_cell.p, stream);
-      kin::adj_transport(view, a, stream);
+      // per-face sums alone read the seeds of the face owners only: the transport runs on those cells (the other
+      // cells' seeds are stale until the next full reduce)
+      if (!want_cells && want_faces)
+        kin::adj_transport(view, a, adj_face_cells.p, n_adj_face_cells, stream);
+      else
+        kin::adj_transport(view, a, nullptr, 0, stream);
       if (want_faces) kin::adj_face_sums(view, a, adj_face.p, stream);
       launched(1 + (want_cells ? 1 : 0) + (want_faces ? 1 : 0));
       KCUDA(cudaGetLastError());
@@ -1690,13 +1712,13 @@ struct Backend final : KinHandle {
         KCUDA(cudaMemcpyAsync(face_sums, adj_face.p, sizeof(double) * n_face, cudaMemcpyDeviceToHost, stream));
       KCUDA(cudaStreamSynchronize(stream));
     } else {
-      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
+      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 or mixed-precision handle");
     }
   }
 
   void adjoint_update(const double* coef, int64_t n_coef, double* res_cell, int64_t n_res, int32_t run_passes,
                       double* op_out, int64_t n_op) override {
-    if constexpr (std::is_same<S, double>::value && std::is_same<M, double>::value) {
+    if constexpr (std::is_same<M, double>::value) {
       KCHECK(adj_on, "adjoint_begin first");
       KCHECK(n_coef == static_cast<int64_t>(nc) * kin::kAdjCoefs && n_res == nc, "adjoint_update: array lengths");
       KCHECK(op_out == nullptr || n_op == static_cast<int64_t>(nc) * nv, "adjoint_update: operator output length");
@@ -1707,8 +1729,7 @@ struct Backend final : KinHandle {
       if (op_out != nullptr) {
         for (int64_t c0 = 0; c0 < nc; c0 += staging_cells) {
           const int cnt = static_cast<int>(std::min<int64_t>(staging_cells, nc - c0));
-          kin::Launch<double, double>::export_f(reinterpret_cast<const double*>(r.p), staging.p, adj_inv2.p, c0, cnt,
-                                                nv, stream);
+          kin::Launch<S, M>::export_f(r.p, staging.p, adj_inv2.p, c0, cnt, nv, stream);
           launched();
           KCUDA(cudaMemcpyAsync(op_out + c0 * nv, staging.p, sizeof(double) * cnt * nv, cudaMemcpyDeviceToHost,
                                 stream));
@@ -1727,13 +1748,13 @@ struct Backend final : KinHandle {
       KCUDA(cudaStreamSynchronize(stream));
       check_status(h_err);
     } else {
-      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 handle");
+      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 or mixed-precision handle");
     }
   }
 
   void adjoint_end() override {
-    for (auto* b : {&adj_lam, &adj_lfb, &adj_hmax, &adj_hmin, &adj_mu, &adj_coef, &adj_cell, &adj_face, &adj_res})
-      b->release();
+    for (auto* b : {&adj_lam, &adj_lfb, &adj_hmax, &adj_hmin}) b->release();
+    for (auto* b : {&adj_mu, &adj_coef, &adj_cell, &adj_face, &adj_res}) b->release();
     adj_imax.release();
     adj_imin.release();
     adj_rev.release();
@@ -1742,6 +1763,8 @@ struct Backend final : KinHandle {
     adj_inv2.release();
     adj_flip.release();
     adj_face_axis.release();
+    adj_face_cells.release();
+    n_adj_face_cells = 0;
     adj_on = false;
   }
 };

@@ -332,11 +332,18 @@ __global__ void __launch_bounds__(kFaceThreads)
 // ---------------------------------------------------------------------------------------------------------
 // limited gradients and steady residual of one velocity chunk (k_gradient / k_residual,
 // kinetic_cuda_kernels.cu:343-372; limited_gradient / residual_value, kinetic_kernels.hpp:161-201, 238-278).
-// grid: (cell, velocity tile of kTileThreads * kTileIters). The CTA stages its cell's CSR entries in shared
-// memory once; every thread then carries its kTileIters velocities through each entry together, so an entry is
+// grid: (kCellsPerCta cells, velocity tile of 32 * U). The CTA stages its cells' CSR entries in shared memory
+// once; every thread then carries its U velocities (the kernel shape) through each entry together, so an entry is
 // read once per thread (not once per velocity) and the velocities give independent FP64 chains. The arithmetic
 // of every velocity is that of the reference routines, entry by entry in CSR order.
 // ---------------------------------------------------------------------------------------------------------
+// stencil extrema: FP32 min / max instructions, FP64 compare and select (as kmax / kmin; measured faster on B200 than
+// fmax / fmin of doubles in the gradient kernel)
+__device__ __forceinline__ double ext_max(double a, double b) { return kmax(a, b); }
+__device__ __forceinline__ float ext_max(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double ext_min(double a, double b) { return kmin(a, b); }
+__device__ __forceinline__ float ext_min(float a, float b) { return fminf(a, b); }
+
 constexpr int kCellsPerCta = 8;   // consecutive cells of one gradient / residual CTA
 constexpr int kStageMulti = 96;   // CSR entries of those cells staged in shared memory
 
@@ -448,8 +455,8 @@ __device__ __forceinline__ void limited_gradient_tile(const View<S, M>& v, int c
       sx[u] += c.c[0] * d;
       sy[u] += c.c[1] * d;
       sz[u] += c.c[2] * d;
-      fmax[u] = kmax(fmax[u], fk[u]);
-      fmin[u] = kmin(fmin[u], fk[u]);
+      fmax[u] = ext_max(fmax[u], fk[u]);
+      fmin[u] = ext_min(fmin[u], fk[u]);
     }
   });
   if (v.limiter_mode == kLimNone && v.positivity == 0) {
@@ -900,9 +907,9 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep_pass(View<S, M> v, S
 
 // ---------------------------------------------------------------------------------------------------------
 // staged LU-SGS block pass (k_sweep_tiles): the recurrence of k_sweep_pass, organised for instruction economy.
-//  * One CTA of kTileThreadsSweep threads per (direction group, block, tile of 32 * kU velocities); a thread carries
-//    SweepTile<M>::kU velocities (lane, lane + 32, ...) through every stencil entry, so the per-entry work that does not
-//    depend on the velocity (entry fetch, kind decode, addressing) is shared by SweepTile<M>::kU velocities.
+//  * One CTA of kTileThreadsSweep threads per (direction group, block, tile of 32 * KU velocities); a thread carries
+//    KU velocities (lane, lane + 32, ...; KU is the kernel shape) through every stencil entry, so the per-entry work
+//    that does not depend on the velocity (entry fetch, kind decode, addressing) is shared by KU velocities.
 //  * The chain's levels are split on the host into sub-levels of at most kStageCells cells and kStageEntries
 //    entries, stored contiguously with each entry's kind for this chain precomputed (periodic, boundary,
 //    in-block lower, in-block upper, other block); the next sub-level is copied into shared memory with
@@ -949,12 +956,15 @@ __device__ __forceinline__ void stage_sublevel(const SweepArgs<S, M>& a, const i
   cp_async_commit();
 }
 
-template <class M>
-__device__ __forceinline__ M pos_part(M af) { return af > M(0) ? af : M(0); }
-template <class M>
-__device__ __forceinline__ M neg_part(M af) { return af > M(0) ? M(0) : af; }
+// the upwind split of a = xi . S: max(a, 0) and min(a, 0) (the reference's branch a > 0 adds a to the outflow sum
+// and couples through a otherwise; the values are the same, zero's sign aside). FP32: one min / max instruction
+// each; FP64: compare and select (measured faster on B200 than fmax / fmin of doubles in these kernels)
+__device__ __forceinline__ double pos_part(double af) { return af > 0.0 ? af : 0.0; }
+__device__ __forceinline__ float pos_part(float af) { return fmaxf(af, 0.0f); }
+__device__ __forceinline__ double neg_part(double af) { return af > 0.0 ? 0.0 : af; }
+__device__ __forceinline__ float neg_part(float af) { return fminf(af, 0.0f); }
 
-// forward value of SweepTile<M>::kU velocities of one cell; First: first block pass (no previous Delta f)
+// forward value of KU velocities of one cell; First: first block pass (no previous Delta f)
 template <class S, class M, int NE, bool First, int KU>
 __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
                                                   const StageE<M>* E, int4 p, const int (&t)[KU],

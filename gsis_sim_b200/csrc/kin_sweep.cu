@@ -70,10 +70,11 @@ __device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, uint3
                : "memory");
 }
 
-template <class M>
-__device__ __forceinline__ M pos_part_r(M af) { return af > M(0) ? af : M(0); }
-template <class M>
-__device__ __forceinline__ M neg_part_r(M af) { return af > M(0) ? M(0) : af; }
+// the upwind split max(a, 0) / min(a, 0) of a = xi . S (FP32: min / max instructions; FP64: compare and select)
+__device__ __forceinline__ double pos_part_r(double af) { return af > 0.0 ? af : 0.0; }
+__device__ __forceinline__ float pos_part_r(float af) { return fmaxf(af, 0.0f); }
+__device__ __forceinline__ double neg_part_r(double af) { return af > 0.0 ? 0.0 : af; }
+__device__ __forceinline__ float neg_part_r(float af) { return fminf(af, 0.0f); }
 
 template <class P>
 struct ResidentStage {

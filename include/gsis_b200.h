@@ -310,8 +310,11 @@ int kin_gsis_correction_extrema(KinHandle* h, const double* w_half, const double
 int kin_gsis_correction_apply(KinHandle* h, const double* w_half, const double* w_new, int64_t n, const double* ext,
                               int64_t n_ext, int32_t* replaced_flags, int64_t* replaced);
 
-/* ---- discrete adjoint of the converged fixed point (no reference counterpart; FP64 handles, one velocity chunk,
-   continuous equilibrium, no Maxwell walls) ----------------------------------------------------------------------
+/* ---- discrete adjoint of the converged fixed point (no reference counterpart; FP64 or mixed-precision handles, one
+   velocity chunk, no Maxwell walls) --------------------------------------------------------------------------------
+   On a mixed-precision handle lambda, the transport seeds and O_f are stored in FP32 and the block passes run in
+   FP32 arithmetic (as the forward's sweeps), while O(y) is evaluated in FP64 arithmetic from the stored values (as
+   the forward's residual); all sums returned to the host are FP64. FP32 handles are refused (KIN_E_ARG).
    The adjoint y = (lambda [cell][velocity], nu [diffuse wall face]) of an objective J solves O(y) = 0 with
    O(y) = y^T dF/dx - dJ/dx, F = (steady residual R of residual_value, rho_Gamma - Phi of the wall densities). The
    handle evaluates O in pieces; the host finishes the per-cell and per-face algebra (gsis_sim_b200/adjoint.py).
@@ -339,7 +342,9 @@ int kin_adjoint_get(KinHandle* h, double* lambda, int64_t n);
    f_spec = the owner's reconstructed face value at the reflected velocity; zero elsewhere); and (13 in all)
    sum_in w an M c / area (3). cell_sums = NULL with n_cell = 0 skips the per-cell sums, face_sums = NULL
    with n_face = 0 the per-face sums; the transposed transport (the seeds that kin_adjoint_update gathers) always
-   runs. */
+   runs, on every cell, except with cell_sums = NULL and face_sums given: then it runs on the owner cells of wall and
+   pressure faces only (all the per-face sums read) and the other cells keep their seeds of the previous call, so a
+   kin_adjoint_update must follow a call that ran the full transport. */
 int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,
                        double* face_sums, int64_t n_face);
 /* Finish O_f(y) with the per-cell moment-expansion coefficients coef (8 per cell: a0, a (3), a2, b (3); the term

@@ -19,7 +19,7 @@ from gsis_sim_b200.solver import KineticSolver
 
 
 def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="periodic_slab", limiter="venkatakrishnan",
-                 eps="relative", half=False, quarter=False, alpha=1.0, equilibrium="continuous"):
+                 eps="relative", half=False, quarter=False, alpha=1.0, equilibrium="continuous", precision="fp64"):
     """Pressure-driven channel (inlet p 1, outlet p 0.5, diffuse walls) in the adjoint's scope; `half`: symmetry
     plane at y = 0 instead of the lower wall; `quarter`: a duct quarter, symmetry planes at y = 0 and z = 0, walls at
     y = 1 and z = 0.7 (a flow that varies in y and z)."""
@@ -35,7 +35,7 @@ def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="perio
         bcs.append(ks.BC("sym", "symmetry"))
     if quarter:
         bcs.append(ks.BC("symz", "symmetry"))
-    kp = ks.KineticParams(precision="fp64", pressure_boundary_reconstruction="cell", limiter=limiter,
+    kp = ks.KineticParams(precision=precision, pressure_boundary_reconstruction="cell", limiter=limiter,
                           limiter_eps=eps, sweep_blocks=1, equilibrium=equilibrium)
     setup, host = ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, Kn=0.3), bcs,
                                          ks.VelocityGrid(n=nv), kp)
