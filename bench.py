@@ -35,7 +35,10 @@ HBM_FALLBACK_GBS = 6650.0
 # 12^3 velocities (profiles/gradient_residual_sweep_tiles_tube63k_12cube_fp64.md, FP64;
 # profiles/residual_tube63k_12cube_mixed.md, mixed); the LU-SGS figure is that of the first block pass. Scaled by
 # the units of a full launch for roofline.traffic.
-DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 34.9, ("fp64", "k_residual"): 57.5, ("mixed", "k_residual"): 23.7}
+# ncu DRAM bytes per (cell, velocity) of one launch on the 62,848-cell tube at 12^3 (gradient_residual_sweep_tiles_*
+# summaries); the block passes: the mean of pass 1 and pass 2 (one launch each)
+DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 36.4, ("fp64", "k_residual"): 56.7, ("fp64", "k_sweep_tiles"): 46.55,
+                       ("mixed", "k_gradient"): 16.8, ("mixed", "k_residual"): 23.7, ("mixed", "k_sweep_tiles"): 21.9}
 DRAM_SOURCE = "ncu DRAM bytes per cell-velocity of the 62,848-cell 12^3 capture, scaled to this launch"
 
 
@@ -382,7 +385,8 @@ def tube_adjoint(args, local):
 
     def mixed_gradient(mesh_kw, timed):
         setup, host = case("mixed", mesh_kw)
-        prob = MassFlowProblem(setup, host, tol=args.fwd_tol, max_iterations=args.max_iters, device=local)
+        prob = MassFlowProblem(setup, host, tol=args.fwd_tol, max_iterations=args.max_iters, device=local,
+                               stall_iterations=args.stall)
         Tw = wall_temperature_field(prob)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -390,15 +394,17 @@ def tube_adjoint(args, local):
         torch.cuda.synchronize()
         t_fwd = time.perf_counter() - t0
         it_fwd = sol.iteration
+        r_fwd = prob.last_residual
         t0 = time.perf_counter()
         ka = KineticAdjoint(sol)
-        res = ka.solve(tol=args.adj_tol, max_iterations=args.adj_max_iters)
+        res = ka.solve(tol=args.adj_tol, max_iterations=args.adj_max_iters, stall_iterations=args.stall)
         torch.cuda.synchronize()
         t_adj = time.perf_counter() - t0
         ka.close()
         prob.release(sol)
         out = {"cells": setup.n_cells, "velocities": setup.nv, "wall_faces": len(prob.wall_faces), "M_dot": J,
-               "forward_seconds": t_fwd, "forward_iterations": it_fwd, "adjoint_seconds": t_adj,
+               "forward_seconds": t_fwd, "forward_iterations": it_fwd, "forward_residual": r_fwd,
+               "adjoint_seconds": t_adj,
                "adjoint_iterations": res.iterations, "adjoint_residual": res.residual,
                "ratio": t_adj / t_fwd}
         return out, res.dJ_dTw[prob.wall_faces].copy(), Tw, setup, host
@@ -452,10 +458,15 @@ def tube_adjoint(args, local):
                 Js.append(Jv)
             fd = (Js[0] - Js[1]) / (2 * h)
             ad = float(g @ v)
-            dirs.append({"adjoint": ad, "fd": fd, "rel_error": abs(ad - fd) / abs(fd)})
+            ad64 = float(g64 @ v)
+            dirs.append({"adjoint": ad, "fd": fd, "rel_error": abs(ad - fd) / abs(fd),
+                         "fp64_adjoint": ad64, "fp64_rel_error": abs(ad64 - fd) / abs(fd)})
         line["fd_check"] = {"mesh": "coarse tube (same geometry), 1,312 cells" if mk == COARSE_TUBE
                             else "the tube above", "run": fd_run, "step": h, "directions": dirs,
                             "max_rel_error": max(d["rel_error"] for d in dirs),
+                            "max_rel_error_fp64_adjoint": max(d["fp64_rel_error"] for d in dirs),
+                            "max_error_over_gradient_norm": max(abs(d["adjoint"] - d["fd"]) for d in dirs) /
+                            float(np.linalg.norm(g)),
                             "fd_seconds": time.perf_counter() - t0,
                             "fd_solver": "FP64 forward, residual 1e-12, central differences"}
     return line
@@ -593,6 +604,9 @@ def main():
     ap.add_argument("--adj-mesh", default="full", choices=["full", "coarse"],
                     help="mesh of the timed tube adjoint: the benchmark tube (--nx) or the 1,312-cell coarse tube")
     ap.add_argument("--adj-max-iters", type=int, default=2000, help="outer iterations of the adjoint solve at most")
+    ap.add_argument("--stall", type=int, default=None,
+                    help="--tube-adjoint: stop the mixed solves at their FP32 floor (no 1%% progress in this many "
+                    "iterations)")
     ap.add_argument("--fd-mesh", default="coarse", choices=["coarse", "same", "none"])
     ap.add_argument("--fd-tw-step", type=float, default=1e-5, help="step of the directional wall-temperature differences")
     args = ap.parse_args()
