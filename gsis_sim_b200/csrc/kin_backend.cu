@@ -1736,7 +1736,8 @@ struct Backend final : KinHandle {
         }
       }
       if (run_passes) {
-        // the forward block passes on lambda (reversed storage) with R = O_f(y): lambda += -P^-T O_f(y)
+        // the forward block passes on lambda (reversed storage) with R = O_f(y): lambda += -P^-T O_f(y). The
+        // adjoint keeps its arrays with rows of nv (= chunk) values, so the passes get that row stride.
         kin::View<S, P> av = sweep_view();
         av.f = adj_lam.p;
         run_block_passes(av, *chunks.front(), chunk, false);

@@ -47,12 +47,37 @@ __global__ void __launch_bounds__(kCellThreads)
 
 // ---------------------------------------------------------------------------------------------------------
 // 13 shifted sums in FP64 -> 15 moments (CpuBackend::compute_moments, kinetic_backend_cpu.cpp:92-120)
+// One warp per cell, kMomentWarps cells per CTA: each lane sums velocities lane, lane + 32, ... (every load of f a
+// 128- or 256-byte segment; four loads issued ahead of their sums), then a butterfly of warp shuffles combines the
+// lanes in a fixed order (bitwise reproducible, no shared memory or barrier).
 // ---------------------------------------------------------------------------------------------------------
+constexpr int kMomentWarps = 8;
+
+__device__ __forceinline__ void moment_terms(double f, double cx, double cy, double cz, double (&acc)[kMomentSums]) {
+  const double t1 = f * cx, t2 = f * cy, t3 = f * cz;
+  const double fc2 = f * (cx * cx + cy * cy + cz * cz);
+  acc[0] += f;
+  acc[1] += t1;
+  acc[2] += t2;
+  acc[3] += t3;
+  acc[4] += t1 * cx;
+  acc[5] += t2 * cy;
+  acc[6] += t3 * cz;
+  acc[7] += t1 * cy;
+  acc[8] += t2 * cz;
+  acc[9] += t1 * cz;
+  acc[10] += fc2 * cx;
+  acc[11] += fc2 * cy;
+  acc[12] += fc2 * cz;
+}
+
 template <class S, class M, bool Finalize>
-__global__ void __launch_bounds__(kCellThreads)
+__global__ void __launch_bounds__(32 * kMomentWarps, 4)
     k_moments(View<S, M> v, double* __restrict__ shift, double* __restrict__ out) {
-  __shared__ double sh[kMomentSums * (kCellThreads / 32)];
-  const int c = blockIdx.x;
+  constexpr int kAhead = 4;
+  const int c = blockIdx.x * kMomentWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= v.n_cells) return;
   const double u0x = shift[3 * static_cast<int64_t>(c) + 0];
   const double u0y = shift[3 * static_cast<int64_t>(c) + 1];
   const double u0z = shift[3 * static_cast<int64_t>(c) + 2];
@@ -61,41 +86,38 @@ __global__ void __launch_bounds__(kCellThreads)
   double acc[kMomentSums];
 #pragma unroll
   for (int k = 0; k < kMomentSums; ++k) acc[k] = 0.0;
-  for (int q = threadIdx.x; q < v.nv; q += kCellThreads) {
-    double f = static_cast<double>(fc[q]);
-    if (!uniform) f *= v.wts[q];
-    const double cx = v.xid_x[q] - u0x, cy = v.xid_y[q] - u0y, cz = v.xid_z[q] - u0z;
-    const double t1 = f * cx, t2 = f * cy, t3 = f * cz;
-    const double fc2 = f * (cx * cx + cy * cy + cz * cz);
-    acc[0] += f;
-    acc[1] += t1;
-    acc[2] += t2;
-    acc[3] += t3;
-    acc[4] += t1 * cx;
-    acc[5] += t2 * cy;
-    acc[6] += t3 * cz;
-    acc[7] += t1 * cy;
-    acc[8] += t2 * cz;
-    acc[9] += t1 * cz;
-    acc[10] += fc2 * cx;
-    acc[11] += fc2 * cy;
-    acc[12] += fc2 * cz;
-  }
-  block_sum<kMomentSums, kCellThreads>(acc, sh);
-  if (!Finalize) {  // raw sums of one velocity shard (kin_moment_sums); the shift stays
-    if (threadIdx.x == 0) {
-      for (int k = 0; k < kMomentSums; ++k) out[kMomentSums * static_cast<int64_t>(c) + k] = acc[k];
+  for (int q0 = 0; q0 < v.nv; q0 += 32 * kAhead) {
+    S fs[kAhead];
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) {
+      const int q = q0 + 32 * j + lane;
+      fs[j] = q < v.nv ? __ldcs(fc + q) : S(0);
     }
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) {
+      const int q = q0 + 32 * j + lane;
+      if (q >= v.nv) break;
+      double f = static_cast<double>(fs[j]);
+      if (!uniform) f *= v.wts[q];
+      moment_terms(f, v.xid_x[q] - u0x, v.xid_y[q] - u0y, v.xid_z[q] - u0z, acc);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMomentSums; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  }
+  if (lane != 0) return;
+  if (!Finalize) {  // raw sums of one velocity shard (kin_moment_sums); the shift stays
+    for (int k = 0; k < kMomentSums; ++k) out[kMomentSums * static_cast<int64_t>(c) + k] = acc[k];
     return;
   }
-  if (threadIdx.x == 0) {
-    double* m = out + 15 * static_cast<int64_t>(c);
-    finalize_moments(acc, uniform ? v.weight : 1.0, u0x, u0y, u0z, m);
-    if (m[0] > 0.0) {
-      shift[3 * static_cast<int64_t>(c) + 0] = m[1];
-      shift[3 * static_cast<int64_t>(c) + 1] = m[2];
-      shift[3 * static_cast<int64_t>(c) + 2] = m[3];
-    }
+  double* m = out + 15 * static_cast<int64_t>(c);
+  finalize_moments(acc, uniform ? v.weight : 1.0, u0x, u0y, u0z, m);
+  if (m[0] > 0.0) {
+    shift[3 * static_cast<int64_t>(c) + 0] = m[1];
+    shift[3 * static_cast<int64_t>(c) + 1] = m[2];
+    shift[3 * static_cast<int64_t>(c) + 2] = m[3];
   }
 }
 
@@ -1313,12 +1335,14 @@ void Launch<S, M>::set_equilibrium(const View<S, M>& v, const double* states, do
 
 template <class S, class M>
 void Launch<S, M>::moments(const View<S, M>& v, double* shift, double* out, cudaStream_t st) {
-  if (v.n_cells > 0) k_moments<S, M, true><<<v.n_cells, kCellThreads, 0, st>>>(v, shift, out);
+  if (v.n_cells > 0)
+    k_moments<S, M, true><<<ceil_div(v.n_cells, kMomentWarps), 32 * kMomentWarps, 0, st>>>(v, shift, out);
 }
 
 template <class S, class M>
 void Launch<S, M>::moment_sums(const View<S, M>& v, double* shift, double* out, cudaStream_t st) {
-  if (v.n_cells > 0) k_moments<S, M, false><<<v.n_cells, kCellThreads, 0, st>>>(v, shift, out);
+  if (v.n_cells > 0)
+    k_moments<S, M, false><<<ceil_div(v.n_cells, kMomentWarps), 32 * kMomentWarps, 0, st>>>(v, shift, out);
 }
 
 template <class S, class M>
