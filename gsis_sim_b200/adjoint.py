@@ -483,7 +483,8 @@ class MassFlowProblem:
     def __init__(self, setup: abi.SetupArrays, host, delta: float | None = None, tol: float = 1e-12,
                  max_iterations: int = 20000,
                  adjoint_tol: float = 1e-12, adjoint_max_iterations: int = 20000,
-                 initial=(1.0, (0.0, 0.0, 0.0), 1.0), device: int = 0, stall_iterations: int | None = None):
+                 initial=(1.0, (0.0, 0.0, 0.0), 1.0), device: int = 0, stall_iterations: int | None = None,
+                 polish_iterations: int = 20):
         self.setup, self.host = setup, host
         self.mu0_0 = float(setup["mu0"])
         self.delta0 = 1.0 / (math.sqrt(2.0) * self.mu0_0) if delta is None else float(delta)
@@ -498,34 +499,23 @@ class MassFlowProblem:
         # mixed precision: accept the storage floor (the residual no longer falls below 0.99 of its best value for
         # this many iterations) as convergence of the forward and adjoint solves
         self.stall_iterations = stall_iterations
+        # mixed precision: FP64 CIS iterations from the converged mixed state before the adjoint (polish_state)
+        self.polish_iterations = int(polish_iterations)
+        self.last_polish = None
 
     def solve(self, delta: float, T_wall=None, alpha=None):
         """Converged forward solve at (delta, T_wall, alpha) -> (solver, M_dot). T_wall: one temperature per wall
         face (None: the patch temperatures). alpha: one accommodation per wall face, which must be 1: the adjoint
         gives the derivative at alpha = 1 from below (alpha <= 1), and walls with alpha < 1 are Maxwell walls, outside
         its scope."""
-        from .backend import B200Backend
-        from .solver import KineticSolver
-
         if not delta > 0:
             raise ValueError(f"delta must be positive, got {delta}")
         if alpha is not None and np.any(np.asarray(alpha, float).reshape(-1) != 1.0):
             raise AdjointScopeError("the accommodation derivative is taken at alpha = 1 (from below); alpha < 1 makes "
                                     "the walls Maxwell walls, outside the adjoint's scope")
-        s = abi.SetupArrays(dict(self.setup.arrays), dict(self.setup.scalars))  # arrays shared, scalars own
-        s["mu0"] = self.mu0_0 if float(delta) == self.delta0 else self.mu0_0 * (self.delta0 / float(delta))
-        be = B200Backend(s, device=self.device)
+        sol = self._solver(delta, T_wall)
+        be = sol.backend
         try:
-            sol = KineticSolver(s, self.host, be)
-            if T_wall is not None:
-                Tw = np.asarray(T_wall, float).reshape(-1)
-                if Tw.shape != self.wall_faces.shape:
-                    raise ValueError(f"T_wall: {Tw.shape[0]} values for {len(self.wall_faces)} wall faces")
-                T = np.ones(s.n_bfaces)
-                T[self.wall_faces] = Tw
-                sol.set_wall_temperature(T)
-            rho, u, T0 = self.initial
-            sol.initialize_uniform(rho, u, T0)
             r = math.inf
             best, since_best, stalled = math.inf, 0, False
             for _ in range(self.max_iterations):
@@ -548,15 +538,76 @@ class MassFlowProblem:
             raise
         return sol, sol.mass_flow()[2]
 
+    def _solver(self, delta: float, T_wall=None, precision: int | None = None):
+        """A KineticSolver on a new B200Backend at (delta, T_wall), initialised to the problem's uniform state."""
+        from .backend import B200Backend
+        from .solver import KineticSolver
+
+        s = abi.SetupArrays(dict(self.setup.arrays), dict(self.setup.scalars))  # arrays shared, scalars own
+        s["mu0"] = self.mu0_0 if float(delta) == self.delta0 else self.mu0_0 * (self.delta0 / float(delta))
+        if precision is not None:
+            s["precision"] = precision
+        be = B200Backend(s, device=self.device)
+        try:
+            sol = KineticSolver(s, self.host, be)
+            if T_wall is not None:
+                Tw = np.asarray(T_wall, float).reshape(-1)
+                if Tw.shape != self.wall_faces.shape:
+                    raise ValueError(f"T_wall: {Tw.shape[0]} values for {len(self.wall_faces)} wall faces")
+                T = np.ones(s.n_bfaces)
+                T[self.wall_faces] = Tw
+                sol.set_wall_temperature(T)
+            rho, u, T0 = self.initial
+            sol.initialize_uniform(rho, u, T0)
+        except BaseException:
+            be.close()
+            raise
+        return sol
+
+    def polish_state(self, sol, delta: float):
+        """FP64 defect correction of a converged mixed-precision state before its adjoint: `polish_iterations` CIS
+        iterations of the FP64 solver from the mixed solver's f, whose result (rounded to FP32) replaces it in a new
+        mixed-precision solver; `sol` is released (the two handles are not held at the same time: at full size
+        they do not fit one device together). Returns the new solver.
+
+        Why: the mixed solve stops at its storage floor, where every value of f sits within an ulp of FP32 but the
+        pattern of roundings is not monotone between neighbours. In flat regions that creates stencil extrema that
+        the FP64 state does not have, and the limiter's derivative there (of order 1 / (g . ds)) makes the
+        linearised iteration unstable: on the 134,528-cell tube the FP64 adjoint at the mixed state diverges, while
+        the mixed adjoint at the FP64 state rounded to FP32 converges like the FP64 one. Twenty FP64 iterations
+        (residual 7.5e-8 -> 4e-10) remove the pattern; five do not."""
+        if int(sol.s["precision"]) != abi.KIN_PREC_MIXED or self.polish_iterations <= 0:
+            return sol
+        f = sol.distribution()
+        Tw = None if sol.wall_T is None else np.asarray(sol.wall_T, float)[self.wall_faces].copy()
+        self.release(sol)
+        s64 = self._solver(delta, Tw, precision=abi.KIN_PREC_FP64)
+        history = []
+        try:
+            s64.set_distribution(f)
+            for _ in range(self.polish_iterations):
+                history.append(s64.sweep().residual)
+            f = s64.distribution()
+        finally:
+            self.release(s64)
+        out = self._solver(delta, Tw)
+        out.set_distribution(f)
+        self.last_polish = history
+        return out
+
     def gradients(self, sol, delta: float):
         """(dM_dot/d delta, dM_dot/dT_w per wall face, dM_dot/d alpha per wall face at alpha = 1) at a converged
-        solve; the alpha derivative is NaN on wall faces not aligned with a coordinate axis."""
+        solve; the alpha derivative is NaN on wall faces not aligned with a coordinate axis. A mixed-precision state
+        is first polished in FP64 (polish_state; `sol` is then released here and the caller's release is a no-op)."""
+        sol = self.polish_state(sol, delta)
         ka = KineticAdjoint(sol)
         try:
             res = ka.solve(tol=self.adjoint_tol, max_iterations=self.adjoint_max_iterations,
                            stall_iterations=self.stall_iterations)
         finally:
             ka.close()
+            if sol is not None and int(sol.s["precision"]) == abi.KIN_PREC_MIXED and self.polish_iterations > 0:
+                self.release(sol)
         if not (res.residual < self.adjoint_tol or
                 (self.stall_iterations is not None and res.iterations < self.adjoint_max_iterations)):
             raise FloatingPointError(f"adjoint stopped at residual {res.residual:.3e} after {res.iterations} "
