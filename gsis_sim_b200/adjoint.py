@@ -599,14 +599,17 @@ class MassFlowProblem:
         """(dM_dot/d delta, dM_dot/dT_w per wall face, dM_dot/d alpha per wall face at alpha = 1) at a converged
         solve; the alpha derivative is NaN on wall faces not aligned with a coordinate axis. A mixed-precision state
         is first polished in FP64 (polish_state; `sol` is then released here and the caller's release is a no-op)."""
+        polished = int(sol.s["precision"]) == abi.KIN_PREC_MIXED and self.polish_iterations > 0
         sol = self.polish_state(sol, delta)
-        ka = KineticAdjoint(sol)
         try:
-            res = ka.solve(tol=self.adjoint_tol, max_iterations=self.adjoint_max_iterations,
-                           stall_iterations=self.stall_iterations)
+            ka = KineticAdjoint(sol)
+            try:
+                res = ka.solve(tol=self.adjoint_tol, max_iterations=self.adjoint_max_iterations,
+                               stall_iterations=self.stall_iterations)
+            finally:
+                ka.close()
         finally:
-            ka.close()
-            if sol is not None and int(sol.s["precision"]) == abi.KIN_PREC_MIXED and self.polish_iterations > 0:
+            if polished:
                 self.release(sol)
         if not (res.residual < self.adjoint_tol or
                 (self.stall_iterations is not None and res.iterations < self.adjoint_max_iterations)):

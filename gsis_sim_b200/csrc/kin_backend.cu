@@ -1361,6 +1361,7 @@ struct Backend final : KinHandle {
       a.R = r.p;
       a.dprev = prev;
       a.out = out;
+      a.diag_store = gx.p;  // free during the passes (the gradient is dead after the residual)
       a.update_f = last ? 1 : 0;
       if (resident) {
         a.Rs = gx.p;

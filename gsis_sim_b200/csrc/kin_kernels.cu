@@ -1035,10 +1035,14 @@ __device__ __forceinline__ void tile_forward_cell(const View<S, M>& v, const Swe
     const M am_out = First ? ext[u] : M(0), Lout = First ? M(0) : ext[u];
     const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out;
     a.out[crow + t[u]] = static_cast<S>((-own[u] - Lout - lo[u]) / D);
+    // the block passes run with S = M (FP64, or FP32 storage and arithmetic in the fp32 and mixed precisions), so
+    // the backward reads back exactly this D
+    a.diag_store[crow + t[u]] = static_cast<S>(D);
   }
 }
 
-// backward value of KU velocities of one cell (and f += Delta f in the last pass)
+// backward value of KU velocities of one cell (and f += Delta f in the last pass); the diagonal is the forward
+// sweep's, read back, so only the in-block upper entries are visited
 template <class S, class M, int NE, bool First, int KU>
 __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const SweepArgs<S, M>& a,
                                                    const StageE<M>* E, int4 p, const int (&t)[KU],
@@ -1055,36 +1059,32 @@ __device__ __forceinline__ void tile_backward_cell(const View<S, M>& v, const Sw
   }
   const int64_t crow = static_cast<int64_t>(p.x) * a.stride;
   const int64_t frow = static_cast<int64_t>(p.x) * v.nv + a.k0;
-  M own[KU], fv[KU];
+  M own[KU], fv[KU], D[KU];
 #pragma unroll
   for (int u = 0; u < KU; ++u) {
     own[u] = ok[u] ? static_cast<M>(a.out[crow + t[u]]) : M(0);
+    D[u] = ok[u] ? static_cast<M>(a.diag_store[crow + t[u]]) : M(1);
     fv[u] = (ok[u] && a.update_f) ? static_cast<M>(__ldcs(v.f + frow + t[u])) : M(0);
   }
-  const M diag = v.cp[p.x].diag;
-  M ap[KU], up[KU], am_out[KU];
+  M up[KU];
 #pragma unroll
-  for (int u = 0; u < KU; ++u) ap[u] = up[u] = am_out[u] = M(0);
+  for (int u = 0; u < KU; ++u) up[u] = M(0);
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
     if (j >= p.z) break;
     const StageE<M>& e = E[p.y + j];
-    const uint32_t kind = e.code >> kKindShift;
-    if (kind == kKindPeriodic) continue;
+    if ((e.code >> kKindShift) != kKindUpper) continue;
     const M s0 = e.s[0], s1 = e.s[1], s2 = e.s[2];
 #pragma unroll
     for (int u = 0; u < KU; ++u) {
       const M af = x[u] * s0 + y[u] * s1 + z[u] * s2;
-      ap[u] += pos_part(af);
-      if (kind == kKindUpper) up[u] += neg_part(af) * val[j][u];
-      else if (First && kind == kKindOther) am_out[u] -= neg_part(af);
+      up[u] += neg_part(af) * val[j][u];
     }
   }
 #pragma unroll
   for (int u = 0; u < KU; ++u) {
     if (!ok[u]) continue;
-    const M D = diag + v.diag_scale * ap[u] + v.interface_damping * am_out[u];
-    const M df = own[u] - up[u] / D;
+    const M df = own[u] - up[u] / D[u];
     a.out[crow + t[u]] = static_cast<S>(df);
     if (a.update_f) __stcs(v.f + frow + t[u], static_cast<S>(fv[u] + df));
   }

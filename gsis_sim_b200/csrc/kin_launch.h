@@ -46,6 +46,9 @@ struct SweepArgs {
   const S* R;                  // steady residual of the chunk
   const S* dprev;              // Delta f of the previous pass (nullptr in the first pass)
   S* out;                      // Delta f* then Delta f
+  // k_sweep_tiles: the diagonal D of every (cell, velocity), written by the forward sweep and read by the backward
+  // one instead of being summed again (a chunk-sized work array that is free during the passes)
+  S* diag_store;
   int32_t update_f;
   int32_t k0;
   int32_t stride;

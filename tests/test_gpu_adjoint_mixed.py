@@ -104,3 +104,34 @@ def test_gpu_mixed_adjoint_gradients_match_fp64(kw):
         g = float(rmx.dJ_dTw[w] @ v)
         print(f"direction: adjoint {g:.10e}, FP64 difference {fd:.10e}, relative {abs(g - fd) / abs(fd):.2e}")
         assert abs(g - fd) <= 1e-4 * abs(fd)
+
+
+@pytest.mark.timeout(900)
+def test_gpu_mixed_mass_flow_autograd_with_fp64_polish():
+    """mass_flow through torch.autograd on a mixed-precision problem: the forward stops at the mixed solve's storage
+    floor, the backward polishes that state with FP64 iterations (MassFlowProblem.polish_state) and runs the mixed
+    adjoint; the delta and per-face T_w gradients equal the FP64 adjoint's at the FP64 fixed point to 1e-4."""
+    from gsis_sim_b200.adjoint import KineticAdjoint, MassFlowProblem, mass_flow
+
+    sol64, setup64, host64 = _solution("fp64", 1e-13)
+    try:
+        ka = KineticAdjoint(sol64)
+        r64 = ka.solve(tol=1e-12, max_iterations=4000)
+        ka.close()
+    finally:
+        sol64.backend.close()
+    setup, host = channel_case(precision="mixed")
+    prob = MassFlowProblem(setup, host, tol=1e-12, adjoint_tol=1e-8, initial=(0.75, (0.0, 0.0, 0.0), 1.0),
+                           stall_iterations=40, polish_iterations=20)
+    delta = torch.tensor(prob.delta0, dtype=torch.float64, requires_grad=True)
+    T = torch.tensor(prob.T_patch, dtype=torch.float64, requires_grad=True)
+    J = mass_flow(prob, delta, T)
+    gd, gT = torch.autograd.grad(J, (delta, T))
+    assert prob.last_polish is not None and len(prob.last_polish) == 20
+    ref_d = r64.dJ_ddelta(float(setup64["mu0"]), prob.delta0)
+    w = prob.wall_faces
+    e_d = abs(float(gd) - ref_d) / abs(ref_d)
+    e_T = np.max(np.abs(gT.numpy() - r64.dJ_dTw[w])) / np.max(np.abs(r64.dJ_dTw[w]))
+    print(f"mixed autograd with polish: delta {e_d:.2e}, T_w {e_T:.2e}, polish residuals "
+          f"{prob.last_polish[0]:.2e} -> {prob.last_polish[-1]:.2e}")
+    assert e_d <= 1e-4 and e_T <= 1e-4
