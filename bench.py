@@ -11,8 +11,15 @@ boundary sums, then 4 x (gradient, residual, 2 LU-SGS block passes) with wall re
 metric = cell-velocity updates per second = n_cells * n_velocities * inner_sweeps / step time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32|mixed] [--impl b200|reference]
-Under torchrun (N > 1) every rank runs an independent replica of the case on its own GPU (the kinetic path of one
-case does not shard across GPUs here; value = all ranks' updates / the slowest rank's time).
+Under torchrun (N > 1) every rank runs an independent replica of the case on its own GPU (value = all ranks'
+updates / the slowest rank's time); with --shard the ranks split one case's velocities instead (strong scaling).
+
+The default line (one GPU) also carries, besides the FP64 figures and every kernel's roofline: the mixed-precision
+leg on the same tube, the adjoint / forward ratio on the channel of the adjoint check (median of 3), the reference's
+own CUDA backend rebuilt for sm_100a on the same tube and GPU, and the reference's CPU path on the host cores.
+Other metrics: --time-to-mdot (solve time to M_dot within 1e-4 of the converged FP64 value, FP64 against mixed),
+--adjoint (the channel adjoint with finite differences, --adjoint-fd), --tube-adjoint (the mixed-precision tube
+adjoint at a per-face wall-temperature field, checked by FP64 directional differences).
 """
 from __future__ import annotations
 
@@ -278,8 +285,9 @@ def run_time_to_mdot(args, local):
 
     torch.cuda.set_device(local)
     out = {}
-    ref = None
-    for prec in ("fp64", "mixed"):
+    ref = args.mdot_fp64
+    precisions = ("mixed",) if ref is not None else ("fp64", "mixed")
+    for prec in precisions:
         args.precision = prec
         setup, host, _ = build_case(args)
         n_cells = setup.n_cells
@@ -305,14 +313,15 @@ def run_time_to_mdot(args, local):
         out[prec] = hist
         if args.history:
             np.savetxt(f"{args.history}_{prec}.txt", np.array(hist), header="wall_s mdot residual")
-    t64 = settle_time(out["fp64"], ref, args.mdot_tol)
+    t64 = settle_time(out["fp64"], ref, args.mdot_tol) if "fp64" in out else args.fp64_seconds
     tmx = settle_time(out["mixed"], ref, args.mdot_tol)
     line = {"metric": f"solve time to M_dot within {args.mdot_tol:g} of the converged FP64 M_dot (mixed)",
             "value": tmx, "unit": "s", "higher_is_better": False, "fp64_seconds": t64,
             "speedup_mixed_vs_fp64": (t64 / tmx) if (t64 and tmx) else None, "mdot_fp64_converged": ref,
             "mdot_mixed_final": out["mixed"][-1][1],
             "mdot_mixed_rel_error": abs(out["mixed"][-1][1] - ref) / abs(ref),
-            "iterations": {"fp64": len(out["fp64"]), "mixed": len(out["mixed"])},
+            "iterations": {k: len(v) for k, v in out.items()},
+            "fp64_from": "this run" if "fp64" in out else "--mdot-fp64 / --fp64-seconds of an earlier FP64 run",
             "seconds_per_iteration": {k: out[k][-1][0] / len(out[k]) for k in out},
             "final_residual": {k: out[k][-1][2] for k in out},
             "data": "synthetic", "config": workload_config(args, n_cells=n_cells)}
@@ -588,6 +597,10 @@ def main():
                     help="split the case's velocities over the ranks (strong scaling) instead of one replica per rank")
     ap.add_argument("--time-to-mdot", action="store_true")
     ap.add_argument("--mdot-tol", type=float, default=1e-4)
+    ap.add_argument("--mdot-fp64", type=float, default=None,
+                    help="--time-to-mdot: the converged FP64 M_dot of an earlier run (then only the mixed solve runs)")
+    ap.add_argument("--fp64-seconds", type=float, default=None,
+                    help="--time-to-mdot with --mdot-fp64: that run's FP64 time to the tolerance")
     ap.add_argument("--max-iters", type=int, default=2000)
     ap.add_argument("--history", default=None, help="write per-iteration (wall s, M_dot, residual) to <prefix>_<prec>.txt")
     # third headline metric: adjoint / forward wall-time ratio on the channel

@@ -424,7 +424,7 @@ __device__ __forceinline__ M venkat_face_sel(M d2, M dmax, M dmin, M eps2) {
   const M den = d1 * d1 + M(2) * d2 * d2 + d1 * d2 + eps2;
   const bool sided = pos || neg;
   M r = (sided && !(den > M(0))) ? M(0) : M(1);
-  if (sided && den > M(0) && num < den) r = kclamp(num / den, M(0), M(1));
+  if (sided && den > M(0) && num < den) r = kclamp(limiter_quotient(num, den), M(0), M(1));
   return r;
 }
 

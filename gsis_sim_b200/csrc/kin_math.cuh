@@ -149,6 +149,18 @@ __host__ __device__ inline CellParams<M> make_cell_params(const double* m, doubl
 }
 
 // Venkatakrishnan limiter of one face (venkatakrishnan_face, src/physics/limiter.hpp:17-31)
+// num / den with subnormal operands first scaled by 2^64 (exact, so the correctly rounded quotient is unchanged):
+// the FP32 limiter of states with tiny differences (far velocity tails, near-vacuum regions; d^2 below 1e-38)
+// would otherwise divide subnormals, which the division handles off its fast path. Used where 0 <= num < den.
+__host__ __device__ inline float limiter_quotient(float num, float den) {
+  if (den < 0x1p-100f) {
+    num *= 0x1p64f;
+    den *= 0x1p64f;
+  }
+  return num / den;
+}
+__host__ __device__ inline double limiter_quotient(double num, double den) { return num / den; }
+
 template <class M>
 __host__ __device__ inline M venkat_face(M d2, M dmax, M dmin, M eps2) {
   M d1;
@@ -164,7 +176,7 @@ __host__ __device__ inline M venkat_face(M d2, M dmax, M dmin, M eps2) {
   if (!(den > M(0))) return M(0);
   // num >= den > 0: the quotient rounds to >= 1 and the clamp gives exactly 1, so the division can be skipped
   if (num >= den) return M(1);
-  return kclamp(num / den, M(0), M(1));
+  return kclamp(limiter_quotient(num, den), M(0), M(1));
 }
 
 // ---- discrete equilibrium (src/kinetic/discrete_equilibrium.hpp) -------------------------------------------
