@@ -42,10 +42,11 @@ HBM_FALLBACK_GBS = 6650.0
 # 12^3 velocities (profiles/gradient_residual_sweep_tiles_tube63k_12cube_fp64.md, FP64;
 # profiles/residual_tube63k_12cube_mixed.md, mixed); the LU-SGS figure is that of the first block pass. Scaled by
 # the units of a full launch for roofline.traffic.
-# ncu DRAM bytes per (cell, velocity) of one launch on the 62,848-cell tube at 12^3 (gradient_residual_sweep_tiles_*
-# summaries); the block passes: the mean of pass 1 and pass 2 (one launch each)
-DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 36.4, ("fp64", "k_residual"): 56.7, ("fp64", "k_sweep_tiles"): 46.55,
-                       ("mixed", "k_gradient"): 16.8, ("mixed", "k_residual"): 23.7, ("mixed", "k_sweep_tiles"): 21.9}
+# ncu DRAM bytes per (cell, velocity) of one launch on the 62,848-cell tube at 12^3 (the gradient_residual_sweep_tiles_*
+# and sweep_tiles_moments_* summaries); the block passes: the mean of pass 1 and pass 2 (one launch each, with the
+# stored diagonal)
+DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 36.4, ("fp64", "k_residual"): 56.7, ("fp64", "k_sweep_tiles"): 66.65,
+                       ("mixed", "k_gradient"): 16.8, ("mixed", "k_residual"): 23.7}
 DRAM_SOURCE = "ncu DRAM bytes per cell-velocity of the 62,848-cell 12^3 capture, scaled to this launch"
 
 
