@@ -60,6 +60,6 @@ EXPORTED_SYMBOLS = [
     "kin_gsis_correction", "kin_internal_face_mass_flux", "kin_take_timings", "kin_deq_counts",
     "kin_set_stream", "kin_launch_count", "kin_device_f", "kin_velocity_permutation", "kin_schedule_info", "kin_discrete_maxwell",
     "kin_discrete_maxwell_noalloc", "kin_moment_sums", "kin_set_moments", "kin_adjoint_begin", "kin_adjoint_set",
-    "kin_adjoint_get", "kin_adjoint_reduce", "kin_adjoint_update", "kin_adjoint_end", "kin_gsis_correction_extrema",
+    "kin_adjoint_get", "kin_adjoint_reduce", "kin_adjoint_face_moment_seeds", "kin_adjoint_update", "kin_adjoint_end", "kin_gsis_correction_extrema",
     "kin_gsis_correction_apply", "kin_device_sums", "kin_finalize_moments", "kin_read_sums",
 ]

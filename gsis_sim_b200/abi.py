@@ -245,6 +245,7 @@ def declare_backend_api(lib, prefix: str, handle_type=C.c_void_p):
         "adjoint_set": [h, _dp, C.c_int64],
         "adjoint_get": [h, _dp, C.c_int64],
         "adjoint_reduce": [h, _dp, C.c_int64, _dp, C.c_int64, _dp, C.c_int64],
+        "adjoint_face_moment_seeds": [h, _dp, C.c_int64],
         "adjoint_update": [h, _dp, C.c_int64, _dp, C.c_int64, C.c_int32, _dp, C.c_int64],
         "adjoint_end": [h],
     }

@@ -4,13 +4,19 @@ wall face at alpha = 1) on the B200 backend.
 There is no reference counterpart; the steady problem differentiated is the one the reference's CIS iteration
 converges to (src/kinetic/kinetic_solver.cpp prepare + sweep, src/kinetic/kinetic_kernels.hpp):
 
-  F(x; p) = ( R(f, rho_Gamma)                 residual_value with the limited LSQ gradient, Shakhov target of the
-                                              cell moments, inflow of walls / pressure faces ("cell" reconstruction)
-              rho_Gamma - Phi(f, rho_Gamma) ) zero net mass flux of every diffuse wall face
+  F(x; p) = ( R(f, rho_Gamma, fs)             residual_value with the limited LSQ gradient, Shakhov target of the
+                                              cell moments, inflow of walls / pressure faces
+              rho_Gamma - Phi(f, rho_Gamma)   zero net mass flux of every diffuse wall face
+              fs - FS(f, fs) )                the face states of the boundary sums (process_boundary_sums,
+                                              src/kinetic/kinetic_solver.cpp:280-335), which the "limited" pressure-
+                                              boundary reconstruction (the reference default) reads: W_b is the owner's
+                                              (p, u, T) reconstructed at the face from its stencil, whose boundary
+                                              entries carry those face states (:172-260); absent with the "cell"
+                                              reconstruction (W_b = the owner's state)
   J = M_dot = 1/2 (mdot_in + mdot_out) sqrt(2/pi)   (tube_mass_flow_json, src/kinetic/kinetic_output.cpp:273-284)
 
-The adjoint y = (lambda, nu) solves O(y) = y^T dF/dx - dJ/dx = 0 by the preconditioned fixed-point iteration
-  lambda <- lambda - P^-T O_f(y),   nu <- nu - O_nu(y)
+The adjoint y = (lambda, nu, kappa) solves O(y) = y^T dF/dx - dJ/dx = 0 by the preconditioned fixed-point iteration
+  lambda <- lambda - P^-T O_f(y),   nu <- nu - O_nu(y),   kappa <- kappa - O_kappa(y)
 where P^-T is the forward LU-SGS block passes run on velocity-reversed storage (the transposed sweep; the device does
 it, kin_adjoint_update). Then dJ/dp = dJ/dp|_x - y^T dF/dp. The transposed transport, the per-cell sums against the
 Shakhov target and the per-face sums against the inflow Maxwellians run on the device (csrc/kin_adjoint.cu); this
@@ -31,8 +37,15 @@ FP64 residual with FP32 sweeps. Its fixed point holds to the FP32 storage of lam
 
 Scope (`check_scope`): FP64 or mixed-precision backend with one velocity chunk; a tensor velocity grid when the equilibrium is discrete
 (every grid of the reference is one) and no failed Newton solve; diffuse walls, pressure inlets / outlets with
-pressure_boundary_reconstruction = "cell", vacuum, symmetry, periodic faces; no Maxwell walls, mass-flow inlets,
-positivity limiter or closed-domain scaling.
+the "limited" (default) or "cell" pressure-boundary reconstruction, vacuum, symmetry, periodic faces; no Maxwell
+walls, mass-flow inlets, positivity limiter or closed-domain scaling.
+
+Face states (limited reconstruction): the device adds the seeds -kappa^T dFS/df on the outgoing reconstructed face
+values (kin_adjoint_face_moment_seeds: weights of w psi, psi = (1, xi, |xi|^2 / 2); at symmetry faces also the
+mirrored incoming half); the host carries the rest: the wall density rho_Gamma = -sm0 / sm5 in the walls' face
+moments (an extra weight in mu), the pressure faces' own incoming halves (a loop back through W_b), the vector-
+Jacobian product of the reconstruction (PressureReconstruction) and the wall-temperature and accommodation terms of
+the gradients.
 """
 from __future__ import annotations
 
@@ -159,6 +172,159 @@ def collision_moment_adjoint(m, volume, mu0, omega, cell_sums):
     return rho_b, u_b, T_b, q_b, coll
 
 
+class PressureReconstruction:
+    """W_ib = (p, u, T) of every pressure face by the "limited" reconstruction of update_pressure_inflow
+    (src/kinetic/kinetic_solver.cpp:172-260) as a function of the cell states and the face states of the boundary
+    sums, with its vector-Jacobian product. The owner's (p, u, T) plus phi * (grad . dx_b): grad the LSQ gradient over
+    the owner's stencil, whose internal entries carry the neighbour's state, whose boundary entries carry the face
+    state (rho T, u, T) where it is positive (periodic entries and the others the owner's own value); phi the
+    Venkatakrishnan limiter with epsilon^2 = K^3 V over the non-periodic entries; the owner's own state where the
+    result is not positive. The stencil arrays are the solver's (KineticSolver._build_pressure_stencils)."""
+
+    def __init__(self, sol):
+        h = sol.h
+        self.nc, self.nb = sol.nc, sol.nb
+        self.faces = sol.pres_faces
+        self.own = sol.bowner[self.faces]
+        self.mask, self.other, self.bface = sol.ps_mask, sol.ps_other, sol.ps_bface
+        self.lsq, self.dx, self.periodic = sol.ps_lsq, sol.ps_dx, sol.ps_periodic
+        fb = sol.bf_global[self.faces]
+        self.dxb = h.face_center[fb] - h.cell_center[self.own]
+        self.eps2 = h.limiter_k ** 3 * sol.volume[self.own]
+        self.limit = int(sol.s["limiter_mode"]) != abi.LIMITER_NONE
+
+    def forward(self, m, fs):
+        """W_ib (n_pressure, 5) from the cell moments m (nc, 15) and the face states fs (nb, 5: rho, u, T)."""
+        state = np.stack([m[:, 5], m[:, 1], m[:, 2], m[:, 3], m[:, 4]], -1)
+        self.state, self.fs = state, fs
+        wi = state[self.own]
+        internal = self.mask & (self.other >= 0)
+        bmask = self.mask & (self.bface >= 0)
+        f = fs[np.where(bmask, self.bface, 0)]
+        use = bmask & ~self.periodic & (f[..., 0] > 0) & (f[..., 4] > 0)
+        wk = np.broadcast_to(wi[:, None, :], self.mask.shape + (5,)).copy()
+        wk[internal] = state[self.other[internal]]
+        wk[use] = np.stack([f[use][:, 0] * f[use][:, 4], f[use][:, 1], f[use][:, 2], f[use][:, 3], f[use][:, 4]], -1)
+        grad = np.einsum("fek,fea->fka", np.where(self.mask[..., None], wk - wi[:, None, :], 0.0), self.lsq)
+        wm = np.where(self.mask[..., None], wk, np.nan)
+        # the bounds start from the owner's value; a stencil entry takes over only when strictly beyond it (the
+        # reference's std::max / std::min keep the earlier value on a tie)
+        xmax, xmin = np.nanmax(wm, axis=1), np.nanmin(wm, axis=1)
+        self.amax = np.where(xmax > wi, np.nanargmax(np.where(np.isnan(wm), -np.inf, wm), axis=1), -1)
+        self.amin = np.where(xmin < wi, np.nanargmin(np.where(np.isnan(wm), np.inf, wm), axis=1), -1)
+        wmax, wmin = np.maximum(wi, xmax), np.minimum(wi, xmin)
+        phi = np.ones_like(wi)
+        self.estar = np.full(wi.shape, -1)
+        if self.limit:
+            proj = np.einsum("fka,fea->fke", grad, self.dx)
+            dmax, dmin = (wmax - wi)[..., None], (wmin - wi)[..., None]
+            d1 = np.where(proj > 0, dmax, np.where(proj < 0, dmin, 0.0))
+            e2 = self.eps2[:, None, None]
+            num = (d1 * d1 + e2) + 2.0 * d1 * proj
+            den = d1 * d1 + 2.0 * proj * proj + d1 * proj + e2
+            with np.errstate(divide="ignore", invalid="ignore"):
+                v = np.clip(num / den, 0.0, 1.0)
+            v = np.where(den > 0, v, 0.0)
+            v = np.where(proj == 0, 1.0, v)
+            v = np.where((self.mask & ~self.periodic)[:, None, :], v, 1.0)
+            vmin = v.min(axis=2)
+            phi = np.minimum(1.0, vmin)
+            e = np.argmin(v, axis=2)
+            self.estar = np.where(vmin < 1.0, e, -1)
+            self.proj, self.d1, self.num, self.den = proj, d1, num, den
+        wib = wi + phi * np.einsum("fka,fa->fk", grad, self.dxb)
+        self.good = (wib[:, 0] > 0) & (wib[:, 4] > 0)
+        self.wi, self.wk, self.use, self.internal, self.grad, self.phi = wi, wk, use, internal, grad, phi
+        return np.where(self.good[:, None], wib, wi)
+
+    def vjp(self, wb):
+        """Seeds wb (n_pressure, 5) on W_ib -> (seeds (nc, 5) on the cells' (p, u, T), seeds (nb, 5) on the face
+        states (rho, u, T)) at the point of the last forward."""
+        npf, E = self.mask.shape
+        wi_bar = np.where(self.good[:, None], 0.0, wb)
+        wg = np.where(self.good[:, None], wb, 0.0)
+        wi_bar = wi_bar + wg
+        wk_bar = np.zeros((npf, E, 5))
+        grad_bar = (wg * self.phi)[:, :, None] * self.dxb[:, None, :]
+        if self.limit:
+            phi_bar = wg * np.einsum("fka,fa->fk", self.grad, self.dxb)
+            f_i, k_i = np.nonzero(self.estar >= 0)
+            e = self.estar[f_i, k_i]
+            p = self.proj[f_i, k_i, e]
+            d1 = self.d1[f_i, k_i, e]
+            num, den = self.num[f_i, k_i, e], self.den[f_i, k_i, e]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                ok = (p != 0) & (den > 0) & (num < den) & (num / den > 0)
+            den2 = np.where(ok, den * den, 1.0)
+            dv_dp = np.where(ok, (2.0 * d1 * den - num * (4.0 * p + d1)) / den2, 0.0)
+            dv_dd1 = np.where(ok, ((2.0 * d1 + 2.0 * p) * den - num * (2.0 * d1 + p)) / den2, 0.0)
+            pb = phi_bar[f_i, k_i] * dv_dp
+            np.add.at(grad_bar, (f_i, k_i), pb[:, None] * self.dx[f_i, e])
+            d1b = phi_bar[f_i, k_i] * dv_dd1
+            # d1 = wmax - wi (proj > 0) or wmin - wi (proj < 0); wmax / wmin is the owner's value or one entry
+            for sel, arg in ((p > 0, self.amax), (p < 0, self.amin)):
+                fi_, ki_, db = f_i[sel], k_i[sel], d1b[sel]
+                a = arg[fi_, ki_]
+                np.add.at(wi_bar, (fi_, ki_), -db)
+                on = a >= 0
+                np.add.at(wi_bar, (fi_[~on], ki_[~on]), db[~on])
+                np.add.at(wk_bar, (fi_[on], a[on], ki_[on]), db[on])
+        # grad = sum_e lsq_e (wk_e - wi) over the stencil
+        g_e = np.einsum("fka,fea->fek", grad_bar, self.lsq) * self.mask[..., None]
+        wk_bar += g_e
+        wi_bar -= g_e.sum(axis=1)
+        cell_bar = np.zeros((self.nc, 5))
+        fs_bar = np.zeros((self.nb, 5))
+        np.add.at(cell_bar, self.own, wi_bar)
+        np.add.at(cell_bar, self.other[self.internal], wk_bar[self.internal])
+        # entries that carry the owner's own value (periodic, no face state, padding)
+        own_val = ~self.internal & ~self.use
+        np.add.at(cell_bar, np.broadcast_to(self.own[:, None], self.mask.shape)[own_val], wk_bar[own_val])
+        # face states: wk = (rho T, u, T)
+        b = self.bface[self.use]
+        fsv = self.fs[b]
+        wu = wk_bar[self.use]
+        fsb = np.column_stack([wu[:, 0] * fsv[:, 4], wu[:, 1:4], wu[:, 4] + wu[:, 0] * fsv[:, 0]])
+        np.add.at(fs_bar, b, fsb)
+        return cell_bar, fs_bar
+
+
+def face_moment_state_adjoint(mom, fs_bar):
+    """Seeds on the face moments mom = (m0, m1, m2, m3, m4) (sums of w psi f, psi = (1, xi, |xi|^2 / 2)) of the seeds
+    fs_bar on the face state (rho, u, T) = (m0, m_a / m0, (2 m4 / m0 - |u|^2) / 3) of process_boundary_sums
+    (src/kinetic/kinetic_solver.cpp:280-335); zero where m0 <= 0 (face state 0)."""
+    pos = mom[:, 0] > 0
+    m0 = np.where(pos, mom[:, 0], 1.0)
+    u = mom[:, 1:4] / m0[:, None]
+    kr, ku, kT = fs_bar[:, 0], fs_bar[:, 1:4], fs_bar[:, 4]
+    out = np.empty_like(mom)
+    out[:, 0] = kr - np.sum(ku * u, 1) / m0 + kT * (-2.0 * mom[:, 4] / (3.0 * m0 * m0) + (2.0 / 3.0) * np.sum(u * u, 1) / m0)
+    out[:, 1:4] = ku / m0[:, None] - (2.0 / 3.0) * kT[:, None] * u / m0[:, None]
+    out[:, 4] = 2.0 * kT / (3.0 * m0)
+    return np.where(pos[:, None], out, 0.0)
+
+
+def inflow_moment_derivatives(xi, w, normals, states):
+    """Per face: D[k, j] = sum_{xi.n < 0} w psi_k(xi) dM/dtheta_j and d5[j] = sum_{xi.n < 0} w (xi.n) dM/dtheta_j for
+    the Maxwellian M of theta = (rho, u (3), T), psi = (1, xi, |xi|^2 / 2): the derivatives of the incoming halves of
+    a face's moment and flux sums (k_boundary_sums) with respect to its inflow state."""
+    n = len(states)
+    D = np.zeros((n, 5, 5))
+    d5 = np.zeros((n, 5))
+    psi = np.column_stack([np.ones(len(xi)), xi, 0.5 * np.sum(xi * xi, 1)])
+    for i in range(n):
+        rho, u, T = states[i, 0], states[i, 1:4], states[i, 4]
+        an = xi @ normals[i]
+        m = an < 0
+        c = xi[m] - u
+        c2 = np.sum(c * c, 1)
+        M = w[m] * rho / (2.0 * math.pi * T) ** 1.5 * np.exp(-c2 / (2.0 * T))
+        dM = np.column_stack([M / rho, M[:, None] * c / T, M * (c2 / (2.0 * T * T) - 1.5 / T)])  # (nin, 5)
+        D[i] = psi[m].T @ dM
+        d5[i] = an[m] @ dM
+    return D, d5
+
+
 @dataclass
 class AdjointResult:
     J: float
@@ -199,6 +365,15 @@ class KineticAdjoint:
         self.sgn[(bk != abi.BC_PRESSURE) & (bk != abi.BC_VACUUM)] = 0.0
         self.nu = np.zeros(len(self.wall))
         self.history = []
+        # the "limited" pressure-boundary reconstruction (the reference default): W_b also reads the neighbours'
+        # states and the face states of the boundary sums, whose adjoint kappa (nb, 5) is iterated like nu
+        self.limited = h.pressure_boundary_reconstruction != "cell" and len(self.pres) > 0
+        self.kappa = np.zeros((self.nb, 5))
+        self.fs_seed = np.zeros((self.nb, 5))
+        if self.limited:
+            self.recon = PressureReconstruction(solver)
+            self.wib = self.recon.forward(solver.moments_, solver.face_state)
+            self._face_state_constants()
         self._discrete_chains()
 
     # ---- derivatives through the discrete equilibrium ---------------------------------------------------------
@@ -242,15 +417,62 @@ class KineticAdjoint:
                 self.deq_wall = sel  # indices into self.wall
                 self.wall_deq = InflowDerivatives(grid, ws[sel])
 
+    def _face_state_constants(self):
+        """The face moments mom = sm[10:15] + s_in sm[15:20] of the last boundary sums (process_boundary_sums:
+        s_in = rho_Gamma = -sm0 / sm5 on diffuse walls, 0 on vacuum faces, 1 elsewhere) and the derivatives of the
+        incoming halves with respect to the inflow state of the pressure faces and of the walls whose face state a
+        pressure face reads."""
+        sol = self.sol
+        sm = sol.bsums
+        sm0, sm5 = sm[:, 0], sm[:, 5]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            self.wall_pos = (sm5 < 0) & (-sm0 / sm5 > 0)
+            rg = np.where(self.wall_pos, -sm0 / sm5, 0.0)
+        s_in = np.ones(self.nb)
+        bk = sol.bkind
+        s_in[bk == abi.BC_DIFFUSE_WALL] = rg[bk == abi.BC_DIFFUSE_WALL]
+        s_in[bk == abi.BC_VACUUM] = 0.0
+        self.fs_mom = sm[:, 10:15] + s_in[:, None] * sm[:, 15:20]
+        r = self.recon
+        read = np.unique(r.bface[r.use]) if r.use.any() else np.zeros(0, np.int64)
+        self.fs_read = read  # the boundary faces whose face state a pressure face reads
+        self.fs_walls = read[bk[read] == abi.BC_DIFFUSE_WALL]
+        s = sol.s
+        xi = np.stack([np.asarray(s["xi_x"]), np.asarray(s["xi_y"]), np.asarray(s["xi_z"])], 1)
+        w = np.asarray(s["weights"]) if s.get("weights") is not None else np.full(sol.nv, float(s["weight"]))
+        nrm = sol.h.face_normal[sol.bf_global]
+        # the inflow states as the device holds them (after the discrete-Maxwellian correction)
+        self.Dp, _ = inflow_moment_derivatives(xi, w, nrm[self.pres], sol.inflow[self.pres][:, 1:6])
+        self.Dw, self.d5w = inflow_moment_derivatives(xi, w, nrm[self.fs_walls], sol.inflow[self.fs_walls][:, 1:6])
+
+    def _mom_bar(self):
+        """Seeds on the face moments from kappa (zero on faces no pressure face reads)."""
+        return face_moment_state_adjoint(self.fs_mom, self.kappa)
+
+    def _face_moment_seeds(self):
+        """The seeds of -kappa^T dFS/df (F_fs = fs - FS(f, ...)): per face the weights of w psi on the outgoing
+        reconstructed values (and the mirrored incoming half of symmetry faces) for the device, and for diffuse walls
+        the extra weight of w a on the outgoing values through rho_Gamma = -sm0 / sm5 (added to mu)."""
+        mb = self._mom_bar()
+        mu_extra = np.zeros(self.nb)
+        sol = self.sol
+        w = sol.bkind == abi.BC_DIFFUSE_WALL
+        with np.errstate(divide="ignore", invalid="ignore"):
+            c0 = np.where(w & self.wall_pos, np.sum(mb * sol.bsums[:, 15:20], 1) / sol.bsums[:, 5], 0.0)
+        mu_extra[w] = c0[w] / sol.barea[w]
+        return -mb, mu_extra
+
     def _pressure_states(self):
-        """(rho_b, u_b, T_b) of the pressure faces from their owner cells (update_pressure_inflow, "cell"
-        reconstruction, src/kinetic/kinetic_solver.cpp:172-260)."""
+        """(rho_b, u_b, T_b) of the pressure faces from W_ib (update_pressure_inflow, src/kinetic/kinetic_solver.cpp:
+        172-260): the owner cell's state ("cell" reconstruction) or its limited reconstruction at the face."""
         sol = self.sol
         h = sol.h
         b = self.pres
         m = sol.moments_
         o = sol.bowner[b]
         p_o, u_o, T_o = m[o, 5], m[o, 1:4], m[o, 4]
+        if self.limited:
+            p_o, u_o, T_o = self.wib[:, 0], self.wib[:, 1:4], self.wib[:, 4]
         patch = sol.bpatch[b]
         p_b = h.patch_dbl[patch, 1]
         inlet = np.isin(sol.ptype[patch], _INLETS)
@@ -277,8 +499,6 @@ class KineticAdjoint:
             raise AdjointScopeError("Maxwell walls (accommodation < 1)")
         if np.any(sol.ptype == BOUNDARY_TYPES.index("mass_flow_inlet")):
             raise AdjointScopeError("mass-flow inlets")
-        if np.any(sol.bkind == abi.BC_PRESSURE) and h.pressure_boundary_reconstruction != "cell":
-            raise AdjointScopeError('pressure boundaries need pressure_boundary_reconstruction = "cell"')
         if float(s["cold_bgk_temperature"]) > 0.0:
             raise AdjointScopeError("cold-BGK switch")
         if sol.discrete_eq:
@@ -299,9 +519,14 @@ class KineticAdjoint:
             mu[w] = np.where(pos, self.nu / (sol.barea[w] * sm5[w]), 0.0)
         j = self.sgn != 0
         mu[j] = -C_J * self.sgn[j]
+        if self.limited:
+            mu = mu + self._mu_extra
         return mu
 
     def _reduce(self, cells: bool = True, faces: bool = True):
+        if self.limited:
+            mom_seeds, self._mu_extra = self._face_moment_seeds()
+            self.sol.backend.adjoint_face_moment_seeds(mom_seeds)
         cell, face = self.sol.backend.adjoint_reduce(self._mu(), cells=cells, faces=faces)
         from .backend import ADJ_CELL_SUMS, ADJ_FACE_SUMS
 
@@ -314,47 +539,87 @@ class KineticAdjoint:
             cell = out
         return (cell if cells else None), (face.reshape(max(self.nb, 0), ADJ_FACE_SUMS) if faces else None)
 
+    def _pressure_chain(self, face):
+        """Seeds on the cells' (p, u, T) (nc, 5) of the pressure faces' inflow: from the device's sums of the seeds
+        on the incoming values (face), through the correction to the discrete Maxwellian, the acoustic correction
+        (App. A.2) and W_ib; with the limited reconstruction also the seeds on the face states (self.fs_seed), which
+        include the pressure faces' own incoming halves read by their face states (-kappa^T dFS/dW_b)."""
+        sol = self.sol
+        m = sol.moments_
+        cell_bar = np.zeros((self.nc, 5))
+        self.fs_seed = np.zeros((self.nb, 5))
+        b = self.pres
+        if len(b) == 0:
+            return cell_bar
+        inf = sol.inflow[b]
+        rb, Tb = inf[:, 1], inf[:, 5]
+        S = face[b]
+        rho_bar = S[:, 0] / rb
+        u_bar = S[:, 1:4] / Tb[:, None]
+        T_bar = S[:, 4] / (2.0 * Tb * Tb) - 1.5 * S[:, 0] / Tb
+        if self.limited:
+            th = -np.einsum("fk,fkj->fj", self._mom_bar()[b], self.Dp)
+            rho_bar, u_bar, T_bar = rho_bar + th[:, 0], u_bar + th[:, 1:4], T_bar + th[:, 4]
+        if len(self.deq_pres):
+            # through the correction of W_b to its discrete Maxwellian
+            k = np.searchsorted(b, self.deq_pres)
+            tb = self.pres_deq.pullback(np.column_stack([rho_bar[k], u_bar[k], T_bar[k]]))
+            rho_bar, u_bar, T_bar = rho_bar.copy(), u_bar.copy(), T_bar.copy()
+            rho_bar[k], u_bar[k], T_bar[k] = tb[:, 0], tb[:, 1:4], tb[:, 4]
+        o = sol.bowner[b]
+        h = sol.h
+        n = h.face_normal[sol.bf_global[b]]
+        patch = sol.bpatch[b]
+        inlet = np.isin(sol.ptype[patch], _INLETS)
+        if self.limited:
+            p_i, u_i, T_i = self.wib[:, 0], self.wib[:, 1:4], self.wib[:, 4]
+        else:
+            p_i, u_i, T_i = m[o, 5], m[o, 1:4], m[o, 4]
+        p_bar, ui_bar, Ti_bar = pressure_face_adjoint(p_i, u_i, T_i, n, h.patch_dbl[patch, 1], inlet,
+                                                      h.patch_dbl[patch, 6] > 0.5, h.gamma, rho_bar, u_bar, T_bar)
+        wb = np.column_stack([p_bar, ui_bar, Ti_bar])
+        if self.limited:
+            cell_bar, self.fs_seed = self.recon.vjp(wb)
+        else:
+            np.add.at(cell_bar, o, wb)
+        return cell_bar
+
     def _coefficients(self, cell, face):
         sol = self.sol
         m = sol.moments_
-        rho, u, T, p = m[:, 0], m[:, 1:4], m[:, 4], m[:, 5]
+        rho, T = m[:, 0], m[:, 4]
         rho_b, u_b, T_b, q_b, coll = collision_moment_adjoint(m, sol.volume, float(sol.s["mu0"]),
                                                               float(sol.s["omega"]), cell)
         if len(self.pres):
-            b = self.pres
-            inf = sol.inflow[b]
-            rb, Tb = inf[:, 1], inf[:, 5]
-            S = face[b]
-            rho_bar = S[:, 0] / rb
-            u_bar = S[:, 1:4] / Tb[:, None]
-            T_bar = S[:, 4] / (2.0 * Tb * Tb) - 1.5 * S[:, 0] / Tb
-            if len(self.deq_pres):
-                # through the correction of W_b to its discrete Maxwellian
-                k = np.searchsorted(b, self.deq_pres)
-                tb = self.pres_deq.pullback(np.column_stack([rho_bar[k], u_bar[k], T_bar[k]]))
-                rho_bar, u_bar, T_bar = rho_bar.copy(), u_bar.copy(), T_bar.copy()
-                rho_bar[k], u_bar[k], T_bar[k] = tb[:, 0], tb[:, 1:4], tb[:, 4]
-            o = sol.bowner[b]
-            h = sol.h
-            n = h.face_normal[sol.bf_global[b]]
-            patch = sol.bpatch[b]
-            inlet = np.isin(sol.ptype[patch], _INLETS)
-            p_bar, uo_bar, To_bar = pressure_face_adjoint(p[o], u[o], T[o], n, h.patch_dbl[patch, 1], inlet,
-                                                          h.patch_dbl[patch, 6] > 0.5, h.gamma, rho_bar, u_bar, T_bar)
+            cb = self._pressure_chain(face)
             # p = rho T
-            np.add.at(rho_b, o, p_bar * T[o])
-            np.add.at(T_b, o, p_bar * rho[o] + To_bar)
-            np.add.at(u_b, o, uo_bar)
+            rho_b = rho_b + cb[:, 0] * T
+            T_b = T_b + cb[:, 0] * rho + cb[:, 4]
+            u_b = u_b + cb[:, 1:4]
         return moment_expansion_coefficients(m, rho_b, u_b, T_b, q_b), coll
 
+    def _refresh_kappa(self, face):
+        """kappa <- -(the face-state rows of y^T dF/dx - dJ/dx without kappa) (Jacobi on the face-state equations)."""
+        if self.limited:
+            self._pressure_chain(face)
+            k_old = self.kappa
+            self.kappa = -self.fs_seed
+            return float(np.sqrt(np.sum((self.kappa - k_old) ** 2))), float(np.sqrt(np.sum(self.kappa ** 2)))
+        return 0.0, 0.0
+
     def operator(self, lam=None, nu=None, with_objective=True):
-        """O(y) (or y^T dF/dx without the objective term) for the given lambda (storage order) and nu; returns
-        (O_f (nc, nv), O_nu (n_wall,))."""
+        """O(y) (or y^T dF/dx without the objective term) for the given lambda (storage order) and auxiliary adjoint
+        nu: the wall densities' (n_wall), followed with the limited pressure reconstruction by the face states'
+        kappa (n_bfaces x 5). Returns (O_f (nc, nv), O_aux in the layout of nu)."""
         be = self.sol.backend
+        nw = len(self.wall)
         if lam is not None:
             be.adjoint_set(np.asarray(lam, float))
         if nu is not None:
-            self.nu = np.asarray(nu, float).copy()
+            nu = np.asarray(nu, float).ravel()
+            self.nu = nu[:nw].copy()
+            if self.limited and len(nu) > nw:
+                self.kappa = nu[nw:].reshape(self.nb, 5).copy()
         sgn = self.sgn
         if not with_objective:
             self.sgn = np.zeros_like(sgn)
@@ -364,7 +629,10 @@ class KineticAdjoint:
             _, op = be.adjoint_update(coef, run_passes=False, want_operator=True)
         finally:
             self.sgn = sgn
-        return op.reshape(self.nc, self.nv), face[self.wall, 0] + self.nu
+        o_aux = face[self.wall, 0] + self.nu
+        if self.limited:
+            o_aux = np.concatenate([o_aux, (self.kappa + self.fs_seed).ravel()])
+        return op.reshape(self.nc, self.nv), o_aux
 
     # ---- the solve -----------------------------------------------------------------------------------------------
     def solve(self, tol: float = 1e-10, max_iterations: int = 5000, inner: int | None = None,
@@ -391,9 +659,11 @@ class KineticAdjoint:
             # wall adjoint first, from the current lambda (the transpose of the forward's rho_Gamma = Phi(f) before
             # each sweep; a one-sweep lag on these strongly coupled unknowns can make the iteration unstable)
             nu_old = self.nu
-            if walls:
+            dk = (0.0, 0.0)
+            if walls or self.limited:
                 _, face = self._reduce(cells=False)
                 self.nu = -face[self.wall, 0]
+                dk = self._refresh_kappa(face)
             cell, face = self._reduce()
             coef, _ = self._coefficients(cell, face)
             res_cell, _ = be.adjoint_update(coef, run_passes=True)
@@ -402,13 +672,15 @@ class KineticAdjoint:
             r = math.sqrt(float(np.sum(res_cell)))
             if ref is None:
                 ref = max(r, 1e-300)
-            res = max(r / ref, dnu / max(float(np.sqrt(np.sum(nu_new ** 2))), 1e-300) if len(nu_new) else 0.0)
+            res = max(r / ref, dnu / max(float(np.sqrt(np.sum(nu_new ** 2))), 1e-300) if len(nu_new) else 0.0,
+                      dk[0] / max(dk[1], 1e-300) if self.limited else 0.0)
             self.history.append(r)
             if callback is not None:
                 callback(it, r)
             if not math.isfinite(r):
                 raise FloatingPointError(f"adjoint iteration diverged at outer iteration {it}")
-            if r / ref < tol and (len(nu_new) == 0 or dnu <= tol * max(float(np.abs(nu_new).max()), 1e-300)):
+            if r / ref < tol and (len(nu_new) == 0 or dnu <= tol * max(float(np.abs(nu_new).max()), 1e-300)) and \
+                    (not self.limited or dk[0] <= tol * max(dk[1], 1e-300)):
                 break
             if r < 0.99 * best:
                 best, since_best = r, 0
@@ -417,9 +689,10 @@ class KineticAdjoint:
             if stall_iterations is not None and since_best >= stall_iterations:
                 break
             for _ in range(1, inner):
-                if walls:
+                if walls or self.limited:
                     _, face = self._reduce(cells=False)
                     self.nu = -face[self.wall, 0]
+                    self._refresh_kappa(face)
                 # the transport's seeds with the new nu (the coupling sums stay frozen over the inner sweeps)
                 self._reduce(cells=False, faces=False)
                 be.adjoint_update(coef, run_passes=True)
@@ -447,6 +720,19 @@ class KineticAdjoint:
                 pos = (sm5 < 0) & (-sm0 / sm5 > 0)
                 dPhi = np.where(pos[:, None], (sm0 / (sm5 * sm5))[:, None] * D5, 0.0)
             th = -(dR - self.nu[:, None] * dPhi)
+            if self.limited and len(self.fs_walls):
+                # + kappa^T dFS/dtheta: the face states of walls a pressure face reads, through the incoming half
+                # rho_Gamma sm[15:20] (rho_Gamma = -sm0 / sm5)
+                fw = self.fs_walls
+                k = np.searchsorted(w, fw)
+                mb = self._mom_bar()[fw]
+                sm0f, sm5f = sol.bsums[fw, 0], sol.bsums[fw, 5]
+                pos_f = self.wall_pos[fw]
+                rgf = np.where(pos_f, -sm0f / np.where(pos_f, sm5f, -1.0), 0.0)
+                drg = np.where(pos_f, sm0f / np.where(pos_f, sm5f * sm5f, 1.0), 0.0)
+                smi = sol.bsums[fw, 15:20]
+                th[k] += rgf[:, None] * np.einsum("fk,fkj->fj", mb, self.Dw) + \
+                    (drg * np.sum(mb * smi, 1))[:, None] * self.d5w
             if len(self.deq_wall):
                 # through the correction of (1, u_w, T_w) to its discrete Maxwellian
                 th[self.deq_wall] = self.wall_deq.pullback(th[self.deq_wall])
@@ -459,6 +745,15 @@ class KineticAdjoint:
             with np.errstate(divide="ignore", invalid="ignore"):
                 nu_t = np.where(pos, self.nu * S[:, 9] / sm5, 0.0)
             dA[w] = np.where(self.axis[w] >= 0, S[:, 7] + S[:, 8] + nu_t, np.nan)
+            if self.limited and len(self.fs_walls):
+                # + kappa^T dFS/dalpha: rho_Gamma = -(sm0 + (1 - alpha) S_spec) / sm5 and the specular part
+                # (1 - alpha) sum_in w psi f_spec of the wall's face moments
+                fw = self.fs_walls
+                mb = self._mom_bar()[fw]
+                Sf = face[fw]
+                pos_f = self.wall_pos[fw]
+                ratio = np.where(pos_f, Sf[:, 9] / np.where(pos_f, sol.bsums[fw, 5], -1.0), 0.0)
+                dA[fw] += np.sum(mb * (ratio[:, None] * sol.bsums[fw, 15:20] - Sf[:, 13:18]), 1)
         J = sol.mass_flow()[2]
         return AdjointResult(J=J, dJ_dmu0=dmu, dJ_dTw=dTw, dJ_dalpha=dA, iterations=iterations, residual=residual,
                              history=list(self.history))

@@ -15,7 +15,7 @@ from . import abi
 from ._lib import load_library
 
 
-ADJ_FACE_SUMS = 13  # per boundary face sums of kin_adjoint_reduce
+ADJ_FACE_SUMS = 18  # per boundary face sums of kin_adjoint_reduce
 ADJ_CELL_SUMS = 19  # per cell sums of kin_adjoint_reduce
 
 
@@ -107,6 +107,15 @@ class KineticBackendABI:
                    abi.as_ptr(cell, C.c_double) if cells else None, cell.size if cells else 0,
                    abi.as_ptr(face, C.c_double) if faces else None, self.n_bfaces * ADJ_FACE_SUMS if faces else 0)
         return cell, (face[:self.n_bfaces * ADJ_FACE_SUMS] if faces else None)
+
+    def adjoint_face_moment_seeds(self, seeds) -> None:
+        """Seeds (n_bfaces, 5) on the boundary faces' moment sums for the following adjoint_reduce calls; None
+        removes them."""
+        if seeds is None:
+            self._call("adjoint_face_moment_seeds", None, 0)
+            return
+        a = np.ascontiguousarray(seeds, dtype=np.float64).ravel()
+        self._call("adjoint_face_moment_seeds", abi.as_ptr(a, C.c_double), a.size)
 
     def adjoint_update(self, coef, run_passes: bool = True, want_operator: bool = False):
         c = np.ascontiguousarray(coef, dtype=np.float64).ravel()

@@ -25,6 +25,11 @@ __device__ __forceinline__ double ld(const S* p, int64_t i) {
   return static_cast<double>(p[i]);
 }
 
+// seed weight of the face moment sums sum_q w psi(xi_q) f_b(q), psi = (1, xi, |xi|^2 / 2), at one velocity
+__device__ __forceinline__ double face_moment_seed(const double* __restrict__ m, double x, double y, double z) {
+  return m[0] + m[1] * x + m[2] * y + m[3] * z + m[4] * (0.5 * (x * x + y * y + z * z));
+}
+
 template <class S>
 __device__ __forceinline__ double entry_value(const View<S, double>& v, const CsrE<double>& c, int cell, int q,
                                               double x, double y, double z, double fi) {
@@ -174,9 +179,16 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_transport(View<S, double> v
           const int qm = v.mirror_map[b.mirror * nv + q];
           const double am = v.xi_x[qm] * c.s[0] + v.xi_y[qm] * c.s[1] + v.xi_z[qm] * c.s[2];
           sig = (ae >= 0.0 ? ae * li : 0.0) + (am < 0.0 ? am * lam_at(a, nv, cell, qm) : 0.0);
+          // face moment sums: this value is the outgoing half at q and the incoming half at qm (mirror weights are
+          // equal on every grid of the reference)
+          if (a.mom_mu != nullptr && ae >= 0.0) {
+            sig += wq * face_moment_seed(a.mom_mu + 5 * c.bface, x, y, z);
+            if (am < 0.0) sig += wq * face_moment_seed(a.mom_mu + 5 * c.bface, v.xi_x[qm], v.xi_y[qm], v.xi_z[qm]);
+          }
         } else {
           if (ae < 0.0) continue;  // incoming inflow value: k_adj_faces
           sig = ae * (li + (a.mu != nullptr ? wq * a.mu[c.bface] : 0.0));
+          if (a.mom_mu != nullptr) sig += wq * face_moment_seed(a.mom_mu + 5 * c.bface, x, y, z);
         }
       }
       lf += sig;
@@ -263,8 +275,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_transport(View<S, double> v
 // diffuse wall aligned with an axis, the partially specular inflow rho M + (1 - alpha) f_spec of a Maxwell wall
 // (maxwell_inflow / reflected_value, src/kinetic/kinetic_kernels.hpp:86-133) gives the accommodation derivative at
 // alpha = 1 from A1 = sum_in a lambda f_spec (f_spec: the owner's reconstructed face value at the reflected
-// velocity), A2 = sum_in s_grad f_o(reflected) (the first-order specular value of the gradient) and
-// S_spec = sum_in w an f_spec.
+// velocity), A2 = sum_in s_grad f_o(reflected) (the first-order specular value of the gradient),
+// S_spec = sum_in w an f_spec and, for the face state of the limited pressure-boundary reconstruction,
+// sum_in w psi f_spec (5).
 template <class S>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<S, double> v, AdjView<S> a, double* __restrict__ out) {
   __shared__ double sh[kAdjFaceSums * (kAdjThreads / 32)];
@@ -319,6 +332,13 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_faces(View<S, double> v, Ad
         s[7] += ae * lam_at(a, nv, o, q) * fspec;
         s[8] += sgrad * fr;
         s[9] += wq * ae / bf.area * fspec;
+        // the specular part's share of the face moment sums (the accommodation derivative of the face state)
+        const double wf = wq * fspec;
+        s[13] += wf;
+        s[14] += wf * x;
+        s[15] += wf * y;
+        s[16] += wf * z;
+        s[17] += wf * (0.5 * (x * x + y * y + z * z));
       }
     }
   }

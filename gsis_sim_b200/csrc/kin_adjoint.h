@@ -29,7 +29,8 @@ namespace kin {
 // the discrete one also sum lambda E F psi (5) and sum lambda E psi (5), the derivative sums then at fixed
 // (beta, gamma) (the host finishes the chain through the Newton solve)
 constexpr int kAdjCellSums = 19;
-constexpr int kAdjFaceSums = 13;  // S0, S1 (3), S2, S5, S6, A1, A2, S_spec, S6 c (3) (k_adj_faces)
+// S0, S1 (3), S2, S5, S6, A1, A2, S_spec, S6 c (3), sum_in w psi f_spec (5) (k_adj_faces)
+constexpr int kAdjFaceSums = 18;
 constexpr int kAdjCoefs = 8;      // a0, a (3), a2, b (3)
 
 template <class S>
@@ -46,6 +47,9 @@ struct AdjView {
   int8_t* imin;
   S* lfb;                  // seeds that land on f[cell][q] itself
   const double* mu;        // per boundary face: seed weight of the outgoing face values (nu and objective terms)
+  const double* mom_mu;    // per boundary face (5), nullptr if none: seed of the face moment sums
+                           // sum_q w psi(xi_q) f_b(q), psi = (1, xi, |xi|^2 / 2) (the face states that the limited
+                           // pressure-boundary reconstruction reads)
   const int32_t* flip;     // [axis][q]: position of xi with component `axis` negated (3 x nv)
   const int32_t* face_axis;  // per boundary face: the axis its normal is aligned with, -1 if none
   const double* coef;      // per cell: moment expansion coefficients (kAdjCoefs)

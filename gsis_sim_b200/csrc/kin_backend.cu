@@ -219,6 +219,7 @@ struct KinHandle {
   virtual void adjoint_get(double* lam, int64_t n) = 0;
   virtual void adjoint_reduce(const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell, double* face_sums,
                               int64_t n_face) = 0;
+  virtual void adjoint_face_moment_seeds(const double* seeds, int64_t n) = 0;
   virtual void adjoint_update(const double* coef, int64_t n_coef, double* res_cell, int64_t n_res, int32_t run_passes,
                               double* op_out, int64_t n_op) = 0;
   virtual void adjoint_end() = 0;
@@ -355,6 +356,8 @@ struct Backend final : KinHandle {
   bool adj_on = false;
   DevBuf<S> adj_lam, adj_lfb, adj_hmax, adj_hmin;  // of the storage type (FP32 in mixed precision)
   DevBuf<double> adj_mu, adj_coef, adj_cell, adj_face, adj_res;
+  DevBuf<double> adj_mom;  // per boundary face (5): seeds of the face moment sums (limited pressure reconstruction)
+  bool adj_mom_on = false;
   DevBuf<int8_t> adj_imax, adj_imin;
   DevBuf<int32_t> adj_rev, adj_rev_entry, adj_perm2, adj_inv2, adj_flip, adj_face_axis;
   DevBuf<int32_t> adj_face_cells;  // owners of wall and pressure faces (the transport the per-face sums need)
@@ -1652,6 +1655,7 @@ struct Backend final : KinHandle {
     a.imin = adj_imin.p;
     a.lfb = adj_lfb.p;
     a.mu = adj_mu.p;
+    a.mom_mu = adj_mom_on ? adj_mom.p : nullptr;
     a.flip = adj_flip.p;
     a.face_axis = adj_face_axis.p;
     a.coef = adj_coef.p;
@@ -1717,6 +1721,23 @@ struct Backend final : KinHandle {
     }
   }
 
+  void adjoint_face_moment_seeds(const double* seeds, int64_t n) override {
+    if constexpr (std::is_same<M, double>::value) {
+      KCHECK(adj_on, "adjoint_begin first");
+      if (seeds == nullptr || n == 0) {
+        adj_mom_on = false;
+        return;
+      }
+      KCHECK(n == 5 * static_cast<int64_t>(nb), "adjoint_face_moment_seeds: length must be 5 * n_bfaces");
+      if (adj_mom.n < static_cast<size_t>(n)) adj_mom.alloc(static_cast<size_t>(n));
+      KCUDA(cudaMemcpyAsync(adj_mom.p, seeds, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+      KCUDA(cudaStreamSynchronize(stream));
+      adj_mom_on = true;
+    } else {
+      throw KinError(KIN_E_ARG, "the adjoint needs an FP64 or mixed-precision handle");
+    }
+  }
+
   void adjoint_update(const double* coef, int64_t n_coef, double* res_cell, int64_t n_res, int32_t run_passes,
                       double* op_out, int64_t n_op) override {
     if constexpr (std::is_same<M, double>::value) {
@@ -1756,7 +1777,8 @@ struct Backend final : KinHandle {
 
   void adjoint_end() override {
     for (auto* b : {&adj_lam, &adj_lfb, &adj_hmax, &adj_hmin}) b->release();
-    for (auto* b : {&adj_mu, &adj_coef, &adj_cell, &adj_face, &adj_res}) b->release();
+    for (auto* b : {&adj_mu, &adj_coef, &adj_cell, &adj_face, &adj_res, &adj_mom}) b->release();
+    adj_mom_on = false;
     adj_imax.release();
     adj_imin.release();
     adj_rev.release();
@@ -1904,6 +1926,9 @@ int kin_adjoint_get(KinHandle* h, double* lam, int64_t n) { return guard(h, [&] 
 int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,
                        double* face_sums, int64_t n_face) {
   return guard(h, [&] { h->adjoint_reduce(mu, n_mu, cell_sums, n_cell, face_sums, n_face); });
+}
+int kin_adjoint_face_moment_seeds(KinHandle* h, const double* seeds, int64_t n) {
+  return guard(h, [&] { h->adjoint_face_moment_seeds(seeds, n); });
 }
 int kin_adjoint_update(KinHandle* h, const double* coef, int64_t n_coef, double* res_cell, int64_t n_res,
                        int32_t run_passes, double* op_out, int64_t n_op) {

@@ -339,14 +339,21 @@ int kin_adjoint_get(KinHandle* h, double* lambda, int64_t n);
    other cells); per boundary face: S0, S1 (3), S2 of the seeds on the incoming inflow values against the inflow
    Maxwellian (M, M c, M c^2) and S5, S6 = sum_in w an M {c^2, 1} / area; A1 = sum_in a lambda f_spec,
    A2 = sum_in s_grad f_owner(reflected velocity), S_spec = sum_in w an f_spec (axis-aligned diffuse walls,
-   f_spec = the owner's reconstructed face value at the reflected velocity; zero elsewhere); and (13 in all)
-   sum_in w an M c / area (3). cell_sums = NULL with n_cell = 0 skips the per-cell sums, face_sums = NULL
+   f_spec = the owner's reconstructed face value at the reflected velocity; zero elsewhere); sum_in w an M c / area
+   (3); and (18 in all) sum_in w psi f_spec (5, psi = (1, xi, |xi|^2 / 2), axis-aligned diffuse walls). cell_sums = NULL with n_cell = 0 skips the per-cell sums, face_sums = NULL
    with n_face = 0 the per-face sums; the transposed transport (the seeds that kin_adjoint_update gathers) always
    runs, on every cell, except with cell_sums = NULL and face_sums given: then it runs on the owner cells of wall and
    pressure faces only (all the per-face sums read) and the other cells keep their seeds of the previous call, so a
    kin_adjoint_update must follow a call that ran the full transport. */
 int kin_adjoint_reduce(KinHandle* h, const double* mu, int64_t n_mu, double* cell_sums, int64_t n_cell,
                        double* face_sums, int64_t n_face);
+/* Seeds on the moment sums of the boundary faces' distributions (the face states of the boundary sums, which the
+   "limited" pressure-boundary reconstruction reads: src/kinetic/kinetic_solver.cpp:172-260, 280-335): seeds[5 b + k]
+   (n = 5 n_bfaces) is the weight of the seed w_q psi_k(xi_q) on the outgoing reconstructed face value of boundary face
+   b at velocity q, psi = (1, xi_x, xi_y, xi_z, |xi|^2 / 2); at a symmetry face the value also carries the incoming
+   half at the mirrored velocity. Kept for the following kin_adjoint_reduce calls; seeds = NULL with n = 0 removes
+   them. Extends the adjoint of the "cell" reconstruction, which needs none; no reference counterpart. */
+int kin_adjoint_face_moment_seeds(KinHandle* h, const double* seeds, int64_t n);
 /* Finish O_f(y) with the per-cell moment-expansion coefficients coef (8 per cell: a0, a (3), a2, b (3); the term
    w_q (a0 + a.c + a2 c^2 + b.c c^2), c = xi_q - u_cell), return sum_q O_f^2 per cell in res_cell and, if op_out is not
    NULL, O_f(y) itself (storage order); with run_passes != 0 then update lambda by the LU-SGS block passes of the

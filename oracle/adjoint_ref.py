@@ -5,12 +5,17 @@ The steady discrete problem that the CIS iteration of the reference converges to
 prepare + sweep, src/kinetic/kinetic_kernels.hpp) is written here as one differentiable map in torch (float64, CPU),
 and its transposed Jacobian is taken by autograd:
 
-  unknowns   x = (f [cell][velocity], rho_Gamma [diffuse wall face])
-  equations  R(f, rho_Gamma; p) = 0       the residual of residual_value (kinetic_kernels.hpp:238-278) with the
+  unknowns   x = (f [cell][velocity], rho_Gamma [diffuse wall face], with the "limited" pressure-boundary
+             reconstruction also fs [boundary face][rho, u, T])
+  equations  R(f, rho_Gamma, fs; p) = 0   the residual of residual_value (kinetic_kernels.hpp:238-278) with the
                                           limited LSQ gradient (:161-201), the Shakhov target of the cell moments
                                           (make_cell_params :451-471) and the inflow of the boundary faces
              rho_Gamma - Phi(f, rho_Gamma) = 0   zero net mass flux of each diffuse wall face
                                           (process_boundary_sums, kinetic_solver.cpp:280-335)
+             fs - FS(f, fs) = 0           the face states of the boundary sums (the same function), which the limited
+                                          reconstruction of the pressure faces' W_b reads (update_pressure_inflow,
+                                          kinetic_solver.cpp:172-260); FS of a pressure face depends on fs through
+                                          its own inflow
   objective  J = M_dot = 1/2 (mdot_in + mdot_out) sqrt(2/pi) from the patch flows of the boundary sums
   parameters p = (mu_hat0, T_w per boundary face, accommodation alpha per wall face at 1: the partially specular
              inflow rho M + (1 - alpha) f_spec of axis-aligned walls, maxwell_inflow / reflected_value,
@@ -20,8 +25,8 @@ The adjoint y solves (dF/dx)^T y = dJ/dx (GMRES over autograd vector-Jacobian pr
 dJ/dp = dJ/dp|_x - y^T dF/dp.
 
 Scope (the same as the B200 adjoint; `check_scope` raises outside it): diffuse walls, pressure inlets / outlets with
-the "cell" boundary reconstruction (W_b from the owner cell, App. A.2 acoustic correction), vacuum, symmetry and
-periodic faces; Venkatakrishnan limiter (absolute or relative epsilon) or none; no positivity limiter, no closed-domain
+the "limited" or the "cell" boundary reconstruction (W_b reconstructed at the face, or the owner cell's state; App.
+A.2 acoustic correction), vacuum, symmetry and periodic faces; Venkatakrishnan limiter (absolute or relative epsilon) or none; no positivity limiter, no closed-domain
 scaling, no mass-flow inlets, no Maxwell walls.
 
 Equilibrium: the continuous Maxwellian, or the discrete one (kinetic.equilibrium = "discrete", the reference default):
@@ -134,6 +139,55 @@ class SteadyMap:
         self.baligned = torch.as_tensor(aligned)
         self.eflip = self.bflip[self.bface]  # (nc, E, nv)
         self.setup, self.host = setup, host
+        self.n_wall = len(self.wall_idx)
+        # per boundary face: the storage position of the mirrored velocity (symmetry faces), q elsewhere
+        self.bmirror = torch.as_tensor(np.where((bkind == BC_SYMMETRY)[:, None], q[None, :] ^ mx[:, None],
+                                                q[None, :]))
+        # the "limited" pressure-boundary reconstruction (the reference default): the face states of the boundary
+        # sums become auxiliary unknowns
+        self.limited = (host.pressure_boundary_reconstruction != "cell" and bool(torch.any(self.bkind == BC_PRESSURE)))
+        if self.limited:
+            self._pressure_stencils(s, host)
+        self.n_aux = self.n_wall + (5 * self.nb if self.limited else 0)
+
+    def _pressure_stencils(self, s, host):
+        """Padded CSR stencils of the owners of the pressure faces (update_pressure_inflow, kinetic_solver.cpp:172-260)
+        with the host geometry the solver uses."""
+        pres = np.flatnonzero(self.bkind.numpy() == BC_PRESSURE)
+        off = np.asarray(s["csr_offsets"], np.int64)
+        own = np.asarray(s["bface_owner"], np.int64)[pres]
+        cnt = off[own + 1] - off[own]
+        E = int(cnt.max())
+        ent = off[own][:, None] + np.arange(E)[None, :]
+        mask = np.arange(E)[None, :] < cnt[:, None]
+        ent = np.where(mask, ent, 0)
+        other = np.where(mask, np.asarray(s["csr_other"])[ent], -1)
+        bface = np.where(mask, np.asarray(s["csr_bface"])[ent], -1)
+        bkind = np.asarray(s["bface_kind"])
+        periodic = mask & (bface >= 0) & (bkind[np.maximum(bface, 0)] == BC_PERIODIC)
+        fk = np.asarray(host.csr_faces)[ent]
+        cc = np.asarray(host.cell_center, float)
+        fg = host.n_internal_faces + pres
+        self.p_idx = torch.as_tensor(pres)
+        self.p_own = torch.as_tensor(own)
+        self.p_mask = torch.as_tensor(mask)
+        self.p_internal = torch.as_tensor(mask & (other >= 0))
+        self.p_other = torch.as_tensor(np.maximum(other, 0))
+        self.p_bmask = torch.as_tensor(mask & (bface >= 0) & ~periodic)
+        self.p_bface = torch.as_tensor(np.maximum(bface, 0))
+        self.p_periodic = torch.as_tensor(periodic)
+        self.p_lsq = _t(np.asarray(host.lsq, float)[ent])                                   # (np, E, 3)
+        self.p_dx = _t(np.asarray(host.face_center, float)[fk] - cc[own][:, None, :])       # (np, E, 3)
+        self.p_dxb = _t(np.asarray(host.face_center, float)[fg] - cc[own])                  # (np, 3)
+        self.p_eps2 = _t(host.limiter_k ** 3 * np.asarray(s["volume"], float)[own])
+        self.p_limit = int(s["limiter_mode"]) != LIMITER_NONE
+
+    def split_aux(self, z):
+        """The auxiliary unknowns (rho_Gamma of the walls, then the face states (nb, 5) with the limited
+        reconstruction) of one vector."""
+        rg = z[:self.n_wall]
+        fs = z[self.n_wall:].view(self.nb, 5) if self.limited else None
+        return rg, fs
 
     # ---- scope ---------------------------------------------------------------------------------------------------
     def check_scope(self, solver=None):
@@ -146,8 +200,6 @@ class SteadyMap:
             raise ScopeError("Maxwell walls (alpha < 1)")
         if "mass_flow_inlet" in self.ptype_names:
             raise ScopeError("mass-flow inlets")
-        if torch.any(self.bkind == BC_PRESSURE) and h.pressure_boundary_reconstruction != "cell":
-            raise ScopeError('pressure boundaries need pressure_boundary_reconstruction = "cell"')
         if int(s["deq_fallback_collisionless"]) and solver is not None and solver.discrete_eq:
             if solver.backend.deq_counts()[1] > 0:
                 raise ScopeError("a cell's discrete equilibrium failed (collisionless fallback)")
@@ -266,15 +318,60 @@ class SteadyMap:
         coll = self.volume * p / (mu0 * T ** self.omega)
         return coll, fS, (rho, u, T, p, q)
 
-    def inflow(self, mom, rho_gamma, Tw):
+    def limited_state(self, mom, fs):
+        """W_ib = (p, u, T) of the pressure faces' owners reconstructed at the face (update_pressure_inflow,
+        kinetic_solver.cpp:172-260): LSQ gradient over the owner's stencil, whose boundary entries carry the face
+        state (rho, u, T) of the last boundary sums where it is positive (periodic entries and the others the owner's
+        own value); Venkatakrishnan limiter with the absolute epsilon^2 = K^3 V; the owner's value where the
+        reconstruction is not positive. (np, 5)"""
+        rho, u, T, p, q = mom
+        st = torch.cat([p[:, None], u, T[:, None]], 1)  # (nc, 5): p, u, T
+        wi = st[self.p_own]
+        fsw = torch.stack([fs[:, 0] * fs[:, 4], fs[:, 1], fs[:, 2], fs[:, 3], fs[:, 4]], 1)[self.p_bface]
+        fsd = fs.detach()[self.p_bface]
+        use = self.p_bmask & (fsd[..., 0] > 0) & (fsd[..., 4] > 0)
+        wiE = wi[:, None, :].expand(-1, self.p_mask.shape[1], -1)
+        wk = torch.where(self.p_internal[..., None], st[self.p_other], torch.where(use[..., None], fsw, wiE))
+        wk = torch.where(self.p_mask[..., None], wk, wiE)
+        grad = torch.einsum("fek,fea->fka", wk - wi[:, None, :], self.p_lsq)  # (np, 5, 3)
+        wmax = torch.maximum(wi, wk.amax(1))
+        wmin = torch.minimum(wi, wk.amin(1))
+        phi = torch.ones_like(wi)
+        if self.p_limit:
+            proj = torch.einsum("fka,fea->fke", grad, self.p_dx)  # (np, 5, E)
+            dmax = (wmax - wi)[..., None]
+            dmin = (wmin - wi)[..., None]
+            d1 = torch.where(proj > 0, dmax.expand_as(proj), torch.where(proj < 0, dmin.expand_as(proj),
+                                                                          torch.zeros_like(proj)))
+            e2 = self.p_eps2[:, None, None]
+            num = (d1 * d1 + e2) + 2.0 * d1 * proj
+            den = d1 * d1 + 2.0 * proj * proj + d1 * proj + e2
+            ok = den > 0
+            v = torch.clamp(num / torch.where(ok, den, torch.ones_like(den)), 0.0, 1.0)
+            v = torch.where(ok, v, torch.zeros_like(v))
+            v = torch.where(proj == 0, torch.ones_like(v), v)
+            active = (self.p_mask & ~self.p_periodic)[:, None, :]
+            v = torch.where(active, v, torch.ones_like(v))
+            phi = torch.clamp(v.amin(2), max=1.0)
+        wib = wi + phi * torch.einsum("fka,fa->fk", grad, self.p_dxb)
+        good = (wib.detach()[:, 0] > 0) & (wib.detach()[:, 4] > 0)
+        return torch.where(good[:, None], wib, wi)
+
+    def inflow(self, mom, rho_gamma, Tw, fs=None):
         """(scale (nb,), Maxwellian values (nb, nv)) of every boundary face; walls at rest-frame density 1 with the
-        wall velocity and temperature Tw, pressure faces W_b of the owner cell (App. A.2, kinetic_solver.cpp:172-260,
-        "cell" reconstruction)."""
+        wall velocity and temperature Tw, pressure faces W_b (App. A.2, kinetic_solver.cpp:172-260) from the owner
+        cell ("cell" reconstruction) or from its limited reconstruction at the face with the face states fs."""
         rho, u, T, p, q = mom
         nb = self.nb
         own = self.bowner
-        # pressure: (p_ib, u_ib, T_ib) = owner state
+        # pressure: (p_ib, u_ib, T_ib) = owner state, or its reconstruction at the face
         p_ib, u_ib, T_ib = p[own], u[own], T[own]
+        if self.limited:
+            wib = self.limited_state(mom, fs)
+            pi = self.p_idx
+            p_ib = p_ib.index_put((pi,), wib[:, 0])
+            u_ib = u_ib.index_put((pi,), wib[:, 1:4])
+            T_ib = T_ib.index_put((pi,), wib[:, 4])
         rho_ib = p_ib / T_ib
         cs = torch.sqrt(self.gamma * T_ib)
         T_b = torch.where(self.inlet_face, self.T_patch, T_ib)
@@ -391,14 +488,53 @@ class SteadyMap:
         sspec = torch.where(out, torch.zeros_like(fb), self.w * an * spec).sum(1)
         return sm0, sm5, sspec
 
+    def face_states(self, f, g, M, sm0, sm5, sspec, alpha):
+        """face_state (rho, u, T) of every boundary face from the moment sums of the face distribution
+        (k_boundary_sums, kinetic_cuda_kernels.cu:275-323, and process_boundary_sums, kinetic_solver.cpp:280-335):
+        the outgoing half the reconstructed face values, the incoming half the mirrored face values (symmetry), the
+        inflow Maxwellian (pressure), rho_Gamma times the unit wall Maxwellian (walls; rho_Gamma = -sm0 / sm5 of
+        these sums, plus the specular part (1 - alpha) f_spec of a Maxwell wall) or nothing (vacuum). (nb, 5)"""
+        own = self.bowner
+        an = self.bn @ self.xi.T  # (nb, nv)
+        fb = f[own] + (g[own] * self.bd[:, None, :]).sum(-1)
+        out = (an >= 0) | (self.bkind == BC_PERIODIC)[:, None]
+        psi = torch.cat([torch.ones(self.nv, 1, dtype=torch.float64), self.xi,
+                         0.5 * (self.xi * self.xi).sum(-1, keepdim=True)], 1)  # (nv, 5)
+        zero = torch.zeros_like(fb)
+        smo = torch.where(out, self.w * fb, zero) @ psi
+        fin = torch.where((self.bkind == BC_SYMMETRY)[:, None], torch.gather(fb, 1, self.bmirror), M)
+        smi = torch.where(out, zero, self.w * fin) @ psi
+        wall = self.wall
+        rg = torch.where(sm5 < 0, torch.clamp(-(sm0 + (1.0 - alpha) * sspec) / torch.where(sm5 < 0, sm5,
+                                                                                            -torch.ones_like(sm5)),
+                                               min=0.0), torch.zeros_like(sm5))
+        in_scale = torch.where(wall, rg, torch.where(self.bkind == BC_VACUUM, torch.zeros_like(rg),
+                                                     torch.ones_like(rg)))
+        mom = smo + in_scale[:, None] * smi
+        # the specular part of a wall with alpha < 1: (1 - alpha) sum_in w psi f_spec
+        fr = torch.gather(f[own], 1, self.bflip)
+        gr = torch.gather(g[own], 1, self.bflip[..., None].expand(-1, -1, 3))
+        spec = fr + (gr * self.bd[:, None, :]).sum(-1)
+        spec_mom = torch.where(out, zero, self.w * spec) @ psi
+        mom = mom + torch.where(wall[:, None], (1.0 - alpha)[:, None] * spec_mom, torch.zeros_like(mom))
+        pos = mom.detach()[:, 0] > 0
+        m0 = torch.where(pos, mom[:, 0], torch.ones_like(mom[:, 0]))
+        u = mom[:, 1:4] / m0[:, None]
+        T = (2.0 * mom[:, 4] / m0 - (u * u).sum(1)) / 3.0
+        fs = torch.cat([mom[:, :1], u, T[:, None]], 1)
+        return torch.where(pos[:, None], fs, torch.zeros_like(fs))
+
     # ---- the map -------------------------------------------------------------------------------------------------
-    def evaluate(self, f, rho_gamma, mu0, Tw, alpha=None):
-        """(R (nc, nv), wall equations rho_Gamma - Phi (n_wall,), J = M_dot). alpha (per boundary face, walls only;
-        default 1): the accommodation, with the specular part of axis-aligned walls (a Maxwell wall)."""
+    def evaluate(self, f, aux, mu0, Tw, alpha=None):
+        """(R (nc, nv), auxiliary equations (n_aux,), J = M_dot). aux: the auxiliary unknowns (split_aux): rho_Gamma
+        of the walls with their zero-net-flux equations rho_Gamma - Phi, and with the limited reconstruction the face
+        states with fs - FS(f, fs). alpha (per boundary face, walls only; default 1): the accommodation, with the
+        specular part of axis-aligned walls (a Maxwell wall)."""
         if alpha is None:
             alpha = torch.ones(self.nb, dtype=torch.float64)
+        rho_gamma, fs = self.split_aux(aux)
         coll, fS, mom = self.target(f, mu0)
-        scale, M = self.inflow(mom, rho_gamma, Tw)
+        scale, M = self.inflow(mom, rho_gamma, Tw, fs)
         fk, a, infl = self._entry_f(f, scale, M, alpha)
         g = self.gradient(f, fk)
         R = self.residual(f, g, fk, a, infl, coll, fS, alpha, scale, M)
@@ -406,6 +542,8 @@ class SteadyMap:
         wi = self.wall_idx
         phi = torch.clamp(-(sm0[wi] + (1.0 - alpha[wi]) * sspec[wi]) / sm5[wi], min=0.0)
         Fw = rho_gamma - phi
+        if self.limited:
+            Fw = torch.cat([Fw, (fs - self.face_states(f, g, M, sm0, sm5, sspec, alpha)).ravel()])
         in_scale = scale  # pressure 1, vacuum 0, walls rho_Gamma
         flow = self.barea * (sm0 + in_scale * sm5)
         mdot_in = -flow[self.inlet_face].sum()
@@ -418,16 +556,24 @@ class SteadyMap:
         return torch.tensor(self.mu0, dtype=torch.float64), Tw
 
 
-def state_of(solver):
-    """(f, rho_Gamma of the wall faces) of a KineticSolver (internal numbering, storage order)."""
+def state_of(solver, limited=None):
+    """(f, auxiliary unknowns) of a KineticSolver (internal numbering, storage order): rho_Gamma of the wall faces,
+    followed by the face states (nb, 5) of the last boundary sums when the pressure faces use the limited
+    reconstruction (limited=None: decided from the solver's set-up)."""
     f = torch.as_tensor(np.asarray(solver.backend.get_distribution(), float))
     wall = np.flatnonzero(solver.bkind == BC_DIFFUSE_WALL)
-    return f, torch.as_tensor(solver.inflow[wall, 0].copy())
+    aux = [np.asarray(solver.inflow[wall, 0], float)]
+    if limited is None:
+        limited = solver.h.pressure_boundary_reconstruction != "cell" and bool(np.any(solver.bkind == BC_PRESSURE))
+    if limited:
+        aux.append(np.asarray(solver.face_state, float).ravel())
+    return f, torch.as_tensor(np.concatenate(aux))
 
 
 def adjoint_gradient(sm: SteadyMap, f, rho_gamma, tol=1e-12, maxiter=4000):
     """dJ/d(mu_hat0), dJ/dT_w and dJ/dalpha (per boundary face; alpha at 1, the derivative from below) at the fixed
-    point (f, rho_Gamma), with the adjoint solved by GMRES. Returns (dJ_dmu0, dJ_dTw (nb,), info) with
+    point (f, auxiliary unknowns of state_of: rho_Gamma, and the face states with the limited reconstruction), with
+    the adjoint solved by GMRES. Returns (dJ_dmu0, dJ_dTw (nb,), info) with
     info = (J, ||F||, gmres iterations, y, dJ_dalpha (nb,))."""
     from scipy.sparse.linalg import LinearOperator, gmres
 
@@ -473,7 +619,8 @@ def adjoint_gradient(sm: SteadyMap, f, rho_gamma, tol=1e-12, maxiter=4000):
 
 
 def transposed_jacobian_product(sm: SteadyMap, f, rho_gamma, y_f, y_w):
-    """(dF/dx)^T y at (f, rho_Gamma): the adjoint residual operator the B200 kernels compute. Returns (x_f, x_w)."""
+    """(dF/dx)^T y at (f, auxiliary unknowns): the adjoint residual operator the B200 kernels compute; y_w in the
+    layout of the auxiliary unknowns. Returns (x_f, x_w)."""
     mu0, Tw = sm.params_of()
     f = f.clone().requires_grad_(True)
     rg = rho_gamma.clone().requires_grad_(True)

@@ -19,7 +19,8 @@ from gsis_sim_b200.solver import KineticSolver
 
 
 def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="periodic_slab", limiter="venkatakrishnan",
-                 eps="relative", half=False, quarter=False, alpha=1.0, equilibrium="continuous", precision="fp64"):
+                 eps="relative", half=False, quarter=False, alpha=1.0, equilibrium="continuous", precision="fp64",
+                 reconstruction="cell"):
     """Pressure-driven channel (inlet p 1, outlet p 0.5, diffuse walls) in the adjoint's scope; `half`: symmetry
     plane at y = 0 instead of the lower wall; `quarter`: a duct quarter, symmetry planes at y = 0 and z = 0, walls at
     y = 1 and z = 0.7 (a flow that varies in y and z)."""
@@ -35,7 +36,7 @@ def channel_case(mu_scale=1.0, Tw=1.0, n=(5, 3, 1), nv=(10, 10, 10), side="perio
         bcs.append(ks.BC("sym", "symmetry"))
     if quarter:
         bcs.append(ks.BC("symz", "symmetry"))
-    kp = ks.KineticParams(precision=precision, pressure_boundary_reconstruction="cell", limiter=limiter,
+    kp = ks.KineticParams(precision=precision, pressure_boundary_reconstruction=reconstruction, limiter=limiter,
                           limiter_eps=eps, sweep_blocks=1, equilibrium=equilibrium)
     setup, host = ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, Kn=0.3), bcs,
                                          ks.VelocityGrid(n=nv), kp)
@@ -64,23 +65,28 @@ def _oracle_solution(**kw):
 
 
 @pytest.mark.timeout(600)
-@pytest.mark.parametrize("equilibrium", ["continuous", "discrete"])
-def test_reference_adjoint_matches_finite_differences(equilibrium):
+@pytest.mark.parametrize("equilibrium,reconstruction", [("continuous", "cell"), ("discrete", "cell"),
+                                                        ("discrete", "limited")])
+def test_reference_adjoint_matches_finite_differences(equilibrium, reconstruction):
     """discrete: the reference default; on this 10^3 grid the Newton solve of the discrete Maxwellian is active in
-    every cell and for every wall and pressure-face inflow state."""
+    every cell and for every wall and pressure-face inflow state. limited: the reference's default pressure-boundary
+    reconstruction (W_b reconstructed at the face from the owner's stencil, with the face states of the boundary sums
+    as auxiliary unknowns)."""
     from oracle import adjoint_ref as ar
 
-    eq = dict(equilibrium=equilibrium)
+    eq = dict(equilibrium=equilibrium, reconstruction=reconstruction)
     sol, setup, host = _oracle_solution(**eq)
     if equilibrium == "discrete":
         assert sol.backend.deq_counts()[0] == sol.nc
     sm = ar.SteadyMap(setup, host)
+    assert sm.limited == (reconstruction == "limited")
     sm.check_scope(sol)
     f, rg = ar.state_of(sol)
+    assert rg.numel() == sm.n_aux
     mu0, Tw = sm.params_of()
     R, Fw, J = sm.evaluate(f, rg, mu0, Tw)
     # the torch map is the fixed point the oracle converged to
-    assert float(R.abs().max()) < 1e-13 and float(Fw.abs().max()) < 1e-13
+    assert float(R.abs().max()) < 1e-13 and float(Fw.abs().max()) < 1e-12
     assert abs(float(J) - sol.mass_flow()[2]) < 1e-14
     dmu, dTw, info = ar.adjoint_gradient(sm, f, rg)
     h = 1e-5
@@ -211,6 +217,76 @@ def test_pressure_face_adjoint_matches_autograd():
     assert np.allclose(Tb, gT.numpy(), rtol=1e-12, atol=1e-14)
 
 
+@pytest.mark.timeout(600)
+def test_limited_pressure_reconstruction_matches_autograd():
+    """PressureReconstruction (the "limited" W_b of update_pressure_inflow) equals the reference adjoint's torch form
+    in value at the oracle's converged state of the half channel (limiter active on some pressure faces), and its
+    vector-Jacobian product equals torch autograd with respect to the cell states and the face states."""
+    from oracle import adjoint_ref as ar
+
+    sol, setup, host = _oracle_solution(half=True, reconstruction="limited", equilibrium="discrete")
+    r = adj.PressureReconstruction(sol)
+    wib = r.forward(sol.moments_, sol.face_state)
+    assert np.any(r.estar >= 0) and np.all(r.good)
+    sm = ar.SteadyMap(setup, host)
+    m = sol.moments_
+    p = torch.tensor(m[:, 5], requires_grad=True)
+    u = torch.tensor(m[:, 1:4], requires_grad=True)
+    T = torch.tensor(m[:, 4], requires_grad=True)
+    fs = torch.tensor(sol.face_state, requires_grad=True)
+    wt = sm.limited_state((torch.tensor(m[:, 0]), u, T, p, None), fs)
+    assert np.max(np.abs(wt.detach().numpy() - wib)) <= 1e-14 * np.max(np.abs(wib))
+    wb = np.random.default_rng(3).standard_normal(wib.shape)
+    gp, gu, gT, gfs = torch.autograd.grad(wt, (p, u, T, fs), grad_outputs=torch.as_tensor(wb))
+    cell_bar, fs_bar = r.vjp(wb)
+    ref_cell = np.column_stack([gp.numpy(), gu.numpy(), gT.numpy()])
+    assert np.max(np.abs(cell_bar - ref_cell)) <= 1e-12 * np.max(np.abs(ref_cell))
+    assert np.max(np.abs(fs_bar - gfs.numpy())) <= 1e-12 * np.max(np.abs(gfs.numpy()))
+    assert np.max(np.abs(fs_bar)) > 0
+
+
+def test_face_state_and_inflow_derivatives():
+    """face_moment_state_adjoint against torch autograd of (rho, u, T) of the face moments; inflow_moment_derivatives
+    against central differences of the incoming-half sums of the Maxwellian."""
+    rng = np.random.default_rng(5)
+    mom = np.column_stack([0.5 + rng.random(6), 0.2 * rng.standard_normal((6, 3)), 2.0 + rng.random(6)])
+    mom[2, 0] = -1.0  # no face state
+    kap = rng.standard_normal((6, 5))
+    mt = torch.tensor(mom, requires_grad=True)
+    m0 = mt[:, 0]
+    ut = mt[:, 1:4] / m0[:, None]
+    Tt = (2.0 * mt[:, 4] / m0 - (ut * ut).sum(1)) / 3.0
+    fs = torch.cat([m0[:, None], ut, Tt[:, None]], 1)
+    (g,) = torch.autograd.grad(fs, mt, grad_outputs=torch.as_tensor(kap))
+    ref = g.numpy()
+    ref[2] = 0.0
+    out = adj.face_moment_state_adjoint(mom, kap)
+    assert np.max(np.abs(out - ref)) <= 1e-13 * np.max(np.abs(ref))
+    gr = np.linspace(-4.5, 4.5, 10)
+    xi = np.stack(np.meshgrid(gr, gr, gr, indexing="ij"), -1).reshape(-1, 3)
+    w = np.full(len(xi), (gr[1] - gr[0]) ** 3)
+    nrm = np.array([[1.0, 0.0, 0.0], [0.0, -0.6, 0.8]])
+    st = np.array([[1.0, 0.1, -0.2, 0.05, 1.1], [0.8, 0.0, 0.3, -0.1, 0.9]])
+    D, d5 = adj.inflow_moment_derivatives(xi, w, nrm, st)
+    psi = np.column_stack([np.ones(len(xi)), xi, 0.5 * np.sum(xi * xi, 1)])
+
+    def sums(n, s):
+        an = xi @ n
+        c = xi - s[1:4]
+        M = w * s[0] / (2 * np.pi * s[4]) ** 1.5 * np.exp(-np.sum(c * c, 1) / (2 * s[4]))
+        m = an < 0
+        return np.concatenate([psi[m].T @ M[m], [an[m] @ M[m]]])
+
+    h = 1e-6
+    for i in range(2):
+        for j in range(5):
+            e = np.zeros(5)
+            e[j] = h
+            fd = (sums(nrm[i], st[i] + e) - sums(nrm[i], st[i] - e)) / (2 * h)
+            assert np.max(np.abs(fd[:5] - D[i, :, j])) <= 1e-7 * max(np.max(np.abs(D[i])), 1.0)
+            assert abs(fd[5] - d5[i, j]) <= 1e-7 * max(np.max(np.abs(d5[i])), 1.0)
+
+
 def test_index_maps():
     setup, host = channel_case()
     xi = np.stack([setup["xi_x"], setup["xi_y"], setup["xi_z"]], 1)
@@ -229,14 +305,16 @@ def test_index_maps():
 
 
 @pytest.mark.timeout(600)
-def test_reversed_velocity_sweeps_solve_the_adjoint():
+@pytest.mark.parametrize("reconstruction", ["cell", "limited"])
+def test_reversed_velocity_sweeps_solve_the_adjoint(reconstruction):
     """The iteration scheme of gsis_sim_b200.adjoint on the CPU: the exact operator O(y) of the reference adjoint,
-    the wall adjoint recomputed from the current lambda, and the forward LU-SGS block passes (the oracle's) run on
-    velocity-reversed storage as the transposed preconditioner. It converges, and to the GMRES adjoint's gradients."""
+    the wall adjoint (and, with the limited pressure reconstruction, the face-state adjoint) recomputed from the
+    current lambda, and the forward LU-SGS block passes (the oracle's) run on velocity-reversed storage as the
+    transposed preconditioner. It converges, and to the GMRES adjoint's gradients."""
     from oracle import adjoint_ref as ar
     from oracle.kinetic_oracle import OracleBackend
 
-    sol, setup, host = _oracle_solution()
+    sol, setup, host = _oracle_solution(reconstruction=reconstruction)
     sm = ar.SteadyMap(setup, host)
     f, rg = ar.state_of(sol)
     mu0, Tw = sm.params_of()

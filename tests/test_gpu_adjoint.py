@@ -2,7 +2,9 @@
 oracle/adjoint_ref.py (the steady map transposed by torch autograd, itself pinned against finite differences in
 tests/test_adjoint.py), at the fixed point the B200 forward solver converged to:
 * the operator y^T dF/dx (and the objective term dJ/dx) for random adjoint states, to 1e-10, with the continuous
-  and with the discrete equilibrium (the Newton solve active in every cell and inflow state);
+  and with the discrete equilibrium (the Newton solve active in every cell and inflow state), and with the "cell"
+  and the "limited" pressure-boundary reconstruction (the reference default: W_b reconstructed at the face from the
+  owner's stencil and the face states of the boundary sums);
 * the converged adjoint's dM_dot/d mu_hat0, dM_dot/dT_w and dM_dot/d alpha (at alpha = 1), to 1e-8 against the
   reference adjoint and to 1e-5 against finite differences of the B200 forward solver (alpha: one-sided, through
   Maxwell-wall solves)."""
@@ -30,8 +32,12 @@ def _gpu_solution(**kw):
 # the gradient test covers (side="symmetry").
 @pytest.mark.parametrize("kw", [dict(), dict(half=True), dict(limiter="none"), dict(eps="absolute"),
                                 dict(n=(5, 3, 3), quarter=True), dict(n=(5, 3, 3), quarter=True, limiter="none"),
-                                dict(equilibrium="discrete"), dict(n=(5, 3, 3), quarter=True, equilibrium="discrete")])
+                                dict(equilibrium="discrete"), dict(n=(5, 3, 3), quarter=True, equilibrium="discrete"),
+                                dict(half=True, equilibrium="discrete", reconstruction="limited"),
+                                dict(n=(5, 3, 3), quarter=True, reconstruction="limited")])
 def test_gpu_adjoint_operator_matches_reference(kw):
+    """With the limited pressure reconstruction the auxiliary adjoint also carries the face states' kappa (5 per
+    boundary face; random on the faces a pressure face reads, zero on the others, whose face states nothing reads)."""
     from gsis_sim_b200.adjoint import KineticAdjoint
     from oracle import adjoint_ref as ar
 
@@ -41,9 +47,15 @@ def test_gpu_adjoint_operator_matches_reference(kw):
         ka = KineticAdjoint(sol)
         sm = ar.SteadyMap(setup, host)
         f, rg = ar.state_of(sol)
+        assert len(rg) == sm.n_aux and ka.limited == sm.limited
         rng = np.random.default_rng(11)
         lam = rng.standard_normal((sol.nc, sol.nv))
-        nu = rng.standard_normal(len(ka.wall))
+        nu = rng.standard_normal(sm.n_aux)
+        if ka.limited:
+            kap = np.zeros((sol.nb, 5))
+            kap[ka.fs_read] = nu[len(ka.wall):].reshape(sol.nb, 5)[ka.fs_read]
+            nu[len(ka.wall):] = kap.ravel()
+            assert len(ka.fs_read) > 0
         op_f, op_w = ka.operator(lam, nu, with_objective=False)
         ref_f, ref_w = ar.transposed_jacobian_product(sm, f, rg, lam, nu)
         scale = np.max(np.abs(ref_f))
@@ -102,7 +114,8 @@ def test_gpu_adjoint_operator_on_tube_mesh():
 
 
 @pytest.mark.timeout(900)
-@pytest.mark.parametrize("kw", [dict(), dict(side="symmetry"), dict(equilibrium="discrete")])
+@pytest.mark.parametrize("kw", [dict(), dict(side="symmetry"), dict(equilibrium="discrete"),
+                                dict(half=True, equilibrium="discrete", reconstruction="limited")])
 def test_gpu_adjoint_gradients_match_reference_and_finite_differences(kw):
     from gsis_sim_b200.adjoint import KineticAdjoint
     from oracle import adjoint_ref as ar
