@@ -330,18 +330,23 @@ def run_time_to_mdot(args, local):
     print(json.dumps(line), flush=True)
 
 
-def channel_case(delta=5.0, Tw=1.0, nv=24, n=(64, 32, 1), alpha=1.0):
+# the adjoint's discretisation choices: the reference's defaults (discrete equilibrium, "limited" pressure-boundary
+# reconstruction) or the simpler continuous equilibrium with the owner cell's state at pressure faces
+ADJ_SCHEMES = {"default": dict(equilibrium="discrete", pressure_boundary_reconstruction="limited"),
+               "continuous-cell": dict(equilibrium="continuous", pressure_boundary_reconstruction="cell")}
+
+
+def channel_case(delta=5.0, Tw=1.0, nv=24, n=(64, 32, 1), alpha=1.0, scheme="default"):
     """Pressure-driven channel: box n[0] x n[1] x 1 on x in [0, 4], y in [0, 1], one cell thick with periodic sides;
     inlet p 1, outlet p 0.5, T 1; walls at T_w with accommodation alpha (diffuse at 1); nv^3 uniform velocities on
-    [-5, 5]^3; FP64 with the continuous equilibrium and the "cell" pressure-boundary reconstruction (the adjoint's
-    scope)."""
+    [-5, 5]^3; FP64; the equilibrium and pressure-boundary reconstruction of ADJ_SCHEMES[scheme]."""
     from gsis_sim_b200 import kinetic_setup as ks
     from gsis_sim_b200.mesh import box_mesh
 
     m = box_mesh(n, (0.0, 0.0, 0.0), (4.0, 1.0, 1.0 / n[1]), ("inlet", "outlet", "wall", "wall", "side", "side"))
     bcs = [ks.BC("inlet", "pressure_inlet", T=1.0, p=1.0), ks.BC("outlet", "pressure_outlet", p=0.5),
            ks.BC("wall", "diffuse_wall", T=Tw, alpha=alpha), ks.BC("side", "periodic_slab")]
-    kp = ks.KineticParams(precision="fp64", equilibrium="continuous", pressure_boundary_reconstruction="cell")
+    kp = ks.KineticParams(precision="fp64", **ADJ_SCHEMES[scheme])
     return ks.build_kinetic_setup(m, ks.Gas(omega=0.81), ks.Conditions(L_ref=1.0, T0=273.15, delta_rp=delta), bcs,
                                   ks.VelocityGrid(n=(nv, nv, nv)), kp)
 
@@ -510,19 +515,18 @@ def adjoint_ratio(args, local):
         delta = 10.0
 
         def make(d):
-            return tube.tube_case(delta=d, nv=args.adj_nv, precision="fp64", equilibrium="continuous",
-                                  pressure_boundary_reconstruction="cell")
+            return tube.tube_case(delta=d, nv=args.adj_nv, precision="fp64", **ADJ_SCHEMES[args.adj_scheme])
 
         workload = (f"kinetic CIS, O-grid tube + reservoir 134528 cells, inlet p 1 / outlet p 0.01, diffuse walls, "
-                    f"{args.adj_nv}^3 velocities on [-5,5]^3, delta 10, continuous equilibrium")
+                    f"{args.adj_nv}^3 velocities on [-5,5]^3, delta 10, {args.adj_scheme} scheme")
     else:
         delta = 5.0
 
         def make(d, Tw=1.0, alpha=1.0):
-            return channel_case(delta=d, nv=args.adj_nv, Tw=Tw, alpha=alpha)
+            return channel_case(delta=d, nv=args.adj_nv, Tw=Tw, alpha=alpha, scheme=args.adj_scheme)
 
         workload = (f"kinetic CIS, channel 64x32x1 cells x in [0,4], inlet p 1 / outlet p 0.5, diffuse walls, "
-                    f"{args.adj_nv}^3 velocities on [-5,5]^3, delta 5, continuous equilibrium")
+                    f"{args.adj_nv}^3 velocities on [-5,5]^3, delta 5, {args.adj_scheme} scheme")
     setup, host = make(delta)
     sol, t_fwd, it_fwd = converge_channel(setup, host, local, args.fwd_tol, args.max_iters)
     torch.cuda.synchronize()
@@ -549,7 +553,8 @@ def adjoint_ratio(args, local):
             "dM_dot_dT_w_max_abs": float(np.max(np.abs(res.dJ_dTw))),
             "n_wall_faces": int(np.count_nonzero(res.dJ_dTw)), "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload, "cells": setup.n_cells, "velocities": setup.nv,
-                       "forward_tol": args.fwd_tol, "adjoint_tol": args.adj_tol}}
+                       "forward_tol": args.fwd_tol, "adjoint_tol": args.adj_tol,
+                       "scheme": dict(ADJ_SCHEMES[args.adj_scheme])}}
     if args.adjoint_fd:
         h = args.fd_step
 
@@ -611,6 +616,9 @@ def main():
     ap.add_argument("--fd-step", type=float, default=1e-6, help="relative step of the central differences")
     ap.add_argument("--adj-nv", type=int, default=24)
     ap.add_argument("--adjoint-case", default="channel", choices=["channel", "tube"])
+    ap.add_argument("--adj-scheme", default="default", choices=sorted(ADJ_SCHEMES),
+                    help="equilibrium and pressure-boundary reconstruction of the adjoint legs (default: the "
+                         "reference's defaults, discrete equilibrium and limited reconstruction)")
     ap.add_argument("--adj-inner", type=int, default=None, help="adjoint sweeps per coupling update (default: the "
                     "set-up's inner_sweeps, as the forward)")
     ap.add_argument("--fwd-tol", type=float, default=1e-10)
