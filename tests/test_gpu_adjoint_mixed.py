@@ -35,8 +35,11 @@ def _solution(precision, tol, **kw):
     return sol, setup, host
 
 
-@pytest.mark.parametrize("kw", [dict(), dict(equilibrium="discrete"), dict(n=(5, 3, 3), quarter=True)])
+@pytest.mark.parametrize("kw", [dict(), dict(equilibrium="discrete"), dict(n=(5, 3, 3), quarter=True),
+                                dict(half=True, equilibrium="discrete", reconstruction="limited")])
 def test_gpu_mixed_adjoint_operator_matches_reference(kw):
+    """With the limited pressure reconstruction the auxiliary adjoint also carries the face states' kappa (random on
+    the faces a pressure face reads)."""
     from gsis_sim_b200.adjoint import KineticAdjoint
     from oracle import adjoint_ref as ar
 
@@ -48,7 +51,11 @@ def test_gpu_mixed_adjoint_operator_matches_reference(kw):
         f, rg = ar.state_of(sol)
         rng = np.random.default_rng(17)
         lam = rng.standard_normal((sol.nc, sol.nv)).astype(np.float32).astype(np.float64)
-        nu = rng.standard_normal(len(ka.wall))
+        nu = rng.standard_normal(sm.n_aux)
+        if ka.limited:
+            kap = np.zeros((sol.nb, 5))
+            kap[ka.fs_read] = nu[len(ka.wall):].reshape(sol.nb, 5)[ka.fs_read]
+            nu[len(ka.wall):] = kap.ravel()
         op_f, op_w = ka.operator(lam, nu, with_objective=False)
         ref_f, ref_w = ar.transposed_jacobian_product(sm, f, rg, lam, nu)
         err_f = np.max(np.abs(op_f - ref_f)) / np.max(np.abs(ref_f))
