@@ -274,6 +274,18 @@ class KineticSolver:
         bmask = mask & (self.ps_bface >= 0)
         periodic[bmask] = self.pk[self.bpatch[self.ps_bface[bmask]]] == abi.BC_PERIODIC
         self.ps_periodic = periodic
+        # gathers of update_pressure_inflow, fixed for the set-up
+        self.ps_owner = own
+        self.ps_internal = mask & (self.ps_other >= 0)
+        self.ps_int_cells = self.ps_other[self.ps_internal]
+        self.ps_fs_entries = bmask & ~periodic  # entries that may carry a face state
+        self.ps_fs_faces = self.ps_bface[self.ps_fs_entries]
+        fb = self.bf_global[pres]
+        self.ps_dxb = self.h.face_center[fb] - self.h.cell_center[own] if len(pres) else np.zeros((0, 3))
+        self.ps_eps2 = self.h.limiter_k ** 3 * self.volume[own]
+        self.ps_normal = self.h.face_normal[fb]
+        ptype = self.ptype[self.bpatch[pres]]
+        self.ps_inlet = (ptype == T_PRESSURE_INLET) | (ptype == T_MASS_FLOW_INLET)
 
     def update_pressure_inflow(self):
         """update_pressure_inflow (src/kinetic/kinetic_solver.cpp:172-260): W_b from the limited reconstruction of
@@ -282,32 +294,29 @@ class KineticSolver:
         if len(pres) == 0:
             return
         h = self.h
-        K = h.limiter_k
         limit = int(self.s["limiter_mode"]) != abi.LIMITER_NONE
+        cols = [5, 1, 2, 3, 4]  # (p, u, T) of the moments
         m = self.moments_
-        state = lambda c: np.stack([m[c, 5], m[c, 1], m[c, 2], m[c, 3], m[c, 4]], -1)  # noqa: E731
-        ci = self.bowner[pres]
-        wi = state(ci)
-        wk = np.broadcast_to(wi[:, None, :], (len(pres),) + self.ps_other.shape[1:] + (5,)).copy()
-        internal = self.ps_other >= 0
-        wk[internal] = state(self.ps_other[internal])
-        bmask = self.ps_mask & (self.ps_bface >= 0)
+        wi = m[self.ps_owner][:, cols]
+        wk = np.repeat(wi[:, None, :], self.ps_mask.shape[1], axis=1)  # padding and other entries: the cell's value
+        wk[self.ps_internal] = m[self.ps_int_cells][:, cols]
         if self.has_face_state:
-            fs = self.face_state[np.where(bmask, self.ps_bface, 0)]
-            use = bmask & ~self.ps_periodic & (fs[..., 0] > 0) & (fs[..., 4] > 0)
-            wk[use] = np.stack([fs[use][:, 0] * fs[use][:, 4], fs[use][:, 1], fs[use][:, 2], fs[use][:, 3],
-                                fs[use][:, 4]], -1)
-        d = np.where(self.ps_mask[..., None], wk - wi[:, None, :], 0.0)
-        grad = np.einsum("fek,fea->fka", d, self.ps_lsq)  # (faces, 5, 3)
+            fs = self.face_state[self.ps_fs_faces]
+            ok = (fs[:, 0] > 0) & (fs[:, 4] > 0)
+            fs = fs[ok]
+            use = self.ps_fs_entries.copy()
+            use[use] = ok
+            wk[use] = np.stack([fs[:, 0] * fs[:, 4], fs[:, 1], fs[:, 2], fs[:, 3], fs[:, 4]], -1)
+        d = wk - wi[:, None, :]  # zero on the padding
+        grad = np.matmul(d.transpose(0, 2, 1), self.ps_lsq)  # (faces, 5, 3): sum_e d_e c_e
         # the bounds start from the cell's own value (wmax = wmin = wi before the stencil loop)
-        wmax = np.maximum(wi, np.where(self.ps_mask[..., None], wk, wi[:, None, :]).max(axis=1))
-        wmin = np.minimum(wi, np.where(self.ps_mask[..., None], wk, wi[:, None, :]).min(axis=1))
-        fb = self.bf_global[pres]
-        dxb = h.face_center[fb] - h.cell_center[ci]
-        eps2 = K ** 3 * self.volume[ci]
+        wmax = np.maximum(wi, wk.max(axis=1))
+        wmin = np.minimum(wi, wk.min(axis=1))
+        dxb = self.ps_dxb
+        eps2 = self.ps_eps2
         phi = np.ones((len(pres), 5))
         if limit:
-            proj = np.einsum("fka,fea->fke", grad, self.ps_dx)  # (faces, 5, E)
+            proj = np.matmul(grad, self.ps_dx.transpose(0, 2, 1))  # (faces, 5, E): grad . dx_e
             dmax = (wmax - wi)[..., None]
             dmin = (wmin - wi)[..., None]
             d1 = np.where(proj > 0, dmax, np.where(proj < 0, dmin, 0.0))
@@ -321,7 +330,7 @@ class KineticSolver:
             active = (self.ps_mask & ~self.ps_periodic)[:, None, :]
             v = np.where(active, v, 1.0)
             phi = np.minimum(1.0, v.min(axis=2))
-        wib = wi + phi * np.einsum("fka,fa->fk", grad, dxb)
+        wib = wi + phi * np.matmul(grad, dxb[:, :, None])[..., 0]
         bad = ~((wib[:, 0] > 0) & (wib[:, 4] > 0))
         wib[bad] = wi[bad]
         if h.pressure_boundary_reconstruction == "cell":
@@ -329,9 +338,8 @@ class KineticSolver:
         p_ib, u_ib, T_ib = wib[:, 0], wib[:, 1:4], wib[:, 4]
         rho_ib = p_ib / T_ib
         cs = np.sqrt(h.gamma * T_ib)
-        n = h.face_normal[fb]
-        ptype = self.ptype[self.bpatch[pres]]
-        inlet = (ptype == T_PRESSURE_INLET) | (ptype == T_MASS_FLOW_INLET)
+        n = self.ps_normal
+        inlet = self.ps_inlet
         p_b = h.patch_dbl[self.bpatch[pres], 1]
         T_b = np.where(inlet, h.patch_dbl[self.bpatch[pres], 0], T_ib)
         du = (p_ib - p_b) / (rho_ib * cs)
@@ -392,10 +400,12 @@ class KineticSolver:
     def compute_epsilon(self):
         """eq. (59) with the u floor (compute_epsilon, src/kinetic/kinetic_solver.cpp:338-363)."""
         V = self.volume
-        a, b = self.moments_, self.prev_moments
-        num = [np.sum((a[:, 0] - b[:, 0]) ** 2 * V), np.sum(np.sum((a[:, 1:4] - b[:, 1:4]) ** 2, 1) * V),
-               np.sum((a[:, 4] - b[:, 4]) ** 2 * V)]
-        den = [np.sum(b[:, 0] ** 2 * V), np.sum(np.sum(b[:, 1:4] ** 2, 1) * V), np.sum(b[:, 4] ** 2 * V)]
+        a, b = self.moments_[:, :5], self.prev_moments[:, :5]
+        d = a - b
+        n5 = (d * d).T @ V  # per moment: sum_c (a - b)^2 V
+        d5 = (b * b).T @ V
+        num = [n5[0], n5[1] + n5[2] + n5[3], n5[4]]
+        den = [d5[0], d5[1] + d5[2] + d5[3], d5[4]]
         fl = self.h.convergence_u_floor
         den[1] = max(den[1], fl * fl * np.sum(V))
         ratio = lambda n, d: math.sqrt(n / d) if d > 0 else (1.0 if n > 0 else 0.0)  # noqa: E731
@@ -514,7 +524,8 @@ class KineticSolver:
         V = self.volume
         self.info.residual = math.sqrt(float(np.sum(self.residual_cell / V)) * self._weight_scale() / float(np.sum(V)))
         self.info.has_residual = True
-        self.prev_moments = self.moments_.copy()
+        # prepare() replaces moments_ by a new array (and scales only that one), so the reference is enough
+        self.prev_moments = self.moments_
         self.has_prev = True
         self.version += 1
         self.iteration += 1
