@@ -48,6 +48,11 @@ HBM_FALLBACK_GBS = 6650.0
 DRAM_BYTES_PER_UNIT = {("fp64", "k_gradient"): 36.4, ("fp64", "k_residual"): 56.7, ("fp64", "k_sweep_tiles"): 66.65,
                        ("mixed", "k_gradient"): 16.8, ("mixed", "k_residual"): 23.7}
 DRAM_SOURCE = "ncu DRAM bytes per cell-velocity of the 62,848-cell 12^3 capture, scaled to this launch"
+# thread instructions per (cell, velocity) (smsp__inst_executed.sum x 32 / units) from the same captures: gradient,
+# residual, first and second LU-SGS block pass of the tile kernel
+INSTR_PER_UNIT = {"fp64": (697.0, 450.5, 440.6, 472.4), "mixed": (439.5, 443.8, 364.7, 373.3)}
+B200_SMS = 148
+ISSUE_PER_SM_CLOCK = 4 * 32  # 4 schedulers, one warp instruction (32 threads) each per cycle
 
 
 def peaks():
@@ -868,8 +873,30 @@ def step_fraction(run, precision, steps, hbm):
     per_unit = run["inner"] * (3 * s + 2 * s + 3 * s * (run["passes"] - 1)) + s
     t_step = run["device_s"] / steps
     achieved = per_unit * units / t_step / 1e9
-    return {"bytes_per_unit_per_iteration": per_unit, "seconds_per_iteration": t_step, "achieved": achieved,
-            "frac": achieved / hbm}
+    out = {"bytes_per_unit_per_iteration": per_unit, "seconds_per_iteration": t_step, "achieved": achieved,
+           "frac": achieved / hbm}
+    instr = INSTR_PER_UNIT.get(precision)
+    if instr is not None and run["passes"] == 2 and not os.environ.get("KIN_SWEEP_KERNEL"):
+        # the issue-rate bound: the sweeps at one instruction per scheduler per cycle, the other phases as measured
+        t = run["timings"]
+        sweep_phases = sum(t.get(k, 0.0) for k in ("gradient", "residual", "sweep_forward", "sweep_backward"))
+        other = max(0.0, (run["device_s"] - sweep_phases) / steps)
+        rate = B200_SMS * ISSUE_PER_SM_CLOCK * sm_max_mhz() * 1e6
+        t_min = run["inner"] * sum(instr) * units / rate + other
+        bound = per_unit * units / t_min / 1e9 / hbm
+        out["issue_bound"] = {"thread_instructions_per_unit_per_inner_sweep": sum(instr),
+                              "issue_rate_per_s": rate, "min_seconds_per_iteration": t_min, "max_frac": bound,
+                              "frac_of_bound": out["frac"] / bound,
+                              "source": "ncu instruction counts of the 62,848-cell 12^3 capture"}
+    return out
+
+
+def sm_max_mhz():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f).get("sm_max_mhz", 1965.0))
+    return 1965.0
 
 
 def mixed_leg(args, local, hbm):

@@ -17,7 +17,7 @@ def test_settle_time_empty_and_never():
 
 
 def _run(precision="fp64", inner=4, passes=2, steps=2):
-    return {"n_cells": 1000, "nv": 512, "inner": inner, "passes": passes, "device_s": 0.5 * steps,
+    return {"n_cells": 1000, "nv": 512, "inner": inner, "passes": passes, "device_s": 0.42 * steps,
             "timings": {"gradient": 0.1 * steps, "residual": 0.12 * steps, "sweep_forward": 0.2 * steps,
                         "sweep_backward": 0.0}, "lout_bytes_per_unit": None}
 
@@ -27,9 +27,15 @@ def test_step_fraction_counts_the_path_bytes_per_unit():
     moments: 264 B in FP64 and 132 B in FP32 storage at 4 inner sweeps and 2 block passes."""
     r = bench.step_fraction(_run(), "fp64", 2, 6000.0)
     assert r["bytes_per_unit_per_iteration"] == 264
-    assert abs(r["achieved"] - 264 * 1000 * 512 / 0.5 / 1e9) < 1e-12
+    assert abs(r["achieved"] - 264 * 1000 * 512 / 0.42 / 1e9) < 1e-12
     assert abs(r["frac"] - r["achieved"] / 6000.0) < 1e-15
     assert bench.step_fraction(_run(), "mixed", 2, 6000.0)["bytes_per_unit_per_iteration"] == 132
+    # the issue-rate bound: the sweeps at the full issue rate plus the other phases as measured (none here)
+    ib = r["issue_bound"]
+    rate = 148 * 128 * bench.sm_max_mhz() * 1e6
+    t_min = 4 * sum(bench.INSTR_PER_UNIT["fp64"]) * 1000 * 512 / rate
+    assert abs(ib["min_seconds_per_iteration"] - t_min) <= 1e-12 * t_min
+    assert abs(ib["max_frac"] - 264 * 1000 * 512 / t_min / 1e9 / 6000.0) <= 1e-9 * ib["max_frac"]
 
 
 def test_kernel_rooflines_divide_algorithmic_bytes_by_the_launch_time():
